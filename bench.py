@@ -1,0 +1,445 @@
+#!/usr/bin/env python
+"""Benchmark: SLQ logdet probe*steps/s on B200 (mixed precision, batched).
+
+Workload (one "step" = one SLQ logdet run over one block of probes on the
+resident matrix): the sparse SPD correlation matrix of the BASELINE's second
+configuration -- n = 262144 points uniform in [0,1]^2 (numpy PCG64 seed 1),
+kernel exp(-r/0.005) zeroed below 0.05 -- with the diagonal shift 0.1 in place
+of the configuration's 1e-3, which leaves the matrix indefinite (smallest Ritz
+value -0.0548, logdet undefined); 48.07M nonzeros, FP32 values, int32
+indices.  256 Rademacher probes (parity stream, seed 0), lanczos_degree 50,
+full reorthogonalisation.  Inputs (matrix 385 MB, Krylov basis 13.4 GB) are
+larger than L2 (126 MB), so no flush is needed between steps.
+
+value      probe*Lanczos-steps per second, whole job, device-timed (CUDA
+           events), matrix resident in HBM.
+e2e        same metric through the public API from host scipy arrays: the
+           CSR upload (host -> device) and the result readback are inside the
+           timed region.
+roofline   dominant kernel class: algorithmic bytes per launch / mean launch
+           time (CUDA events inside the timed region), vs the measured HBM
+           copy bandwidth.
+cpu_baseline  the reference's own CPU SLQ (oracle/_ref, built from its
+           sources) on the host cores, on a bounded sample of the workload.
+
+--impl reference times that reference CPU implementation alone.
+Multi-GPU: torchrun, one rank per GPU; each rank runs its own probes
+(disjoint probe indices), no collective on the data path (weak scaling).
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("SLQ logdet probe·steps/s on 1 B200, mixed+batched vs plain "
+          "FP64, at 1e-3 rel err")
+UNIT = "probe*steps/s"
+# FP64 oracle of the workload's logdet: sparse LU (scipy splu, MMD_AT_PLUS_A,
+# symmetric mode) of the float64 matrix; tests/golden/make_c2_oracle.py
+ORACLE_FILE = os.path.join(ROOT, "tests", "golden", "c2prime_oracle.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine",
+                    choices=["engine", "reference"])
+    ap.add_argument("--n", type=int, default=262144)
+    ap.add_argument("--probes", type=int, default=256)
+    ap.add_argument("--degree", type=int, default=50)
+    ap.add_argument("--orthogonalize", type=int, default=-1)
+    ap.add_argument("--shift", type=float, default=0.1)
+    ap.add_argument("--fp64-probes", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def build_matrix(args, dtype):
+    from imate_b200.sample_matrices import correlation_matrix
+    return correlation_matrix(args.n, scale=0.005, threshold=0.05,
+                              shift=args.shift, seed=1, dtype=dtype)
+
+
+def workload_config(args, nnz):
+    return {
+        "workload": "sparse SPD correlation matrix (exp(-r/0.005), cut 0.05, "
+                    "diag shift %g), SLQ logdet" % args.shift,
+        "n": args.n, "nnz": int(nnz), "value_dtype": "float32",
+        "index_dtype": "int32", "probes_per_step": args.probes,
+        "lanczos_degree": args.degree,
+        "orthogonalize": args.orthogonalize, "rng": "parity",
+        "l2": "inputs larger than L2 (matrix 385 MB, basis >13 GB)",
+    }
+
+
+def load_oracle(args):
+    try:
+        with open(ORACLE_FILE) as f:
+            d = json.load(f)
+        if d["n"] == args.n and abs(d["shift"] - args.shift) < 1e-15:
+            return d["logdet"]
+    except (OSError, KeyError, ValueError):
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# reference CPU SLQ (oracle/_ref) -- CPU baseline and the reference arm
+# ---------------------------------------------------------------------------
+
+def reference_sample(A, args, probes, threads, seed=0):
+    """Time the reference CPU estimator on `probes` probes; returns
+    (probe*steps/s, seconds, kind)."""
+    from oracle import ref
+    if ref.available():
+        r = ref.trace_estimator(A, "log", min_num_samples=probes,
+                                max_num_samples=probes, error_rtol=0.0,
+                                lanczos_degree=args.degree,
+                                orthogonalize=args.orthogonalize, seed=seed,
+                                num_threads=threads)
+        secs = r["alg_wall_time"]
+        # the reference does not report per-sample Krylov sizes; breakdown
+        # does not occur on this matrix, so every probe runs all steps
+        return probes * args.degree / secs, secs, "reference"
+    from oracle import oracle
+    t = time.perf_counter()
+    r = oracle.trace_estimator(A.astype(np.float64), "log",
+                               min_num_samples=probes,
+                               max_num_samples=probes, error_rtol=0.0,
+                               lanczos_degree=args.degree,
+                               orthogonalize=args.orthogonalize, seed=seed)
+    secs = time.perf_counter() - t
+    return float(np.sum(r["lanczos_sizes"][:probes])) / secs, secs, "port"
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    A = build_matrix(args, "float32")
+    threads = cpu_threads()
+    probes = threads  # one probe per host thread per step
+    for _ in range(args.warmup):
+        reference_sample(A, args, probes, threads)
+    vals, secs = [], 0.0
+    kind = "reference"
+    for s in range(args.steps):
+        v, t, kind = reference_sample(A, args, probes, threads, seed=s)
+        vals.append(v)
+        secs += t
+    value = probes * args.degree * args.steps / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": workload_config(args, A.nnz),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                         "kind": kind,
+                         "sample": "%d probes x %d Lanczos steps per step, "
+                                   "num_threads=%d" % (probes, args.degree,
+                                                       threads)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap")
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# engine arm
+# ---------------------------------------------------------------------------
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kind):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/*.txt lines 'traffic <kind> <bytes_per_launch>')."""
+    pdir = os.path.join(ROOT, "profiles")
+    try:
+        for fn in sorted(os.listdir(pdir)):
+            if not fn.endswith(".txt"):
+                continue
+            with open(os.path.join(pdir, fn)) as f:
+                for line in f:
+                    parts = line.split()
+                    if len(parts) == 3 and parts[0] == "traffic" and \
+                            parts[1] == kind:
+                        return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
+def run_engine_arm(args):
+    import torch
+    import torch.distributed as dist
+    import imate_b200 as ib
+    from imate_b200 import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    A32 = build_matrix(args, "float32")
+    Aop = ib.Matrix(A32)
+    Aop.get_device_operator()  # one-time upload, outside the timed region
+    eng = ib.EngineOptions(block_size=args.probes, rng="parity")
+    kw = dict(method="slq", gpu=True, return_info=True,
+              min_num_samples=args.probes, max_num_samples=args.probes,
+              error_rtol=0.0, lanczos_degree=args.degree,
+              orthogonalize=args.orthogonalize, seed=0)
+
+    def step(i, op=Aop):
+        # disjoint probe indices per rank and step (parity stream offsets)
+        eng.first_probe = (rank * (args.warmup + args.steps) + i) * args.probes
+        return ib.logdet(op, engine=eng, **kw)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    _lib.profile_begin()
+    ev0.record()
+    probe_steps = 0
+    launches = 0
+    estimates = []
+    for i in range(args.steps):
+        tr, info = step(args.warmup + i)
+        probe_steps += int(np.sum(info["engine"]["lanczos_size"]
+                                  [:args.probes]))
+        launches += int(info["engine"]["gpu_launches"])
+        estimates.append(float(tr))
+    ev1.record()
+    torch.cuda.synchronize()
+    kstats = _lib.profile_end()
+    clk = clocks.stop()
+    elapsed = ev0.elapsed_time(ev1) * 1e-3
+    if world > 1:
+        t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+        ps = torch.tensor([probe_steps], dtype=torch.float64, device="cuda")
+        dist.all_reduce(ps, op=dist.ReduceOp.SUM)
+        total_probe_steps = float(ps.item())
+    else:
+        total_probe_steps = float(probe_steps)
+    value = total_probe_steps / elapsed
+
+    # roofline of the dominant kernel class
+    dom = max(kstats, key=lambda k: kstats[k][1])
+    nl, ms, by = kstats[dom]
+    achieved = (by / nl) / (ms / nl * 1e-3) / 1e9 if nl else 0.0
+    peak, peak_kind = peaks()
+    traffic = ncu_traffic(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": peak_kind,
+                "bytes_per_launch": by / nl if nl else 0.0,
+                "ms_per_launch": ms / nl if nl else 0.0,
+                "share_of_kernel_time": ms / max(1e-12, sum(
+                    v[1] for v in kstats.values())),
+                "kernels": {k: {"launches": v[0], "ms": v[1],
+                                "GB/s": (v[2] / (v[1] * 1e-3) / 1e9)
+                                if v[1] > 0 else None}
+                            for k, v in kstats.items() if v[0]}}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": workload_config(args, A32.nnz),
+        "roofline": roofline, "gpu_launches": launches, "clocks": clk,
+    }
+
+    # accuracy vs the FP64 oracle
+    oracle_val = load_oracle(args)
+    est = float(np.mean(estimates))
+    line["accuracy"] = {
+        "estimate_mean": est,
+        "fp64_oracle": oracle_val,
+        "rel_err_vs_oracle": (abs(est - oracle_val) / abs(oracle_val)
+                              if oracle_val else None),
+        "probes_in_mean": args.probes * args.steps * world,
+        "note": "precision error (mixed vs FP64 on identical probes) is in "
+                "fp64_plain.rel_diff_same_probes",
+    }
+
+    if rank == 0:
+        # plain FP64 per-probe path (block width 1) on the same matrix
+        A64 = A32.astype(np.float64)
+        Aop64 = ib.Matrix(A64)
+        Aop64.get_device_operator()
+        e64 = ib.EngineOptions(block_size=1, rng="parity")
+        nprb = args.fp64_probes
+        kw64 = dict(kw, min_num_samples=nprb, max_num_samples=nprb)
+        ib.logdet(Aop64, engine=e64, **dict(kw64, min_num_samples=1,
+                                              max_num_samples=1))
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        tr64, info64 = ib.logdet(Aop64, engine=e64, **kw64)
+        e1.record()
+        torch.cuda.synchronize()
+        t64 = e0.elapsed_time(e1) * 1e-3
+        ps64 = int(np.sum(info64["engine"]["lanczos_size"][:nprb]))
+        # same probes in mixed precision
+        e32 = ib.EngineOptions(block_size=min(args.probes, 256), rng="parity")
+        tr32, info32 = ib.logdet(Aop, engine=e32, **kw64)
+        s64 = np.asarray(info64["convergence"]["samples"][:nprb], float)
+        s32 = np.asarray(info32["convergence"]["samples"][:nprb], float)
+        v64 = ps64 / t64
+        line["fp64_plain"] = {
+            "value": v64, "unit": UNIT, "probes": nprb, "block_size": 1,
+            "dtype": "f64", "speedup_mixed_batched": value / world / v64,
+            "rel_diff_same_probes": float(np.max(np.abs(s32 - s64) /
+                                                 np.abs(s64))),
+        }
+        del Aop64
+
+        # end to end through the public API from host arrays
+        if not args.no_e2e:
+            h2d = A32.data.nbytes + A32.indices.nbytes + A32.indptr.nbytes
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e_ps = 0
+            nsteps = max(1, min(args.steps, 3))
+            for i in range(nsteps):
+                fresh = ib.Matrix(A32)
+                eng.first_probe = i * args.probes
+                tr, info = ib.logdet(fresh, engine=eng, **kw)
+                e_ps += int(np.sum(info["engine"]["lanczos_size"]
+                                   [:args.probes]))
+                del fresh
+            torch.cuda.synchronize()
+            te = time.perf_counter() - t0
+            line["e2e"] = {"value": e_ps / te, "unit": UNIT,
+                           "h2d_bytes_per_step": int(h2d),
+                           "d2h_bytes_per_step": int(args.probes * 8 * 2),
+                           "steps": nsteps,
+                           "path": "imate_b200.logdet(scipy CSR on host)"}
+
+        if not args.no_cpu_baseline:
+            threads = cpu_threads()
+            probes = min(threads, 64)
+            v, secs, kind = reference_sample(A32, args, probes, threads)
+            line["cpu_baseline"] = {
+                "value": v, "unit": UNIT, "cores": threads, "kind": kind,
+                "sample": "%d probes x %d steps, FP32, full reorth, %.1f s"
+                          % (probes, args.degree, secs)}
+        print(json.dumps(line), flush=True)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_engine_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,172 @@
+"""ctypes binding of ``libslq_b200.so`` (declarations in ``include/slq.h``).
+
+Replaces imate's runtime loader of the CUDA libraries
+(``imate/_cuda_dynamic_loading/dynamic_loading.h:97-110``): the engine is one
+in-tree shared library, linked against the CUDA runtime only, and loading it
+fails loudly when it is missing -- there is no CPU fallback.
+"""
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libslq_b200.so")
+
+SLQ_OK = 0
+STATUS_NAMES = {
+    0: "OK", 1: "BAD_ARG", 2: "BAD_CSR", 3: "WORKSPACE", 4: "CUDA",
+    5: "NAN", 6: "EIGEN", 7: "UNSUPPORTED",
+}
+SLQ_F32, SLQ_F64 = 0, 1
+SLQ_CSR, SLQ_CSC = 0, 1
+FUNC_IDS = {"log": 0, "inv": 1, "id": 2}
+RNG_IDS = {"parity": 0, "fast": 1}
+MAX_DEGREE = 256
+
+# every symbol include/slq.h declares
+EXPORTS = (
+    "slq_operator_workspace_bytes", "slq_operator_create",
+    "slq_operator_destroy", "slq_operator_dot", "slq_run_workspace_bytes",
+    "slq_run", "slq_generate_probes", "slq_generate_probes_workspace_bytes",
+    "slq_nodes_weights", "slq_check_convergence", "slq_average_estimates",
+    "slq_erfinv", "slq_xoshiro_jump_ahead", "slq_device_info",
+    "slq_last_error", "slq_abi_version", "slq_profile_begin",
+    "slq_profile_end",
+)
+
+
+class SlqError(RuntimeError):
+    """A status other than SLQ_OK returned by the engine."""
+
+    def __init__(self, status, message):
+        self.status = status
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, status),
+                                     message))
+
+
+class SlqParams(ctypes.Structure):
+    _fields_ = [
+        ("func", ctypes.c_int),
+        ("gram", ctypes.c_int),
+        ("exponent", ctypes.c_double),
+        ("orthogonalize", ctypes.c_int),
+        ("seed", ctypes.c_int64),
+        ("lanczos_degree", ctypes.c_int),
+        ("lanczos_tol", ctypes.c_double),
+        ("min_num_samples", ctypes.c_int),
+        ("max_num_samples", ctypes.c_int),
+        ("error_atol", ctypes.c_double),
+        ("error_rtol", ctypes.c_double),
+        ("confidence_level", ctypes.c_double),
+        ("outlier_significance_level", ctypes.c_double),
+        ("block_size", ctypes.c_int),
+        ("rng", ctypes.c_int),
+        ("first_probe", ctypes.c_int64),
+    ]
+
+
+KERNEL_KINDS = ("spmm", "dots", "reorth", "finalize", "eig", "probe", "other")
+
+
+class SlqKernelStat(ctypes.Structure):
+    _fields_ = [
+        ("launches", ctypes.c_int64),
+        ("milliseconds", ctypes.c_double),
+        ("bytes", ctypes.c_double),
+    ]
+
+
+class SlqResult(ctypes.Structure):
+    _fields_ = [
+        ("trace", ctypes.c_void_p),
+        ("error", ctypes.c_void_p),
+        ("samples", ctypes.c_void_p),
+        ("processed_samples_indices", ctypes.c_void_p),
+        ("num_samples_used", ctypes.c_void_p),
+        ("num_outliers", ctypes.c_void_p),
+        ("converged", ctypes.c_void_p),
+        ("lanczos_size", ctypes.c_void_p),
+        ("alpha", ctypes.c_void_p),
+        ("beta", ctypes.c_void_p),
+        ("all_converged", ctypes.c_int32),
+        ("num_blocks", ctypes.c_int32),
+        ("num_probes_computed", ctypes.c_int64),
+        ("gpu_launches", ctypes.c_int64),
+        ("alg_wall_time", ctypes.c_float),
+    ]
+
+
+_lib = None
+
+
+def _declare(lib):
+    vp, sz, i32, i64, d = (ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
+                           ctypes.c_int64, ctypes.c_double)
+    psz = ctypes.POINTER(ctypes.c_size_t)
+    sig = {
+        "slq_operator_workspace_bytes": (i32, [i64, i64, i64, i32, i32, i32,
+                                               psz]),
+        "slq_operator_create": (i32, [vp, vp, vp, i64, i64, i64, i32, i32,
+                                      i32, i32, i32, vp, sz, vp,
+                                      ctypes.POINTER(vp)]),
+        "slq_operator_destroy": (i32, [vp]),
+        "slq_operator_dot": (i32, [vp, i32, d, vp, vp, i32, vp]),
+        "slq_run_workspace_bytes": (i32, [vp, ctypes.POINTER(SlqParams), i32,
+                                          psz]),
+        "slq_run": (i32, [vp, ctypes.POINTER(SlqParams), vp, i32, vp, sz, vp,
+                          ctypes.POINTER(SlqResult)]),
+        "slq_generate_probes": (i32, [i64, i32, i64, i64, i32, i32, i32, vp,
+                                      vp, sz, vp]),
+        "slq_generate_probes_workspace_bytes": (i32, [i64, i32, psz]),
+        "slq_nodes_weights": (i32, [vp, vp, vp, i32, i32, i32, vp, vp, vp,
+                                    vp]),
+        "slq_check_convergence": (i32, [vp, i32, i32, vp, i32, d, d, d, vp,
+                                        vp, vp]),
+        "slq_average_estimates": (None, [d, d, i32, i32, vp, vp, vp, vp, vp,
+                                         vp]),
+        "slq_erfinv": (d, [d]),
+        "slq_xoshiro_jump_ahead": (None, [vp, ctypes.c_uint64]),
+        "slq_device_info": (i32, [vp, vp, vp]),
+        "slq_last_error": (ctypes.c_char_p, []),
+        "slq_profile_begin": (i32, []),
+        "slq_profile_end": (i32, [ctypes.POINTER(SlqKernelStat)]),
+        "slq_abi_version": (i32, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def load():
+    """Load the engine library; raises ImportError if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            "libslq_b200.so is missing: build it with "
+            "`python -m imate_b200._build` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(LIB_PATH)
+    _declare(lib)
+    _lib = lib
+    return lib
+
+
+def profile_begin():
+    check(load().slq_profile_begin())
+
+
+def profile_end():
+    """Per-kernel-class stats since profile_begin():
+    {kind: (launches, milliseconds, bytes)}."""
+    stats = (SlqKernelStat * len(KERNEL_KINDS))()
+    check(load().slq_profile_end(stats))
+    return {k: (int(s.launches), float(s.milliseconds), float(s.bytes))
+            for k, s in zip(KERNEL_KINDS, stats)}
+
+
+def check(status):
+    if status != SLQ_OK:
+        msg = load().slq_last_error()
+        raise SlqError(status, msg.decode() if msg else "")

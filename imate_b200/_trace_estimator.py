@@ -1,0 +1,532 @@
+"""Host side of the SLQ estimator.
+
+Mirrors imate's dispatcher for ``method='slq'``
+(``imate/_trace_estimator/trace_estimator.pyx:38-390`` with
+``trace_estimator_utilities.py:24-373``): the same argument checks and
+defaults, the same outputs and the same ``info`` dictionary, with the sample
+loop, Krylov recurrences, eigen-solves and quadrature running in
+``libslq_b200.so`` on the GPU.  Only ``gpu=True`` is served; there is no CPU
+path.
+"""
+
+import ctypes
+import numbers
+import time
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+from .__version__ import __version__
+from .linear_operator import LinearOperator, Matrix
+
+__all__ = ["trace_estimator", "EngineOptions"]
+
+
+class EngineOptions:
+    """Engine settings beyond imate's keyword arguments.
+
+    block_size : probes advanced together on the device (power of two,
+        <= 1024 for float32, <= 512 for float64); 0 picks
+        min(256, next power of two >= max_num_samples).
+    rng : 'parity' reproduces the reference's xoshiro256** Rademacher stream
+        bit for bit; 'fast' uses a counter-based hash (no host set-up).
+    first_probe : global index of the first probe (sample i uses probe
+        first_probe + i of the stream), so that shards of one estimate can
+        run on different devices without sharing probes.
+    return_coefficients : put the per-sample Lanczos coefficients in
+        info['engine']['alpha'] / ['beta'].
+    """
+
+    def __init__(self, block_size=0, rng="parity", return_coefficients=False,
+                 first_probe=0):
+        self.block_size = int(block_size)
+        self.rng = rng
+        self.return_coefficients = bool(return_coefficients)
+        self.first_probe = int(first_probe)
+
+
+def _is_int(x):
+    return isinstance(x, (int, np.integer)) and not isinstance(x, bool)
+
+
+def _is_float(x):
+    return isinstance(x, (int, float, np.integer, np.floating)) and \
+        not isinstance(x, bool)
+
+
+def get_operator(A, gram):
+    """Wrap the input as an operator (trace_estimator_utilities.py:24-55)."""
+    if isinstance(A, np.ndarray) or sp.issparse(A):
+        if A.ndim != 2:
+            raise ValueError("Input matrix should be a 2-dimensional array.")
+        if not gram and A.shape[0] != A.shape[1]:
+            raise ValueError("Input matrix should be a square matrix.")
+        return Matrix(A)
+    if isinstance(A, LinearOperator):
+        if not gram and A.get_num_rows() != A.get_num_columns():
+            raise ValueError("Input operator should have the same number of "
+                             "rows and columns.")
+        return A
+    raise TypeError('The linear operator "A" should be either a '
+                    'numpy.ndarray, a scipy.sparse array, or an instance of '
+                    'a class derived from the "LinearOperator" class.')
+
+
+def get_operator_parameters(parameters, data_type_name):
+    """Normalise ``parameters`` (trace_estimator_utilities.py:62-101)."""
+    if parameters is None:
+        return None, 0
+    if np.isscalar(parameters):
+        return parameters, 1
+    if isinstance(parameters, (list, np.ndarray)):
+        arr = np.asarray(parameters, dtype=data_type_name)
+        if arr.ndim != 1:
+            raise ValueError('"parameters", if given as an array, should be a '
+                             'one-dimensional array. Current dimension of '
+                             'parameters is %d.' % arr.ndim)
+        return arr, arr.size
+    raise TypeError('"parameters" type should be either "None", a scalar, a '
+                    'flat list, or one-dimensional "numpy.ndarray.')
+
+
+def find_num_inquiries(Aop, parameters_size):
+    """Number of parameter sets (trace_estimator_utilities.py:338-373)."""
+    k = Aop.get_num_parameters()
+    if k == 0:
+        return 1
+    if parameters_size < k:
+        raise ValueError("Not enough parameters are provided. The given "
+                         "parameter size is %d, which should be larger than "
+                         "%d, the number of parameters of the linear "
+                         "operator." % (parameters_size, k))
+    if parameters_size % k != 0:
+        raise ValueError("Parameters size (given %d) is not an integer-"
+                         "multiple of %d, the number of the parameters of the "
+                         "linear operator." % (parameters_size, k))
+    return parameters_size // k
+
+
+def check_arguments(gram, exponent, min_num_samples, max_num_samples,
+                    error_atol, error_rtol, confidence_level,
+                    outlier_significance_level, lanczos_degree, lanczos_tol,
+                    orthogonalize, seed, num_threads, num_gpu_devices,
+                    verbose, plot, gpu):
+    """Type and range checks of imate's SLQ keyword arguments
+    (trace_estimator_utilities.py:108-305).  Returns (error_atol,
+    error_rtol) with None mapped to 0."""
+
+    def flag(name, v):
+        if v is None:
+            raise TypeError('"%s" cannot be None.' % name)
+        if not np.isscalar(v):
+            raise TypeError('"%s" should be a scalar value.' % name)
+        if not isinstance(v, bool):
+            raise TypeError('"%s" should be boolean.' % name)
+
+    def count(name, v, minimum, none_error=ValueError):
+        if v is None:
+            raise none_error('"%s" cannot be None.' % name)
+        if not np.isscalar(v):
+            raise TypeError('"%s" should be a scalar value.' % name)
+        if not _is_int(v):
+            raise TypeError('"%s" should be an integer.' % name)
+        if v < minimum:
+            raise ValueError('"%s" should be at least %d.' % (name, minimum))
+
+    flag("gram", gram)
+    if exponent is None:
+        raise TypeError('"exponent" cannot be None.')
+    if not np.isscalar(exponent):
+        raise TypeError('"exponent" should be a scalar value.')
+    if isinstance(exponent, complex):
+        raise TypeError('"exponent" cannot be a complex number.')
+    count("min_num_samples", min_num_samples, 1)
+    count("max_num_samples", max_num_samples, 1)
+    if min_num_samples > max_num_samples:
+        raise ValueError('"min_num_samples" cannot be greater than '
+                         '"max_num_samples".')
+
+    def tolerance(name, v):
+        if v is None:
+            return 0.0
+        if not np.isscalar(v):
+            raise TypeError('"%s" should be a scalar value.' % name)
+        if not isinstance(v, (int, float)) or isinstance(v, bool):
+            raise TypeError('"%s" should be a float number.' % name)
+        if v < 0.0:
+            raise ValueError('"%s" cannot be negative.' % name)
+        return v
+
+    error_atol = tolerance("error_atol", error_atol)
+    error_rtol = tolerance("error_rtol", error_rtol)
+
+    if confidence_level is None:
+        raise TypeError('"confidence_level" cannot be None.')
+    if not np.isscalar(confidence_level):
+        raise TypeError('"confidence_level" should be a scalar.')
+    if not isinstance(confidence_level, (int, float)) or \
+            isinstance(confidence_level, bool):
+        raise TypeError('"confidence_level" should be a float number.')
+    if not 0.0 <= confidence_level <= 1.0:
+        raise ValueError('"confidence_level" should be between 0 and 1.')
+
+    osl = outlier_significance_level
+    if osl is None:
+        raise TypeError('"outlier_significance_level" cannot be None.')
+    if not np.isscalar(osl):
+        raise TypeError('"outlier_significance_level" should be a scalar.')
+    if not _is_float(osl):
+        raise TypeError('"outlier_significance_level" must be a float number.')
+    if not 0.0 <= osl <= 1.0:
+        raise ValueError('"outlier_significance_level" must be in [0, 1] '
+                         'interval.')
+    if osl > 1.0 - confidence_level:
+        raise ValueError('The sum of "confidence_level" and '
+                         '"outlier_significance_level" should be less than 1.')
+
+    count("lanczos_degree", lanczos_degree, 1, none_error=TypeError)
+    if lanczos_tol is not None:
+        if not np.isscalar(lanczos_tol):
+            raise TypeError('"lanczos_tol" should be a scalar value.')
+        if not _is_float(lanczos_tol):
+            raise TypeError('"lanczos_tol" should be a float number.')
+        if lanczos_tol < 0.0:
+            raise ValueError('"lancozs_tol" cannot be negative.')
+
+    if orthogonalize is None:
+        raise TypeError('"orthogonalize" cannot be None.')
+    if not np.isscalar(orthogonalize):
+        raise TypeError('"orthogonalize" should be a scalar value.')
+    if not _is_int(orthogonalize):
+        raise TypeError('"orthogonalize" should be an integer.')
+    if orthogonalize > lanczos_degree:
+        raise ValueError('"orthogonalize", if positive, should be at most '
+                         'equal to "lanczos_degree".')
+
+    if seed is not None:
+        if not np.isscalar(seed):
+            raise TypeError('"seed" should be a None or a scalar value.')
+        if not _is_int(seed):
+            raise TypeError('"seed" should be None or an integer.')
+
+    for name, v in (("num_threads", num_threads),
+                    ("num_gpu_devices", num_gpu_devices)):
+        if v is None:
+            raise TypeError('"%s" cannot be None.' % name)
+        if not np.isscalar(v):
+            raise TypeError('"%s" should be a scalar value.' % name)
+        if not _is_int(v):
+            raise TypeError('"%s" should be an integer.' % name)
+        if v < 0:
+            raise ValueError('"%s" should be a non-negative integer.' % name)
+
+    flag("verbose", verbose)
+    flag("plot", plot)
+    flag("gpu", gpu)
+    return error_atol, error_rtol
+
+
+def _clock_seed():
+    # a non-negative seed from the high-resolution clock (the reference maps
+    # seed=None to -1, which seeds SplitMix64 from the clock,
+    # split_mix_64.cpp:33-41)
+    return int(time.perf_counter_ns() & 0x7FFFFFFF)
+
+
+def trace_estimator(A, parameters, func, gram, exponent, min_num_samples,
+                    max_num_samples, error_atol, error_rtol,
+                    confidence_level, outlier_significance_level,
+                    lanczos_degree, lanczos_tol, orthogonalize, seed,
+                    num_threads, num_gpu_devices, verbose, plot, gpu,
+                    options=None):
+    """SLQ estimate of trace(f(A^p)) (or of f((A^T A)^p) with gram) on the
+    GPU.  ``func`` is 'log', 'inv' or 'id'.  Returns (trace, info) like
+    ``trace_estimator.pyx``."""
+    import torch
+
+    if options is None:
+        options = EngineOptions()
+    if not gpu:
+        raise ValueError('This engine runs SLQ on the GPU only: call with '
+                         '"gpu=True" (imate\'s CPU path serves gpu=False).')
+    if func not in _lib.FUNC_IDS:
+        raise ValueError("unknown matrix function %r" % (func,))
+    if options.rng not in _lib.RNG_IDS:
+        raise ValueError('rng must be "parity" or "fast"')
+
+    Aop = get_operator(A, gram)
+    data_type_name = Aop.get_data_type_name()
+    dtype_str = data_type_name.decode()
+    parameters, parameters_size = get_operator_parameters(parameters,
+                                                          dtype_str)
+    num_inquiries = find_num_inquiries(Aop, parameters_size)
+    error_atol, error_rtol = check_arguments(
+        gram, exponent, min_num_samples, max_num_samples, error_atol,
+        error_rtol, confidence_level, outlier_significance_level,
+        lanczos_degree, lanczos_tol, orthogonalize, seed, num_threads,
+        num_gpu_devices, verbose, plot, gpu)
+    if lanczos_degree > _lib.MAX_DEGREE:
+        raise ValueError('"lanczos_degree" is at most %d on this engine.'
+                         % _lib.MAX_DEGREE)
+    if seed is None:
+        seed_used = _clock_seed()
+    else:
+        seed_used = int(seed)
+        if seed_used < 0:
+            seed_used = _clock_seed()
+    if lanczos_tol is None:
+        lanczos_tol = float(np.finfo(dtype_str).eps)
+    if num_threads < 1:
+        import os
+        num_threads = os.cpu_count() or 1
+
+    lib = _lib.load()
+    if not torch.cuda.is_available():
+        raise RuntimeError("no CUDA device is available for the SLQ engine")
+
+    init_wall = time.perf_counter()
+    init_proc = time.process_time()
+
+    affine = Aop.get_num_parameters() > 0
+    if affine:
+        t_values = np.atleast_1d(np.asarray(parameters, dtype=np.float64))
+    else:
+        t_values = np.zeros(1)
+
+    # gram with several shifts: the shift relation does not hold for
+    # (A + tI)^T (A + tI), so each t gets its own Krylov runs
+    if gram and affine and num_inquiries > 1:
+        groups = [[j] for j in range(num_inquiries)]
+    else:
+        groups = [list(range(num_inquiries))]
+
+    q = num_inquiries
+    m = int(lanczos_degree)
+    trace = np.full(q, np.nan)
+    error = np.full(q, np.nan)
+    samples = np.full((max_num_samples, q), np.nan)
+    processed = np.zeros(max_num_samples, dtype=np.int32)
+    num_samples_used = np.zeros(q, dtype=np.int32)
+    num_outliers = np.zeros(q, dtype=np.int32)
+    converged = np.zeros(q, dtype=np.int32)
+    lanczos_size = np.zeros((max_num_samples, len(groups)), dtype=np.int32)
+    alphas = betas = None
+    if options.return_coefficients:
+        alphas = np.full((len(groups), max_num_samples, m), np.nan)
+        betas = np.full((len(groups), max_num_samples, m), np.nan)
+    all_converged = True
+    alg_wall_time = 0.0
+    engine = dict(block_size=None, rng=options.rng, num_blocks=0,
+                  num_probes_computed=0, gpu_launches=0)
+
+    dev_op = Aop.get_device_operator(need_transpose=bool(gram))
+    stream = torch.cuda.current_stream(dev_op.device)
+    for gi, group in enumerate(groups):
+        gq = len(group)
+        prm = _lib.SlqParams(
+            func=_lib.FUNC_IDS[func], gram=int(bool(gram)),
+            exponent=float(exponent), orthogonalize=int(orthogonalize),
+            seed=seed_used, lanczos_degree=m, lanczos_tol=float(lanczos_tol),
+            min_num_samples=int(min_num_samples),
+            max_num_samples=int(max_num_samples),
+            error_atol=float(error_atol), error_rtol=float(error_rtol),
+            confidence_level=float(confidence_level),
+            outlier_significance_level=float(outlier_significance_level),
+            block_size=options.block_size, rng=_lib.RNG_IDS[options.rng],
+            first_probe=options.first_probe)
+        ws_bytes = ctypes.c_size_t(0)
+        _lib.check(lib.slq_run_workspace_bytes(dev_op.handle,
+                                               ctypes.byref(prm), gq,
+                                               ctypes.byref(ws_bytes)))
+        workspace = torch.empty(int(ws_bytes.value), dtype=torch.uint8,
+                                device=dev_op.device)
+        g_trace = np.zeros(gq)
+        g_error = np.zeros(gq)
+        g_samples = np.zeros((max_num_samples, gq))
+        g_order = np.zeros(max_num_samples, dtype=np.int32)
+        g_used = np.zeros(gq, dtype=np.int32)
+        g_out = np.zeros(gq, dtype=np.int32)
+        g_conv = np.zeros(gq, dtype=np.int32)
+        g_size = np.zeros(max_num_samples, dtype=np.int32)
+        g_alpha = np.zeros((max_num_samples, m)) if alphas is not None \
+            else None
+        g_beta = np.zeros((max_num_samples, m)) if betas is not None \
+            else None
+        ptr = (lambda a: a.ctypes.data if a is not None else None)
+        res = _lib.SlqResult(
+            trace=ptr(g_trace), error=ptr(g_error), samples=ptr(g_samples),
+            processed_samples_indices=ptr(g_order),
+            num_samples_used=ptr(g_used), num_outliers=ptr(g_out),
+            converged=ptr(g_conv), lanczos_size=ptr(g_size),
+            alpha=ptr(g_alpha), beta=ptr(g_beta))
+        t_g = np.ascontiguousarray(t_values[group], dtype=np.float64)
+        status = lib.slq_run(dev_op.handle, ctypes.byref(prm),
+                             t_g.ctypes.data, gq, workspace.data_ptr(),
+                             workspace.numel(), stream.cuda_stream,
+                             ctypes.byref(res))
+        del workspace
+        if status == 6:  # eigen-solve failure: report, do not hide
+            import warnings
+            warnings.warn("SLQ: " + lib.slq_last_error().decode())
+        elif status != _lib.SLQ_OK:
+            _lib.check(status)
+        for k, j in enumerate(group):
+            trace[j] = g_trace[k]
+            error[j] = g_error[k]
+            samples[:, j] = g_samples[:, k]
+            num_samples_used[j] = g_used[k]
+            num_outliers[j] = g_out[k]
+            converged[j] = g_conv[k]
+        processed = g_order if gi == 0 else processed
+        lanczos_size[:, gi] = g_size
+        if alphas is not None:
+            alphas[gi] = g_alpha
+            betas[gi] = g_beta
+        all_converged = all_converged and bool(res.all_converged)
+        alg_wall_time += float(res.alg_wall_time)
+        engine["num_blocks"] += int(res.num_blocks)
+        engine["num_probes_computed"] += int(res.num_probes_computed)
+        engine["gpu_launches"] += int(res.gpu_launches)
+
+    b = options.block_size
+    if b <= 0:
+        b = min(256, 1 << max(0, (max_num_samples - 1).bit_length()))
+    bmax = 512 if dtype_str == "float64" else 1024
+    b = min(1 << max(0, (b - 1).bit_length()), bmax,
+            1 << max(0, (max_num_samples - 1).bit_length()))
+    engine["block_size"] = b
+
+    tot_wall_time = time.perf_counter() - init_wall
+    cpu_proc_time = time.process_time() - init_proc
+
+    props = torch.cuda.get_device_properties(dev_op.device)
+    out_dtype = np.dtype(dtype_str)
+    trace_out = trace.astype(out_dtype)
+    error_out = error.astype(out_dtype)
+    samples_out = samples.astype(out_dtype)
+    info = {
+        "matrix": {
+            "data_type": data_type_name,
+            "gram": gram,
+            "exponent": exponent,
+            "size": (Aop.get_num_rows(), Aop.get_num_columns()),
+            "sparse": Aop.is_sparse(),
+            "nnz": Aop.get_nnz(),
+            "density": Aop.get_density(),
+            "num_inquiries": num_inquiries,
+            "num_operator_parameters": Aop.get_num_parameters(),
+            "parameters": parameters,
+        },
+        "error": {
+            "absolute_error": None,
+            "relative_error": None,
+            "error_atol": error_atol,
+            "error_rtol": error_rtol,
+            "confidence_level": confidence_level,
+            "outlier_significance_level": outlier_significance_level,
+        },
+        "convergence": {
+            "converged": None,
+            "all_converged": bool(all_converged),
+            "min_num_samples": min_num_samples,
+            "max_num_samples": max_num_samples,
+            "num_samples_used": None,
+            "num_outliers": None,
+            "samples": None,
+            "samples_mean": None,
+            "samples_processed_order": processed,
+        },
+        "time": {
+            "tot_wall_time": tot_wall_time,
+            "alg_wall_time": alg_wall_time,
+            "cpu_proc_time": cpu_proc_time,
+        },
+        "device": {
+            "num_cpu_threads": num_threads,
+            "num_gpu_devices": 1,
+            "num_gpu_multiprocessors": props.multi_processor_count,
+            "num_gpu_threads_per_multiprocessor":
+                props.max_threads_per_multi_processor,
+        },
+        "solver": {
+            "version": __version__,
+            "lanczos_degree": lanczos_degree,
+            "lanczos_tol": lanczos_tol,
+            "orthogonalize": orthogonalize,
+            "seed": seed_used if seed is not None and seed >= 0 else -1,
+            "method": "slq",
+        },
+        "engine": dict(engine, lanczos_size=lanczos_size[:, 0]
+                       if len(groups) == 1 else lanczos_size),
+    }
+    if alphas is not None:
+        info["engine"]["alpha"] = alphas[0] if len(groups) == 1 else alphas
+        info["engine"]["beta"] = betas[0] if len(groups) == 1 else betas
+
+    output_is_array = not (parameters is None or np.isscalar(parameters))
+    eps = np.finfo(float).eps
+    if output_is_array:
+        info["error"]["absolute_error"] = error_out
+        info["error"]["relative_error"] = error_out / (np.abs(trace_out) + eps)
+        info["convergence"]["converged"] = converged.astype(bool)
+        info["convergence"]["num_samples_used"] = num_samples_used
+        info["convergence"]["num_outliers"] = num_outliers
+        info["convergence"]["samples"] = samples_out
+        info["convergence"]["samples_mean"] = trace_out
+    else:
+        info["error"]["absolute_error"] = error_out[0]
+        info["error"]["relative_error"] = \
+            error_out[0] / (np.abs(trace_out[0]) + eps)
+        info["convergence"]["converged"] = bool(converged[0])
+        info["convergence"]["num_samples_used"] = num_samples_used[0]
+        info["convergence"]["num_outliers"] = num_outliers[0]
+        info["convergence"]["samples"] = samples_out[:, 0]
+        info["convergence"]["samples_mean"] = trace_out[0]
+
+    if verbose:
+        print_summary(info)
+    if plot:
+        import warnings
+        warnings.warn("plot=True: convergence plots are not produced by the "
+                      "B200 engine (no plotting stack)")
+
+    if output_is_array:
+        return trace_out, info
+    return trace_out[0], info
+
+
+def print_summary(info):
+    """Results table in the spirit of imate's verbose output
+    (trace_estimator_utilities.py:380)."""
+    conv = info["convergence"]
+    err = info["error"]
+    q = info["matrix"]["num_inquiries"]
+    tr = np.atleast_1d(conv["samples_mean"])
+    ae = np.atleast_1d(err["absolute_error"])
+    re = np.atleast_1d(err["relative_error"]) * 100.0
+    used = np.atleast_1d(conv["num_samples_used"])
+    outl = np.atleast_1d(conv["num_outliers"])
+    cv = np.atleast_1d(conv["converged"])
+    params = info["matrix"]["parameters"]
+    print("=" * 78)
+    print("i   parameter        trace      abs. error   rel. error   "
+          "num  out  converged")
+    print("=" * 78)
+    for i in range(q):
+        pv = "none" if params is None else "%.4e" % np.atleast_1d(params)[i]
+        print("%-3d %-12s %+12.5e  %10.3e  %9.3f%%  %4d %4d  %s"
+              % (i + 1, pv, tr[i], ae[i], re[i], used[i], outl[i],
+                 bool(cv[i])))
+    t = info["time"]
+    d = info["device"]
+    print("-" * 78)
+    print("alg wall time %.4f s   total wall time %.4f s   GPU: %d SMs"
+          % (t["alg_wall_time"], t["tot_wall_time"],
+             d["num_gpu_multiprocessors"]))
+    s = info["solver"]
+    e = info["engine"]
+    print("lanczos degree %d   orthogonalize %s   block %s   rng %s   "
+          "kernels %d" % (s["lanczos_degree"], s["orthogonalize"],
+                          e["block_size"], e["rng"], e["gpu_launches"]))
+    print("=" * 78)

@@ -1,0 +1,1249 @@
+// B200 SLQ engine: operator set-up, the block Krylov driver and the C ABI
+// declared in include/slq.h.
+//
+// The reference GPU path (imate/_cu_trace_estimator/cu_trace_estimator.cu)
+// runs one probe at a time per device: a host-generated probe is copied to
+// the device, every Lanczos step issues a cuSPARSE SpMV and a series of
+// cuBLAS level-1 calls whose dot/nrm2 results return to the host, and the
+// tridiagonal eigen-solve runs in host LAPACK.  Here a block of b probes
+// advances together and stays on the device: probes are generated in place,
+// each Krylov step is one SpMM over the block plus fused update /
+// reorthogonalisation passes whose reductions are finalised on the device,
+// and the eigen-solve and quadrature run on the device.  The host reads b
+// samples per block and replays the reference's sequential stopping rule.
+
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/slq.h"
+#include "slq_kernels.cuh"
+#include "slq_rng.h"
+
+using namespace slq;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+
+namespace {
+
+thread_local std::string g_error;
+
+slq_status fail(slq_status s, const std::string& msg)
+{
+    g_error = msg;
+    return s;
+}
+
+#define SLQ_CK(call)                                                        \
+    do {                                                                    \
+        cudaError_t e_ = (call);                                            \
+        if (e_ != cudaSuccess)                                              \
+            return fail(SLQ_ERR_CUDA, std::string(#call) + ": " +           \
+                                          cudaGetErrorString(e_));          \
+    } while (0)
+
+#define SLQ_LAUNCH_CK()                                                     \
+    do {                                                                    \
+        cudaError_t e_ = cudaGetLastError();                                \
+        if (e_ != cudaSuccess)                                              \
+            return fail(SLQ_ERR_CUDA, std::string("kernel launch: ") +      \
+                                          cudaGetErrorString(e_));          \
+    } while (0)
+
+#define SLQ_TRY(expr)                                                       \
+    do {                                                                    \
+        slq_status s_ = (expr);                                             \
+        if (s_ != SLQ_OK) return s_;                                        \
+    } while (0)
+
+// Bump allocator over a caller-provided device buffer (256-byte aligned
+// pieces).  With base == nullptr it only measures.
+struct Carver {
+    char* base;
+    size_t cap;
+    size_t off = 0;
+    Carver(void* b, size_t c) : base(static_cast<char*>(b)), cap(c) {}
+    template <typename T>
+    T* take(size_t count)
+    {
+        off = (off + 255) & ~static_cast<size_t>(255);
+        T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+        off += count * sizeof(T);
+        return p;
+    }
+    bool fits() const { return off <= cap; }
+};
+
+int g_num_sms = 0;
+
+slq_status device_sms(int* sms)
+{
+    if (g_num_sms == 0)
+    {
+        int dev = 0;
+        SLQ_CK(cudaGetDevice(&dev));
+        SLQ_CK(cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    *sms = g_num_sms;
+    return SLQ_OK;
+}
+
+inline bool is_pow2(int x) { return x > 0 && (x & (x - 1)) == 0; }
+
+inline int next_pow2(int x)
+{
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+inline size_t dsize(int dtype) { return dtype == SLQ_F64 ? 8 : 4; }
+
+// Per-kernel event timing (slq_profile_begin / slq_profile_end).
+struct ProfRecord {
+    int kind;
+    cudaEvent_t start, stop;
+    double bytes;
+};
+
+struct Profiler {
+    bool on = false;
+    std::vector<ProfRecord> records;
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    cudaEvent_t next_event()
+    {
+        if (used == pool.size())
+        {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+            pool.push_back(e);
+        }
+        return pool[used++];
+    }
+};
+
+thread_local Profiler g_prof;
+
+// Brackets one launch with events when profiling is on.
+struct ProfScope {
+    int kind;
+    double bytes;
+    cudaStream_t st;
+    cudaEvent_t start = nullptr;
+    ProfScope(int k, double by, cudaStream_t s) : kind(k), bytes(by), st(s)
+    {
+        if (g_prof.on)
+        {
+            start = g_prof.next_event();
+            if (start) cudaEventRecord(start, st);
+        }
+    }
+    ~ProfScope()
+    {
+        if (g_prof.on && start)
+        {
+            cudaEvent_t stop = g_prof.next_event();
+            if (stop)
+            {
+                cudaEventRecord(stop, st);
+                g_prof.records.push_back({kind, start, stop, bytes});
+            }
+        }
+    }
+};
+
+}  // namespace
+
+extern "C" slq_status slq_profile_begin(void)
+{
+    g_prof.records.clear();
+    g_prof.used = 0;
+    g_prof.on = true;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_profile_end(slq_kernel_stat* stats)
+{
+    if (!stats) return fail(SLQ_ERR_BAD_ARG, "profile_end: stats is NULL");
+    for (int k = 0; k < SLQ_K_COUNT; ++k) stats[k] = {0, 0.0, 0.0};
+    g_prof.on = false;
+    if (!g_prof.records.empty())
+        SLQ_CK(cudaEventSynchronize(g_prof.records.back().stop));
+    for (const ProfRecord& r : g_prof.records)
+    {
+        float ms = 0.0f;
+        SLQ_CK(cudaEventElapsedTime(&ms, r.start, r.stop));
+        stats[r.kind].launches += 1;
+        stats[r.kind].milliseconds += ms;
+        stats[r.kind].bytes += r.bytes;
+    }
+    g_prof.records.clear();
+    g_prof.used = 0;
+    return SLQ_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// operator
+// ---------------------------------------------------------------------------
+
+struct slq_op {
+    int dtype;
+    int affine;
+    int64_t nrows, ncols, nnz;
+    // CSR of A (rows = nrows) and CSR of A^T (rows = ncols)
+    const void* a_data = nullptr;
+    const int32_t* a_ind = nullptr;
+    const int32_t* a_ptr = nullptr;
+    const void* t_data = nullptr;
+    const int32_t* t_ind = nullptr;
+    const int32_t* t_ptr = nullptr;
+};
+
+namespace {
+
+// Plan of the transpose of an R x C CSR matrix into caller memory.
+struct TransposeBufs {
+    int32_t* t_ptr;
+    int32_t* t_ind;
+    void* t_data;
+    int32_t* row_of;
+    int32_t* keys_out;
+    int32_t* iota;
+    int32_t* perm;
+    void* temp;
+    size_t temp_bytes;
+};
+
+slq_status transpose_layout(Carver& c, int64_t R, int64_t C, int64_t nnz,
+                            int dtype, TransposeBufs* t)
+{
+    size_t temp_bytes = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(
+        nullptr, temp_bytes, static_cast<const int32_t*>(nullptr),
+        static_cast<int32_t*>(nullptr), static_cast<const int32_t*>(nullptr),
+        static_cast<int32_t*>(nullptr), static_cast<int>(std::max<int64_t>(nnz, 1)));
+    if (e != cudaSuccess)
+        return fail(SLQ_ERR_CUDA, std::string("cub sort sizing: ") + cudaGetErrorString(e));
+    t->t_ptr = c.take<int32_t>(C + 1);
+    t->t_ind = c.take<int32_t>(nnz);
+    t->t_data = c.take<char>(nnz * dsize(dtype));
+    t->row_of = c.take<int32_t>(nnz);
+    t->keys_out = c.take<int32_t>(nnz);
+    t->iota = c.take<int32_t>(nnz);
+    t->perm = c.take<int32_t>(nnz);
+    t->temp = c.take<char>(temp_bytes);
+    t->temp_bytes = temp_bytes;
+    (void)R;
+    return SLQ_OK;
+}
+
+// Deterministic transpose: stable radix sort of (column, position) pairs
+// keeps the original row order inside every output row.
+slq_status transpose_csr(const int32_t* ptr, const int32_t* ind, const void* data,
+                         int64_t R, int64_t C, int64_t nnz, int dtype,
+                         TransposeBufs* t, cudaStream_t st)
+{
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
+    const int grid = sms * 4;
+    if (nnz > 0)
+    {
+        k_row_ids<<<grid, 256, 0, st>>>(ptr, R, t->row_of);
+        SLQ_LAUNCH_CK();
+        k_iota<<<grid, 256, 0, st>>>(t->iota, nnz);
+        SLQ_LAUNCH_CK();
+        int end_bit = 1;
+        while ((int64_t(1) << end_bit) <= C && end_bit < 31) ++end_bit;
+        size_t tb = t->temp_bytes;
+        cudaError_t e = cub::DeviceRadixSort::SortPairs(
+            t->temp, tb, ind, t->keys_out, t->iota, t->perm,
+            static_cast<int>(nnz), 0, end_bit, st);
+        if (e != cudaSuccess)
+            return fail(SLQ_ERR_CUDA, std::string("cub sort: ") + cudaGetErrorString(e));
+        if (dtype == SLQ_F64)
+            k_gather_transpose<double><<<grid, 256, 0, st>>>(
+                t->perm, t->row_of, static_cast<const double*>(data), nnz, t->t_ind,
+                static_cast<double*>(t->t_data));
+        else
+            k_gather_transpose<float><<<grid, 256, 0, st>>>(
+                t->perm, t->row_of, static_cast<const float*>(data), nnz, t->t_ind,
+                static_cast<float*>(t->t_data));
+        SLQ_LAUNCH_CK();
+    }
+    k_bounds<<<std::max<int64_t>(1, std::min<int64_t>(grid, (C + 256) / 256)), 256, 0, st>>>(
+        t->keys_out, nnz, C, t->t_ptr);
+    SLQ_LAUNCH_CK();
+    return SLQ_OK;
+}
+
+}  // namespace
+
+extern "C" slq_status slq_operator_workspace_bytes(int64_t num_rows, int64_t num_cols,
+                                                   int64_t nnz, int dtype, int format,
+                                                   int need_transpose, size_t* bytes)
+{
+    if (!bytes || num_rows < 0 || num_cols < 0 || nnz < 0)
+        return fail(SLQ_ERR_BAD_ARG, "operator_workspace_bytes: bad argument");
+    Carver c(nullptr, 0);
+    TransposeBufs t;
+    c.take<int32_t>(1);  // index-check flag
+    const bool build = (format == SLQ_CSC) || need_transpose;
+    if (build)
+    {
+        const int64_t R = (format == SLQ_CSC) ? num_cols : num_rows;
+        const int64_t C = (format == SLQ_CSC) ? num_rows : num_cols;
+        SLQ_TRY(transpose_layout(c, R, C, nnz, dtype, &t));
+    }
+    *bytes = c.off + 256;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_operator_create(const void* data, const int32_t* indices,
+                                          const int32_t* indptr, int64_t num_rows,
+                                          int64_t num_cols, int64_t nnz, int dtype,
+                                          int format, int affine, int need_transpose,
+                                          int check_indices, void* workspace,
+                                          size_t workspace_bytes, void* stream,
+                                          slq_op** out)
+{
+    if (!out) return fail(SLQ_ERR_BAD_ARG, "operator_create: out is NULL");
+    *out = nullptr;
+    if (dtype != SLQ_F32 && dtype != SLQ_F64)
+        return fail(SLQ_ERR_BAD_ARG, "operator_create: dtype must be SLQ_F32 or SLQ_F64");
+    if (format != SLQ_CSR && format != SLQ_CSC)
+        return fail(SLQ_ERR_BAD_ARG, "operator_create: format must be SLQ_CSR or SLQ_CSC");
+    if (num_rows <= 0 || num_cols <= 0 || nnz < 0 || nnz > INT32_MAX ||
+        num_rows > INT32_MAX || num_cols > INT32_MAX)
+        return fail(SLQ_ERR_BAD_ARG, "operator_create: sizes out of range (int32 indices)");
+    if (!indptr || (nnz > 0 && (!indices || !data)))
+        return fail(SLQ_ERR_BAD_ARG, "operator_create: NULL array");
+    if (affine && num_rows != num_cols)
+        return fail(SLQ_ERR_BAD_ARG, "operator_create: A + tI needs a square matrix");
+    size_t need = 0;
+    SLQ_TRY(slq_operator_workspace_bytes(num_rows, num_cols, nnz, dtype, format,
+                                         need_transpose, &need));
+    if (!workspace || workspace_bytes < need)
+        return fail(SLQ_ERR_WORKSPACE, "operator_create: workspace too small (need " +
+                                           std::to_string(need) + " bytes)");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Carver c(workspace, workspace_bytes);
+    int32_t* flag = c.take<int32_t>(1);
+
+    // stored arrays: CSR over `srows` rows, `scols` columns
+    const int64_t srows = (format == SLQ_CSC) ? num_cols : num_rows;
+    const int64_t scols = (format == SLQ_CSC) ? num_rows : num_cols;
+    if (check_indices)
+    {
+        int sms = 0;
+        SLQ_TRY(device_sms(&sms));
+        SLQ_CK(cudaMemsetAsync(flag, 0, sizeof(int32_t), st));
+        k_check_csr<<<sms * 4, 256, 0, st>>>(indptr, indices, srows, scols, nnz, flag);
+        SLQ_LAUNCH_CK();
+        int32_t h = 0;
+        SLQ_CK(cudaMemcpyAsync(&h, flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        SLQ_CK(cudaStreamSynchronize(st));
+        if (h & 1) return fail(SLQ_ERR_BAD_CSR, "index pointer must start at 0 and end at nnz");
+        if (h & 2) return fail(SLQ_ERR_BAD_CSR, "index pointer must be non-decreasing");
+        if (h & 4) return fail(SLQ_ERR_BAD_CSR, "index out of range");
+    }
+
+    slq_op* op = new slq_op();
+    op->dtype = dtype;
+    op->affine = affine;
+    op->nrows = num_rows;
+    op->ncols = num_cols;
+    op->nnz = nnz;
+    const bool build = (format == SLQ_CSC) || need_transpose;
+    TransposeBufs t;
+    if (build)
+    {
+        slq_status s = transpose_layout(c, srows, scols, nnz, dtype, &t);
+        if (s == SLQ_OK)
+            s = transpose_csr(indptr, indices, data, srows, scols, nnz, dtype, &t, st);
+        if (s != SLQ_OK)
+        {
+            delete op;
+            return s;
+        }
+    }
+    if (format == SLQ_CSR)
+    {
+        op->a_data = data;
+        op->a_ind = indices;
+        op->a_ptr = indptr;
+        if (build)
+        {
+            op->t_data = t.t_data;
+            op->t_ind = t.t_ind;
+            op->t_ptr = t.t_ptr;
+        }
+    }
+    else
+    {   // CSC arrays are the CSR of A^T; their transpose is the CSR of A
+        op->t_data = data;
+        op->t_ind = indices;
+        op->t_ptr = indptr;
+        op->a_data = t.t_data;
+        op->a_ind = t.t_ind;
+        op->a_ptr = t.t_ptr;
+    }
+    *out = op;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_operator_destroy(slq_op* op)
+{
+    delete op;
+    return SLQ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct Launcher {
+    cudaStream_t st;
+    int sms;
+    int64_t launches = 0;
+};
+
+template <typename VT, int LV, int KS>
+slq_status spmm_inst(Launcher& L, int grid, const int32_t* ptr, const int32_t* ind,
+                     const VT* vals, int64_t nrows, int b, const VT* X,
+                     const double* sx, double shift, VT* Y, const VT* Z,
+                     const double* zc, const double* zs, int epi, double* partials,
+                     int64_t nnz, int64_t xrows)
+{
+    // compulsory traffic: matrix once, X once, Y written once, Z read once
+    const double s = sizeof(VT);
+    const double bytes = nnz * (s + 4.0) + (nrows + 1) * 4.0 + double(xrows) * b * s +
+                         double(nrows) * b * s * (Z ? 2.0 : 1.0);
+    ProfScope prof(SLQ_K_SPMM, bytes, L.st);
+    static bool attr = false;
+    const size_t smem = (epi != 0) ? 8 * static_cast<size_t>(b) * sizeof(double) : 0;
+    if (!attr)
+    {
+        SLQ_CK(cudaFuncSetAttribute(k_spmm<VT, LV, KS>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        attr = true;
+    }
+    k_spmm<VT, LV, KS><<<grid, 256, smem, L.st>>>(ptr, ind, vals, nrows, b, X, sx, shift, Y, Z,
+                                                  zc, zs, epi, partials);
+    SLQ_LAUNCH_CK();
+    ++L.launches;
+    return SLQ_OK;
+}
+
+template <typename VT>
+int spmm_grid(const Launcher& L, int64_t nrows)
+{
+    const int64_t g = (nrows + 7) / 8;
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(g, int64_t(L.sms) * 4)));
+}
+
+template <typename VT>
+slq_status spmm(Launcher& L, int grid, const int32_t* ptr, const int32_t* ind, const VT* vals,
+                int64_t nrows, int b, const VT* X, const double* sx, double shift, VT* Y,
+                const VT* Z, const double* zc, const double* zs, int epi, double* partials,
+                int64_t nnz, int64_t xrows)
+{
+#define SLQ_SPMM_CASE(BB, LV, KS)                                                         \
+    case BB:                                                                              \
+        return spmm_inst<VT, LV, KS>(L, grid, ptr, ind, vals, nrows, b, X, sx, shift, Y,  \
+                                     Z, zc, zs, epi, partials, nnz, xrows);
+    switch (b)
+    {
+        SLQ_SPMM_CASE(1, 1, 32)
+        SLQ_SPMM_CASE(2, 1, 16)
+        SLQ_SPMM_CASE(4, 1, 8)
+        SLQ_SPMM_CASE(8, 1, 4)
+        SLQ_SPMM_CASE(16, 1, 2)
+        SLQ_SPMM_CASE(32, 1, 1)
+        SLQ_SPMM_CASE(64, 2, 1)
+        SLQ_SPMM_CASE(128, 4, 1)
+        SLQ_SPMM_CASE(256, 8, 1)
+        SLQ_SPMM_CASE(512, 16, 1)
+        SLQ_SPMM_CASE(1024, 32, 1)
+        default:
+            return fail(SLQ_ERR_BAD_ARG, "block width must be a power of two <= 1024");
+    }
+#undef SLQ_SPMM_CASE
+}
+
+template <typename VT>
+constexpr int vec_of(int b)
+{
+    return (sizeof(VT) == 4) ? (b >= 4 ? 4 : 1) : (b >= 2 ? 2 : 1);
+}
+
+// Geometry shared by k_update_dots and k_reorth.
+struct StreamGeom {
+    int VEC, PT, P;
+};
+
+template <typename VT>
+StreamGeom stream_geom(int b)
+{
+    StreamGeom g;
+    g.VEC = vec_of<VT>(b);
+    g.PT = std::min(b, 64 * g.VEC);
+    g.P = g.PT / g.VEC;
+    return g;
+}
+
+template <typename VT>
+int dots_grid(const Launcher& L, int64_t n, int b, int J)
+{
+    const StreamGeom g = stream_geom<VT>(b);
+    const int G = std::max(1, (J + DOT_K - 1) / DOT_K);
+    const int RS = std::max(1, 256 / (g.P * G));
+    const int64_t gx = (n + RS - 1) / RS;
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(gx, int64_t(L.sms) * 2)));
+}
+
+template <typename VT>
+int reorth_grid(const Launcher& L, int64_t n, int b)
+{
+    const StreamGeom g = stream_geom<VT>(b);
+    const int RS = std::max(1, 512 / g.P);
+    const int64_t gx = (n + RS - 1) / RS;
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(gx, int64_t(L.sms) * 2)));
+}
+
+template <typename VT>
+slq_status update_dots(Launcher& L, int grid, int64_t n, int b, const VT* W, VT* Wout,
+                       int do_update, const VT* Vj, const double* sj, const double* aj,
+                       const VT* Vm, const double* sm, const double* bm, const VT* basis,
+                       int64_t slot_elems, int bs, int last, int J, double* partials)
+{
+    const StreamGeom g = stream_geom<VT>(b);
+    const int G = std::max(1, (J + DOT_K - 1) / DOT_K);
+    const int RS = std::max(1, 256 / (g.P * G));
+    const int threads = g.P * G * RS;
+    const size_t smem = (RS > 1) ? static_cast<size_t>(RS) * J * g.PT * sizeof(double) : 0;
+    dim3 grd(grid, b / g.PT);
+    const double vb = double(n) * b * sizeof(VT);
+    ProfScope prof(SLQ_K_DOTS, vb * (1 + J + (do_update ? (Vm ? 3 : 2) : 0)), L.st);
+#define SLQ_DOTS(VECV)                                                                    \
+    {                                                                                     \
+        static bool attr = false;                                                         \
+        if (!attr)                                                                        \
+        {                                                                                 \
+            SLQ_CK(cudaFuncSetAttribute(k_update_dots<VT, VECV>,                          \
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                                        200 * 1024));                                     \
+            attr = true;                                                                  \
+        }                                                                                 \
+        k_update_dots<VT, VECV><<<grd, threads, smem, L.st>>>(                            \
+            n, b, g.PT, G, RS, W, Wout, do_update, Vj, sj, aj, Vm, sm, bm, basis,         \
+            slot_elems, bs, last, J, partials);                                           \
+    }
+    if (g.VEC == 4) SLQ_DOTS(4)
+    else if (g.VEC == 2) SLQ_DOTS(2)
+    else SLQ_DOTS(1)
+#undef SLQ_DOTS
+    SLQ_LAUNCH_CK();
+    ++L.launches;
+    return SLQ_OK;
+}
+
+template <typename VT>
+slq_status reorth(Launcher& L, int grid, int64_t n, int b, const VT* Win, VT* Wout,
+                  int do_update, const VT* Vj, const double* sj, const double* aj,
+                  const VT* Vm, const double* sm, const double* bm, const VT* basis,
+                  int64_t slot_elems, int bs, int last, int J, const VT* coef,
+                  int want_norm, double* partials)
+{
+    const StreamGeom g = stream_geom<VT>(b);
+    const int RS = std::max(1, 512 / g.P);
+    const int threads = g.P * RS;
+    const size_t smem = ((static_cast<size_t>(J) * g.PT * sizeof(VT) + 15) / 16) * 16 +
+                        static_cast<size_t>(RS) * g.PT * sizeof(double);
+    dim3 grd(grid, b / g.PT);
+    const double vb = double(n) * b * sizeof(VT);
+    ProfScope prof(SLQ_K_REORTH, vb * (2 + J + (do_update ? (Vm ? 2 : 1) : 0)), L.st);
+#define SLQ_REORTH(VECV)                                                                  \
+    {                                                                                     \
+        static bool attr = false;                                                         \
+        if (!attr)                                                                        \
+        {                                                                                 \
+            SLQ_CK(cudaFuncSetAttribute(k_reorth<VT, VECV>,                               \
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                                        200 * 1024));                                     \
+            attr = true;                                                                  \
+        }                                                                                 \
+        k_reorth<VT, VECV><<<grd, threads, smem, L.st>>>(                                 \
+            n, b, g.PT, RS, Win, Wout, do_update, Vj, sj, aj, Vm, sm, bm, basis,          \
+            slot_elems, bs, last, J, coef, want_norm, partials);                          \
+    }
+    if (g.VEC == 4) SLQ_REORTH(4)
+    else if (g.VEC == 2) SLQ_REORTH(2)
+    else SLQ_REORTH(1)
+#undef SLQ_REORTH
+    SLQ_LAUNCH_CK();
+    ++L.launches;
+    return SLQ_OK;
+}
+
+template <typename VT>
+slq_status finalize(Launcher& L, const double* partials, int nparts, int cols, int mode,
+                    double* out, VT* coef, const double* scales, int b, int bs, int last,
+                    double* next_scale, int32_t* active, int32_t* size, int check_break,
+                    double thr, int step)
+{
+    const int grid = (cols + 31) / 32;
+    ProfScope prof(SLQ_K_FINALIZE, double(nparts) * cols * 8.0, L.st);
+    k_finalize<VT><<<grid, 1024, 0, L.st>>>(partials, nparts, cols, mode, out, coef, scales, b,
+                                           bs, last, next_scale, active, size, check_break, thr,
+                                           step);
+    SLQ_LAUNCH_CK();
+    ++L.launches;
+    return SLQ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// run plan and workspace
+// ---------------------------------------------------------------------------
+
+struct RunPlan {
+    int gram, orth, m, bs, b, q;
+    int64_t nv, nu;       // probe length, U length (gram)
+    int64_t wpp;          // parity words per probe
+    int cw, nchunks;      // parity chunking
+    size_t partial_cols;  // max partial buffer doubles
+};
+
+struct RunBufs {
+    void* V;
+    void* U;
+    void* W;
+    void* W2;
+    double* scale_v;
+    double* scale_u;
+    double* alpha;
+    double* beta;
+    void* coef;
+    int32_t* active;
+    int32_t* size;
+    int32_t* status;
+    double* partials;
+    double* samples;
+    double* params;
+    uint64_t* starts;
+    uint64_t* chunk_polys;
+};
+
+int buffer_size(int gram, int orth, int m)
+{
+    if (gram)
+    {
+        if (orth == 0) return 2;
+        if (orth < 0 || orth > m - 1) return m;
+        return orth + 1;
+    }
+    if (orth == 0 || orth == 1) return 2;
+    if (orth < 0 || orth > m) return m;
+    return orth;
+}
+
+slq_status make_plan(const slq_op* op, const slq_params* p, int q, RunPlan* r)
+{
+    if (!op || !p) return fail(SLQ_ERR_BAD_ARG, "NULL operator or params");
+    if (p->lanczos_degree < 1 || p->lanczos_degree > SLQ_MAX_DEGREE)
+        return fail(SLQ_ERR_BAD_ARG, "lanczos_degree must be in [1, " +
+                                         std::to_string(SLQ_MAX_DEGREE) + "]");
+    if (p->min_num_samples < 1 || p->max_num_samples < 1 ||
+        p->min_num_samples > p->max_num_samples)
+        return fail(SLQ_ERR_BAD_ARG, "need 1 <= min_num_samples <= max_num_samples");
+    if (p->func < SLQ_FUNC_LOG || p->func > SLQ_FUNC_ID)
+        return fail(SLQ_ERR_BAD_ARG, "unknown matrix function");
+    if (p->seed < 0) return fail(SLQ_ERR_BAD_ARG, "seed must be >= 0");
+    if (p->first_probe < 0) return fail(SLQ_ERR_BAD_ARG, "first_probe must be >= 0");
+    if (q < 1) return fail(SLQ_ERR_BAD_ARG, "num_inquiries must be >= 1");
+    if (q > 1 && !op->affine)
+        return fail(SLQ_ERR_BAD_ARG, "several inquiries need an affine operator");
+    if (q > 1 && p->gram)
+        return fail(SLQ_ERR_UNSUPPORTED,
+                    "eigenvalue shift across inquiries is not valid for gram operators");
+    if (!p->gram && op->nrows != op->ncols)
+        return fail(SLQ_ERR_BAD_ARG, "non-gram runs need a square matrix");
+    if (p->gram && !op->t_ptr)
+        return fail(SLQ_ERR_BAD_ARG, "gram runs need an operator created with need_transpose");
+    if (p->orthogonalize > p->lanczos_degree)
+        return fail(SLQ_ERR_BAD_ARG, "orthogonalize must be at most lanczos_degree");
+    if (p->rng != SLQ_RNG_PARITY && p->rng != SLQ_RNG_FAST)
+        return fail(SLQ_ERR_BAD_ARG, "unknown rng mode");
+    r->gram = p->gram ? 1 : 0;
+    r->orth = p->orthogonalize;
+    r->m = p->lanczos_degree;
+    r->bs = buffer_size(r->gram, r->orth, r->m);
+    r->q = q;
+    r->nv = r->gram ? op->ncols : op->nrows;
+    r->nu = r->gram ? op->nrows : 0;
+    const int bmax = (op->dtype == SLQ_F64) ? 512 : 1024;
+    int b = p->block_size;
+    if (b <= 0) b = std::min(next_pow2(p->max_num_samples), 256);
+    b = std::min(next_pow2(b), bmax);
+    b = std::min(b, next_pow2(p->max_num_samples));
+    r->b = b;
+    r->wpp = r->nv / 64 + 1;
+    r->cw = 64;
+    while ((r->wpp + r->cw - 1) / r->cw > 65535) r->cw *= 2;
+    r->nchunks = static_cast<int>((r->wpp + r->cw - 1) / r->cw);
+    return SLQ_OK;
+}
+
+template <typename VT>
+void carve(Carver& c, const RunPlan& r, int sms, RunBufs* B)
+{
+    const int64_t vslot = r.nv * r.b;
+    const int64_t uslot = r.nu * r.b;
+    B->V = c.take<VT>(static_cast<size_t>(r.bs) * vslot);
+    B->U = r.gram ? c.take<VT>(static_cast<size_t>(r.bs) * uslot) : nullptr;
+    B->W = r.gram ? nullptr : c.take<VT>(vslot);
+    B->W2 = (!r.gram && r.orth != 0) ? c.take<VT>(vslot) : nullptr;
+    B->scale_v = c.take<double>(static_cast<size_t>(r.bs) * r.b);
+    B->scale_u = c.take<double>(static_cast<size_t>(r.bs) * r.b);
+    B->alpha = c.take<double>(static_cast<size_t>(r.m) * r.b);
+    B->beta = c.take<double>(static_cast<size_t>(r.m) * r.b);
+    B->coef = c.take<VT>(static_cast<size_t>(r.bs) * r.b);
+    B->active = c.take<int32_t>(r.b);
+    B->size = c.take<int32_t>(r.b);
+    B->status = c.take<int32_t>(r.b);
+    // partial sums: SpMM grid <= 4*sms, stream kernels <= 2*sms (x J <= MAX_J)
+    const size_t pcols = std::max<size_t>(static_cast<size_t>(sms) * 4 * r.b,
+                                          static_cast<size_t>(sms) * 2 * MAX_J * r.b);
+    B->partials = c.take<double>(pcols);
+    B->samples = c.take<double>(static_cast<size_t>(r.b) * r.q);
+    B->params = c.take<double>(r.q);
+    B->starts = c.take<uint64_t>(static_cast<size_t>(r.b) * 4);
+    B->chunk_polys = c.take<uint64_t>(static_cast<size_t>(r.nchunks) * 4);
+}
+
+template <typename VT>
+slq_status launch_probes(Launcher& L, const RunPlan& r, int rng, int64_t seed, int64_t first,
+                         int count, const RunBufs& B, VT* X)
+{
+    dim3 grid((r.b + 127) / 128, r.nchunks);
+    ProfScope prof(SLQ_K_PROBE, double(r.nv) * r.b * sizeof(VT), L.st);
+    if (rng == SLQ_RNG_PARITY)
+        k_probe_parity<VT><<<grid, 128, 0, L.st>>>(r.nv, r.b, count, r.wpp, r.cw, B.starts,
+                                                   B.chunk_polys, X);
+    else
+        k_probe_fast<VT><<<grid, 128, 0, L.st>>>(r.nv, r.b, count, first,
+                                                 static_cast<uint64_t>(seed) * 0xd1342543de82ef95ULL,
+                                                 r.wpp, r.cw, X);
+    SLQ_LAUNCH_CK();
+    ++L.launches;
+    return SLQ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// one probe block: Lanczos (symmetric) or Golub-Kahn (gram)
+// ---------------------------------------------------------------------------
+
+template <typename VT>
+slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, const RunPlan& r,
+                        const RunBufs& B, int count, double shift)
+{
+    const int b = r.b;
+    const int bs = r.bs;
+    const int m = r.m;
+    const int64_t vslot = r.nv * b;
+    const int64_t uslot = r.nu * b;
+    VT* V = static_cast<VT*>(B.V);
+    VT* U = static_cast<VT*>(B.U);
+    VT* W = static_cast<VT*>(B.W);
+    VT* W2 = static_cast<VT*>(B.W2);
+    VT* coef = static_cast<VT*>(B.coef);
+    const VT* Aval = static_cast<const VT*>(op->a_data);
+    const VT* Tval = static_cast<const VT*>(op->t_data);
+    const double thr = p->lanczos_tol * std::sqrt(static_cast<double>(r.nv));
+    auto sv_of = [&](int vec) { return B.scale_v + static_cast<int64_t>(((vec % bs) + bs) % bs) * b; };
+    auto su_of = [&](int vec) { return B.scale_u + static_cast<int64_t>(((vec % bs) + bs) % bs) * b; };
+    auto Vs = [&](int vec) { return V + static_cast<int64_t>(((vec % bs) + bs) % bs) * vslot; };
+    auto Us = [&](int vec) { return U + static_cast<int64_t>(((vec % bs) + bs) % bs) * uslot; };
+
+    // dots + finalize(COEF) + reorth over chunks of MAX_J basis vectors;
+    // returns the number of partial rows of the norm partials in *nparts.
+    auto reorthogonalize = [&](int64_t n, VT* w_in_first, VT* w_work, VT* w_out, int do_update,
+                               const VT* Vj, const double* sj, const double* aj, const VT* Vm,
+                               const double* sm, const double* bm, const VT* basis,
+                               int64_t slot_elems, const double* scales, int last, int J,
+                               int* nparts) -> slq_status {
+        const int dg = dots_grid<VT>(L, n, b, std::min(J, MAX_J));
+        for (int c0 = 0; c0 < J; c0 += MAX_J)
+        {
+            const int Jc = std::min(MAX_J, J - c0);
+            const bool first = (c0 == 0);
+            SLQ_TRY(update_dots<VT>(L, dg, n, b, first ? w_in_first : w_work, w_work,
+                                    first ? do_update : 0, Vj, sj, aj, Vm, sm, bm, basis,
+                                    slot_elems, bs, last - c0, Jc, B.partials));
+            SLQ_TRY(finalize<VT>(L, B.partials, dg, Jc * b, FIN_COEF, nullptr,
+                                 coef + static_cast<int64_t>(c0) * b, scales, b, bs, last - c0,
+                                 nullptr, nullptr, nullptr, 0, 0.0, 0));
+        }
+        const int rg = reorth_grid<VT>(L, n, b);
+        for (int c0 = 0; c0 < J; c0 += MAX_J)
+        {
+            const int Jc = std::min(MAX_J, J - c0);
+            const bool lastc = (c0 + MAX_J >= J);
+            SLQ_TRY(reorth<VT>(L, rg, n, b, w_work, lastc ? w_out : w_work, 0, nullptr, nullptr,
+                               nullptr, nullptr, nullptr, nullptr, basis, slot_elems, bs,
+                               last - c0, Jc, coef + static_cast<int64_t>(c0) * b,
+                               lastc ? 1 : 0, B.partials));
+        }
+        *nparts = rg;
+        return SLQ_OK;
+    };
+
+    if (!r.gram)
+    {
+        const int sg = spmm_grid<VT>(L, r.nv);
+        for (int j = 0; j < m; ++j)
+        {
+            VT* vj = Vs(j);
+            SLQ_TRY(spmm<VT>(L, sg, op->a_ptr, op->a_ind, Aval, r.nv, b, vj, sv_of(j), shift, W,
+                             nullptr, nullptr, nullptr, 1, B.partials, op->nnz, r.nv));
+            double* aj = B.alpha + static_cast<int64_t>(j) * b;
+            SLQ_TRY(finalize<VT>(L, B.partials, sg, b, FIN_STORE, aj, nullptr, nullptr, b, bs, 0,
+                                 nullptr, nullptr, nullptr, 0, 0.0, j));
+            const VT* vm = (j > 0) ? Vs(j - 1) : nullptr;
+            const double* sm = (j > 0) ? sv_of(j - 1) : nullptr;
+            const double* bm = (j > 0) ? B.beta + static_cast<int64_t>(j - 1) * b : nullptr;
+            int J = 0;
+            if (r.orth != 0)
+                J = static_cast<int>(std::min<int64_t>((j < bs) ? j + 1 : bs, r.nv));
+            int nparts = 0;
+            if (J == 0)
+            {
+                const int rg = reorth_grid<VT>(L, r.nv, b);
+                SLQ_TRY(reorth<VT>(L, rg, r.nv, b, W, Vs(j + 1), 1, vj, sv_of(j), aj, vm, sm, bm,
+                                   V, vslot, bs, j, 0, coef, 1, B.partials));
+                nparts = rg;
+            }
+            else
+            {
+                SLQ_TRY(reorthogonalize(r.nv, W, W2, Vs(j + 1), 1, vj, sv_of(j), aj, vm, sm, bm,
+                                        V, vslot, B.scale_v, j, J, &nparts));
+            }
+            SLQ_TRY(finalize<VT>(L, B.partials, nparts, b, FIN_NORM,
+                                 B.beta + static_cast<int64_t>(j) * b, nullptr, nullptr, b, bs, 0,
+                                 sv_of(j + 1), B.active, B.size, 1, thr, j));
+        }
+    }
+    else
+    {
+        const int sgu = spmm_grid<VT>(L, r.nu);
+        const int sgv = spmm_grid<VT>(L, r.nv);
+        for (int j = 0; j < m; ++j)
+        {
+            int no = 0;
+            if (r.orth != 0) no = (j < bs) ? j : bs - 1;
+            // u_j = A v_j - beta_{j-1} u_{j-1}
+            const int Ju = (j > 0) ? static_cast<int>(std::min<int64_t>(no, r.nu)) : 0;
+            VT* uj = Us(j);
+            SLQ_TRY(spmm<VT>(L, sgu, op->a_ptr, op->a_ind, Aval, r.nu, b, Vs(j), sv_of(j), shift,
+                             uj, (j > 0) ? Us(j - 1) : nullptr,
+                             (j > 0) ? B.beta + static_cast<int64_t>(j - 1) * b : nullptr,
+                             (j > 0) ? su_of(j - 1) : nullptr, Ju > 0 ? 0 : 2, B.partials,
+                             op->nnz, r.nv));
+            int nparts = sgu;
+            if (Ju > 0)
+                SLQ_TRY(reorthogonalize(r.nu, uj, uj, uj, 0, nullptr, nullptr, nullptr, nullptr,
+                                        nullptr, nullptr, U, uslot, B.scale_u, j - 1, Ju,
+                                        &nparts));
+            double* aj = B.alpha + static_cast<int64_t>(j) * b;
+            SLQ_TRY(finalize<VT>(L, B.partials, nparts, b, FIN_NORM, aj, nullptr, nullptr, b, bs,
+                                 0, su_of(j), B.active, B.size, 0, 0.0, j));
+            // v_{j+1} = A^T u_j - alpha_j v_j
+            const int Jv = static_cast<int>(std::min<int64_t>(no, r.nv));
+            VT* vn = Vs(j + 1);
+            SLQ_TRY(spmm<VT>(L, sgv, op->t_ptr, op->t_ind, Tval, r.nv, b, uj, su_of(j), shift, vn,
+                             Vs(j), aj, sv_of(j), Jv > 0 ? 0 : 2, B.partials, op->nnz, r.nu));
+            nparts = sgv;
+            if (Jv > 0)
+                SLQ_TRY(reorthogonalize(r.nv, vn, vn, vn, 0, nullptr, nullptr, nullptr, nullptr,
+                                        nullptr, nullptr, V, vslot, B.scale_v, j, Jv, &nparts));
+            SLQ_TRY(finalize<VT>(L, B.partials, nparts, b, FIN_NORM,
+                                 B.beta + static_cast<int64_t>(j) * b, nullptr, nullptr, b, bs, 0,
+                                 sv_of(j + 1), B.active, B.size, 1, thr, j));
+        }
+    }
+    return SLQ_OK;
+}
+
+template <typename VT>
+slq_status run_typed(slq_op* op, const slq_params* p, const double* parameters, int q,
+                     void* workspace, size_t workspace_bytes, cudaStream_t st, slq_result* res)
+{
+    RunPlan r;
+    SLQ_TRY(make_plan(op, p, q, &r));
+    Launcher L;
+    L.st = st;
+    SLQ_TRY(device_sms(&L.sms));
+    Carver c(workspace, workspace_bytes);
+    RunBufs B;
+    carve<VT>(c, r, L.sms, &B);
+    if (!c.fits() || !workspace)
+        return fail(SLQ_ERR_WORKSPACE, "run: workspace too small (need " + std::to_string(c.off) +
+                                           " bytes)");
+
+    const int max_s = p->max_num_samples;
+    const int m = r.m;
+    const int b = r.b;
+    std::vector<double> params(q, 0.0);
+    if (op->affine && parameters)
+        for (int j = 0; j < q; ++j) params[j] = parameters[j];
+    const double shift = op->affine ? params[0] : 0.0;
+    SLQ_CK(cudaMemcpyAsync(B.params, params.data(), sizeof(double) * q, cudaMemcpyHostToDevice, st));
+
+    // parity stream set-up on the host: state of probe 0 and the per-chunk
+    // advance polynomials
+    uint64_t cur[4] = {0, 0, 0, 0};
+    Poly256 advance = {{1, 0, 0, 0}};
+    if (p->rng == SLQ_RNG_PARITY)
+    {
+        if (!self_check())
+            return fail(SLQ_ERR_CUDA, "xoshiro256 jump polynomial self-check failed");
+        stream_state(p->seed, cur);
+        jump_ahead(cur, static_cast<uint64_t>(p->first_probe) * static_cast<uint64_t>(r.wpp));
+        advance = jump_poly(static_cast<uint64_t>(r.wpp));
+        std::vector<uint64_t> polys(static_cast<size_t>(r.nchunks) * 4);
+        Poly256 step = jump_poly(static_cast<uint64_t>(r.cw));
+        Poly256 acc = {{1, 0, 0, 0}};
+        for (int cidx = 0; cidx < r.nchunks; ++cidx)
+        {
+            for (int k = 0; k < 4; ++k) polys[static_cast<size_t>(cidx) * 4 + k] = acc.w[k];
+            acc = poly_mulmod(acc, step);
+        }
+        SLQ_CK(cudaMemcpyAsync(B.chunk_polys, polys.data(), polys.size() * sizeof(uint64_t),
+                               cudaMemcpyHostToDevice, st));
+    }
+
+    // outputs
+    for (int64_t i = 0; i < static_cast<int64_t>(max_s) * q; ++i) res->samples[i] = NAN;
+    for (int i = 0; i < max_s; ++i)
+    {
+        res->processed_samples_indices[i] = 0;
+        if (res->lanczos_size) res->lanczos_size[i] = 0;
+    }
+    for (int j = 0; j < q; ++j)
+    {
+        res->converged[j] = 0;
+        res->num_samples_used[j] = 0;
+        res->num_outliers[j] = 0;
+        res->trace[j] = NAN;
+        res->error[j] = NAN;
+    }
+    if (res->alpha)
+        for (int64_t i = 0; i < static_cast<int64_t>(max_s) * m; ++i) res->alpha[i] = NAN;
+    if (res->beta)
+        for (int64_t i = 0; i < static_cast<int64_t>(max_s) * m; ++i) res->beta[i] = NAN;
+
+    cudaEvent_t ev0, ev1;
+    SLQ_CK(cudaEventCreate(&ev0));
+    SLQ_CK(cudaEventCreate(&ev1));
+    SLQ_CK(cudaEventRecord(ev0, st));
+
+    std::vector<double> hs(static_cast<size_t>(b) * q);
+    std::vector<int32_t> hsize(b), hstat(b);
+    std::vector<double> ha, hb;
+    if (res->alpha || res->beta)
+    {
+        ha.resize(static_cast<size_t>(m) * b);
+        hb.resize(static_cast<size_t>(m) * b);
+    }
+    std::vector<uint64_t> hstarts(static_cast<size_t>(b) * 4);
+    const double s0 = 1.0 / std::sqrt(static_cast<double>(r.nv));
+    int nproc = 0;
+    int all = 0;
+    int blocks = 0;
+    int64_t computed = 0;
+    slq_status status = SLQ_OK;
+    bool eig_failed = false;
+    for (int g = 0; g < max_s && !all; g += b)
+    {
+        const int count = std::min(b, max_s - g);
+        if (p->rng == SLQ_RNG_PARITY)
+        {
+            for (int pi = 0; pi < count; ++pi)
+            {
+                for (int k = 0; k < 4; ++k) hstarts[static_cast<size_t>(pi) * 4 + k] = cur[k];
+                apply_poly(advance, cur);
+            }
+            SLQ_CK(cudaMemcpyAsync(B.starts, hstarts.data(),
+                                   sizeof(uint64_t) * 4 * static_cast<size_t>(count),
+                                   cudaMemcpyHostToDevice, st));
+        }
+        SLQ_TRY(launch_probes<VT>(L, r, p->rng, p->seed, p->first_probe + g, count, B,
+                                  static_cast<VT*>(B.V)));
+        {
+        ProfScope prof(SLQ_K_OTHER, 0.0, st);
+        k_init_block<<<(b + 127) / 128, 128, 0, st>>>(count, b, m, s0, B.scale_v, B.active,
+                                                     B.size);
+        SLQ_LAUNCH_CK();
+        ++L.launches;
+        }
+        SLQ_TRY(krylov_block<VT>(L, op, p, r, B, count, shift));
+        {
+        ProfScope prof(SLQ_K_EIG, double(m) * b * 16.0 + double(count) * q * 8.0, st);
+        k_eig_quad<<<(count + 127) / 128, 128, 0, st>>>(
+            count, b, m, B.alpha, B.beta, B.size, r.gram, p->func, p->exponent, B.params, q,
+            static_cast<double>(r.nv), B.samples, nullptr, nullptr, B.status);
+        SLQ_LAUNCH_CK();
+        ++L.launches;
+        }
+        SLQ_CK(cudaMemcpyAsync(hs.data(), B.samples, sizeof(double) * count * q,
+                               cudaMemcpyDeviceToHost, st));
+        SLQ_CK(cudaMemcpyAsync(hsize.data(), B.size, sizeof(int32_t) * count,
+                               cudaMemcpyDeviceToHost, st));
+        SLQ_CK(cudaMemcpyAsync(hstat.data(), B.status, sizeof(int32_t) * count,
+                               cudaMemcpyDeviceToHost, st));
+        if (!ha.empty())
+        {
+            SLQ_CK(cudaMemcpyAsync(ha.data(), B.alpha, sizeof(double) * m * b,
+                                   cudaMemcpyDeviceToHost, st));
+            SLQ_CK(cudaMemcpyAsync(hb.data(), B.beta, sizeof(double) * m * b,
+                                   cudaMemcpyDeviceToHost, st));
+        }
+        SLQ_CK(cudaStreamSynchronize(st));
+        ++blocks;
+        computed += count;
+        for (int pi = 0; pi < count && !all; ++pi)
+        {
+            const int s = g + pi;
+            for (int j = 0; j < q; ++j)
+                res->samples[static_cast<int64_t>(s) * q + j] = hs[static_cast<size_t>(pi) * q + j];
+            if (res->lanczos_size) res->lanczos_size[s] = hsize[pi];
+            if (hstat[pi] == 2) eig_failed = true;
+            if (!ha.empty())
+                for (int i = 0; i < m; ++i)
+                {
+                    if (res->alpha)
+                        res->alpha[static_cast<int64_t>(s) * m + i] =
+                            (i < hsize[pi]) ? ha[static_cast<size_t>(i) * b + pi] : NAN;
+                    if (res->beta)
+                        res->beta[static_cast<int64_t>(s) * m + i] =
+                            (i < hsize[pi]) ? hb[static_cast<size_t>(i) * b + pi] : NAN;
+                }
+            // with a known eigenvalue relation every inquiry is refreshed by
+            // each sample (c_trace_estimator.cpp:572-583)
+            if (op->affine && q > 1)
+                for (int j = 0; j < q; ++j) res->converged[j] = 0;
+            res->processed_samples_indices[nproc++] = s;
+            all = slq_check_convergence(res->samples, q, p->min_num_samples,
+                                        res->processed_samples_indices, nproc,
+                                        p->confidence_level, p->error_atol, p->error_rtol,
+                                        res->error, res->num_samples_used, res->converged);
+        }
+    }
+    SLQ_CK(cudaEventRecord(ev1, st));
+    SLQ_CK(cudaEventSynchronize(ev1));
+    float ms = 0.0f;
+    SLQ_CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+
+    slq_average_estimates(p->confidence_level, p->outlier_significance_level, q, max_s,
+                          res->num_samples_used, res->processed_samples_indices, res->samples,
+                          res->num_outliers, res->trace, res->error);
+    res->all_converged = all;
+    res->num_blocks = blocks;
+    res->num_probes_computed = computed;
+    res->gpu_launches = L.launches;
+    res->alg_wall_time = ms * 1e-3f;
+    if (eig_failed) status = fail(SLQ_ERR_EIGEN, "tridiagonal eigen-solve did not converge");
+    return status;
+}
+
+}  // namespace
+
+extern "C" slq_status slq_run_workspace_bytes(const slq_op* op, const slq_params* p,
+                                              int num_inquiries, size_t* bytes)
+{
+    if (!bytes) return fail(SLQ_ERR_BAD_ARG, "bytes is NULL");
+    RunPlan r;
+    SLQ_TRY(make_plan(op, p, num_inquiries, &r));
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
+    Carver c(nullptr, 0);
+    RunBufs B;
+    if (op->dtype == SLQ_F64) carve<double>(c, r, sms, &B);
+    else carve<float>(c, r, sms, &B);
+    *bytes = c.off + 256;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_run(slq_op* op, const slq_params* p, const double* parameters,
+                              int num_inquiries, void* workspace, size_t workspace_bytes,
+                              void* stream, slq_result* result)
+{
+    if (!result || !result->trace || !result->error || !result->samples ||
+        !result->processed_samples_indices || !result->num_samples_used ||
+        !result->num_outliers || !result->converged)
+        return fail(SLQ_ERR_BAD_ARG, "run: result arrays missing");
+    if (!op) return fail(SLQ_ERR_BAD_ARG, "run: operator is NULL");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (op->dtype == SLQ_F64)
+        return run_typed<double>(op, p, parameters, num_inquiries, workspace, workspace_bytes, st,
+                                 result);
+    return run_typed<float>(op, p, parameters, num_inquiries, workspace, workspace_bytes, st,
+                            result);
+}
+
+// ---------------------------------------------------------------------------
+// operator product, probes, nodes/weights, device info
+// ---------------------------------------------------------------------------
+
+extern "C" slq_status slq_operator_dot(slq_op* op, int transpose, double t, const void* x,
+                                       void* y, int width, void* stream)
+{
+    if (!op || !x || !y) return fail(SLQ_ERR_BAD_ARG, "operator_dot: NULL argument");
+    if (x == y) return fail(SLQ_ERR_BAD_ARG, "operator_dot: x and y must not alias");
+    if (!is_pow2(width) || width > ((op->dtype == SLQ_F64) ? 512 : 1024))
+        return fail(SLQ_ERR_BAD_ARG, "operator_dot: width must be a power of two");
+    if (transpose && !op->t_ptr)
+        return fail(SLQ_ERR_BAD_ARG, "operator_dot: operator has no transpose");
+    Launcher L;
+    L.st = static_cast<cudaStream_t>(stream);
+    SLQ_TRY(device_sms(&L.sms));
+    const double shift = op->affine ? t : 0.0;
+    const int64_t rows = transpose ? op->ncols : op->nrows;
+    const int32_t* ptr = transpose ? op->t_ptr : op->a_ptr;
+    const int32_t* ind = transpose ? op->t_ind : op->a_ind;
+    const void* val = transpose ? op->t_data : op->a_data;
+    if (op->dtype == SLQ_F64)
+        return spmm<double>(L, spmm_grid<double>(L, rows), ptr, ind,
+                            static_cast<const double*>(val), rows, width,
+                            static_cast<const double*>(x), nullptr, shift,
+                            static_cast<double*>(y), nullptr, nullptr, nullptr, 0, nullptr,
+                            op->nnz, transpose ? op->nrows : op->ncols);
+    return spmm<float>(L, spmm_grid<float>(L, rows), ptr, ind, static_cast<const float*>(val),
+                       rows, width, static_cast<const float*>(x), nullptr, shift,
+                       static_cast<float*>(y), nullptr, nullptr, nullptr, 0, nullptr,
+                       op->nnz, transpose ? op->nrows : op->ncols);
+}
+
+extern "C" slq_status slq_generate_probes_workspace_bytes(int64_t len, int width,
+                                                          size_t* bytes)
+{
+    if (!bytes || len <= 0 || width <= 0) return fail(SLQ_ERR_BAD_ARG, "bad argument");
+    const int64_t wpp = len / 64 + 1;
+    int cw = 64;
+    while ((wpp + cw - 1) / cw > 65535) cw *= 2;
+    const int64_t nchunks = (wpp + cw - 1) / cw;
+    Carver c(nullptr, 0);
+    c.take<uint64_t>(static_cast<size_t>(width) * 4);
+    c.take<uint64_t>(static_cast<size_t>(nchunks) * 4);
+    *bytes = c.off + 256;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_generate_probes(int64_t seed, int rng, int64_t len, int64_t first,
+                                          int count, int width, int dtype, void* out,
+                                          void* workspace, size_t workspace_bytes, void* stream)
+{
+    if (!out || len <= 0 || first < 0 || count < 0 || width <= 0 || count > width ||
+        seed < 0 || (rng != SLQ_RNG_PARITY && rng != SLQ_RNG_FAST))
+        return fail(SLQ_ERR_BAD_ARG, "generate_probes: bad argument");
+    size_t need = 0;
+    SLQ_TRY(slq_generate_probes_workspace_bytes(len, width, &need));
+    if (!workspace || workspace_bytes < need)
+        return fail(SLQ_ERR_WORKSPACE, "generate_probes: workspace too small");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    RunPlan r;
+    r.nv = len;
+    r.b = width;
+    r.wpp = len / 64 + 1;
+    r.cw = 64;
+    while ((r.wpp + r.cw - 1) / r.cw > 65535) r.cw *= 2;
+    r.nchunks = static_cast<int>((r.wpp + r.cw - 1) / r.cw);
+    Carver c(workspace, workspace_bytes);
+    RunBufs B;
+    B.starts = c.take<uint64_t>(static_cast<size_t>(width) * 4);
+    B.chunk_polys = c.take<uint64_t>(static_cast<size_t>(r.nchunks) * 4);
+    if (rng == SLQ_RNG_PARITY)
+    {
+        if (!self_check()) return fail(SLQ_ERR_CUDA, "jump polynomial self-check failed");
+        uint64_t cur[4];
+        stream_state(seed, cur);
+        jump_ahead(cur, static_cast<uint64_t>(first) * static_cast<uint64_t>(r.wpp));
+        const Poly256 adv = jump_poly(static_cast<uint64_t>(r.wpp));
+        std::vector<uint64_t> hs(static_cast<size_t>(width) * 4, 0);
+        for (int pi = 0; pi < count; ++pi)
+        {
+            for (int k = 0; k < 4; ++k) hs[static_cast<size_t>(pi) * 4 + k] = cur[k];
+            apply_poly(adv, cur);
+        }
+        std::vector<uint64_t> polys(static_cast<size_t>(r.nchunks) * 4);
+        const Poly256 step = jump_poly(static_cast<uint64_t>(r.cw));
+        Poly256 acc = {{1, 0, 0, 0}};
+        for (int ci = 0; ci < r.nchunks; ++ci)
+        {
+            for (int k = 0; k < 4; ++k) polys[static_cast<size_t>(ci) * 4 + k] = acc.w[k];
+            acc = poly_mulmod(acc, step);
+        }
+        SLQ_CK(cudaMemcpyAsync(B.starts, hs.data(), hs.size() * 8, cudaMemcpyHostToDevice, st));
+        SLQ_CK(cudaMemcpyAsync(B.chunk_polys, polys.data(), polys.size() * 8,
+                               cudaMemcpyHostToDevice, st));
+        SLQ_CK(cudaStreamSynchronize(st));  // host vectors go out of scope
+    }
+    Launcher L;
+    L.st = st;
+    SLQ_TRY(device_sms(&L.sms));
+    if (dtype == SLQ_F64)
+        return launch_probes<double>(L, r, rng, seed, first, count, B, static_cast<double*>(out));
+    return launch_probes<float>(L, r, rng, seed, first, count, B, static_cast<float*>(out));
+}
+
+extern "C" slq_status slq_nodes_weights(const double* alpha, const double* beta,
+                                        const int32_t* sizes, int count, int m, int gram,
+                                        double* theta, double* tau, int32_t* status,
+                                        void* stream)
+{
+    if (!alpha || !beta || !sizes || !theta || !tau || !status || count <= 0 || m <= 0 ||
+        m > EIG_MAX)
+        return fail(SLQ_ERR_BAD_ARG, "nodes_weights: bad argument");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_eig_quad<<<(count + 127) / 128, 128, 0, st>>>(count, count, m, alpha, beta, sizes, gram, 0,
+                                                   1.0, nullptr, 0, 1.0, nullptr, theta, tau,
+                                                   status);
+    SLQ_LAUNCH_CK();
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_device_info(int* num_devices, int* num_sms, int* max_threads_per_sm)
+{
+    int n = 0;
+    SLQ_CK(cudaGetDeviceCount(&n));
+    if (num_devices) *num_devices = n;
+    if (n > 0)
+    {
+        int dev = 0;
+        SLQ_CK(cudaGetDevice(&dev));
+        if (num_sms) SLQ_CK(cudaDeviceGetAttribute(num_sms, cudaDevAttrMultiProcessorCount, dev));
+        if (max_threads_per_sm)
+            SLQ_CK(cudaDeviceGetAttribute(max_threads_per_sm,
+                                          cudaDevAttrMaxThreadsPerMultiProcessor, dev));
+    }
+    return SLQ_OK;
+}
+
+extern "C" void slq_xoshiro_jump_ahead(uint64_t* state, uint64_t k) { jump_ahead(state, k); }
+
+extern "C" const char* slq_last_error(void) { return g_error.c_str(); }
+
+extern "C" int slq_abi_version(void) { return SLQ_ABI_VERSION; }

@@ -1,0 +1,900 @@
+// Device kernels of the B200 SLQ engine.
+//
+// Data layout.  A probe block is b column vectors stored row-major, [len][b]:
+// element (row r, probe p) at r*b + p, so one matrix row's gather reads b
+// contiguous values (one 128-byte line per 32 FP32 probes) and every vector
+// kernel streams contiguous memory.  A Krylov basis is bs such blocks
+// ("slots") back to back; slot (v mod bs) holds basis vector v, stored
+// unnormalised together with a per-probe scale ([bs][b] doubles) so that a
+// normalisation never needs its own pass over the vector.
+//
+// Precision.  Vector storage and SpMM accumulation use the operator's dtype
+// (FP32 in mixed mode, FP64 in FP64 mode); every reduction (alpha, beta,
+// reorthogonalisation inner products) accumulates in FP64, and the
+// three-term update and reorthogonalisation subtraction are evaluated in
+// FP64 before rounding to storage.  The tridiagonal eigen-solve and the
+// quadrature run in FP64.
+//
+// Reductions are deterministic: each CTA writes its partial sums to a
+// [grid][cols] buffer and k_finalize sums them in a fixed order.
+
+#ifndef SLQ_KERNELS_CUH_
+#define SLQ_KERNELS_CUH_
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace slq {
+
+constexpr unsigned FULL_MASK = 0xffffffffu;
+constexpr int DOT_K = 8;        // basis vectors per thread in k_update_dots
+constexpr int DOT_GMAX = 8;     // basis-vector groups per CTA
+constexpr int MAX_J = DOT_K * DOT_GMAX;  // basis vectors per launch
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+
+template <typename VT, int N>
+__device__ __forceinline__ void load_n(const VT* p, VT (&v)[N])
+{
+    constexpr int BYTES = N * static_cast<int>(sizeof(VT));
+    if constexpr (BYTES % 16 == 0)
+    {
+        const uint4* q = reinterpret_cast<const uint4*>(p);
+#pragma unroll
+        for (int i = 0; i < BYTES / 16; ++i)
+        {
+            uint4 t = q[i];
+            memcpy(reinterpret_cast<char*>(v) + 16 * i, &t, 16);
+        }
+    }
+    else if constexpr (BYTES % 8 == 0)
+    {
+        const uint2* q = reinterpret_cast<const uint2*>(p);
+#pragma unroll
+        for (int i = 0; i < BYTES / 8; ++i)
+        {
+            uint2 t = q[i];
+            memcpy(reinterpret_cast<char*>(v) + 8 * i, &t, 8);
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int i = 0; i < N; ++i) v[i] = p[i];
+    }
+}
+
+// read-only path for gathers from a buffer no thread of the kernel writes
+template <typename VT, int N>
+__device__ __forceinline__ void ldg_n(const VT* p, VT (&v)[N])
+{
+    constexpr int BYTES = N * static_cast<int>(sizeof(VT));
+    if constexpr (BYTES % 16 == 0)
+    {
+        const uint4* q = reinterpret_cast<const uint4*>(p);
+#pragma unroll
+        for (int i = 0; i < BYTES / 16; ++i)
+        {
+            uint4 t = __ldg(q + i);
+            memcpy(reinterpret_cast<char*>(v) + 16 * i, &t, 16);
+        }
+    }
+    else if constexpr (BYTES % 8 == 0)
+    {
+        const uint2* q = reinterpret_cast<const uint2*>(p);
+#pragma unroll
+        for (int i = 0; i < BYTES / 8; ++i)
+        {
+            uint2 t = __ldg(q + i);
+            memcpy(reinterpret_cast<char*>(v) + 8 * i, &t, 8);
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int i = 0; i < N; ++i) v[i] = __ldg(p + i);
+    }
+}
+
+template <typename VT, int N>
+__device__ __forceinline__ void store_n(VT* p, const VT (&v)[N])
+{
+    constexpr int BYTES = N * static_cast<int>(sizeof(VT));
+    if constexpr (BYTES % 16 == 0)
+    {
+        uint4* q = reinterpret_cast<uint4*>(p);
+#pragma unroll
+        for (int i = 0; i < BYTES / 16; ++i)
+        {
+            uint4 t;
+            memcpy(&t, reinterpret_cast<const char*>(v) + 16 * i, 16);
+            q[i] = t;
+        }
+    }
+    else if constexpr (BYTES % 8 == 0)
+    {
+        uint2* q = reinterpret_cast<uint2*>(p);
+#pragma unroll
+        for (int i = 0; i < BYTES / 8; ++i)
+        {
+            uint2 t;
+            memcpy(&t, reinterpret_cast<const char*>(v) + 8 * i, 8);
+            q[i] = t;
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int i = 0; i < N; ++i) p[i] = v[i];
+    }
+}
+
+__device__ __forceinline__ int64_t min64(int64_t a, int64_t b) { return a < b ? a : b; }
+
+__device__ __forceinline__ int ring_slot(int vec, int bs)
+{
+    int s = vec % bs;
+    return s < 0 ? s + bs : s;
+}
+
+// ---------------------------------------------------------------------------
+// CSR SpMM: Y = sx * (A X) [+ shift * sx * X] [- zc * zs * Z]
+//
+// One warp per matrix row; the row's b probe columns are split over the
+// lanes: P = b / LV lanes, each owning LV consecutive probes, and KS = 32/P
+// lane slices that walk alternate nonzeros of the row (KS > 1 only for
+// b < 32).  Column indices and values are read coalesced 32 at a time and
+// broadcast by shuffle; each nonzero then costs one contiguous LV-wide
+// gather per lane (the whole warp reads b contiguous values of X).  The
+// epilogue applies the per-probe scale and the Krylov recurrence's axpy and
+// accumulates the FP64 partial of alpha (Lanczos) or of the squared norm.
+//
+// epi: 0 store only, 1 alpha partial <sx X[r], Y[r]>, 2 norm partial |Y[r]|^2
+// ---------------------------------------------------------------------------
+
+template <typename VT, int LV, int KS>
+__global__ void __launch_bounds__(256)
+k_spmm(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+       const VT* __restrict__ vals, int64_t nrows, int b,
+       const VT* __restrict__ X, const double* __restrict__ sx, double shift,
+       VT* __restrict__ Y, const VT* __restrict__ Z,
+       const double* __restrict__ zc, const double* __restrict__ zs, int epi,
+       double* __restrict__ partials)
+{
+    constexpr int P = 32 / KS;
+    extern __shared__ double smem_spmm[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int pl = lane % P;
+    const int ks = lane / P;
+    const int p0 = pl * LV;
+
+    double sxr[LV], zcr[LV], part[LV];
+#pragma unroll
+    for (int v = 0; v < LV; ++v)
+    {
+        sxr[v] = sx ? sx[p0 + v] : 1.0;
+        zcr[v] = Z ? zc[p0 + v] * zs[p0 + v] : 0.0;
+        part[v] = 0.0;
+    }
+
+    const int64_t gw = static_cast<int64_t>(blockIdx.x) * nwarps + warp;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * nwarps;
+    for (int64_t row = gw; row < nrows; row += stride)
+    {
+        const int k0 = indptr[row];
+        const int k1 = indptr[row + 1];
+        VT acc[LV];
+#pragma unroll
+        for (int v = 0; v < LV; ++v) acc[v] = VT(0);
+
+        for (int base = k0; base < k1; base += 32)
+        {
+            const int kk = base + lane;
+            int c = 0;
+            VT a = VT(0);
+            if (kk < k1)
+            {
+                c = __ldg(indices + kk);
+                a = __ldg(vals + kk);
+            }
+            const int cnt = min(32, k1 - base);
+            int t = 0;
+            // four nonzeros per lane slice in flight
+            for (; t + 4 * KS <= cnt; t += 4 * KS)
+            {
+                int cc[4];
+                VT aa[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                {
+                    cc[u] = __shfl_sync(FULL_MASK, c, t + u * KS + ks);
+                    aa[u] = __shfl_sync(FULL_MASK, a, t + u * KS + ks);
+                }
+                VT x[4][LV];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    ldg_n<VT, LV>(X + static_cast<int64_t>(cc[u]) * b + p0, x[u]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int v = 0; v < LV; ++v) acc[v] += aa[u] * x[u][v];
+            }
+            for (; t < cnt; t += KS)
+            {
+                const int src = t + ks;
+                const int cc = __shfl_sync(FULL_MASK, c, src & 31);
+                const VT aa = __shfl_sync(FULL_MASK, a, src & 31);
+                if (src < cnt)
+                {
+                    VT x[LV];
+                    ldg_n<VT, LV>(X + static_cast<int64_t>(cc) * b + p0, x);
+#pragma unroll
+                    for (int v = 0; v < LV; ++v) acc[v] += aa * x[v];
+                }
+            }
+        }
+        if constexpr (KS > 1)
+        {
+#pragma unroll
+            for (int off = P; off < 32; off <<= 1)
+#pragma unroll
+                for (int v = 0; v < LV; ++v)
+                    acc[v] += __shfl_xor_sync(FULL_MASK, acc[v], off);
+        }
+        if (ks == 0)
+        {
+            const int64_t o = row * b + p0;
+            VT xr[LV], zr[LV], yr[LV];
+            if (shift != 0.0 || epi == 1) ldg_n<VT, LV>(X + o, xr);
+            if (Z) ldg_n<VT, LV>(Z + o, zr);
+#pragma unroll
+            for (int v = 0; v < LV; ++v)
+            {
+                double y = static_cast<double>(acc[v]) * sxr[v];
+                if (shift != 0.0)
+                    y += shift * (sxr[v] * static_cast<double>(xr[v]));
+                if (Z) y -= zcr[v] * static_cast<double>(zr[v]);
+                yr[v] = static_cast<VT>(y);
+                const double ys = static_cast<double>(yr[v]);
+                if (epi == 1)
+                    part[v] += (sxr[v] * static_cast<double>(xr[v])) * ys;
+                else if (epi == 2)
+                    part[v] += ys * ys;
+            }
+            store_n<VT, LV>(Y + o, yr);
+        }
+    }
+
+    if (epi == 0) return;
+    // CTA reduction over warps, fixed order
+    if (ks == 0)
+#pragma unroll
+        for (int v = 0; v < LV; ++v) smem_spmm[warp * b + p0 + v] = part[v];
+    __syncthreads();
+    for (int p = threadIdx.x; p < b; p += blockDim.x)
+    {
+        double s = 0.0;
+        for (int w = 0; w < nwarps; ++w) s += smem_spmm[w * b + p];
+        partials[static_cast<int64_t>(blockIdx.x) * b + p] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused Lanczos three-term update and reorthogonalisation inner products.
+//
+// w = W - alpha_j (s_j v_j) - beta_{j-1} (s_{j-1} v_{j-1})  (if do_update;
+// written to Wout, a buffer no thread of the launch reads) and, for the J
+// basis vectors last, last-1, ..., partial sums of <v_i, w> (unscaled;
+// k_finalize applies s_i).
+//
+// CTA = probe tile of PT = P*VEC probes (blockIdx.y) x G basis-vector groups
+// x RS row lanes.  A thread owns VEC probes and the basis vectors
+// g, g+G, ..., so it keeps DOT_K x VEC FP64 accumulators and no intra-CTA
+// reduction is needed across basis vectors; only the RS row lanes are summed
+// through shared memory at the end.
+// ---------------------------------------------------------------------------
+
+template <typename VT, int VEC>
+__global__ void __launch_bounds__(512)
+k_update_dots(int64_t n, int b, int PT, int G, int RS, const VT* W,
+              VT* __restrict__ Wout, int do_update,
+              const VT* Vj, const double* __restrict__ sj,
+              const double* __restrict__ aj, const VT* Vm,
+              const double* __restrict__ sm, const double* __restrict__ bm,
+              const VT* basis, int64_t slot_elems, int bs, int last, int J,
+              double* __restrict__ partials)
+{
+    extern __shared__ double smem_dots[];
+    const int P = PT / VEC;
+    const int tid = threadIdx.x;
+    const int pv = tid % P;
+    const int t2 = tid / P;
+    const int rs = t2 % RS;
+    const int g = t2 / RS;
+    const int pl = pv * VEC;                       // probe within tile
+    const int p0 = blockIdx.y * PT + pl;           // probe within block
+
+    double acc[DOT_K][VEC];
+#pragma unroll
+    for (int k = 0; k < DOT_K; ++k)
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) acc[k][e] = 0.0;
+
+    double cj[VEC], cm[VEC];
+#pragma unroll
+    for (int e = 0; e < VEC; ++e)
+    {
+        cj[e] = do_update ? aj[p0 + e] * sj[p0 + e] : 0.0;
+        cm[e] = (do_update && Vm) ? bm[p0 + e] * sm[p0 + e] : 0.0;
+    }
+    const VT* vptr[DOT_K];
+#pragma unroll
+    for (int k = 0; k < DOT_K; ++k)
+    {
+        const int i = g + k * G;
+        vptr[k] = (i < J) ? basis + static_cast<int64_t>(ring_slot(last - i, bs)) * slot_elems
+                          : nullptr;
+    }
+
+    for (int64_t r = static_cast<int64_t>(blockIdx.x) * RS + rs; r < n;
+         r += static_cast<int64_t>(gridDim.x) * RS)
+    {
+        const int64_t o = r * b + p0;
+        VT wv[VEC];
+        load_n<VT, VEC>(W + o, wv);
+        double w[VEC];
+        if (do_update)
+        {
+            VT a[VEC], m[VEC];
+            load_n<VT, VEC>(Vj + o, a);
+            if (Vm) load_n<VT, VEC>(Vm + o, m);
+#pragma unroll
+            for (int e = 0; e < VEC; ++e)
+            {
+                double t = static_cast<double>(wv[e]) - cj[e] * static_cast<double>(a[e]);
+                if (Vm) t -= cm[e] * static_cast<double>(m[e]);
+                wv[e] = static_cast<VT>(t);
+            }
+            if (g == 0) store_n<VT, VEC>(Wout + o, wv);
+        }
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) w[e] = static_cast<double>(wv[e]);
+#pragma unroll
+        for (int k = 0; k < DOT_K; ++k)
+        {
+            if (vptr[k])
+            {
+                VT v[VEC];
+                load_n<VT, VEC>(vptr[k] + o, v);
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) acc[k][e] += static_cast<double>(v[e]) * w[e];
+            }
+        }
+    }
+
+    // reduce the RS row lanes; layout red[rs][i][pl + e]
+    if (RS > 1)
+    {
+#pragma unroll
+        for (int k = 0; k < DOT_K; ++k)
+        {
+            const int i = g + k * G;
+            if (i < J)
+#pragma unroll
+                for (int e = 0; e < VEC; ++e)
+                    smem_dots[(static_cast<int64_t>(rs) * J + i) * PT + pl + e] = acc[k][e];
+        }
+        __syncthreads();
+        const int nthreads = blockDim.x;
+        for (int idx = tid; idx < J * PT; idx += nthreads)
+        {
+            double s = 0.0;
+            for (int q = 0; q < RS; ++q) s += smem_dots[static_cast<int64_t>(q) * J * PT + idx];
+            const int i = idx / PT;
+            const int pp = idx % PT;
+            partials[(static_cast<int64_t>(blockIdx.x) * J + i) * b + blockIdx.y * PT + pp] = s;
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int k = 0; k < DOT_K; ++k)
+        {
+            const int i = g + k * G;
+            if (i < J)
+#pragma unroll
+                for (int e = 0; e < VEC; ++e)
+                    partials[(static_cast<int64_t>(blockIdx.x) * J + i) * b + p0 + e] = acc[k][e];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Reorthogonalisation update (and the plain three-term update):
+// w = Win [- alpha_j s_j v_j - beta_{j-1} s_{j-1} v_{j-1}] - sum_i c_i v_i,
+// written to Wout (may alias Win or a basis slot: every element is read
+// before the same thread writes it), with FP64 partials of |w|^2.
+// c_i = h_i s_i, [J][b] in VT, staged in shared memory per probe tile.
+// ---------------------------------------------------------------------------
+
+template <typename VT, int VEC>
+__global__ void __launch_bounds__(512)
+k_reorth(int64_t n, int b, int PT, int RS, const VT* Win, VT* Wout,
+         int do_update, const VT* Vj, const double* __restrict__ sj,
+         const double* __restrict__ aj, const VT* Vm,
+         const double* __restrict__ sm, const double* __restrict__ bm,
+         const VT* basis, int64_t slot_elems, int bs, int last, int J,
+         const VT* __restrict__ coef, int want_norm,
+         double* __restrict__ partials)
+{
+    extern __shared__ unsigned char smem_raw[];
+    VT* cs = reinterpret_cast<VT*>(smem_raw);                 // [J][PT]
+    double* red = reinterpret_cast<double*>(smem_raw + ((J * PT * sizeof(VT) + 15) / 16) * 16);
+    const int P = PT / VEC;
+    const int tid = threadIdx.x;
+    const int pv = tid % P;
+    const int rs = tid / P;
+    const int pl = pv * VEC;
+    const int p0 = blockIdx.y * PT + pl;
+
+    for (int idx = tid; idx < J * PT; idx += blockDim.x)
+        cs[idx] = coef[static_cast<int64_t>(idx / PT) * b + blockIdx.y * PT + idx % PT];
+    __syncthreads();
+
+    double cj[VEC], cm[VEC], nacc[VEC];
+#pragma unroll
+    for (int e = 0; e < VEC; ++e)
+    {
+        cj[e] = do_update ? aj[p0 + e] * sj[p0 + e] : 0.0;
+        cm[e] = (do_update && Vm) ? bm[p0 + e] * sm[p0 + e] : 0.0;
+        nacc[e] = 0.0;
+    }
+
+    for (int64_t r = static_cast<int64_t>(blockIdx.x) * RS + rs; r < n;
+         r += static_cast<int64_t>(gridDim.x) * RS)
+    {
+        const int64_t o = r * b + p0;
+        VT wv[VEC];
+        load_n<VT, VEC>(Win + o, wv);
+        double w[VEC];
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) w[e] = static_cast<double>(wv[e]);
+        if (do_update)
+        {
+            VT a[VEC], m[VEC];
+            load_n<VT, VEC>(Vj + o, a);
+            if (Vm) load_n<VT, VEC>(Vm + o, m);
+#pragma unroll
+            for (int e = 0; e < VEC; ++e)
+            {
+                w[e] -= cj[e] * static_cast<double>(a[e]);
+                if (Vm) w[e] -= cm[e] * static_cast<double>(m[e]);
+            }
+        }
+        int i = 0;
+        for (; i + 4 <= J; i += 4)
+        {
+            VT v[4][VEC];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                load_n<VT, VEC>(basis + static_cast<int64_t>(ring_slot(last - i - u, bs)) * slot_elems + o, v[u]);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int e = 0; e < VEC; ++e)
+                    w[e] -= static_cast<double>(cs[(i + u) * PT + pl + e]) * static_cast<double>(v[u][e]);
+        }
+        for (; i < J; ++i)
+        {
+            VT v[VEC];
+            load_n<VT, VEC>(basis + static_cast<int64_t>(ring_slot(last - i, bs)) * slot_elems + o, v);
+#pragma unroll
+            for (int e = 0; e < VEC; ++e)
+                w[e] -= static_cast<double>(cs[i * PT + pl + e]) * static_cast<double>(v[e]);
+        }
+#pragma unroll
+        for (int e = 0; e < VEC; ++e)
+        {
+            wv[e] = static_cast<VT>(w[e]);
+            const double d = static_cast<double>(wv[e]);
+            nacc[e] += d * d;
+        }
+        store_n<VT, VEC>(Wout + o, wv);
+    }
+
+    if (!want_norm) return;
+    const int RSn = blockDim.x / P;
+#pragma unroll
+    for (int e = 0; e < VEC; ++e) red[rs * PT + pl + e] = nacc[e];
+    __syncthreads();
+    for (int pp = tid; pp < PT; pp += blockDim.x)
+    {
+        double s = 0.0;
+        for (int q = 0; q < RSn; ++q) s += red[q * PT + pp];
+        partials[static_cast<int64_t>(blockIdx.x) * b + blockIdx.y * PT + pp] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic column sums of a [nparts][cols] partials buffer, followed by
+// the per-column finalisation of one Krylov quantity.
+//   FIN_STORE : out[col] = sum                        (alpha_j, Lanczos)
+//   FIN_COEF  : col = i*b + p -> coef[col] = sum * s_i(p)^2 (reorth coefs)
+//   FIN_NORM  : nrm = sqrt(sum); out[p] = nrm; next_scale[p] = active ? 1/nrm
+//               : 0; with check_break, probes whose nrm < thr stop at size
+//               step+1 (the breakdown test of c_lanczos_tridiagonalization
+//               .cpp:225-228).
+// 32 x 32 threads: 32 columns per CTA, 32 partial rows per column.
+// ---------------------------------------------------------------------------
+
+enum { FIN_STORE = 0, FIN_COEF = 1, FIN_NORM = 2 };
+
+template <typename VT>
+__global__ void __launch_bounds__(1024)
+k_finalize(const double* __restrict__ partials, int nparts, int cols, int mode,
+           double* __restrict__ out, VT* __restrict__ coef,
+           const double* __restrict__ scales, int b, int bs, int last,
+           double* __restrict__ next_scale, int32_t* __restrict__ active,
+           int32_t* __restrict__ size, int check_break, double thr, int step)
+{
+    __shared__ double red[32][33];
+    const int cx = threadIdx.x & 31;
+    const int cy = threadIdx.x >> 5;
+    const int col = blockIdx.x * 32 + cx;
+    double s = 0.0;
+    if (col < cols)
+        for (int q = cy; q < nparts; q += 32)
+            s += partials[static_cast<int64_t>(q) * cols + col];
+    red[cy][cx] = s;
+    __syncthreads();
+    if (cy != 0 || col >= cols) return;
+    double t = 0.0;
+    for (int q = 0; q < 32; ++q) t += red[q][cx];
+
+    if (mode == FIN_STORE)
+    {
+        out[col] = t;
+    }
+    else if (mode == FIN_COEF)
+    {
+        const int i = col / b;
+        const int p = col % b;
+        const double si = scales[static_cast<int64_t>(ring_slot(last - i, bs)) * b + p];
+        coef[col] = static_cast<VT>(t * si * si);
+    }
+    else
+    {
+        const int p = col;
+        const double nrm = sqrt(t);
+        out[p] = nrm;
+        int act = active[p];
+        if (act && check_break && nrm < thr)
+        {
+            size[p] = step + 1;
+            act = 0;
+            active[p] = 0;
+        }
+        next_scale[p] = act ? 1.0 / nrm : 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Nodes, weights and quadrature, one thread per probe.
+//
+// Implicit QL with Wilkinson shifts on the symmetric tridiagonal T (the
+// Jacobi matrix of Lanczos, or B^T B for Golub-Kahn's upper bidiagonal B),
+// tracking only the first row of the eigenvector matrix (Golub & Welsch):
+// theta = eigenvalues, tau = first eigenvector entries.  The sample of
+// inquiry j is  nscale * sum_i tau_i^2 f((theta_i - t_0 + t_j)^p)
+// (c_trace_estimator.cpp:564-629).
+// ---------------------------------------------------------------------------
+
+constexpr int EIG_MAX = 256;
+
+__device__ __forceinline__ double apply_func(int func, double x)
+{
+    if (func == 0) return log(x);
+    if (func == 1) return 1.0 / x;
+    return x;
+}
+
+__device__ int ql_first_row(double* d, double* e, double* z, int k)
+{
+    for (int i = 0; i < k; ++i) z[i] = (i == 0) ? 1.0 : 0.0;
+    if (k <= 1) return 0;
+    e[k - 1] = 0.0;
+    const double eps = 2.220446049250313e-16;
+    for (int l = 0; l < k; ++l)
+    {
+        int iter = 0;
+        for (;;)
+        {
+            int mm;
+            for (mm = l; mm < k - 1; ++mm)
+            {
+                const double dd = fabs(d[mm]) + fabs(d[mm + 1]);
+                if (fabs(e[mm]) <= eps * dd) break;
+            }
+            if (mm == l) break;
+            if (++iter > 60) return 1;
+            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            double r = hypot(g, 1.0);
+            g = d[mm] - d[l] + e[l] / (g + (g >= 0.0 ? r : -r));
+            double s = 1.0, c = 1.0, p = 0.0;
+            bool deflated = false;
+            for (int i = mm - 1; i >= l; --i)
+            {
+                const double f = s * e[i];
+                const double bb = c * e[i];
+                r = hypot(f, g);
+                e[i + 1] = r;
+                if (r == 0.0)
+                {
+                    d[i + 1] -= p;
+                    e[mm] = 0.0;
+                    deflated = true;
+                    break;
+                }
+                s = f / r;
+                c = g / r;
+                g = d[i + 1] - p;
+                r = (d[i] - g) * s + 2.0 * c * bb;
+                p = s * r;
+                d[i + 1] = g + p;
+                g = c * r - bb;
+                const double zf = z[i + 1];
+                z[i + 1] = s * z[i] + c * zf;
+                z[i] = c * z[i] - s * zf;
+            }
+            if (deflated) continue;
+            d[l] -= p;
+            e[l] = g;
+            e[mm] = 0.0;
+        }
+    }
+    return 0;
+}
+
+__global__ void __launch_bounds__(128)
+k_eig_quad(int count, int b, int m, const double* __restrict__ alpha,
+           const double* __restrict__ beta, const int32_t* __restrict__ size,
+           int gram, int func, double exponent,
+           const double* __restrict__ params, int q, double nscale,
+           double* __restrict__ samples, double* __restrict__ theta_out,
+           double* __restrict__ tau_out, int32_t* __restrict__ status)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    double d[EIG_MAX], e[EIG_MAX], z[EIG_MAX];
+    const int k = size[p];
+    for (int i = 0; i < k; ++i)
+    {
+        const double a = alpha[static_cast<int64_t>(i) * b + p];
+        const double bt = beta[static_cast<int64_t>(i) * b + p];
+        if (gram)
+        {
+            const double bp = (i > 0) ? beta[static_cast<int64_t>(i - 1) * b + p] : 0.0;
+            d[i] = a * a + bp * bp;
+            e[i] = (i < k - 1) ? a * bt : 0.0;
+        }
+        else
+        {
+            d[i] = a;
+            e[i] = (i < k - 1) ? bt : 0.0;
+        }
+    }
+    int st = ql_first_row(d, e, z, k);
+    bool bad = false;
+    for (int i = 0; i < k; ++i)
+        if (!isfinite(d[i]) || !isfinite(z[i])) bad = true;
+    if (theta_out)
+        for (int i = 0; i < k; ++i)
+        {
+            theta_out[static_cast<int64_t>(i) * b + p] = d[i];
+            tau_out[static_cast<int64_t>(i) * b + p] = z[i];
+        }
+    const double t0 = (q > 0) ? params[0] : 0.0;
+    for (int j = 0; j < q; ++j)
+    {
+        double acc = 0.0;
+        for (int i = 0; i < k; ++i)
+        {
+            const double th = (j > 0) ? d[i] - t0 + params[j] : d[i];
+            acc += z[i] * z[i] * apply_func(func, pow(th, exponent));
+        }
+        samples[static_cast<int64_t>(p) * q + j] = nscale * acc;
+    }
+    status[p] = st ? 2 : (bad ? 1 : 0);
+}
+
+// ---------------------------------------------------------------------------
+// Rademacher probe generation into a [len][b] block.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint64_t xoshiro_next_dev(uint64_t* s)
+{
+    const uint64_t x = s[1] * 5;
+    const uint64_t result = ((x << 7) | (x >> 57)) * 9;
+    const uint64_t t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = (s[3] << 45) | (s[3] >> 19);
+    return result;
+}
+
+// Parity mode: probe p (0 <= p < count) is words [0, wpp) of the stream
+// state starts[p]; block (x = probe tile, y = chunk) thread advances to word
+// chunk*cw by the polynomial chunk_polys[chunk] (x^(chunk*cw) mod P) and
+// draws cw words.  Bit j of word w gives element 64 w + j (+1 if set).
+template <typename VT>
+__global__ void __launch_bounds__(128)
+k_probe_parity(int64_t len, int b, int count, int64_t wpp, int cw,
+               const uint64_t* __restrict__ starts,
+               const uint64_t* __restrict__ chunk_polys, VT* __restrict__ X)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= b) return;
+    const int64_t w0 = static_cast<int64_t>(blockIdx.y) * cw;
+    const int64_t w1 = min64(w0 + cw, wpp);
+    if (p >= count)
+    {
+        for (int64_t idx = w0 * 64; idx < min64(w1 * 64, len); ++idx) X[idx * b + p] = VT(0);
+        return;
+    }
+    uint64_t s[4];
+    for (int k = 0; k < 4; ++k) s[k] = starts[static_cast<int64_t>(p) * 4 + k];
+    if (blockIdx.y > 0)
+    {
+        const uint64_t* q = chunk_polys + static_cast<int64_t>(blockIdx.y) * 4;
+        uint64_t acc[4] = {0, 0, 0, 0};
+        for (int i = 0; i < 256; ++i)
+        {
+            if ((q[i >> 6] >> (i & 63)) & 1ULL)
+                for (int k = 0; k < 4; ++k) acc[k] ^= s[k];
+            xoshiro_next_dev(s);
+        }
+        for (int k = 0; k < 4; ++k) s[k] = acc[k];
+    }
+    for (int64_t w = w0; w < w1; ++w)
+    {
+        const uint64_t bits = xoshiro_next_dev(s);
+        const int64_t e0 = w * 64;
+        const int ne = static_cast<int>(min64(64, len - e0));
+        for (int j = 0; j < ne; ++j)
+            X[(e0 + j) * b + p] = ((bits >> j) & 1ULL) ? VT(1) : VT(-1);
+    }
+}
+
+// Fast mode: word w of probe g is a SplitMix64 finaliser of a counter built
+// from (seed, g, w); no sequential state, no host set-up.
+__device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(128)
+k_probe_fast(int64_t len, int b, int count, int64_t first, uint64_t key,
+             int64_t wpp, int cw, VT* __restrict__ X)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= b) return;
+    const int64_t w0 = static_cast<int64_t>(blockIdx.y) * cw;
+    const int64_t w1 = min64(w0 + cw, wpp);
+    const uint64_t g = static_cast<uint64_t>(first + p);
+    for (int64_t w = w0; w < w1; ++w)
+    {
+        const uint64_t bits =
+            mix64(key + 0x9e3779b97f4a7c15ULL * (g * 0x100000001b3ULL + static_cast<uint64_t>(w) + 1));
+        const int64_t e0 = w * 64;
+        const int ne = static_cast<int>(min64(64, len - e0));
+        for (int j = 0; j < ne; ++j)
+            X[(e0 + j) * b + p] = (p >= count) ? VT(0)
+                                  : (((bits >> j) & 1ULL) ? VT(1) : VT(-1));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Operator set-up helpers
+// ---------------------------------------------------------------------------
+
+// flag |= 1: indptr[0] != 0 or indptr[rows] != nnz; 2: decreasing indptr;
+// 4: column index out of range
+__global__ void k_check_csr(const int32_t* __restrict__ indptr,
+                            const int32_t* __restrict__ indices, int64_t rows,
+                            int64_t cols, int64_t nnz, int32_t* flag)
+{
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    if (i == 0 && (indptr[0] != 0 || indptr[rows] != nnz)) atomicOr(flag, 1);
+    for (int64_t r = i; r < rows; r += stride)
+        if (indptr[r + 1] < indptr[r]) atomicOr(flag, 2);
+    for (int64_t k = i; k < nnz; k += stride)
+    {
+        const int32_t c = indices[k];
+        if (c < 0 || c >= cols) atomicOr(flag, 4);
+    }
+}
+
+__global__ void k_row_ids(const int32_t* __restrict__ indptr, int64_t rows,
+                          int32_t* __restrict__ row_of)
+{
+    const int64_t r0 = static_cast<int64_t>(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * (blockDim.x / 32);
+    const int lane = threadIdx.x & 31;
+    for (int64_t r = r0; r < rows; r += stride)
+        for (int k = indptr[r] + lane; k < indptr[r + 1]; k += 32) row_of[k] = static_cast<int32_t>(r);
+}
+
+__global__ void k_iota(int32_t* __restrict__ a, int64_t n)
+{
+    const int64_t i0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t i = i0; i < n; i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        a[i] = static_cast<int32_t>(i);
+}
+
+template <typename VT>
+__global__ void k_gather_transpose(const int32_t* __restrict__ perm,
+                                   const int32_t* __restrict__ row_of,
+                                   const VT* __restrict__ data, int64_t nnz,
+                                   int32_t* __restrict__ t_indices,
+                                   VT* __restrict__ t_data)
+{
+    const int64_t i0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t i = i0; i < nnz; i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        const int32_t k = perm[i];
+        t_indices[i] = row_of[k];
+        t_data[i] = data[k];
+    }
+}
+
+// t_indptr[c] = first position of key >= c in the sorted column keys
+__global__ void k_bounds(const int32_t* __restrict__ sorted_keys, int64_t nnz,
+                         int64_t ncols, int32_t* __restrict__ t_indptr)
+{
+    const int64_t c0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t c = c0; c <= ncols; c += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        int64_t lo = 0, hi = nnz;
+        while (lo < hi)
+        {
+            const int64_t mid = (lo + hi) >> 1;
+            if (sorted_keys[mid] < c) lo = mid + 1;
+            else hi = mid;
+        }
+        t_indptr[c] = static_cast<int32_t>(lo);
+    }
+}
+
+__global__ void k_fill_f64(double* __restrict__ a, int64_t n, double v)
+{
+    const int64_t i0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t i = i0; i < n; i += static_cast<int64_t>(gridDim.x) * blockDim.x) a[i] = v;
+}
+
+__global__ void k_init_block(int count, int b, int m, double s0,
+                             double* __restrict__ scale0,
+                             int32_t* __restrict__ active,
+                             int32_t* __restrict__ size)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= b) return;
+    const bool real = p < count;
+    scale0[p] = real ? s0 : 0.0;
+    active[p] = real ? 1 : 0;
+    size[p] = m;
+}
+
+}  // namespace slq
+
+#endif  // SLQ_KERNELS_CUH_

@@ -1,0 +1,218 @@
+"""Linear operators: ``Matrix`` and ``AffineMatrixFunction``.
+
+Mirror of imate's operator classes for the GPU SLQ path
+(``imate/linear_operator/matrix.py:286-352``,
+``imate/linear_operator/affine_matrix_function.py:278-360``): they hold the
+host matrix and lazily create a device operator on first use, reusing it in
+later calls.  Device arrays are PyTorch CUDA tensors; the engine
+(``libslq_b200.so``) wraps them without copying and derives A^T (for
+``gram=True``) or the CSR of A (for CSC input) into a PyTorch-allocated
+workspace, with a deterministic device transpose.
+"""
+
+import ctypes
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+
+__all__ = ["LinearOperator", "Matrix", "AffineMatrixFunction"]
+
+
+def _dtype_code(dtype):
+    if dtype == np.float32:
+        return _lib.SLQ_F32
+    if dtype == np.float64:
+        return _lib.SLQ_F64
+    # py_cu_matrix.pyx:136-142 raises TypeError for other types on GPU
+    raise TypeError('Data type should be either "float32" or "float64" on '
+                    'GPU; got "%s".' % dtype)
+
+
+class _DeviceOperator:
+    """An ``slq_op`` plus the tensors it points into (kept alive here)."""
+
+    def __init__(self, A, affine, need_transpose, check_indices=True):
+        import torch
+        lib = _lib.load()
+        if not torch.cuda.is_available():
+            raise RuntimeError("no CUDA device is available for the SLQ "
+                               "engine (it has no CPU path)")
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        fmt = _lib.SLQ_CSC if A.format == "csc" else _lib.SLQ_CSR
+        if A.format not in ("csr", "csc"):
+            A = A.tocsr()
+            fmt = _lib.SLQ_CSR
+        A = A.copy()
+        A.sort_indices()
+        A.sum_duplicates()
+        self.dtype_code = _dtype_code(A.dtype)
+        self.np_dtype = A.dtype
+        self.shape = A.shape
+        self.nnz = int(A.nnz)
+        if max(A.shape) > np.iinfo(np.int32).max or \
+                self.nnz > np.iinfo(np.int32).max:
+            raise ValueError("matrix too large for 32-bit indices")
+        dev = self.device
+        self.data = torch.from_numpy(np.ascontiguousarray(A.data)).to(dev)
+        self.indices = torch.from_numpy(
+            np.ascontiguousarray(A.indices, dtype=np.int32)).to(dev)
+        self.indptr = torch.from_numpy(
+            np.ascontiguousarray(A.indptr, dtype=np.int32)).to(dev)
+        nbytes = ctypes.c_size_t(0)
+        _lib.check(lib.slq_operator_workspace_bytes(
+            A.shape[0], A.shape[1], self.nnz, self.dtype_code, fmt,
+            int(need_transpose), ctypes.byref(nbytes)))
+        self.workspace = torch.empty(max(int(nbytes.value), 256),
+                                     dtype=torch.uint8, device=dev)
+        self.handle = ctypes.c_void_p(None)
+        stream = torch.cuda.current_stream(dev)
+        _lib.check(lib.slq_operator_create(
+            self.data.data_ptr(), self.indices.data_ptr(),
+            self.indptr.data_ptr(), A.shape[0], A.shape[1], self.nnz,
+            self.dtype_code, fmt, int(affine), int(need_transpose),
+            int(check_indices), self.workspace.data_ptr(),
+            self.workspace.numel(), stream.cuda_stream,
+            ctypes.byref(self.handle)))
+        self.affine = affine
+        self.has_transpose = bool(need_transpose) or fmt == _lib.SLQ_CSC
+        self._lib = lib
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            self._lib.slq_operator_destroy(h)
+            self.handle = ctypes.c_void_p(None)
+
+    def dot(self, x, transpose=False, t=0.0):
+        """y = A x (or A^T x) (+ t x for affine operators) for a torch
+        tensor x of shape [len] or [len, width] on the operator's device."""
+        import torch
+        squeeze = x.dim() == 1
+        X = x.reshape(x.shape[0], -1)
+        width = X.shape[1]
+        wpad = 1
+        while wpad < width:
+            wpad *= 2
+        tdt = torch.float64 if self.dtype_code == _lib.SLQ_F64 else \
+            torch.float32
+        Xp = torch.zeros((X.shape[0], wpad), dtype=tdt, device=self.device)
+        Xp[:, :width] = X
+        rows = self.shape[1] if transpose else self.shape[0]
+        Y = torch.empty((rows, wpad), dtype=tdt, device=self.device)
+        stream = torch.cuda.current_stream(self.device)
+        _lib.check(self._lib.slq_operator_dot(
+            self.handle, int(transpose), float(t), Xp.data_ptr(),
+            Y.data_ptr(), wpad, stream.cuda_stream))
+        Y = Y[:, :width]
+        return Y.reshape(-1) if squeeze else Y
+
+
+class LinearOperator:
+    """Base class (``imate/linear_operator/linear_operator.py``)."""
+
+    def __init__(self):
+        self.A = None
+        self.num_parameters = 0
+        self._device_ops = {}
+        self.data_type_name = None
+
+    def set_data_type_name(self, A):
+        self.data_type_name = str(np.dtype(A.dtype).name).encode()
+
+    def get_data_type_name(self):
+        return self.data_type_name
+
+    def get_num_rows(self):
+        return self.A.shape[0]
+
+    def get_num_columns(self):
+        return self.A.shape[1]
+
+    def is_sparse(self):
+        return sp.issparse(self.A)
+
+    def get_nnz(self):
+        if sp.issparse(self.A):
+            return self.A.nnz
+        return self.A.shape[0] * self.A.shape[1]
+
+    def get_density(self):
+        return self.get_nnz() / (self.A.shape[0] * self.A.shape[1])
+
+    def get_num_parameters(self):
+        return self.num_parameters
+
+    def _affine(self):
+        return False
+
+    def get_device_operator(self, need_transpose=False):
+        """Device operator on the current CUDA device, created on first use
+        and reused (``linear_operator.py:114-147``)."""
+        import torch
+        dev = torch.cuda.current_device() if torch.cuda.is_available() else -1
+        key = (dev, bool(need_transpose))
+        op = self._device_ops.get(key)
+        if op is None and not need_transpose:
+            op = self._device_ops.get((dev, True))
+        if op is None:
+            A = self.A if sp.issparse(self.A) else sp.csr_matrix(self.A)
+            op = _DeviceOperator(A, self._affine(), need_transpose)
+            self._device_ops[key] = op
+        return op
+
+    def release(self):
+        """Drop the cached device copies."""
+        self._device_ops.clear()
+
+
+class Matrix(LinearOperator):
+    """A fixed matrix (``imate/linear_operator/matrix.py``)."""
+
+    def __init__(self, A):
+        super().__init__()
+        if not (sp.issparse(A) or isinstance(A, np.ndarray)):
+            raise TypeError("A should be a numpy array or a scipy sparse "
+                            "matrix.")
+        self.A = A
+        self.num_parameters = 0
+        self.set_data_type_name(A)
+
+
+def _is_identity(B, n):
+    if B is None:
+        return True
+    if np.isscalar(B):
+        return False
+    Bs = sp.csr_matrix(B)
+    if Bs.shape != (n, n):
+        return False
+    Bs = Bs.copy()
+    Bs.eliminate_zeros()
+    d = Bs.diagonal()
+    return Bs.nnz == n and np.all(d == 1)
+
+
+class AffineMatrixFunction(LinearOperator):
+    """A + t B with B = I (``imate/linear_operator/affine_matrix_function.py``).
+
+    With B the identity the eigenvalues of A + t I are those of A shifted by
+    t, so one Krylov run per probe serves every t
+    (``imate/_c_linear_operator/c_affine_matrix_function.cpp:98-113``).  A
+    general B is not served by this engine.
+    """
+
+    def __init__(self, A, B=None):
+        super().__init__()
+        self.A = A
+        self.B = B
+        self.num_parameters = 1
+        self.set_data_type_name(A)
+        if not _is_identity(B, A.shape[0]):
+            raise NotImplementedError(
+                "AffineMatrixFunction with B other than the identity is not "
+                "served by the B200 SLQ engine")
+
+    def _affine(self):
+        return True

@@ -1,0 +1,235 @@
+/*
+ * slq.h -- C ABI of the B200 stochastic Lanczos quadrature engine
+ * (libslq_b200.so).
+ *
+ * The engine replaces the GPU SLQ path of ameli/imate v0.25.2: the linear
+ * operator (imate/_cu_linear_operator/), the trace estimator
+ * (imate/_cu_trace_estimator/), the probe generator (imate/_random_generator/)
+ * and the CUDA loader (imate/_cuda_dynamic_loading/).  All device memory is
+ * owned by the caller (PyTorch tensors in the Python host); the engine only
+ * carves the buffers it is given.  Every entry point returns a status and
+ * never aborts; slq_last_error() describes the last failure of the calling
+ * thread.
+ *
+ * Stream: every call takes a cudaStream_t (passed as void*; NULL = legacy
+ * default stream) and enqueues all device work on it.
+ */
+
+#ifndef SLQ_B200_H_
+#define SLQ_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SLQ_ABI_VERSION 1
+
+typedef enum {
+    SLQ_OK = 0,
+    SLQ_ERR_BAD_ARG = 1,          /* argument out of range / inconsistent   */
+    SLQ_ERR_BAD_CSR = 2,          /* malformed index arrays                 */
+    SLQ_ERR_WORKSPACE = 3,        /* workspace pointer/size too small       */
+    SLQ_ERR_CUDA = 4,             /* a CUDA runtime call failed             */
+    SLQ_ERR_NAN = 5,              /* NaN/Inf in a Lanczos coefficient       */
+    SLQ_ERR_EIGEN = 6,            /* tridiagonal eigen-solve did not converge */
+    SLQ_ERR_UNSUPPORTED = 7       /* valid request this build does not serve */
+} slq_status;
+
+typedef enum { SLQ_F32 = 0, SLQ_F64 = 1 } slq_dtype;
+typedef enum { SLQ_CSR = 0, SLQ_CSC = 1 } slq_format;
+typedef enum { SLQ_FUNC_LOG = 0, SLQ_FUNC_INV = 1, SLQ_FUNC_ID = 2 } slq_func;
+typedef enum { SLQ_RNG_PARITY = 0, SLQ_RNG_FAST = 1 } slq_rng;
+
+/* Opaque operator: a sparse matrix A (or A + t I when affine != 0) resident
+ * on one device. */
+typedef struct slq_op slq_op;
+
+/* Bytes of device workspace slq_operator_create needs for the layouts it
+ * derives (a CSR copy of A^T for gram runs, a CSR copy of A for CSC input).
+ * Replaces the device upload of cuCSRMatrix / cuCSCMatrix
+ * (imate/_cu_linear_operator/cu_csr_matrix.cu:165-224,
+ *  cu_csc_matrix.cu:165-230). */
+slq_status slq_operator_workspace_bytes(int64_t num_rows, int64_t num_cols,
+                                        int64_t nnz, int dtype, int format,
+                                        int need_transpose, size_t* bytes);
+
+/* Wrap caller-owned device arrays (values dtype, int32 indices, int32 index
+ * pointer of length num_rows+1 for CSR / num_cols+1 for CSC) as an operator.
+ * need_transpose requests A^T as well (gram / Golub-Kahn runs).  affine marks
+ * the operator as A + t I (imate.AffineMatrixFunction with B = I; the
+ * eigenvalue shift relation of c_affine_matrix_function.cpp:98-113 holds).
+ * check_indices != 0 validates indptr monotonicity and index range on the
+ * device first (SLQ_ERR_BAD_CSR on failure).  Replaces pycuMatrix.__cinit__
+ * (imate/_cu_linear_operator/py_cu_matrix.pyx:118-200) and
+ * cuCSRMatrix / cuCSCMatrix / cuCSRAffineMatrixFunction construction. */
+slq_status slq_operator_create(const void* data, const int32_t* indices,
+                               const int32_t* indptr, int64_t num_rows,
+                               int64_t num_cols, int64_t nnz, int dtype,
+                               int format, int affine, int need_transpose,
+                               int check_indices, void* workspace,
+                               size_t workspace_bytes, void* stream,
+                               slq_op** out);
+
+/* Release the host-side operator record (device arrays stay with their
+ * owners).  Replaces the cuLinearOperator destructors
+ * (imate/_cu_linear_operator/cu_csr_matrix.cu:95-154). */
+slq_status slq_operator_destroy(slq_op* op);
+
+/* y = A x (transpose=0) or y = A^T x (transpose=1), plus t x for affine
+ * operators, for a block of `width` column vectors stored row-major
+ * ([len][width], contiguous), in the operator's dtype.  Replaces
+ * cuCSRMatrix::dot / transpose_dot (cu_csr_matrix.cu:278-414),
+ * cuCSCMatrix::dot / transpose_dot (cu_csc_matrix.cu:287-470) and
+ * cuCSRAffineMatrixFunction::dot (cu_csr_affine_matrix_function.cu:124-211),
+ * which the reference's tests check against scipy
+ * (imate/_cu_linear_operator/tests/test_cu_matrix.pyx:50-187). */
+slq_status slq_operator_dot(slq_op* op, int transpose, double t,
+                            const void* x, void* y, int width, void* stream);
+
+/* Estimator settings: the keyword arguments of imate's slq methods
+ * (imate/logdet/_slq_method.pyx:24-44, trace_estimator.pyx:38-61) plus the
+ * engine's own block width and probe-generator choice. */
+typedef struct {
+    int func;                      /* slq_func                               */
+    int gram;                      /* Golub-Kahn on A (A^T A) if != 0        */
+    double exponent;               /* p in f(A^p)                            */
+    int orthogonalize;             /* 0 none, <0 full, k last-k              */
+    int64_t seed;                  /* >= 0 (the host maps None to a clock seed) */
+    int lanczos_degree;            /* m, 1..SLQ_MAX_DEGREE                   */
+    double lanczos_tol;            /* breakdown tolerance (eps of dtype)     */
+    int min_num_samples;
+    int max_num_samples;
+    double error_atol;
+    double error_rtol;
+    double confidence_level;
+    double outlier_significance_level;
+    int block_size;                /* probes advanced together; 0 = auto     */
+    int rng;                       /* slq_rng                                */
+    int64_t first_probe;           /* global index of sample 0 (probe shards) */
+} slq_params;
+
+#define SLQ_MAX_DEGREE 256
+
+/* Host-side outputs, caller-allocated (same arrays the reference fills in
+ * py_cu_trace_estimator.pyx:199-247).  samples is [max_num_samples][q]
+ * row-major and NaN where not computed.  lanczos_size is per sample.
+ * alpha/beta (optional, may be NULL) receive the per-sample coefficients,
+ * [max_num_samples][lanczos_degree]. */
+typedef struct {
+    double* trace;                     /* [q]   */
+    double* error;                     /* [q]   */
+    double* samples;                   /* [max][q] */
+    int32_t* processed_samples_indices;/* [max] */
+    int32_t* num_samples_used;         /* [q]   */
+    int32_t* num_outliers;             /* [q]   */
+    int32_t* converged;                /* [q]   */
+    int32_t* lanczos_size;             /* [max] */
+    double* alpha;                     /* [max][m] or NULL */
+    double* beta;                      /* [max][m] or NULL */
+    int32_t all_converged;
+    int32_t num_blocks;                /* probe blocks launched              */
+    int64_t num_probes_computed;       /* incl. the unused tail of a block   */
+    int64_t gpu_launches;              /* kernels launched by the call       */
+    float alg_wall_time;               /* seconds, CUDA events on the stream */
+} slq_result;
+
+/* Device workspace slq_run needs for these settings. */
+slq_status slq_run_workspace_bytes(const slq_op* op, const slq_params* p,
+                                   int num_inquiries, size_t* bytes);
+
+/* The estimator.  parameters (host, length num_inquiries) are the t values
+ * of an affine operator (ignored otherwise; num_inquiries must then be 1).
+ * Replaces cuTraceEstimator<T>::cu_trace_estimator
+ * (imate/_cu_trace_estimator/cu_trace_estimator.cu:197-315) with
+ * _cu_stochastic_lanczos_quadrature (:419-660), cu_lanczos_tridiagonalization
+ * (cu_lanczos_tridiagonalization.cu:119-248), cu_golub_kahn_bidiagonalization
+ * (cu_golub_kahn_bidiagonalization.cu:113-242) and
+ * cuOrthogonalization::gram_schmidt_process (cu_orthogonalization.cu:128-228),
+ * and the host LAPACK eigensolve it called (diagonalization.cpp:89-231). */
+slq_status slq_run(slq_op* op, const slq_params* p, const double* parameters,
+                   int num_inquiries, void* workspace, size_t workspace_bytes,
+                   void* stream, slq_result* result);
+
+/* Probe generator alone: writes probes [first, first+count) of the stream for
+ * (seed, rng) as a row-major block [len][width] of +-1 in the given dtype
+ * (columns >= count are zero).  Replaces
+ * RandomArrayGenerator::generate_random_array
+ * (imate/_random_generator/random_array_generator.cpp:63-165) driven as in
+ * c_trace_estimator.cpp:235,449 with one thread. */
+slq_status slq_generate_probes(int64_t seed, int rng, int64_t len,
+                               int64_t first, int count, int width, int dtype,
+                               void* out, void* workspace,
+                               size_t workspace_bytes, void* stream);
+slq_status slq_generate_probes_workspace_bytes(int64_t len, int width,
+                                               size_t* bytes);
+
+/* Nodes (theta) and weights (tau) of a batch of Jacobi matrices, on the
+ * device, by implicit QL in FP64.  All arrays are device memory in
+ * probe-minor layout: alpha, beta, theta, tau are [m][count] (entry i of
+ * matrix p at i*count + p); sizes [count] gives each matrix's order; status
+ * [count] receives 0, 1 (non-finite result) or 2 (QL did not converge).
+ * gram != 0 treats (alpha, beta) as an upper bidiagonal B and solves B^T B.
+ * Replaces Diagonalization::eigh_tridiagonal / svd_bidiagonal
+ * (imate/_c_trace_estimator/diagonalization.cpp:89-231). */
+slq_status slq_nodes_weights(const double* alpha, const double* beta,
+                             const int32_t* sizes, int count, int m, int gram,
+                             double* theta, double* tau, int32_t* status,
+                             void* stream);
+
+/* Reference-style convergence test and outlier-trimmed averaging on host
+ * arrays (imate/_c_trace_estimator/convergence_tools.cpp:95-376); exported so
+ * the host logic can be checked without a GPU. */
+int slq_check_convergence(const double* samples, int num_inquiries,
+                          int min_num_samples, const int32_t* order,
+                          int num_processed, double confidence_level,
+                          double error_atol, double error_rtol, double* error,
+                          int32_t* num_samples_used, int32_t* converged);
+void slq_average_estimates(double confidence_level,
+                           double outlier_significance_level,
+                           int num_inquiries, int max_num_samples,
+                           const int32_t* num_samples_used,
+                           const int32_t* order, const double* samples,
+                           int32_t* num_outliers, double* trace,
+                           double* error);
+double slq_erfinv(double x);
+
+/* xoshiro256** jump-ahead on the host: advances state (4 words) by k draws.
+ * Exported so the parity probe stream can be checked without a GPU. */
+void slq_xoshiro_jump_ahead(uint64_t* state, uint64_t k);
+
+/* Per-kernel timing.  Between slq_profile_begin() and slq_profile_end()
+ * every kernel the calling thread launches is bracketed by CUDA events on its
+ * stream; slq_profile_end() synchronizes and returns, per kernel class, the
+ * launch count, the summed device time and the summed algorithmic bytes
+ * (compulsory HBM traffic of the operation as launched).  Replaces the
+ * CudaTimer around the reference's sample loop (cuda_timer.cu:28-84) with a
+ * per-kernel breakdown. */
+typedef enum {
+    SLQ_K_SPMM = 0, SLQ_K_DOTS = 1, SLQ_K_REORTH = 2, SLQ_K_FINALIZE = 3,
+    SLQ_K_EIG = 4, SLQ_K_PROBE = 5, SLQ_K_OTHER = 6, SLQ_K_COUNT = 7
+} slq_kernel_kind;
+
+typedef struct {
+    int64_t launches;
+    double milliseconds;
+    double bytes;
+} slq_kernel_stat;
+
+slq_status slq_profile_begin(void);
+slq_status slq_profile_end(slq_kernel_stat* stats /* [SLQ_K_COUNT] */);
+
+/* Device count / properties (replaces query_device.cu:48-64). */
+slq_status slq_device_info(int* num_devices, int* num_sms,
+                           int* max_threads_per_sm);
+
+const char* slq_last_error(void);
+int slq_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SLQ_B200_H_ */

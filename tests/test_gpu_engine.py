@@ -1,0 +1,306 @@
+"""Parity of the CUDA engine with the oracle and with the reference's own
+golden outputs.  Tolerances: bit-exact for probe bits and sample counts;
+1e-10 relative for FP64 Lanczos/Golub-Kahn coefficients, nodes, weights and
+per-probe samples (the accuracy BASELINE's north star states for FP64);
+FP32 operator products within 1e-5 relative of scipy."""
+
+import ctypes
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import imate_b200 as ib
+from imate_b200 import _lib
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+RTOL_FP64 = 1e-10
+
+
+def rel(a, b):
+    a = np.asarray(a, float)
+    b = np.asarray(b, float)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+
+
+def _probes(lib, seed, rng, n, first, count, width, dtype):
+    import torch
+    tdt = torch.float64 if dtype == _lib.SLQ_F64 else torch.float32
+    out = torch.full((n, width), 7.0, dtype=tdt, device="cuda")
+    nb = ctypes.c_size_t(0)
+    _lib.check(lib.slq_generate_probes_workspace_bytes(n, width,
+                                                       ctypes.byref(nb)))
+    ws = torch.empty(nb.value, dtype=torch.uint8, device="cuda")
+    _lib.check(lib.slq_generate_probes(
+        seed, rng, n, first, count, width, dtype, out.data_ptr(),
+        ws.data_ptr(), ws.numel(),
+        torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("n", [1, 63, 64, 65, 1000, 4097, 70001])
+@pytest.mark.parametrize("first,count,width", [(0, 1, 1), (0, 8, 8),
+                                               (5, 50, 64)])
+def test_parity_probes_bit_exact(cuda, n, first, count, width):
+    want = oracle.random_probes(3, n, first + count)[first:]
+    for dt in (_lib.SLQ_F32, _lib.SLQ_F64):
+        got = _probes(cuda, 3, 0, n, first, count, width, dt)
+        assert np.array_equal(got[:, :count].T, want)
+        assert np.all(got[:, count:] == 0)
+
+
+def test_parity_probes_golden(cuda, golden):
+    g = golden("rng.npz")
+    for seed, n in ((0, 65), (3, 1000), (5, 4097)):
+        want = g["probes_seed%d_n%d" % (seed, n)]
+        got = _probes(cuda, seed, 0, n, 0, want.shape[0], 8, _lib.SLQ_F64)
+        assert np.array_equal((got[:, :want.shape[0]].T > 0).astype(np.int8),
+                              want)
+
+
+def test_fast_probes_are_rademacher(cuda):
+    got = _probes(cuda, 11, 1, 100000, 0, 32, 32, _lib.SLQ_F32)
+    assert set(np.unique(got)) == {-1.0, 1.0}
+    assert abs(got.mean()) < 0.01
+    c = np.corrcoef(got.T)
+    assert np.max(np.abs(c - np.eye(32))) < 0.02
+
+
+def _dot(Aop, x, transpose=False, t=0.0):
+    import torch
+    X = torch.from_numpy(x).cuda()
+    return Aop.dot(X, transpose=transpose, t=t).cpu().numpy()
+
+
+@pytest.mark.parametrize("fmt", ["csr", "csc"])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("width", [1, 3, 32, 128])
+def test_operator_products(cuda, fmt, dtype, width):
+    rng = np.random.default_rng(1)
+    A = sp.random(700, 500, density=0.02, format=fmt, random_state=2,
+                  dtype=np.float64).astype(dtype)
+    M = ib.Matrix(A)
+    op = M.get_device_operator(need_transpose=True)
+    x = rng.standard_normal((500, width)).astype(dtype)
+    z = rng.standard_normal((700, width)).astype(dtype)
+    y = _dot(op, x)
+    yt = _dot(op, z, transpose=True)
+    tol = 1e-12 if dtype == np.float64 else 2e-5
+    ref_y = A.astype(np.float64) @ x.astype(np.float64)
+    ref_yt = A.T.astype(np.float64) @ z.astype(np.float64)
+    assert np.max(np.abs(y - ref_y)) <= tol * np.max(np.abs(ref_y))
+    assert np.max(np.abs(yt - ref_yt)) <= tol * np.max(np.abs(ref_yt))
+
+
+def test_affine_operator_product(cuda, corr_small):
+    Aop = ib.AffineMatrixFunction(corr_small)
+    op = Aop.get_device_operator()
+    x = np.random.default_rng(0).standard_normal((corr_small.shape[0], 4))
+    y = _dot(op, x, t=0.75)
+    want = corr_small @ x + 0.75 * x
+    assert np.max(np.abs(y - want)) < 1e-12 * np.max(np.abs(want))
+
+
+def _run(func, A, gram=False, block_size=0, coefficients=True, **kw):
+    eng = ib.EngineOptions(block_size=block_size,
+                           return_coefficients=coefficients)
+    f = {"log": ib.logdet, "inv": ib.traceinv, "id": ib.trace}[func]
+    tr, info = f(A, gram=gram, method="slq", gpu=True, return_info=True,
+                 engine=eng, **kw)
+    return tr, info
+
+
+@pytest.mark.parametrize("orth", [0, -1, 10])
+@pytest.mark.parametrize("block_size", [1, 4, 64])
+def test_golub_kahn_coefficients_match_reference(cuda, golden, orth,
+                                                 block_size):
+    g = golden("krylov.npz")
+    B = ib.toeplitz(2.0, 1.0, 16384)
+    tr, info = _run("log", B, gram=True, block_size=block_size,
+                    min_num_samples=4, max_num_samples=4, lanczos_degree=30,
+                    orthogonalize=orth, seed=0)
+    a = info["engine"]["alpha"]
+    b = info["engine"]["beta"]
+    for p in range(4):
+        key = "c1_orth%d_p%d" % (orth, p)
+        assert rel(a[p], g[key + "_alpha"]) < RTOL_FP64
+        assert rel(b[p], g[key + "_beta"]) < RTOL_FP64
+
+
+@pytest.mark.parametrize("orth", [0, -1, 1, 5])
+@pytest.mark.parametrize("block_size", [1, 8, 256])
+def test_lanczos_coefficients_match_reference(cuda, golden, corr_small, orth,
+                                              block_size):
+    g = golden("krylov.npz")
+    tr, info = _run("log", corr_small, block_size=block_size,
+                    min_num_samples=4, max_num_samples=4, lanczos_degree=20,
+                    orthogonalize=orth, seed=5)
+    a = info["engine"]["alpha"]
+    b = info["engine"]["beta"]
+    for p in range(4):
+        key = "corr_orth%d_p%d" % (orth, p)
+        assert rel(a[p], g[key + "_alpha"]) < RTOL_FP64
+        assert rel(b[p], g[key + "_beta"]) < RTOL_FP64
+
+
+def test_nodes_weights_match_lapack(cuda, golden):
+    import torch
+    g = golden("krylov.npz")
+    keys = [("c1_orth-1_p0", 1), ("c1_orth0_p1", 1), ("corr_orth-1_p2", 0),
+            ("corr_orth5_p3", 0)]
+    for key, gram in keys:
+        a = g[key + "_alpha"]
+        bb = g[key + "_beta"]
+        m = a.size
+        A = torch.from_numpy(a.reshape(m, 1).copy()).cuda()
+        Bt = torch.from_numpy(bb.reshape(m, 1).copy()).cuda()
+        size = torch.tensor([m], dtype=torch.int32, device="cuda")
+        th = torch.zeros((m, 1), dtype=torch.float64, device="cuda")
+        tau = torch.zeros((m, 1), dtype=torch.float64, device="cuda")
+        st = torch.zeros(1, dtype=torch.int32, device="cuda")
+        _lib.check(cuda.slq_nodes_weights(
+            A.data_ptr(), Bt.data_ptr(), size.data_ptr(), 1, m, gram,
+            th.data_ptr(), tau.data_ptr(), st.data_ptr(),
+            torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        assert int(st.item()) == 0
+        t1 = th.cpu().numpy()[:, 0]
+        w1 = tau.cpu().numpy()[:, 0] ** 2
+        i1 = np.argsort(t1)
+        t2 = g[key + "_theta"]
+        w2 = g[key + "_tau"] ** 2
+        i2 = np.argsort(t2)
+        assert rel(t1[i1], t2[i2]) < RTOL_FP64
+        assert np.max(np.abs(w1[i1] - w2[i2])) < RTOL_FP64
+
+
+def _check_estimator(tr, info, g, key):
+    used = int(np.atleast_1d(g[key + "_num_samples_used"])[0])
+    conv = info["convergence"]
+    np.testing.assert_array_equal(np.atleast_1d(conv["num_samples_used"]),
+                                  g[key + "_num_samples_used"])
+    np.testing.assert_array_equal(np.atleast_1d(conv["num_outliers"]),
+                                  g[key + "_num_outliers"])
+    order = g[key + "_processed_samples_indices"][:used]
+    np.testing.assert_array_equal(conv["samples_processed_order"][:used],
+                                  order)
+    s = np.asarray(conv["samples"]).reshape(len(conv["samples"]), -1)
+    assert rel(s[order], g[key + "_samples"][order]) < RTOL_FP64
+    assert rel(np.atleast_1d(tr), g[key + "_trace"]) < RTOL_FP64
+    assert rel(np.atleast_1d(info["error"]["absolute_error"]),
+               g[key + "_error"]) < 1e-6
+
+
+@pytest.mark.parametrize("orth", [0, -1])
+@pytest.mark.parametrize("block_size", [0, 32])
+def test_estimator_toeplitz_matches_reference(cuda, golden, orth, block_size):
+    g = golden("estimator.npz")
+    B = ib.toeplitz(2.0, 1.0, 16384)
+    tr, info = _run("log", B, gram=True, block_size=block_size,
+                    coefficients=False, min_num_samples=50,
+                    max_num_samples=200, error_rtol=1e-3, lanczos_degree=30,
+                    orthogonalize=orth, seed=0)
+    _check_estimator(tr, info, g, "c1_log_orth%d" % orth)
+    exact = ib.toeplitz_logdet(2.0, 1.0, 16384, gram=True)
+    assert abs(tr - exact) / exact < 1e-3
+
+
+@pytest.mark.parametrize("func", ["log", "inv", "id"])
+def test_estimator_functions_match_reference(cuda, golden, corr_small, func):
+    g = golden("estimator.npz")
+    tr, info = _run(func, corr_small, coefficients=False, min_num_samples=10,
+                    max_num_samples=64, error_rtol=1e-2, lanczos_degree=20,
+                    orthogonalize=0, seed=3)
+    _check_estimator(tr, info, g, "corr_%s" % func)
+
+
+def test_estimator_gram_affine_exponent_match_reference(cuda, golden,
+                                                        corr_small):
+    g = golden("estimator.npz")
+    tr, info = _run("log", corr_small, gram=True, coefficients=False,
+                    min_num_samples=10, max_num_samples=40, error_rtol=1e-2,
+                    lanczos_degree=15, orthogonalize=-1, seed=4)
+    _check_estimator(tr, info, g, "corr_gram_log")
+    Aop = ib.AffineMatrixFunction(corr_small)
+    tr, info = _run("inv", Aop, coefficients=False,
+                    parameters=[0.1, 1.0, 10.0], min_num_samples=5,
+                    max_num_samples=30, error_rtol=1e-3, lanczos_degree=20,
+                    orthogonalize=-1, seed=9)
+    _check_estimator(tr, info, g, "corr_affine_inv")
+    tr, info = ib.logdet(corr_small, p=2.0, method="slq", gpu=True,
+                         return_info=True, min_num_samples=5,
+                         max_num_samples=20, error_rtol=1e-2,
+                         lanczos_degree=10, orthogonalize=3, seed=2)
+    _check_estimator(tr, info, g, "corr_log_p2")
+
+
+def test_estimator_matches_oracle_at_random_sizes(cuda):
+    # sizes that exercise partial probe blocks and ragged rows
+    rng = np.random.default_rng(8)
+    for n, seed in ((37, 1), (301, 2), (1025, 3)):
+        M = sp.random(n, n, density=min(1.0, 6.0 / n), random_state=seed,
+                      format="csr")
+        A = (M @ M.T + sp.eye(n) * 0.5).tocsr()
+        for orth, bs in ((0, 4), (-1, 16), (3, 2)):
+            kw = dict(min_num_samples=3, max_num_samples=21, error_rtol=1e-8,
+                      lanczos_degree=12, orthogonalize=orth, seed=seed)
+            tr, info = _run("log", A, block_size=bs, coefficients=False,
+                            **kw)
+            want = oracle.trace_estimator(A, "log", **kw)
+            assert info["convergence"]["num_samples_used"] == \
+                want["num_samples_used"][0]
+            assert rel(info["convergence"]["samples"],
+                       want["samples"][:, 0]) < RTOL_FP64
+    assert rng is not None
+
+
+def test_mixed_precision_toeplitz_accuracy(cuda):
+    B = ib.toeplitz(2.0, 1.0, 16384, dtype="float32")
+    tr, info = ib.logdet(B, gram=True, method="slq", gpu=True,
+                         return_info=True, min_num_samples=50,
+                         max_num_samples=200, error_rtol=1e-3,
+                         lanczos_degree=30, orthogonalize=-1, seed=0)
+    exact = ib.toeplitz_logdet(2.0, 1.0, 16384, gram=True)
+    assert info["matrix"]["data_type"] == b"float32"
+    assert abs(float(tr) - exact) / exact < 1e-3
+    B64 = ib.toeplitz(2.0, 1.0, 16384)
+    tr64, info64 = ib.logdet(B64, gram=True, method="slq", gpu=True,
+                             return_info=True, min_num_samples=50,
+                             max_num_samples=200, error_rtol=1e-3,
+                             lanczos_degree=30, orthogonalize=-1, seed=0)
+    s32 = info["convergence"]["samples"][:145]
+    s64 = info64["convergence"]["samples"][:145]
+    assert rel(s32, s64) < 1e-5
+
+
+def test_bad_csr_is_rejected(cuda):
+    A = sp.csr_matrix(np.eye(4))
+    A.indices[2] = 9
+    with pytest.raises(_lib.SlqError) as e:
+        ib.Matrix(A).get_device_operator()
+    assert e.value.status == 2
+
+
+def test_identity_breaks_down_after_one_step(cuda):
+    A = sp.eye(500, format="csr")
+    tr, info = ib.logdet(A, method="slq", gpu=True, return_info=True,
+                         min_num_samples=5, max_num_samples=5,
+                         lanczos_degree=10, seed=1)
+    assert np.all(info["engine"]["lanczos_size"][:5] == 1)
+    assert abs(tr) < 1e-12
+    tr, info = ib.traceinv(A, method="slq", gpu=True, return_info=True,
+                           min_num_samples=5, max_num_samples=5,
+                           lanczos_degree=10, seed=1)
+    assert abs(tr - 500.0) < 1e-9
+
+
+def test_indefinite_matrix_gives_nan_logdet(cuda):
+    d = np.r_[np.full(50, 2.0), np.full(50, -1.0)]
+    A = sp.diags(d).tocsr()
+    tr, info = ib.logdet(A, method="slq", gpu=True, return_info=True,
+                         min_num_samples=3, max_num_samples=3,
+                         lanczos_degree=8, seed=2)
+    assert np.isnan(tr)
