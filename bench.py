@@ -363,7 +363,7 @@ def run_engine_arm(args):
                 "fp64_plain.rel_diff_same_probes",
     }
 
-    if rank == 0:
+    if rank == 0 and args.fp64_probes > 0:
         # plain FP64 per-probe path (block width 1) on the same matrix
         A64 = A32.astype(np.float64)
         Aop64 = ib.Matrix(A64)
@@ -396,6 +396,7 @@ def run_engine_arm(args):
         }
         del Aop64
 
+    if rank == 0:
         # end to end through the public API from host arrays
         if not args.no_e2e:
             h2d = A32.data.nbytes + A32.indices.nbytes + A32.indptr.nbytes

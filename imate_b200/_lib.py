@@ -105,9 +105,9 @@ def _declare(lib):
     psz = ctypes.POINTER(ctypes.c_size_t)
     sig = {
         "slq_operator_workspace_bytes": (i32, [i64, i64, i64, i32, i32, i32,
-                                               psz]),
+                                               i32, psz]),
         "slq_operator_create": (i32, [vp, vp, vp, i64, i64, i64, i32, i32,
-                                      i32, i32, i32, vp, sz, vp,
+                                      i32, i32, i32, vp, vp, sz, vp,
                                       ctypes.POINTER(vp)]),
         "slq_operator_destroy": (i32, [vp]),
         "slq_operator_dot": (i32, [vp, i32, d, vp, vp, i32, vp]),

@@ -207,6 +207,8 @@ struct slq_op {
     const void* t_data = nullptr;
     const int32_t* t_ind = nullptr;
     const int32_t* t_ptr = nullptr;
+    // symmetric locality permutation: probe element e lives in row inv[e]
+    const int32_t* inv = nullptr;
 };
 
 namespace {
@@ -286,17 +288,96 @@ slq_status transpose_csr(const int32_t* ptr, const int32_t* ind, const void* dat
     return SLQ_OK;
 }
 
+struct PermBufs {
+    int32_t* inv;
+    int32_t* p_ptr;
+    int32_t* p_ind;
+    void* p_data;
+    uint64_t* keys_in;
+    uint64_t* keys_out;
+    int32_t* pos_in;
+    int32_t* pos_out;
+    void* temp;
+    size_t temp_bytes;
+};
+
+slq_status perm_layout(Carver& c, int64_t n, int64_t nnz, int dtype, PermBufs* t)
+{
+    size_t temp_bytes = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(
+        nullptr, temp_bytes, static_cast<const uint64_t*>(nullptr),
+        static_cast<uint64_t*>(nullptr), static_cast<const int32_t*>(nullptr),
+        static_cast<int32_t*>(nullptr), static_cast<int>(std::max<int64_t>(nnz, 1)));
+    if (e != cudaSuccess)
+        return fail(SLQ_ERR_CUDA, std::string("cub sort sizing: ") + cudaGetErrorString(e));
+    t->inv = c.take<int32_t>(n);
+    t->p_ptr = c.take<int32_t>(n + 1);
+    t->p_ind = c.take<int32_t>(nnz);
+    t->p_data = c.take<char>(nnz * dsize(dtype));
+    t->keys_in = c.take<uint64_t>(nnz);
+    t->keys_out = c.take<uint64_t>(nnz);
+    t->pos_in = c.take<int32_t>(nnz);
+    t->pos_out = c.take<int32_t>(nnz);
+    t->temp = c.take<char>(temp_bytes);
+    t->temp_bytes = temp_bytes;
+    return SLQ_OK;
+}
+
+// B = P A P^T with B[i][j] = A[perm[i]][perm[j]]: sort (new row, new column)
+// keys; rows of B come out with ascending column indices.
+slq_status permute_csr(const int32_t* ptr, const int32_t* ind, const void* data,
+                       const int32_t* perm, int64_t n, int64_t nnz, int dtype,
+                       PermBufs* t, cudaStream_t st)
+{
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
+    const int grid = sms * 4;
+    k_inverse_perm<<<grid, 256, 0, st>>>(perm, n, t->inv);
+    SLQ_LAUNCH_CK();
+    if (nnz > 0)
+    {
+        k_perm_keys<<<grid, 256, 0, st>>>(ptr, ind, t->inv, n, t->keys_in, t->pos_in);
+        SLQ_LAUNCH_CK();
+        int bits = 1;
+        while ((int64_t(1) << bits) <= n && bits < 31) ++bits;
+        size_t tb = t->temp_bytes;
+        cudaError_t e = cub::DeviceRadixSort::SortPairs(
+            t->temp, tb, t->keys_in, t->keys_out, t->pos_in, t->pos_out,
+            static_cast<int>(nnz), 0, 32 + bits, st);
+        if (e != cudaSuccess)
+            return fail(SLQ_ERR_CUDA, std::string("cub sort: ") + cudaGetErrorString(e));
+        if (dtype == SLQ_F64)
+            k_perm_gather<double><<<grid, 256, 0, st>>>(
+                t->keys_out, t->pos_out, static_cast<const double*>(data), nnz, t->p_ind,
+                static_cast<double*>(t->p_data));
+        else
+            k_perm_gather<float><<<grid, 256, 0, st>>>(
+                t->keys_out, t->pos_out, static_cast<const float*>(data), nnz, t->p_ind,
+                static_cast<float*>(t->p_data));
+        SLQ_LAUNCH_CK();
+    }
+    k_bounds64<<<std::max<int64_t>(1, std::min<int64_t>(grid, (n + 256) / 256)), 256, 0, st>>>(
+        t->keys_out, nnz, n, t->p_ptr);
+    SLQ_LAUNCH_CK();
+    return SLQ_OK;
+}
+
 }  // namespace
 
 extern "C" slq_status slq_operator_workspace_bytes(int64_t num_rows, int64_t num_cols,
                                                    int64_t nnz, int dtype, int format,
-                                                   int need_transpose, size_t* bytes)
+                                                   int need_transpose, int has_perm,
+                                                   size_t* bytes)
 {
     if (!bytes || num_rows < 0 || num_cols < 0 || nnz < 0)
         return fail(SLQ_ERR_BAD_ARG, "operator_workspace_bytes: bad argument");
+    if (has_perm && (format != SLQ_CSR || num_rows != num_cols))
+        return fail(SLQ_ERR_BAD_ARG, "a permutation needs a square CSR matrix");
     Carver c(nullptr, 0);
     TransposeBufs t;
+    PermBufs pb;
     c.take<int32_t>(1);  // index-check flag
+    if (has_perm) SLQ_TRY(perm_layout(c, num_rows, nnz, dtype, &pb));
     const bool build = (format == SLQ_CSC) || need_transpose;
     if (build)
     {
@@ -312,9 +393,9 @@ extern "C" slq_status slq_operator_create(const void* data, const int32_t* indic
                                           const int32_t* indptr, int64_t num_rows,
                                           int64_t num_cols, int64_t nnz, int dtype,
                                           int format, int affine, int need_transpose,
-                                          int check_indices, void* workspace,
-                                          size_t workspace_bytes, void* stream,
-                                          slq_op** out)
+                                          int check_indices, const int32_t* perm,
+                                          void* workspace, size_t workspace_bytes,
+                                          void* stream, slq_op** out)
 {
     if (!out) return fail(SLQ_ERR_BAD_ARG, "operator_create: out is NULL");
     *out = nullptr;
@@ -331,7 +412,7 @@ extern "C" slq_status slq_operator_create(const void* data, const int32_t* indic
         return fail(SLQ_ERR_BAD_ARG, "operator_create: A + tI needs a square matrix");
     size_t need = 0;
     SLQ_TRY(slq_operator_workspace_bytes(num_rows, num_cols, nnz, dtype, format,
-                                         need_transpose, &need));
+                                         need_transpose, perm != nullptr, &need));
     if (!workspace || workspace_bytes < need)
         return fail(SLQ_ERR_WORKSPACE, "operator_create: workspace too small (need " +
                                            std::to_string(need) + " bytes)");
@@ -363,13 +444,32 @@ extern "C" slq_status slq_operator_create(const void* data, const int32_t* indic
     op->nrows = num_rows;
     op->ncols = num_cols;
     op->nnz = nnz;
+    const void* src_data = data;
+    const int32_t* src_ind = indices;
+    const int32_t* src_ptr = indptr;
+    if (perm)
+    {
+        PermBufs pb;
+        slq_status s = perm_layout(c, num_rows, nnz, dtype, &pb);
+        if (s == SLQ_OK)
+            s = permute_csr(indptr, indices, data, perm, num_rows, nnz, dtype, &pb, st);
+        if (s != SLQ_OK)
+        {
+            delete op;
+            return s;
+        }
+        src_data = pb.p_data;
+        src_ind = pb.p_ind;
+        src_ptr = pb.p_ptr;
+        op->inv = pb.inv;
+    }
     const bool build = (format == SLQ_CSC) || need_transpose;
     TransposeBufs t;
     if (build)
     {
         slq_status s = transpose_layout(c, srows, scols, nnz, dtype, &t);
         if (s == SLQ_OK)
-            s = transpose_csr(indptr, indices, data, srows, scols, nnz, dtype, &t, st);
+            s = transpose_csr(src_ptr, src_ind, src_data, srows, scols, nnz, dtype, &t, st);
         if (s != SLQ_OK)
         {
             delete op;
@@ -378,9 +478,9 @@ extern "C" slq_status slq_operator_create(const void* data, const int32_t* indic
     }
     if (format == SLQ_CSR)
     {
-        op->a_data = data;
-        op->a_ind = indices;
-        op->a_ptr = indptr;
+        op->a_data = src_data;
+        op->a_ind = src_ind;
+        op->a_ptr = src_ptr;
         if (build)
         {
             op->t_data = t.t_data;
@@ -705,11 +805,20 @@ slq_status make_plan(const slq_op* op, const slq_params* p, int q, RunPlan* r)
     return SLQ_OK;
 }
 
+// Elements between consecutive basis slots: the block plus 2560 bytes, so
+// that slot strides are not a multiple of a large power of two (the same
+// row of every slot would otherwise fall into the same DRAM channels).
+template <typename VT>
+int64_t slot_stride(int64_t len, int b)
+{
+    return len * b + 2560 / static_cast<int64_t>(sizeof(VT));
+}
+
 template <typename VT>
 void carve(Carver& c, const RunPlan& r, int sms, RunBufs* B)
 {
-    const int64_t vslot = r.nv * r.b;
-    const int64_t uslot = r.nu * r.b;
+    const int64_t vslot = slot_stride<VT>(r.nv, r.b);
+    const int64_t uslot = slot_stride<VT>(r.nu, r.b);
     B->V = c.take<VT>(static_cast<size_t>(r.bs) * vslot);
     B->U = r.gram ? c.take<VT>(static_cast<size_t>(r.bs) * uslot) : nullptr;
     B->W = r.gram ? nullptr : c.take<VT>(vslot);
@@ -734,17 +843,17 @@ void carve(Carver& c, const RunPlan& r, int sms, RunBufs* B)
 
 template <typename VT>
 slq_status launch_probes(Launcher& L, const RunPlan& r, int rng, int64_t seed, int64_t first,
-                         int count, const RunBufs& B, VT* X)
+                         int count, const RunBufs& B, const int32_t* inv, VT* X)
 {
     dim3 grid((r.b + 127) / 128, r.nchunks);
     ProfScope prof(SLQ_K_PROBE, double(r.nv) * r.b * sizeof(VT), L.st);
     if (rng == SLQ_RNG_PARITY)
         k_probe_parity<VT><<<grid, 128, 0, L.st>>>(r.nv, r.b, count, r.wpp, r.cw, B.starts,
-                                                   B.chunk_polys, X);
+                                                   B.chunk_polys, inv, X);
     else
         k_probe_fast<VT><<<grid, 128, 0, L.st>>>(r.nv, r.b, count, first,
                                                  static_cast<uint64_t>(seed) * 0xd1342543de82ef95ULL,
-                                                 r.wpp, r.cw, X);
+                                                 r.wpp, r.cw, inv, X);
     SLQ_LAUNCH_CK();
     ++L.launches;
     return SLQ_OK;
@@ -761,8 +870,8 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
     const int b = r.b;
     const int bs = r.bs;
     const int m = r.m;
-    const int64_t vslot = r.nv * b;
-    const int64_t uslot = r.nu * b;
+    const int64_t vslot = slot_stride<VT>(r.nv, b);
+    const int64_t uslot = slot_stride<VT>(r.nu, b);
     VT* V = static_cast<VT*>(B.V);
     VT* U = static_cast<VT*>(B.U);
     VT* W = static_cast<VT*>(B.W);
@@ -989,7 +1098,7 @@ slq_status run_typed(slq_op* op, const slq_params* p, const double* parameters, 
                                    cudaMemcpyHostToDevice, st));
         }
         SLQ_TRY(launch_probes<VT>(L, r, p->rng, p->seed, p->first_probe + g, count, B,
-                                  static_cast<VT*>(B.V)));
+                                  op->inv, static_cast<VT*>(B.V)));
         {
         ProfScope prof(SLQ_K_OTHER, 0.0, st);
         k_init_block<<<(b + 127) / 128, 128, 0, st>>>(count, b, m, s0, B.scale_v, B.active,
@@ -1205,8 +1314,10 @@ extern "C" slq_status slq_generate_probes(int64_t seed, int rng, int64_t len, in
     L.st = st;
     SLQ_TRY(device_sms(&L.sms));
     if (dtype == SLQ_F64)
-        return launch_probes<double>(L, r, rng, seed, first, count, B, static_cast<double*>(out));
-    return launch_probes<float>(L, r, rng, seed, first, count, B, static_cast<float*>(out));
+        return launch_probes<double>(L, r, rng, seed, first, count, B, nullptr,
+                                     static_cast<double*>(out));
+    return launch_probes<float>(L, r, rng, seed, first, count, B, nullptr,
+                                static_cast<float*>(out));
 }
 
 extern "C" slq_status slq_nodes_weights(const double* alpha, const double* beta,

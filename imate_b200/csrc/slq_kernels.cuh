@@ -737,7 +737,8 @@ template <typename VT>
 __global__ void __launch_bounds__(128)
 k_probe_parity(int64_t len, int b, int count, int64_t wpp, int cw,
                const uint64_t* __restrict__ starts,
-               const uint64_t* __restrict__ chunk_polys, VT* __restrict__ X)
+               const uint64_t* __restrict__ chunk_polys,
+               const int32_t* __restrict__ inv, VT* __restrict__ X)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= b) return;
@@ -745,7 +746,8 @@ k_probe_parity(int64_t len, int b, int count, int64_t wpp, int cw,
     const int64_t w1 = min64(w0 + cw, wpp);
     if (p >= count)
     {
-        for (int64_t idx = w0 * 64; idx < min64(w1 * 64, len); ++idx) X[idx * b + p] = VT(0);
+        for (int64_t idx = w0 * 64; idx < min64(w1 * 64, len); ++idx)
+            X[static_cast<int64_t>(inv ? inv[idx] : idx) * b + p] = VT(0);
         return;
     }
     uint64_t s[4];
@@ -768,7 +770,10 @@ k_probe_parity(int64_t len, int b, int count, int64_t wpp, int cw,
         const int64_t e0 = w * 64;
         const int ne = static_cast<int>(min64(64, len - e0));
         for (int j = 0; j < ne; ++j)
-            X[(e0 + j) * b + p] = ((bits >> j) & 1ULL) ? VT(1) : VT(-1);
+        {
+            const int64_t row = inv ? inv[e0 + j] : e0 + j;
+            X[row * b + p] = ((bits >> j) & 1ULL) ? VT(1) : VT(-1);
+        }
     }
 }
 
@@ -784,7 +789,8 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z)
 template <typename VT>
 __global__ void __launch_bounds__(128)
 k_probe_fast(int64_t len, int b, int count, int64_t first, uint64_t key,
-             int64_t wpp, int cw, VT* __restrict__ X)
+             int64_t wpp, int cw, const int32_t* __restrict__ inv,
+             VT* __restrict__ X)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= b) return;
@@ -798,8 +804,11 @@ k_probe_fast(int64_t len, int b, int count, int64_t first, uint64_t key,
         const int64_t e0 = w * 64;
         const int ne = static_cast<int>(min64(64, len - e0));
         for (int j = 0; j < ne; ++j)
-            X[(e0 + j) * b + p] = (p >= count) ? VT(0)
-                                  : (((bits >> j) & 1ULL) ? VT(1) : VT(-1));
+        {
+            const int64_t row = inv ? inv[e0 + j] : e0 + j;
+            X[row * b + p] = (p >= count) ? VT(0)
+                             : (((bits >> j) & 1ULL) ? VT(1) : VT(-1));
+        }
     }
 }
 
@@ -873,6 +882,68 @@ __global__ void k_bounds(const int32_t* __restrict__ sorted_keys, int64_t nnz,
             else hi = mid;
         }
         t_indptr[c] = static_cast<int32_t>(lo);
+    }
+}
+
+// Symmetric permutation B = P A P^T of a square CSR matrix: inverse map,
+// 64-bit (new row, new column) sort keys, gather of the sorted entries and
+// row pointers from the sorted keys.
+__global__ void k_inverse_perm(const int32_t* __restrict__ perm, int64_t n,
+                               int32_t* __restrict__ inv)
+{
+    const int64_t i0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t i = i0; i < n; i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        inv[perm[i]] = static_cast<int32_t>(i);
+}
+
+__global__ void k_perm_keys(const int32_t* __restrict__ indptr,
+                            const int32_t* __restrict__ indices,
+                            const int32_t* __restrict__ inv, int64_t rows,
+                            uint64_t* __restrict__ keys, int32_t* __restrict__ pos)
+{
+    const int64_t r0 = static_cast<int64_t>(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * (blockDim.x / 32);
+    const int lane = threadIdx.x & 31;
+    for (int64_t r = r0; r < rows; r += stride)
+    {
+        const uint64_t hi = static_cast<uint64_t>(static_cast<uint32_t>(inv[r])) << 32;
+        for (int k = indptr[r] + lane; k < indptr[r + 1]; k += 32)
+        {
+            keys[k] = hi | static_cast<uint32_t>(inv[indices[k]]);
+            pos[k] = k;
+        }
+    }
+}
+
+template <typename VT>
+__global__ void k_perm_gather(const uint64_t* __restrict__ sorted_keys,
+                              const int32_t* __restrict__ sorted_pos,
+                              const VT* __restrict__ data, int64_t nnz,
+                              int32_t* __restrict__ p_ind, VT* __restrict__ p_data)
+{
+    const int64_t i0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t i = i0; i < nnz; i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        p_ind[i] = static_cast<int32_t>(sorted_keys[i] & 0xffffffffULL);
+        p_data[i] = data[sorted_pos[i]];
+    }
+}
+
+__global__ void k_bounds64(const uint64_t* __restrict__ sorted_keys, int64_t nnz,
+                           int64_t rows, int32_t* __restrict__ p_ptr)
+{
+    const int64_t r0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t r = r0; r <= rows; r += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        const uint64_t key = static_cast<uint64_t>(r) << 32;
+        int64_t lo = 0, hi = nnz;
+        while (lo < hi)
+        {
+            const int64_t mid = (lo + hi) >> 1;
+            if (sorted_keys[mid] < key) lo = mid + 1;
+            else hi = mid;
+        }
+        p_ptr[r] = static_cast<int32_t>(lo);
     }
 }
 

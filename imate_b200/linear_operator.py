@@ -30,16 +30,51 @@ def _dtype_code(dtype):
                     'GPU; got "%s".' % dtype)
 
 
+def locality_order(A, reorder="auto"):
+    """Reverse Cuthill-McKee order of a square sparse matrix, or None.
+
+    'auto' reorders square matrices of order >= 16384 whose nonzeros lie far
+    from the diagonal (mean |i - j| > 256) when RCM shrinks that distance at
+    least fourfold: the SpMM gathers of such matrices then stay inside a
+    window that fits L2.  True always reorders a square matrix, False never.
+    """
+    if reorder is False or A.shape[0] != A.shape[1]:
+        return None
+    from scipy.sparse.csgraph import reverse_cuthill_mckee
+    A = sp.csr_matrix(A)
+    n = A.shape[0]
+    if reorder == "auto":
+        if n < 16384 or A.nnz == 0:
+            return None
+        rows = np.repeat(np.arange(n), np.diff(A.indptr))
+        spread = float(np.mean(np.abs(A.indices - rows)))
+        if spread <= 256.0:
+            return None
+    perm = reverse_cuthill_mckee(A, symmetric_mode=False)
+    if reorder == "auto":
+        inv = np.empty_like(perm)
+        inv[perm] = np.arange(n, dtype=perm.dtype)
+        rows = np.repeat(np.arange(n), np.diff(A.indptr))
+        new_spread = float(np.mean(np.abs(inv[A.indices] - inv[rows])))
+        if new_spread * 4.0 > spread:
+            return None
+    return np.ascontiguousarray(perm, dtype=np.int32)
+
+
 class _DeviceOperator:
     """An ``slq_op`` plus the tensors it points into (kept alive here)."""
 
-    def __init__(self, A, affine, need_transpose, check_indices=True):
+    def __init__(self, A, affine, need_transpose, check_indices=True,
+                 reorder="auto"):
         import torch
         lib = _lib.load()
         if not torch.cuda.is_available():
             raise RuntimeError("no CUDA device is available for the SLQ "
                                "engine (it has no CPU path)")
         self.device = torch.device("cuda", torch.cuda.current_device())
+        perm = locality_order(A, reorder)
+        if perm is not None and A.format != "csr":
+            A = A.tocsr()
         fmt = _lib.SLQ_CSC if A.format == "csc" else _lib.SLQ_CSR
         if A.format not in ("csr", "csc"):
             A = A.tocsr()
@@ -60,10 +95,17 @@ class _DeviceOperator:
             np.ascontiguousarray(A.indices, dtype=np.int32)).to(dev)
         self.indptr = torch.from_numpy(
             np.ascontiguousarray(A.indptr, dtype=np.int32)).to(dev)
+        self.perm = None
+        self.inv = None
+        if perm is not None:
+            self.perm = torch.from_numpy(perm).to(dev)
+            self.inv = torch.empty_like(self.perm)
+            self.inv[self.perm.long()] = torch.arange(
+                perm.size, dtype=torch.int32, device=dev)
         nbytes = ctypes.c_size_t(0)
         _lib.check(lib.slq_operator_workspace_bytes(
             A.shape[0], A.shape[1], self.nnz, self.dtype_code, fmt,
-            int(need_transpose), ctypes.byref(nbytes)))
+            int(need_transpose), int(perm is not None), ctypes.byref(nbytes)))
         self.workspace = torch.empty(max(int(nbytes.value), 256),
                                      dtype=torch.uint8, device=dev)
         self.handle = ctypes.c_void_p(None)
@@ -72,7 +114,9 @@ class _DeviceOperator:
             self.data.data_ptr(), self.indices.data_ptr(),
             self.indptr.data_ptr(), A.shape[0], A.shape[1], self.nnz,
             self.dtype_code, fmt, int(affine), int(need_transpose),
-            int(check_indices), self.workspace.data_ptr(),
+            int(check_indices),
+            self.perm.data_ptr() if self.perm is not None else None,
+            self.workspace.data_ptr(),
             self.workspace.numel(), stream.cuda_stream,
             ctypes.byref(self.handle)))
         self.affine = affine
@@ -98,7 +142,7 @@ class _DeviceOperator:
         tdt = torch.float64 if self.dtype_code == _lib.SLQ_F64 else \
             torch.float32
         Xp = torch.zeros((X.shape[0], wpad), dtype=tdt, device=self.device)
-        Xp[:, :width] = X
+        Xp[:, :width] = X if self.perm is None else X[self.perm.long()]
         rows = self.shape[1] if transpose else self.shape[0]
         Y = torch.empty((rows, wpad), dtype=tdt, device=self.device)
         stream = torch.cuda.current_stream(self.device)
@@ -106,6 +150,8 @@ class _DeviceOperator:
             self.handle, int(transpose), float(t), Xp.data_ptr(),
             Y.data_ptr(), wpad, stream.cuda_stream))
         Y = Y[:, :width]
+        if self.perm is not None:
+            Y = Y[self.inv.long()]
         return Y.reshape(-1) if squeeze else Y
 
 
@@ -149,7 +195,9 @@ class LinearOperator:
 
     def get_device_operator(self, need_transpose=False):
         """Device operator on the current CUDA device, created on first use
-        and reused (``linear_operator.py:114-147``)."""
+        and reused (``linear_operator.py:114-147``).  Square matrices may be
+        stored in a locality order (see ``locality_order``; the ``reorder``
+        attribute, default 'auto')."""
         import torch
         dev = torch.cuda.current_device() if torch.cuda.is_available() else -1
         key = (dev, bool(need_transpose))
@@ -158,7 +206,8 @@ class LinearOperator:
             op = self._device_ops.get((dev, True))
         if op is None:
             A = self.A if sp.issparse(self.A) else sp.csr_matrix(self.A)
-            op = _DeviceOperator(A, self._affine(), need_transpose)
+            op = _DeviceOperator(A, self._affine(), need_transpose,
+                                 reorder=getattr(self, "reorder", "auto"))
             self._device_ops[key] = op
         return op
 
@@ -168,10 +217,16 @@ class LinearOperator:
 
 
 class Matrix(LinearOperator):
-    """A fixed matrix (``imate/linear_operator/matrix.py``)."""
+    """A fixed matrix (``imate/linear_operator/matrix.py``).
 
-    def __init__(self, A):
+    ``reorder`` ('auto', True or False) selects the device storage order of
+    square matrices (see ``locality_order``); results do not depend on it
+    beyond floating-point summation order.
+    """
+
+    def __init__(self, A, reorder="auto"):
         super().__init__()
+        self.reorder = reorder
         if not (sp.issparse(A) or isinstance(A, np.ndarray)):
             raise TypeError("A should be a numpy array or a scipy sparse "
                             "matrix.")
@@ -203,8 +258,9 @@ class AffineMatrixFunction(LinearOperator):
     general B is not served by this engine.
     """
 
-    def __init__(self, A, B=None):
+    def __init__(self, A, B=None, reorder="auto"):
         super().__init__()
+        self.reorder = reorder
         self.A = A
         self.B = B
         self.num_parameters = 1

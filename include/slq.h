@@ -48,13 +48,15 @@ typedef enum { SLQ_RNG_PARITY = 0, SLQ_RNG_FAST = 1 } slq_rng;
 typedef struct slq_op slq_op;
 
 /* Bytes of device workspace slq_operator_create needs for the layouts it
- * derives (a CSR copy of A^T for gram runs, a CSR copy of A for CSC input).
+ * derives: a CSR copy of A^T for gram runs, a CSR copy of A for CSC input,
+ * and the symmetrically permuted matrix when a permutation is given.
  * Replaces the device upload of cuCSRMatrix / cuCSCMatrix
  * (imate/_cu_linear_operator/cu_csr_matrix.cu:165-224,
  *  cu_csc_matrix.cu:165-230). */
 slq_status slq_operator_workspace_bytes(int64_t num_rows, int64_t num_cols,
                                         int64_t nnz, int dtype, int format,
-                                        int need_transpose, size_t* bytes);
+                                        int need_transpose, int has_perm,
+                                        size_t* bytes);
 
 /* Wrap caller-owned device arrays (values dtype, int32 indices, int32 index
  * pointer of length num_rows+1 for CSR / num_cols+1 for CSC) as an operator.
@@ -62,16 +64,27 @@ slq_status slq_operator_workspace_bytes(int64_t num_rows, int64_t num_cols,
  * the operator as A + t I (imate.AffineMatrixFunction with B = I; the
  * eigenvalue shift relation of c_affine_matrix_function.cpp:98-113 holds).
  * check_indices != 0 validates indptr monotonicity and index range on the
- * device first (SLQ_ERR_BAD_CSR on failure).  Replaces pycuMatrix.__cinit__
- * (imate/_cu_linear_operator/py_cu_matrix.pyx:118-200) and
- * cuCSRMatrix / cuCSCMatrix / cuCSRAffineMatrixFunction construction. */
+ * device first (SLQ_ERR_BAD_CSR on failure).
+ *
+ * perm (device int32[num_rows], or NULL; square CSR input only) is a
+ * locality ordering: the engine stores B = P A P^T with B[i][j] =
+ * A[perm[i]][perm[j]] and writes probe element e to row perm^-1[e], so every
+ * inner product -- hence every Lanczos coefficient, node, weight and sample --
+ * is that of A; only the order of floating-point sums changes.  A
+ * bandwidth-reducing order (reverse Cuthill-McKee) keeps each SpMM gather
+ * window inside L2.  slq_operator_dot on such an operator acts on permuted
+ * vectors (y' = B x').
+ *
+ * Replaces pycuMatrix.__cinit__ (imate/_cu_linear_operator/py_cu_matrix.pyx:
+ * 118-200) and cuCSRMatrix / cuCSCMatrix / cuCSRAffineMatrixFunction
+ * construction. */
 slq_status slq_operator_create(const void* data, const int32_t* indices,
                                const int32_t* indptr, int64_t num_rows,
                                int64_t num_cols, int64_t nnz, int dtype,
                                int format, int affine, int need_transpose,
-                               int check_indices, void* workspace,
-                               size_t workspace_bytes, void* stream,
-                               slq_op** out);
+                               int check_indices, const int32_t* perm,
+                               void* workspace, size_t workspace_bytes,
+                               void* stream, slq_op** out);
 
 /* Release the host-side operator record (device arrays stay with their
  * owners).  Replaces the cuLinearOperator destructors

@@ -304,3 +304,41 @@ def test_indefinite_matrix_gives_nan_logdet(cuda):
                          min_num_samples=3, max_num_samples=3,
                          lanczos_degree=8, seed=2)
     assert np.isnan(tr)
+
+
+def test_reordered_operator_products(cuda):
+    A = ib.correlation_matrix(3000, scale=0.02, threshold=0.05, shift=0.1,
+                              seed=5)
+    M = ib.Matrix(A, reorder=True)
+    op = M.get_device_operator(need_transpose=True)
+    assert op.perm is not None
+    x = np.random.default_rng(0).standard_normal((3000, 8))
+    y = _dot(op, x)
+    want = A @ x
+    assert np.max(np.abs(y - want)) < 1e-12 * np.max(np.abs(want))
+
+
+@pytest.mark.parametrize("orth", [0, -1])
+def test_reordered_lanczos_matches_reference(cuda, golden, corr_small, orth):
+    # a symmetric permutation changes only summation order
+    g = golden("krylov.npz")
+    M = ib.Matrix(corr_small, reorder=True)
+    tr, info = _run("log", M, block_size=4, min_num_samples=4,
+                    max_num_samples=4, lanczos_degree=20,
+                    orthogonalize=orth, seed=5)
+    assert M.get_device_operator().perm is not None
+    for p in range(4):
+        key = "corr_orth%d_p%d" % (orth, p)
+        assert rel(info["engine"]["alpha"][p], g[key + "_alpha"]) < RTOL_FP64
+        assert rel(info["engine"]["beta"][p], g[key + "_beta"]) < RTOL_FP64
+
+
+def test_reordered_gram_matches_oracle(cuda, corr_small):
+    M = ib.Matrix(corr_small, reorder=True)
+    kw = dict(min_num_samples=3, max_num_samples=6, error_rtol=1e-9,
+              lanczos_degree=12, orthogonalize=-1, seed=6)
+    tr, info = _run("inv", M, gram=True, block_size=2, coefficients=False,
+                    **kw)
+    want = oracle.trace_estimator(corr_small, "inv", gram=True, **kw)
+    assert rel(info["convergence"]["samples"], want["samples"][:, 0]) < \
+        RTOL_FP64
