@@ -31,7 +31,7 @@ EXPORTS = (
     "slq_nodes_weights", "slq_check_convergence", "slq_average_estimates",
     "slq_erfinv", "slq_xoshiro_jump_ahead", "slq_device_info",
     "slq_last_error", "slq_abi_version", "slq_profile_begin",
-    "slq_profile_end",
+    "slq_profile_end", "slq_generate_probes_noalloc",
 )
 
 
@@ -118,6 +118,8 @@ def _declare(lib):
         "slq_generate_probes": (i32, [i64, i32, i64, i64, i32, i32, i32, vp,
                                       vp, sz, vp]),
         "slq_generate_probes_workspace_bytes": (i32, [i64, i32, psz]),
+        "slq_generate_probes_noalloc": (i32, [i64, i32, i64, i64, i32, i32,
+                                              i32, vp, vp]),
         "slq_nodes_weights": (i32, [vp, vp, vp, i32, i32, i32, vp, vp, vp,
                                     vp]),
         "slq_check_convergence": (i32, [vp, i32, i32, vp, i32, d, d, d, vp,

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1309,6 +1310,118 @@ extern "C" slq_status slq_generate_probes(int64_t seed, int rng, int64_t len, in
         SLQ_CK(cudaMemcpyAsync(B.chunk_polys, polys.data(), polys.size() * 8,
                                cudaMemcpyHostToDevice, st));
         SLQ_CK(cudaStreamSynchronize(st));  // host vectors go out of scope
+    }
+    Launcher L;
+    L.st = st;
+    SLQ_TRY(device_sms(&L.sms));
+    if (dtype == SLQ_F64)
+        return launch_probes<double>(L, r, rng, seed, first, count, B, nullptr,
+                                     static_cast<double*>(out));
+    return launch_probes<float>(L, r, rng, seed, first, count, B, nullptr,
+                                static_cast<float*>(out));
+}
+
+// ---------------------------------------------------------------------------
+// Probe generation that allocates nothing (slq_generate_probes_noalloc).
+//
+// Some callers cannot hand the engine a workspace: code whose device memory
+// is wholly owned by a caching allocator or a fixed-size arena (a direct
+// cudaMalloc there fails or fragments the pool), and latency-critical paths
+// that cannot afford the device-wide synchronisation cudaFree may trigger.
+// For them the generator keeps its scratch -- per-probe xoshiro256** start
+// states and per-chunk jump polynomials -- in a file-scope device array of
+// fixed size.  Every GPU that loads this library holds the array (288 KB)
+// until the process exits.
+// ---------------------------------------------------------------------------
+
+namespace {
+constexpr int NOALLOC_MAX_WIDTH = 1024;    // probes per call
+constexpr int NOALLOC_MAX_CHUNKS = 8192;   // parallel chunks per probe
+constexpr size_t NOALLOC_WORDS =
+    static_cast<size_t>(NOALLOC_MAX_WIDTH + NOALLOC_MAX_CHUNKS) * 4;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+std::mutex g_noalloc_mutex;
+// device address of the scratch array, per device (host code must not use
+// the array's name as a device pointer)
+uint64_t* g_noalloc_dev[NOALLOC_MAX_DEVICES] = {};
+// host staging of the scratch contents (static storage, no heap)
+uint64_t g_noalloc_host[NOALLOC_WORDS];
+}  // namespace
+
+// starts: words [0, 4*NOALLOC_MAX_WIDTH); chunk polynomials after them
+static __device__ __align__(256) uint64_t g_noalloc_scratch[NOALLOC_WORDS];
+
+extern "C" slq_status slq_generate_probes_noalloc(int64_t seed, int rng, int64_t len,
+                                                  int64_t first, int count, int width,
+                                                  int dtype, void* out, void* stream)
+{
+    if (!out || len <= 0 || first < 0 || count < 0 || width <= 0 || count > width ||
+        seed < 0 || (rng != SLQ_RNG_PARITY && rng != SLQ_RNG_FAST) ||
+        (dtype != SLQ_F32 && dtype != SLQ_F64))
+        return fail(SLQ_ERR_BAD_ARG, "generate_probes_noalloc: bad argument");
+    if (width > NOALLOC_MAX_WIDTH)
+        return fail(SLQ_ERR_BAD_ARG,
+                    "generate_probes_noalloc: width " + std::to_string(width) +
+                        " exceeds the static scratch limit of " +
+                        std::to_string(NOALLOC_MAX_WIDTH) + " probes per call");
+    int dev = 0;
+    SLQ_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return fail(SLQ_ERR_BAD_ARG, "generate_probes_noalloc: device index out of range");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_dev[dev])
+    {
+        // first call on this device (the device is current): resolve the
+        // array's device address once
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(SLQ_ERR_CUDA, std::string("cudaGetSymbolAddress: ") +
+                                          cudaGetErrorString(e));
+        g_noalloc_dev[dev] = static_cast<uint64_t*>(ptr);
+    }
+    uint64_t* scratch = g_noalloc_dev[dev];
+
+    RunPlan r;
+    r.nv = len;
+    r.b = width;
+    r.wpp = len / 64 + 1;
+    r.cw = 64;
+    while ((r.wpp + r.cw - 1) / r.cw > NOALLOC_MAX_CHUNKS) r.cw *= 2;
+    r.nchunks = static_cast<int>((r.wpp + r.cw - 1) / r.cw);
+    RunBufs B;
+    B.starts = scratch;
+    B.chunk_polys = scratch + static_cast<size_t>(NOALLOC_MAX_WIDTH) * 4;
+    if (rng == SLQ_RNG_PARITY)
+    {
+        if (!self_check()) return fail(SLQ_ERR_CUDA, "jump polynomial self-check failed");
+        uint64_t cur[4];
+        stream_state(seed, cur);
+        jump_ahead(cur, static_cast<uint64_t>(first) * static_cast<uint64_t>(r.wpp));
+        const Poly256 adv = jump_poly(static_cast<uint64_t>(r.wpp));
+        uint64_t* hs = g_noalloc_host;
+        uint64_t* hp = g_noalloc_host + static_cast<size_t>(NOALLOC_MAX_WIDTH) * 4;
+        for (int pi = 0; pi < count; ++pi)
+        {
+            for (int k = 0; k < 4; ++k) hs[static_cast<size_t>(pi) * 4 + k] = cur[k];
+            apply_poly(adv, cur);
+        }
+        const Poly256 step = jump_poly(static_cast<uint64_t>(r.cw));
+        Poly256 acc = {{1, 0, 0, 0}};
+        for (int ci = 0; ci < r.nchunks; ++ci)
+        {
+            for (int k = 0; k < 4; ++k) hp[static_cast<size_t>(ci) * 4 + k] = acc.w[k];
+            acc = poly_mulmod(acc, step);
+        }
+        SLQ_CK(cudaMemcpyAsync(B.starts, hs, sizeof(uint64_t) * 4 * static_cast<size_t>(count),
+                               cudaMemcpyHostToDevice, st));
+        SLQ_CK(cudaMemcpyAsync(B.chunk_polys, hp,
+                               sizeof(uint64_t) * 4 * static_cast<size_t>(r.nchunks),
+                               cudaMemcpyHostToDevice, st));
+        // the host staging is reused by the next call
+        SLQ_CK(cudaStreamSynchronize(st));
     }
     Launcher L;
     L.st = st;

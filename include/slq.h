@@ -179,6 +179,21 @@ slq_status slq_generate_probes(int64_t seed, int rng, int64_t len,
 slq_status slq_generate_probes_workspace_bytes(int64_t len, int width,
                                                size_t* bytes);
 
+/* The probe generator above without any workspace (no counterpart in the
+ * reference).  For callers that cannot allocate device memory -- code whose
+ * device memory is entirely owned by a caching allocator or a fixed arena,
+ * and latency-critical paths that must not take the synchronisation cudaFree
+ * can cause.  Its scratch (probe start states and jump polynomials) is a
+ * fixed 288 KB array inside the library, held by every GPU that loads it.
+ * Limit: width <= 1024 probes per call (SLQ_ERR_BAD_ARG beyond).  The first
+ * call on a device resolves the array's device address, so make that first
+ * call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU (other streams, other host threads) race; each call
+ * synchronizes its stream after staging the parity-mode scratch. */
+slq_status slq_generate_probes_noalloc(int64_t seed, int rng, int64_t len,
+                                       int64_t first, int count, int width,
+                                       int dtype, void* out, void* stream);
+
 /* Nodes (theta) and weights (tau) of a batch of Jacobi matrices, on the
  * device, by implicit QL in FP64.  All arrays are device memory in
  * probe-minor layout: alpha, beta, theta, tau are [m][count] (entry i of
