@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libslq_b200.so")
 SLQ_OK = 0
 STATUS_NAMES = {
     0: "OK", 1: "BAD_ARG", 2: "BAD_CSR", 3: "WORKSPACE", 4: "CUDA",
-    5: "NAN", 6: "EIGEN", 7: "UNSUPPORTED",
+    5: "NAN", 6: "EIGEN", 7: "UNSUPPORTED", 8: "TIMEOUT",
 }
 SLQ_F32, SLQ_F64 = 0, 1
 SLQ_CSR, SLQ_CSC = 0, 1
@@ -105,9 +105,9 @@ def _declare(lib):
     psz = ctypes.POINTER(ctypes.c_size_t)
     sig = {
         "slq_operator_workspace_bytes": (i32, [i64, i64, i64, i32, i32, i32,
-                                               i32, psz]),
+                                               i32, i32, psz]),
         "slq_operator_create": (i32, [vp, vp, vp, i64, i64, i64, i32, i32,
-                                      i32, i32, i32, vp, vp, sz, vp,
+                                      i32, i32, i32, vp, i32, vp, sz, vp,
                                       ctypes.POINTER(vp)]),
         "slq_operator_destroy": (i32, [vp]),
         "slq_operator_dot": (i32, [vp, i32, d, vp, vp, i32, vp]),

@@ -59,9 +59,9 @@ slq_status fail(slq_status s, const std::string& msg)
                                           cudaGetErrorString(e_));          \
     } while (0)
 
-#define SLQ_TRY(expr)                                                       \
+#define SLQ_TRY(...)                                                        \
     do {                                                                    \
-        slq_status s_ = (expr);                                             \
+        slq_status s_ = (__VA_ARGS__);                                      \
         if (s_ != SLQ_OK) return s_;                                        \
     } while (0)
 
@@ -210,6 +210,14 @@ struct slq_op {
     const int32_t* t_ptr = nullptr;
     // symmetric locality permutation: probe element e lives in row inv[e]
     const int32_t* inv = nullptr;
+    // row-group format (0 = none) of A and of A^T
+    int group_rows = 0;
+    const int32_t* a_gptr = nullptr;
+    const int32_t* a_gcol = nullptr;
+    const void* a_gval = nullptr;
+    const int32_t* t_gptr = nullptr;
+    const int32_t* t_gcol = nullptr;
+    const void* t_gval = nullptr;
 };
 
 namespace {
@@ -363,13 +371,70 @@ slq_status permute_csr(const int32_t* ptr, const int32_t* ind, const void* data,
     return SLQ_OK;
 }
 
+struct GroupBufs {
+    int32_t* counts;
+    int32_t* gptr;
+    int32_t* gcol;
+    void* gval;
+    void* temp;
+    size_t temp_bytes;
+};
+
+// Union entries never exceed nnz, so the format fits in nnz (col + G values).
+slq_status group_layout(Carver& c, int64_t rows, int64_t nnz, int G, int dtype, GroupBufs* t)
+{
+    const int64_t ng = (rows + G - 1) / G;
+    size_t temp_bytes = 0;
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes,
+                                                  static_cast<const int32_t*>(nullptr),
+                                                  static_cast<int32_t*>(nullptr),
+                                                  static_cast<int>(ng + 1));
+    if (e != cudaSuccess)
+        return fail(SLQ_ERR_CUDA, std::string("cub scan sizing: ") + cudaGetErrorString(e));
+    t->counts = c.take<int32_t>(ng + 1);
+    t->gptr = c.take<int32_t>(ng + 1);
+    t->gcol = c.take<int32_t>(std::max<int64_t>(nnz, 1));
+    t->gval = c.take<char>(std::max<int64_t>(nnz, 1) * G * dsize(dtype));
+    t->temp = c.take<char>(temp_bytes);
+    t->temp_bytes = temp_bytes;
+    return SLQ_OK;
+}
+
+slq_status group_build(const int32_t* ptr, const int32_t* ind, const void* val, int64_t rows,
+                       int G, int dtype, GroupBufs* t, cudaStream_t st)
+{
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
+    const int64_t ng = (rows + G - 1) / G;
+    SLQ_CK(cudaMemsetAsync(t->counts, 0, sizeof(int32_t) * (ng + 1), st));
+    k_rg_count<<<sms * 8, 256, 0, st>>>(ptr, ind, rows, G, t->counts, ng);
+    SLQ_LAUNCH_CK();
+    size_t tb = t->temp_bytes;
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(t->temp, tb, t->counts, t->gptr,
+                                                  static_cast<int>(ng + 1), st);
+    if (e != cudaSuccess)
+        return fail(SLQ_ERR_CUDA, std::string("cub scan: ") + cudaGetErrorString(e));
+    if (dtype == SLQ_F64)
+        k_rg_fill<double><<<sms * 8, 256, 0, st>>>(ptr, ind, static_cast<const double*>(val),
+                                                   rows, G, t->gptr, t->gcol,
+                                                   static_cast<double*>(t->gval), ng);
+    else
+        k_rg_fill<float><<<sms * 8, 256, 0, st>>>(ptr, ind, static_cast<const float*>(val), rows,
+                                                  G, t->gptr, t->gcol,
+                                                  static_cast<float*>(t->gval), ng);
+    SLQ_LAUNCH_CK();
+    return SLQ_OK;
+}
+
 }  // namespace
 
 extern "C" slq_status slq_operator_workspace_bytes(int64_t num_rows, int64_t num_cols,
                                                    int64_t nnz, int dtype, int format,
                                                    int need_transpose, int has_perm,
-                                                   size_t* bytes)
+                                                   int group_rows, size_t* bytes)
 {
+    if (group_rows != 0 && group_rows != 4 && group_rows != 8)
+        return fail(SLQ_ERR_BAD_ARG, "group_rows must be 0, 4 or 8");
     if (!bytes || num_rows < 0 || num_cols < 0 || nnz < 0)
         return fail(SLQ_ERR_BAD_ARG, "operator_workspace_bytes: bad argument");
     if (has_perm && (format != SLQ_CSR || num_rows != num_cols))
@@ -386,6 +451,13 @@ extern "C" slq_status slq_operator_workspace_bytes(int64_t num_rows, int64_t num
         const int64_t C = (format == SLQ_CSC) ? num_rows : num_cols;
         SLQ_TRY(transpose_layout(c, R, C, nnz, dtype, &t));
     }
+    if (group_rows)
+    {
+        GroupBufs g;
+        SLQ_TRY(group_layout(c, num_rows, nnz, group_rows, dtype, &g));
+        if (need_transpose || format == SLQ_CSC)
+            SLQ_TRY(group_layout(c, num_cols, nnz, group_rows, dtype, &g));
+    }
     *bytes = c.off + 256;
     return SLQ_OK;
 }
@@ -395,8 +467,8 @@ extern "C" slq_status slq_operator_create(const void* data, const int32_t* indic
                                           int64_t num_cols, int64_t nnz, int dtype,
                                           int format, int affine, int need_transpose,
                                           int check_indices, const int32_t* perm,
-                                          void* workspace, size_t workspace_bytes,
-                                          void* stream, slq_op** out)
+                                          int group_rows, void* workspace,
+                                          size_t workspace_bytes, void* stream, slq_op** out)
 {
     if (!out) return fail(SLQ_ERR_BAD_ARG, "operator_create: out is NULL");
     *out = nullptr;
@@ -413,7 +485,7 @@ extern "C" slq_status slq_operator_create(const void* data, const int32_t* indic
         return fail(SLQ_ERR_BAD_ARG, "operator_create: A + tI needs a square matrix");
     size_t need = 0;
     SLQ_TRY(slq_operator_workspace_bytes(num_rows, num_cols, nnz, dtype, format,
-                                         need_transpose, perm != nullptr, &need));
+                                         need_transpose, perm != nullptr, group_rows, &need));
     if (!workspace || workspace_bytes < need)
         return fail(SLQ_ERR_WORKSPACE, "operator_create: workspace too small (need " +
                                            std::to_string(need) + " bytes)");
@@ -497,6 +569,34 @@ extern "C" slq_status slq_operator_create(const void* data, const int32_t* indic
         op->a_data = t.t_data;
         op->a_ind = t.t_ind;
         op->a_ptr = t.t_ptr;
+    }
+    if (group_rows)
+    {
+        GroupBufs ga;
+        slq_status s = group_layout(c, num_rows, nnz, group_rows, dtype, &ga);
+        if (s == SLQ_OK)
+            s = group_build(op->a_ptr, op->a_ind, op->a_data, num_rows, group_rows, dtype, &ga,
+                            st);
+        if (s == SLQ_OK && op->t_ptr)
+        {
+            GroupBufs gt;
+            s = group_layout(c, num_cols, nnz, group_rows, dtype, &gt);
+            if (s == SLQ_OK)
+                s = group_build(op->t_ptr, op->t_ind, op->t_data, num_cols, group_rows, dtype,
+                                &gt, st);
+            op->t_gptr = gt.gptr;
+            op->t_gcol = gt.gcol;
+            op->t_gval = gt.gval;
+        }
+        if (s != SLQ_OK)
+        {
+            delete op;
+            return s;
+        }
+        op->group_rows = group_rows;
+        op->a_gptr = ga.gptr;
+        op->a_gcol = ga.gcol;
+        op->a_gval = ga.gval;
     }
     *out = op;
     return SLQ_OK;
@@ -714,6 +814,140 @@ slq_status finalize(Launcher& L, const double* partials, int nparts, int cols, i
     return SLQ_OK;
 }
 
+// Operator product on a block: row-group SpMM where the operator has the
+// format and the width suits it (32 <= b <= 256; FP64 b <= 128), else CSR.
+// *grid_out receives the number of partial rows the launch writes.
+template <typename VT, int LV, int G, int NS>
+slq_status spmm_rg_inst(Launcher& L, const int32_t* gptr, const int32_t* gcol, const VT* gval,
+                        int64_t nrows, int b, const VT* X, const double* sx, double shift, VT* Y,
+                        const VT* Z, const double* zc, const double* zs, int epi,
+                        double* partials, int64_t nnz, int64_t xrows, int* grid_out)
+{
+    const double s = sizeof(VT);
+    const double bytes = nnz * (s + 4.0) + (nrows + 1) * 4.0 + double(xrows) * b * s +
+                         double(nrows) * b * s * (Z ? 2.0 : 1.0);
+    ProfScope prof(SLQ_K_SPMM, bytes, L.st);
+    const int64_t ng = (nrows + G - 1) / G;
+    constexpr int GPC = 8 / NS;
+    const int grid = static_cast<int>(
+        std::max<int64_t>(1, std::min<int64_t>((ng + GPC - 1) / GPC, int64_t(L.sms) * 4)));
+    k_spmm_rg<VT, LV, G, NS><<<grid, 256, 0, L.st>>>(gptr, gcol, gval, nrows, ng, b, X, sx, shift, Y,
+                                                 Z, zc, zs, epi, partials);
+    SLQ_LAUNCH_CK();
+    ++L.launches;
+    *grid_out = grid;
+    return SLQ_OK;
+}
+
+template <typename VT>
+slq_status op_spmm(Launcher& L, const slq_op* op, int transpose, int b, const VT* X,
+                   const double* sx, double shift, VT* Y, const VT* Z, const double* zc,
+                   const double* zs, int epi, double* partials, int* grid_out)
+{
+    const int64_t rows = transpose ? op->ncols : op->nrows;
+    const int64_t xrows = transpose ? op->nrows : op->ncols;
+    const int32_t* gptr = transpose ? op->t_gptr : op->a_gptr;
+    const int bmax_rg = (sizeof(VT) == 8) ? 64 : 256;
+    if (op->group_rows && gptr && b >= 32 && b <= bmax_rg)
+    {
+        const int32_t* gcol = transpose ? op->t_gcol : op->a_gcol;
+        const VT* gval = static_cast<const VT*>(transpose ? op->t_gval : op->a_gval);
+#define SLQ_RG(BB, LVV, NSS)                                                                   \
+    if (b == BB)                                                                               \
+    {                                                                                          \
+        if (op->group_rows == 8)                                                               \
+            return spmm_rg_inst<VT, LVV, 8, NSS>(L, gptr, gcol, gval, rows, b, X, sx, shift,   \
+                                                 Y, Z, zc, zs, epi, partials, op->nnz, xrows,  \
+                                                 grid_out);                                    \
+        return spmm_rg_inst<VT, LVV, 4, NSS>(L, gptr, gcol, gval, rows, b, X, sx, shift, Y, Z, \
+                                             zc, zs, epi, partials, op->nnz, xrows, grid_out); \
+    }
+        SLQ_RG(32, 1, 1)
+        SLQ_RG(64, 2, 1)
+        SLQ_RG(128, 4, 1)
+        if constexpr (sizeof(VT) == 4)
+        {
+            SLQ_RG(256, 4, 2)
+        }
+#undef SLQ_RG
+    }
+    const int32_t* ptr = transpose ? op->t_ptr : op->a_ptr;
+    const int32_t* ind = transpose ? op->t_ind : op->a_ind;
+    const VT* val = static_cast<const VT*>(transpose ? op->t_data : op->a_data);
+    const int grid = spmm_grid<VT>(L, rows);
+    *grid_out = grid;
+    return spmm<VT>(L, grid, ptr, ind, val, rows, b, X, sx, shift, Y, Z, zc, zs, epi, partials,
+                    op->nnz, xrows);
+}
+
+// TMA-streamed pass (k_stream): MODE 0 = update + inner products,
+// MODE 1 = (update +) reorthogonalisation update + norm.
+template <typename VT, int MODE>
+slq_status stream_pass(Launcher& L, int64_t n, int b, const VT* W, VT* Wout, int do_update,
+                       const VT* Vj, const double* sj, const double* aj, const VT* Vm,
+                       const double* sm, const double* bm, const VT* basis, int64_t slot_elems,
+                       int bs, int last, int J, const VT* coef, int want_norm,
+                       double* partials, int32_t* error, int* grid_out)
+{
+    constexpr int R = (sizeof(VT) == 4) ? 16 : 8;
+    constexpr size_t SMEM_MAX = 232448;
+    const int PT = std::min(b, STREAM_CONSUMERS);
+    const int T = R * (STREAM_CONSUMERS / PT);
+    const size_t fixed = 256 + STREAM_CONSUMERS * sizeof(double);
+    const size_t extra = (MODE == 0) ? static_cast<size_t>(J) * STREAM_CONSUMERS * 8
+                                     : static_cast<size_t>(J) * PT * 8;
+    if (fixed + extra + 2 * STREAM_TILE_BYTES > SMEM_MAX)
+        return fail(SLQ_ERR_BAD_ARG, "stream pass: too many basis vectors per launch");
+    const int S = static_cast<int>(std::min<size_t>(STREAM_MAX_STAGES,
+                                                    (SMEM_MAX - fixed - extra) / STREAM_TILE_BYTES));
+    const size_t smem = fixed + static_cast<size_t>(S) * STREAM_TILE_BYTES + extra;
+    static bool attr = false;
+    if (!attr)
+    {
+        SLQ_CK(cudaFuncSetAttribute(k_stream<VT, MODE, R>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(SMEM_MAX)));
+        attr = true;
+    }
+    StreamArgs<VT> a;
+    a.n = n;
+    a.b = b;
+    a.PT = PT;
+    a.T = T;
+    a.S = S;
+    a.J = J;
+    a.bs = bs;
+    a.last = last;
+    a.slot_elems = slot_elems;
+    a.W = W;
+    a.Wout = Wout;
+    a.do_update = do_update;
+    a.Vj = Vj;
+    a.sj = sj;
+    a.aj = aj;
+    a.Vm = Vm;
+    a.sm = sm;
+    a.bm = bm;
+    a.basis = basis;
+    a.coef = coef;
+    a.want_norm = want_norm;
+    a.partials = partials;
+    a.error = error;
+    const int gy = b / PT;
+    const int gx = std::max(1, L.sms / gy);
+    const double vb = double(n) * b * sizeof(VT);
+    const int npre = 1 + (do_update ? (Vm ? 2 : 1) : 0);
+    const int skip = (MODE == 0 && do_update) ? (Vm ? 2 : 1) : 0;
+    const int reads = npre + std::max(0, J - skip);
+    const int writes = (MODE == 1 || do_update) ? 1 : 0;
+    ProfScope prof(MODE == 0 ? SLQ_K_DOTS : SLQ_K_REORTH, vb * (reads + writes), L.st);
+    k_stream<VT, MODE, R><<<dim3(gx, gy), STREAM_THREADS, smem, L.st>>>(a);
+    SLQ_LAUNCH_CK();
+    ++L.launches;
+    *grid_out = gx;
+    return SLQ_OK;
+}
+
 // ---------------------------------------------------------------------------
 // run plan and workspace
 // ---------------------------------------------------------------------------
@@ -739,6 +973,7 @@ struct RunBufs {
     int32_t* active;
     int32_t* size;
     int32_t* status;
+    int32_t* error;
     double* partials;
     double* samples;
     double* params;
@@ -812,7 +1047,7 @@ slq_status make_plan(const slq_op* op, const slq_params* p, int q, RunPlan* r)
 template <typename VT>
 int64_t slot_stride(int64_t len, int b)
 {
-    return len * b + 2560 / static_cast<int64_t>(sizeof(VT));
+    return ((len * b + 63) / 64) * 64 + 2560 / static_cast<int64_t>(sizeof(VT));
 }
 
 template <typename VT>
@@ -832,6 +1067,7 @@ void carve(Carver& c, const RunPlan& r, int sms, RunBufs* B)
     B->active = c.take<int32_t>(r.b);
     B->size = c.take<int32_t>(r.b);
     B->status = c.take<int32_t>(r.b);
+    B->error = c.take<int32_t>(1);
     // partial sums: SpMM grid <= 4*sms, stream kernels <= 2*sms (x J <= MAX_J)
     const size_t pcols = std::max<size_t>(static_cast<size_t>(sms) * 4 * r.b,
                                           static_cast<size_t>(sms) * 2 * MAX_J * r.b);
@@ -878,8 +1114,6 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
     VT* W = static_cast<VT*>(B.W);
     VT* W2 = static_cast<VT*>(B.W2);
     VT* coef = static_cast<VT*>(B.coef);
-    const VT* Aval = static_cast<const VT*>(op->a_data);
-    const VT* Tval = static_cast<const VT*>(op->t_data);
     const double thr = p->lanczos_tol * std::sqrt(static_cast<double>(r.nv));
     auto sv_of = [&](int vec) { return B.scale_v + static_cast<int64_t>(((vec % bs) + bs) % bs) * b; };
     auto su_of = [&](int vec) { return B.scale_u + static_cast<int64_t>(((vec % bs) + bs) % bs) * b; };
@@ -893,27 +1127,29 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
                                const double* sm, const double* bm, const VT* basis,
                                int64_t slot_elems, const double* scales, int last, int J,
                                int* nparts) -> slq_status {
-        const int dg = dots_grid<VT>(L, n, b, std::min(J, MAX_J));
         for (int c0 = 0; c0 < J; c0 += MAX_J)
         {
             const int Jc = std::min(MAX_J, J - c0);
             const bool first = (c0 == 0);
-            SLQ_TRY(update_dots<VT>(L, dg, n, b, first ? w_in_first : w_work, w_work,
-                                    first ? do_update : 0, Vj, sj, aj, Vm, sm, bm, basis,
-                                    slot_elems, bs, last - c0, Jc, B.partials));
+            int dg = 0;
+            SLQ_TRY(stream_pass<VT, 0>(L, n, b, first ? w_in_first : w_work, w_work,
+                                       first ? do_update : 0, Vj, sj, aj, Vm, sm, bm, basis,
+                                       slot_elems, bs, last - c0, Jc, nullptr, 0, B.partials,
+                                       B.error, &dg));
             SLQ_TRY(finalize<VT>(L, B.partials, dg, Jc * b, FIN_COEF, nullptr,
                                  coef + static_cast<int64_t>(c0) * b, scales, b, bs, last - c0,
                                  nullptr, nullptr, nullptr, 0, 0.0, 0));
         }
-        const int rg = reorth_grid<VT>(L, n, b);
+        int rg = 0;
         for (int c0 = 0; c0 < J; c0 += MAX_J)
         {
             const int Jc = std::min(MAX_J, J - c0);
             const bool lastc = (c0 + MAX_J >= J);
-            SLQ_TRY(reorth<VT>(L, rg, n, b, w_work, lastc ? w_out : w_work, 0, nullptr, nullptr,
-                               nullptr, nullptr, nullptr, nullptr, basis, slot_elems, bs,
-                               last - c0, Jc, coef + static_cast<int64_t>(c0) * b,
-                               lastc ? 1 : 0, B.partials));
+            SLQ_TRY(stream_pass<VT, 1>(L, n, b, w_work, lastc ? w_out : w_work, 0, nullptr,
+                                       nullptr, nullptr, nullptr, nullptr, nullptr, basis,
+                                       slot_elems, bs, last - c0, Jc,
+                                       coef + static_cast<int64_t>(c0) * b, lastc ? 1 : 0,
+                                       B.partials, B.error, &rg));
         }
         *nparts = rg;
         return SLQ_OK;
@@ -921,12 +1157,12 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
 
     if (!r.gram)
     {
-        const int sg = spmm_grid<VT>(L, r.nv);
         for (int j = 0; j < m; ++j)
         {
             VT* vj = Vs(j);
-            SLQ_TRY(spmm<VT>(L, sg, op->a_ptr, op->a_ind, Aval, r.nv, b, vj, sv_of(j), shift, W,
-                             nullptr, nullptr, nullptr, 1, B.partials, op->nnz, r.nv));
+            int sg = 0;
+            SLQ_TRY(op_spmm<VT>(L, op, 0, b, vj, sv_of(j), shift, W, nullptr, nullptr, nullptr, 1,
+                                B.partials, &sg));
             double* aj = B.alpha + static_cast<int64_t>(j) * b;
             SLQ_TRY(finalize<VT>(L, B.partials, sg, b, FIN_STORE, aj, nullptr, nullptr, b, bs, 0,
                                  nullptr, nullptr, nullptr, 0, 0.0, j));
@@ -939,10 +1175,9 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
             int nparts = 0;
             if (J == 0)
             {
-                const int rg = reorth_grid<VT>(L, r.nv, b);
-                SLQ_TRY(reorth<VT>(L, rg, r.nv, b, W, Vs(j + 1), 1, vj, sv_of(j), aj, vm, sm, bm,
-                                   V, vslot, bs, j, 0, coef, 1, B.partials));
-                nparts = rg;
+                SLQ_TRY(stream_pass<VT, 1>(L, r.nv, b, W, Vs(j + 1), 1, vj, sv_of(j), aj, vm, sm,
+                                           bm, V, vslot, bs, j, 0, coef, 1, B.partials, B.error,
+                                           &nparts));
             }
             else
             {
@@ -956,8 +1191,6 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
     }
     else
     {
-        const int sgu = spmm_grid<VT>(L, r.nu);
-        const int sgv = spmm_grid<VT>(L, r.nv);
         for (int j = 0; j < m; ++j)
         {
             int no = 0;
@@ -965,11 +1198,12 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
             // u_j = A v_j - beta_{j-1} u_{j-1}
             const int Ju = (j > 0) ? static_cast<int>(std::min<int64_t>(no, r.nu)) : 0;
             VT* uj = Us(j);
-            SLQ_TRY(spmm<VT>(L, sgu, op->a_ptr, op->a_ind, Aval, r.nu, b, Vs(j), sv_of(j), shift,
-                             uj, (j > 0) ? Us(j - 1) : nullptr,
-                             (j > 0) ? B.beta + static_cast<int64_t>(j - 1) * b : nullptr,
-                             (j > 0) ? su_of(j - 1) : nullptr, Ju > 0 ? 0 : 2, B.partials,
-                             op->nnz, r.nv));
+            int sgu = 0;
+            SLQ_TRY(op_spmm<VT>(L, op, 0, b, Vs(j), sv_of(j), shift, uj,
+                                (j > 0) ? Us(j - 1) : nullptr,
+                                (j > 0) ? B.beta + static_cast<int64_t>(j - 1) * b : nullptr,
+                                (j > 0) ? su_of(j - 1) : nullptr, Ju > 0 ? 0 : 2, B.partials,
+                                &sgu));
             int nparts = sgu;
             if (Ju > 0)
                 SLQ_TRY(reorthogonalize(r.nu, uj, uj, uj, 0, nullptr, nullptr, nullptr, nullptr,
@@ -981,8 +1215,9 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
             // v_{j+1} = A^T u_j - alpha_j v_j
             const int Jv = static_cast<int>(std::min<int64_t>(no, r.nv));
             VT* vn = Vs(j + 1);
-            SLQ_TRY(spmm<VT>(L, sgv, op->t_ptr, op->t_ind, Tval, r.nv, b, uj, su_of(j), shift, vn,
-                             Vs(j), aj, sv_of(j), Jv > 0 ? 0 : 2, B.partials, op->nnz, r.nu));
+            int sgv = 0;
+            SLQ_TRY(op_spmm<VT>(L, op, 1, b, uj, su_of(j), shift, vn, Vs(j), aj, sv_of(j),
+                                Jv > 0 ? 0 : 2, B.partials, &sgv));
             nparts = sgv;
             if (Jv > 0)
                 SLQ_TRY(reorthogonalize(r.nv, vn, vn, vn, 0, nullptr, nullptr, nullptr, nullptr,
@@ -1019,6 +1254,8 @@ slq_status run_typed(slq_op* op, const slq_params* p, const double* parameters, 
         for (int j = 0; j < q; ++j) params[j] = parameters[j];
     const double shift = op->affine ? params[0] : 0.0;
     SLQ_CK(cudaMemcpyAsync(B.params, params.data(), sizeof(double) * q, cudaMemcpyHostToDevice, st));
+    SLQ_CK(cudaMemsetAsync(B.error, 0, sizeof(int32_t), st));
+    int32_t herr = 0;
 
     // parity stream set-up on the host: state of probe 0 and the per-chunk
     // advance polynomials
@@ -1129,7 +1366,10 @@ slq_status run_typed(slq_op* op, const slq_params* p, const double* parameters, 
             SLQ_CK(cudaMemcpyAsync(hb.data(), B.beta, sizeof(double) * m * b,
                                    cudaMemcpyDeviceToHost, st));
         }
+        SLQ_CK(cudaMemcpyAsync(&herr, B.error, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         SLQ_CK(cudaStreamSynchronize(st));
+        if (herr)
+            return fail(SLQ_ERR_TIMEOUT, "a streaming kernel gave up waiting for its copies");
         ++blocks;
         computed += count;
         for (int pi = 0; pi < count && !all; ++pi)
@@ -1231,20 +1471,13 @@ extern "C" slq_status slq_operator_dot(slq_op* op, int transpose, double t, cons
     L.st = static_cast<cudaStream_t>(stream);
     SLQ_TRY(device_sms(&L.sms));
     const double shift = op->affine ? t : 0.0;
-    const int64_t rows = transpose ? op->ncols : op->nrows;
-    const int32_t* ptr = transpose ? op->t_ptr : op->a_ptr;
-    const int32_t* ind = transpose ? op->t_ind : op->a_ind;
-    const void* val = transpose ? op->t_data : op->a_data;
+    int grid = 0;
     if (op->dtype == SLQ_F64)
-        return spmm<double>(L, spmm_grid<double>(L, rows), ptr, ind,
-                            static_cast<const double*>(val), rows, width,
-                            static_cast<const double*>(x), nullptr, shift,
-                            static_cast<double*>(y), nullptr, nullptr, nullptr, 0, nullptr,
-                            op->nnz, transpose ? op->nrows : op->ncols);
-    return spmm<float>(L, spmm_grid<float>(L, rows), ptr, ind, static_cast<const float*>(val),
-                       rows, width, static_cast<const float*>(x), nullptr, shift,
-                       static_cast<float*>(y), nullptr, nullptr, nullptr, 0, nullptr,
-                       op->nnz, transpose ? op->nrows : op->ncols);
+        return op_spmm<double>(L, op, transpose, width, static_cast<const double*>(x), nullptr,
+                               shift, static_cast<double*>(y), nullptr, nullptr, nullptr, 0,
+                               nullptr, &grid);
+    return op_spmm<float>(L, op, transpose, width, static_cast<const float*>(x), nullptr, shift,
+                          static_cast<float*>(y), nullptr, nullptr, nullptr, 0, nullptr, &grid);
 }
 
 extern "C" slq_status slq_generate_probes_workspace_bytes(int64_t len, int width,

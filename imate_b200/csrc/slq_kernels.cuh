@@ -21,6 +21,7 @@
 #ifndef SLQ_KERNELS_CUH_
 #define SLQ_KERNELS_CUH_
 
+#include <climits>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -964,6 +965,641 @@ __global__ void k_init_block(int count, int b, int m, double s0,
     scale0[p] = real ? s0 : 0.0;
     active[p] = real ? 1 : 0;
     size[p] = m;
+}
+
+
+// ===========================================================================
+// TMA-streamed reorthogonalisation passes (sm_100a).
+//
+// One CTA per SM: a producer warp moves tiles of T rows x PT probes of every
+// vector the pass reads into a ring of S shared-memory stages with
+// cp.async.bulk (completion counted on an mbarrier per stage); eight
+// consumer warps compute from the stages and release them through a second
+// mbarrier per stage.  The copy engine keeps S x 16 KB in flight per SM, so
+// the pass streams at HBM rate without registers spent on loads in flight.
+//
+// Work per row tile, in item order:
+//   dots   : W [, v_j, v_{j-1} (three-term update; written to Wout)],
+//            then the basis vectors last-i (skipping v_j, v_{j-1}, whose
+//            products come from the update registers) -> FP64 partials of
+//            <v_i, w> per (i, probe);
+//   reorth : Win, then the basis vectors last-i: w -= c_i v_i, written to
+//            Wout, FP64 partials of |w|^2.
+// Rows past the last whole tile are done by the last CTA with plain loads.
+//
+// Every mbarrier wait is bounded; a wait that runs out sets *error and the
+// CTA skips the remaining work (it still waits, bounded, for the copies it
+// issued before it leaves).
+// ===========================================================================
+
+constexpr int STREAM_CONSUMERS = 256;            // 8 consumer warps
+constexpr int STREAM_THREADS = STREAM_CONSUMERS + 32;
+constexpr int STREAM_TILE_BYTES = 16384;
+constexpr int STREAM_MAX_STAGES = 8;
+constexpr long long STREAM_SPIN_LIMIT = 1LL << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait: false if the phase did not complete within the limit or
+// another thread of the CTA gave up (abort flag)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          const int* abort_flag)
+{
+    for (long long i = 0; i < STREAM_SPIN_LIMIT; ++i)
+    {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 1023) == 1023 && *reinterpret_cast<const volatile int*>(abort_flag))
+            return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
+                                              uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <typename VT>
+struct StreamArgs {
+    int64_t n;            // rows
+    int b;                // block width (row stride)
+    int PT;               // probes per CTA tile (grid.y = b / PT)
+    int T;                // rows per tile
+    int S;                // stages
+    int J;                // basis vectors (last, last-1, ...)
+    int bs;               // ring slots
+    int last;             // newest basis vector index
+    int64_t slot_elems;   // stride between ring slots (elements)
+    const VT* W;          // dots: input w (pre-update); reorth: input w
+    VT* Wout;             // updated / reorthogonalised w
+    int do_update;        // dots: three-term update first
+    const VT* Vj;
+    const double* sj;
+    const double* aj;
+    const VT* Vm;
+    const double* sm;
+    const double* bm;
+    const VT* basis;
+    const VT* coef;       // reorth: [J][b] coefficients c_i = h_i s_i
+    int want_norm;
+    double* partials;     // dots: [grid.x][J][b]; reorth: [grid.x][b]
+    int32_t* error;       // set to 1 when a wait runs out
+};
+
+// MODE 0: dots, MODE 1: reorth.  R = rows per consumer thread per tile.
+template <typename VT, int MODE, int R>
+__global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<VT> a)
+{
+    // shared memory: barriers (256 B) | norm partials (256 doubles) |
+    // S stages of 16 KB | dots: acc[J][256] doubles, reorth: coef[J][PT]
+    extern __shared__ __align__(128) unsigned char smem_stream[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_stream);
+    uint64_t* empty = full + STREAM_MAX_STAGES;
+    int* abort_flag = reinterpret_cast<int*>(empty + STREAM_MAX_STAGES);
+    double* red = reinterpret_cast<double*>(smem_stream + 256);
+    VT* stages = reinterpret_cast<VT*>(smem_stream + 256 + STREAM_CONSUMERS * 8);
+    const int tile_elems = a.T * a.PT;
+    double* extra = reinterpret_cast<double*>(smem_stream + 256 + STREAM_CONSUMERS * 8 +
+                                              static_cast<size_t>(a.S) * STREAM_TILE_BYTES);
+
+    const int tid = threadIdx.x;
+    const bool producer = tid >= STREAM_CONSUMERS;
+    const int PT = a.PT;
+    const int RSTEP = STREAM_CONSUMERS / PT;
+    const int pl = tid % PT;
+    const int roff = tid / PT;
+    const int p0 = blockIdx.y * PT;
+    const int b = a.b;
+    const int J = a.J;
+
+    // items per tile
+    const bool upd = a.do_update != 0;
+    const int npre = 1 + (upd ? (a.Vm ? 2 : 1) : 0);
+    // dots: basis vectors v_j, v_{j-1} are served from the update registers
+    const int skip = (MODE == 0 && upd) ? (a.Vm ? 2 : 1) : 0;
+    const int nbasis = (J > skip) ? J - skip : 0;
+    const int nitems = npre + nbasis;
+
+    if (tid == 0)
+    {
+        for (int s = 0; s < a.S; ++s)
+        {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], STREAM_CONSUMERS / 32);
+        }
+        abort_flag[0] = 0;
+        abort_flag[1] = 0;  // stays 0: bounded waits on the way out
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (MODE == 0)
+    {
+        for (int i = tid; i < J * STREAM_CONSUMERS; i += STREAM_THREADS) extra[i] = 0.0;
+    }
+    else
+    {
+        for (int i = tid; i < J * PT; i += STREAM_THREADS)
+            extra[i] = static_cast<double>(a.coef[static_cast<int64_t>(i / PT) * b + p0 + i % PT]);
+    }
+    __syncthreads();
+
+    const int64_t ntiles = a.n / a.T;
+    const bool contiguous = (PT == b);
+    const uint32_t tile_bytes = static_cast<uint32_t>(tile_elems * sizeof(VT));
+    auto item_ptr = [&](int item) -> const VT* {
+        if (item == 0) return a.W;
+        if (upd && item == 1) return a.Vj;
+        if (upd && item == 2 && a.Vm) return a.Vm;
+        const int i = skip + (item - npre);
+        return a.basis + static_cast<int64_t>(ring_slot(a.last - i, a.bs)) * a.slot_elems;
+    };
+
+    if (producer)
+    {
+        if ((tid & 31) == 0)
+        {
+            int s = 0;
+            uint32_t phase = 0;
+            int64_t issued = 0;
+            bool ok = true;
+            for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
+            {
+                const int64_t row0 = tile * a.T;
+                for (int item = 0; item < nitems; ++item)
+                {
+                    if (*reinterpret_cast<volatile int*>(abort_flag)) { ok = false; break; }
+                    if (!mbar_wait(&empty[s], phase ^ 1, abort_flag))
+                    {
+                        *abort_flag = 1;
+                        atomicExch(a.error, 1);
+                        ok = false;
+                        break;
+                    }
+                    VT* dst = stages + static_cast<size_t>(s) * (STREAM_TILE_BYTES / sizeof(VT));
+                    const VT* src = item_ptr(item) + row0 * b + p0;
+                    mbar_expect_tx(&full[s], tile_bytes);
+                    if (contiguous)
+                    {
+                        bulk_copy_g2s(dst, src, tile_bytes, &full[s]);
+                    }
+                    else
+                    {
+                        const uint32_t rb = static_cast<uint32_t>(PT * sizeof(VT));
+                        for (int r = 0; r < a.T; ++r)
+                            bulk_copy_g2s(dst + r * PT, src + static_cast<int64_t>(r) * b, rb,
+                                          &full[s]);
+                    }
+                    ++issued;
+                    if (++s == a.S) { s = 0; phase ^= 1; }
+                }
+            }
+            if (!ok)
+            {
+                // let the copies already issued land before the CTA leaves
+                int s2 = 0;
+                uint32_t ph2 = 0;
+                for (int64_t k = 0; k < issued; ++k)
+                {
+                    if (k + a.S >= issued) mbar_wait(&full[s2], ph2, abort_flag + 1);
+                    if (++s2 == a.S) { s2 = 0; ph2 ^= 1; }
+                }
+            }
+        }
+    }
+    else
+    {
+        int s = 0;
+        uint32_t phase = 0;
+        double cj = 0.0, cm = 0.0;
+        if (upd)
+        {
+            cj = a.aj[p0 + pl] * a.sj[p0 + pl];
+            cm = a.Vm ? a.bm[p0 + pl] * a.sm[p0 + pl] : 0.0;
+        }
+        double nacc = 0.0;
+        bool ok = true;
+        const int lane = tid & 31;
+        auto release = [&](int st) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[st]);
+        };
+        for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
+        {
+            const int64_t row0 = tile * a.T;
+            double w[R], vj[R], vm[R];
+            for (int item = 0; item < nitems; ++item)
+            {
+                if (*reinterpret_cast<volatile int*>(abort_flag)) { ok = false; break; }
+                if (!mbar_wait(&full[s], phase, abort_flag))
+                {
+                    *abort_flag = 1;
+                    atomicExch(a.error, 1);
+                    ok = false;
+                    break;
+                }
+                const VT* st = stages + static_cast<size_t>(s) * (STREAM_TILE_BYTES / sizeof(VT));
+                if (item == 0)
+                {
+#pragma unroll
+                    for (int k = 0; k < R; ++k)
+                        w[k] = static_cast<double>(st[(roff + k * RSTEP) * PT + pl]);
+                }
+                else if (upd && item == 1)
+                {
+#pragma unroll
+                    for (int k = 0; k < R; ++k)
+                    {
+                        vj[k] = static_cast<double>(st[(roff + k * RSTEP) * PT + pl]);
+                        w[k] -= cj * vj[k];
+                    }
+                }
+                else if (upd && item == 2 && a.Vm)
+                {
+#pragma unroll
+                    for (int k = 0; k < R; ++k)
+                    {
+                        vm[k] = static_cast<double>(st[(roff + k * RSTEP) * PT + pl]);
+                        w[k] -= cm * vm[k];
+                    }
+                }
+                else
+                {
+                    const int i = skip + (item - npre);
+                    if (MODE == 0)
+                    {
+                        double loc = 0.0;
+#pragma unroll
+                        for (int k = 0; k < R; ++k)
+                            loc += static_cast<double>(st[(roff + k * RSTEP) * PT + pl]) * w[k];
+                        extra[i * STREAM_CONSUMERS + tid] += loc;
+                    }
+                    else
+                    {
+                        const double c = extra[i * PT + pl];
+#pragma unroll
+                        for (int k = 0; k < R; ++k)
+                            w[k] -= c * static_cast<double>(st[(roff + k * RSTEP) * PT + pl]);
+                    }
+                }
+                release(s);
+                if (++s == a.S) { s = 0; phase ^= 1; }
+                if (MODE == 0 && upd && item == npre - 1)
+                {
+                    // updated w: round to storage, store, and serve the
+                    // products with v_j, v_{j-1} from registers
+                    double lj = 0.0, lm = 0.0;
+#pragma unroll
+                    for (int k = 0; k < R; ++k)
+                    {
+                        const VT wr = static_cast<VT>(w[k]);
+                        w[k] = static_cast<double>(wr);
+                        a.Wout[(row0 + roff + k * RSTEP) * b + p0 + pl] = wr;
+                        lj += vj[k] * w[k];
+                        if (a.Vm) lm += vm[k] * w[k];
+                    }
+                    if (J > 0) extra[0 * STREAM_CONSUMERS + tid] += lj;
+                    if (a.Vm && J > 1) extra[1 * STREAM_CONSUMERS + tid] += lm;
+                }
+            }
+            if (MODE == 1 && ok)
+            {
+#pragma unroll
+                for (int k = 0; k < R; ++k)
+                {
+                    const VT wr = static_cast<VT>(w[k]);
+                    const double d = static_cast<double>(wr);
+                    nacc += d * d;
+                    a.Wout[(row0 + roff + k * RSTEP) * b + p0 + pl] = wr;
+                }
+            }
+        }
+
+        // rows past the last whole tile: plain loads, last CTA only
+        const int64_t tail0 = ntiles * a.T;
+        if (ok && blockIdx.x == gridDim.x - 1 && tail0 < a.n)
+        {
+            for (int64_t r = tail0 + roff; r < a.n; r += RSTEP)
+            {
+                const int64_t o = r * b + p0 + pl;
+                double wv = static_cast<double>(a.W[o]);
+                if (upd)
+                {
+                    const double x = static_cast<double>(a.Vj[o]);
+                    wv -= cj * x;
+                    double y = 0.0;
+                    if (a.Vm)
+                    {
+                        y = static_cast<double>(a.Vm[o]);
+                        wv -= cm * y;
+                    }
+                    if (MODE == 0)
+                    {
+                        const VT wr = static_cast<VT>(wv);
+                        wv = static_cast<double>(wr);
+                        a.Wout[o] = wr;
+                        if (J > 0) extra[tid] += x * wv;
+                        if (a.Vm && J > 1) extra[STREAM_CONSUMERS + tid] += y * wv;
+                    }
+                }
+                for (int i = skip; i < J; ++i)
+                {
+                    const VT* vp = a.basis + static_cast<int64_t>(ring_slot(a.last - i, a.bs)) * a.slot_elems;
+                    const double v = static_cast<double>(vp[o]);
+                    if (MODE == 0) extra[i * STREAM_CONSUMERS + tid] += v * wv;
+                    else wv -= extra[i * PT + pl] * v;
+                }
+                if (MODE == 1)
+                {
+                    const VT wr = static_cast<VT>(wv);
+                    const double d = static_cast<double>(wr);
+                    nacc += d * d;
+                    a.Wout[o] = wr;
+                }
+            }
+        }
+        if (MODE == 1) red[tid] = nacc;
+    }
+    __syncthreads();
+
+    if (producer) return;
+    if (MODE == 0)
+    {
+        for (int idx = tid; idx < J * PT; idx += STREAM_CONSUMERS)
+        {
+            const int i = idx / PT;
+            const int q = idx % PT;
+            double sum = 0.0;
+            for (int r = 0; r < RSTEP; ++r) sum += extra[i * STREAM_CONSUMERS + r * PT + q];
+            a.partials[(static_cast<int64_t>(blockIdx.x) * J + i) * b + p0 + q] = sum;
+        }
+    }
+    else if (a.want_norm)
+    {
+        for (int q = tid; q < PT; q += STREAM_CONSUMERS)
+        {
+            double sum = 0.0;
+            for (int r = 0; r < RSTEP; ++r) sum += red[r * PT + q];
+            a.partials[static_cast<int64_t>(blockIdx.x) * b + p0 + q] = sum;
+        }
+    }
+}
+
+
+// ===========================================================================
+// Row-group SpMM.
+//
+// Groups of G consecutive rows (after the locality order, neighbours) share
+// most of their columns.  The row-group format stores, per group, the sorted
+// union of the group's column indices and a dense G-wide value column per
+// union entry (zero where a row lacks the column):
+//   grp_ptr[g] .. grp_ptr[g+1]  union entries of group g
+//   grp_col[u]                  column of entry u
+//   grp_val[u*G + r]            value of row g*G+r at that column
+// One X row gathered from L1/L2 then feeds G rows' FMAs from registers, so
+// the gather traffic per useful FMA drops by ~G x fill.  Row sums run over
+// the same ascending column order as CSR and the padding adds exact zeros,
+// so results are bit-identical to k_spmm.
+// ===========================================================================
+
+// Union size of each group (warp per group; lanes < G hold the row cursors).
+__global__ void k_rg_count(const int32_t* __restrict__ ptr, const int32_t* __restrict__ ind,
+                           int64_t nrows, int G, int32_t* __restrict__ counts, int64_t ngroups)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t ws = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+    for (int64_t g = w0; g < ngroups; g += ws)
+    {
+        const int64_t row = g * G + lane;
+        int k = 0, kend = 0;
+        if (lane < G && row < nrows)
+        {
+            k = ptr[row];
+            kend = ptr[row + 1];
+        }
+        int count = 0;
+        for (;;)
+        {
+            const int head = (k < kend) ? ind[k] : INT_MAX;
+            int mn = head;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1)
+                mn = min(mn, __shfl_xor_sync(FULL_MASK, mn, off));
+            if (mn == INT_MAX) break;
+            ++count;
+            if (head == mn) ++k;
+        }
+        if (lane == 0) counts[g] = count;
+    }
+}
+
+template <typename VT>
+__global__ void k_rg_fill(const int32_t* __restrict__ ptr, const int32_t* __restrict__ ind,
+                          const VT* __restrict__ val, int64_t nrows, int G,
+                          const int32_t* __restrict__ gptr, int32_t* __restrict__ gcol,
+                          VT* __restrict__ gval, int64_t ngroups)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t ws = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+    for (int64_t g = w0; g < ngroups; g += ws)
+    {
+        const int64_t row = g * G + lane;
+        int k = 0, kend = 0;
+        if (lane < G && row < nrows)
+        {
+            k = ptr[row];
+            kend = ptr[row + 1];
+        }
+        int64_t u = gptr[g];
+        for (;;)
+        {
+            const int head = (k < kend) ? ind[k] : INT_MAX;
+            int mn = head;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1)
+                mn = min(mn, __shfl_xor_sync(FULL_MASK, mn, off));
+            if (mn == INT_MAX) break;
+            if (lane == 0) gcol[u] = mn;
+            if (lane < G) gval[u * G + lane] = (head == mn) ? val[k] : VT(0);
+            if (head == mn) ++k;
+            ++u;
+        }
+    }
+}
+
+// Epilogue of one output row (lanes own LV consecutive probes each).
+template <typename VT, int LV>
+__device__ __forceinline__ void spmm_row_epilogue(int64_t row, int b, int p0, const VT (&acc)[LV],
+                                                  const double (&sxr)[LV],
+                                                  const double (&zcr)[LV], double shift,
+                                                  const VT* __restrict__ X, VT* __restrict__ Y,
+                                                  const VT* __restrict__ Z, int epi,
+                                                  double (&part)[LV])
+{
+    const int64_t o = row * b + p0;
+    VT xr[LV], zr[LV], yr[LV];
+    if (shift != 0.0 || epi == 1) ldg_n<VT, LV>(X + o, xr);
+    if (Z) ldg_n<VT, LV>(Z + o, zr);
+#pragma unroll
+    for (int v = 0; v < LV; ++v)
+    {
+        double y = static_cast<double>(acc[v]) * sxr[v];
+        if (shift != 0.0) y += shift * (sxr[v] * static_cast<double>(xr[v]));
+        if (Z) y -= zcr[v] * static_cast<double>(zr[v]);
+        yr[v] = static_cast<VT>(y);
+        const double ys = static_cast<double>(yr[v]);
+        if (epi == 1)
+            part[v] += (sxr[v] * static_cast<double>(xr[v])) * ys;
+        else if (epi == 2)
+            part[v] += ys * ys;
+    }
+    store_n<VT, LV>(Y + o, yr);
+}
+
+// b = 32 * LV * NS probes: NS warps share a row group, each owning a slice
+// of 32 * LV probes (LV <= 4 keeps the G x LV accumulators and two gathers in
+// flight within 128 registers, two CTAs per SM).  8 warps per CTA.
+template <typename VT, int LV, int G, int NS>
+__global__ void __launch_bounds__(256, 2)
+k_spmm_rg(const int32_t* __restrict__ gptr, const int32_t* __restrict__ gcol,
+          const VT* __restrict__ gval, int64_t nrows, int64_t ngroups, int b,
+          const VT* __restrict__ X, const double* __restrict__ sx, double shift,
+          VT* __restrict__ Y, const VT* __restrict__ Z, const double* __restrict__ zc,
+          const double* __restrict__ zs, int epi, double* __restrict__ partials)
+{
+    __shared__ int32_t s_col[8][32];
+    __shared__ __align__(16) VT s_val[8][32][G];
+    __shared__ double s_red[8][256];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int slice = warp % NS;
+    const int p0 = (slice * 32 + lane) * LV;
+    constexpr int GPC = 8 / NS;  // row groups in flight per CTA
+
+    double sxr[LV], zcr[LV], part[LV];
+#pragma unroll
+    for (int v = 0; v < LV; ++v)
+    {
+        sxr[v] = sx ? sx[p0 + v] : 1.0;
+        zcr[v] = Z ? zc[p0 + v] * zs[p0 + v] : 0.0;
+        part[v] = 0.0;
+    }
+
+    const int64_t gw = static_cast<int64_t>(blockIdx.x) * GPC + warp / NS;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * GPC;
+    for (int64_t g = gw; g < ngroups; g += stride)
+    {
+        VT acc[G][LV];
+#pragma unroll
+        for (int r = 0; r < G; ++r)
+#pragma unroll
+            for (int v = 0; v < LV; ++v) acc[r][v] = VT(0);
+        const int u0 = gptr[g];
+        const int u1 = gptr[g + 1];
+        for (int base = u0; base < u1; base += 32)
+        {
+            const int cnt = min(32, u1 - base);
+            if (lane < cnt)
+            {
+                s_col[warp][lane] = __ldg(gcol + base + lane);
+                VT tmp[G];
+                ldg_n<VT, G>(gval + static_cast<int64_t>(base + lane) * G, tmp);
+                store_n<VT, G>(&s_val[warp][lane][0], tmp);
+            }
+            __syncwarp();
+            int t = 0;
+            for (; t + 2 <= cnt; t += 2)
+            {
+                const int c0 = s_col[warp][t];
+                const int c1 = s_col[warp][t + 1];
+                VT x0[LV], x1[LV];
+                ldg_n<VT, LV>(X + static_cast<int64_t>(c0) * b + p0, x0);
+                ldg_n<VT, LV>(X + static_cast<int64_t>(c1) * b + p0, x1);
+                VT a0[G], a1[G];
+                load_n<VT, G>(&s_val[warp][t][0], a0);
+                load_n<VT, G>(&s_val[warp][t + 1][0], a1);
+#pragma unroll
+                for (int r = 0; r < G; ++r)
+#pragma unroll
+                    for (int v = 0; v < LV; ++v)
+                    {
+                        acc[r][v] += a0[r] * x0[v];
+                        acc[r][v] += a1[r] * x1[v];
+                    }
+            }
+            if (t < cnt)
+            {
+                const int c0 = s_col[warp][t];
+                VT x0[LV];
+                ldg_n<VT, LV>(X + static_cast<int64_t>(c0) * b + p0, x0);
+                VT a0[G];
+                load_n<VT, G>(&s_val[warp][t][0], a0);
+#pragma unroll
+                for (int r = 0; r < G; ++r)
+#pragma unroll
+                    for (int v = 0; v < LV; ++v) acc[r][v] += a0[r] * x0[v];
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int r = 0; r < G; ++r)
+        {
+            const int64_t row = g * G + r;
+            if (row < nrows)
+                spmm_row_epilogue<VT, LV>(row, b, p0, acc[r], sxr, zcr, shift, X, Y, Z, epi, part);
+        }
+    }
+
+    if (epi == 0) return;
+    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&s_red[0][0])[i] = 0.0;
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < LV; ++v) s_red[warp][p0 + v] = part[v];
+    __syncthreads();
+    for (int p = threadIdx.x; p < b; p += blockDim.x)
+    {
+        double s = 0.0;
+        for (int w = 0; w < 8; ++w) s += s_red[w][p];
+        partials[static_cast<int64_t>(blockIdx.x) * b + p] = s;
+    }
 }
 
 }  // namespace slq

@@ -35,7 +35,8 @@ typedef enum {
     SLQ_ERR_CUDA = 4,             /* a CUDA runtime call failed             */
     SLQ_ERR_NAN = 5,              /* NaN/Inf in a Lanczos coefficient       */
     SLQ_ERR_EIGEN = 6,            /* tridiagonal eigen-solve did not converge */
-    SLQ_ERR_UNSUPPORTED = 7       /* valid request this build does not serve */
+    SLQ_ERR_UNSUPPORTED = 7,      /* valid request this build does not serve */
+    SLQ_ERR_TIMEOUT = 8           /* a bounded device-side wait ran out     */
 } slq_status;
 
 typedef enum { SLQ_F32 = 0, SLQ_F64 = 1 } slq_dtype;
@@ -56,7 +57,7 @@ typedef struct slq_op slq_op;
 slq_status slq_operator_workspace_bytes(int64_t num_rows, int64_t num_cols,
                                         int64_t nnz, int dtype, int format,
                                         int need_transpose, int has_perm,
-                                        size_t* bytes);
+                                        int group_rows, size_t* bytes);
 
 /* Wrap caller-owned device arrays (values dtype, int32 indices, int32 index
  * pointer of length num_rows+1 for CSR / num_cols+1 for CSC) as an operator.
@@ -75,6 +76,14 @@ slq_status slq_operator_workspace_bytes(int64_t num_rows, int64_t num_cols,
  * window inside L2.  slq_operator_dot on such an operator acts on permuted
  * vectors (y' = B x').
  *
+ * group_rows (0, 4 or 8) additionally stores A (and A^T) in a row-group
+ * format: per group of consecutive rows, the sorted union of their column
+ * indices with a dense value per (union column, row), zero where absent.
+ * One gathered row of a probe block then feeds group_rows rows of FMAs, which
+ * cuts the SpMM's L1/L2 gather traffic for wide blocks (32 <= b <= 256).
+ * Results are bit-identical to the CSR kernel (same summation order; the
+ * padding adds exact zeros).
+ *
  * Replaces pycuMatrix.__cinit__ (imate/_cu_linear_operator/py_cu_matrix.pyx:
  * 118-200) and cuCSRMatrix / cuCSCMatrix / cuCSRAffineMatrixFunction
  * construction. */
@@ -83,8 +92,9 @@ slq_status slq_operator_create(const void* data, const int32_t* indices,
                                int64_t num_cols, int64_t nnz, int dtype,
                                int format, int affine, int need_transpose,
                                int check_indices, const int32_t* perm,
-                               void* workspace, size_t workspace_bytes,
-                               void* stream, slq_op** out);
+                               int group_rows, void* workspace,
+                               size_t workspace_bytes, void* stream,
+                               slq_op** out);
 
 /* Release the host-side operator record (device arrays stay with their
  * owners).  Replaces the cuLinearOperator destructors

@@ -342,3 +342,42 @@ def test_reordered_gram_matches_oracle(cuda, corr_small):
     want = oracle.trace_estimator(corr_small, "inv", gram=True, **kw)
     assert rel(info["convergence"]["samples"], want["samples"][:, 0]) < \
         RTOL_FP64
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("width", [32, 64, 128, 256])
+@pytest.mark.parametrize("group", [4, 8])
+def test_row_group_products_bit_identical_to_csr(cuda, dtype, width, group):
+    A = ib.correlation_matrix(5000, scale=0.02, threshold=0.05, shift=0.1,
+                              seed=7, dtype=dtype)
+    x = np.random.default_rng(1).standard_normal((5000, width)).astype(dtype)
+    plain = ib.Matrix(A, reorder=True, group_rows=0)
+    grouped = ib.Matrix(A, reorder=True, group_rows=group)
+    op0 = plain.get_device_operator(need_transpose=True)
+    op1 = grouped.get_device_operator(need_transpose=True)
+    assert op1.group_rows == group
+    y0 = _dot(op0, x)
+    y1 = _dot(op1, x)
+    assert np.array_equal(y0, y1)
+    assert np.array_equal(_dot(op0, x, transpose=True),
+                          _dot(op1, x, transpose=True))
+    want = A.astype(np.float64) @ x.astype(np.float64)
+    tol = 1e-12 if dtype == np.float64 else 2e-5
+    assert np.max(np.abs(y1 - want)) <= tol * np.max(np.abs(want))
+
+
+@pytest.mark.parametrize("gram", [False, True])
+def test_row_group_estimator_matches_oracle(cuda, gram):
+    A = ib.correlation_matrix(3000, scale=0.03, threshold=0.05, shift=0.2,
+                              seed=9)
+    M = ib.Matrix(A, reorder=True, group_rows=8)
+    kw = dict(min_num_samples=5, max_num_samples=40, error_rtol=1e-9,
+              lanczos_degree=14, orthogonalize=-1, seed=12)
+    tr, info = _run("log", M, gram=gram, block_size=64, coefficients=False,
+                    **kw)
+    assert M.get_device_operator(need_transpose=gram).group_rows == 8
+    want = oracle.trace_estimator(A, "log", gram=gram, **kw)
+    assert info["convergence"]["num_samples_used"] == \
+        want["num_samples_used"][0]
+    assert rel(info["convergence"]["samples"], want["samples"][:, 0]) < \
+        RTOL_FP64
