@@ -13,6 +13,8 @@
 // samples per block and replays the reference's sequential stopping rule.
 
 #include <cub/cub.cuh>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -814,6 +816,67 @@ slq_status finalize(Launcher& L, const double* partials, int nparts, int cols, i
     return SLQ_OK;
 }
 
+// Tensor maps for the TMA row gathers of k_spmm_rgt: one per probe-block
+// buffer, [rows][b] FP32, box = one row of b values.
+PFN_cuTensorMapEncodeTiled_v12000 g_encode_tiled = nullptr;
+
+slq_status row_map(CUtensorMap* m, const float* base, int64_t rows, int b)
+{
+    if (!g_encode_tiled)
+    {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        SLQ_CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess)
+            return fail(SLQ_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+        g_encode_tiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    cuuint64_t dims[2] = {static_cast<cuuint64_t>(b), static_cast<cuuint64_t>(rows)};
+    cuuint64_t strides[1] = {static_cast<cuuint64_t>(b) * sizeof(float)};
+    cuuint32_t box[2] = {static_cast<cuuint32_t>(b), 1};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = g_encode_tiled(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                                const_cast<float*>(base), dims, strides, box, es,
+                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(SLQ_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+    return SLQ_OK;
+}
+
+template <int LV, int G>
+slq_status spmm_rgt_inst(Launcher& L, const CUtensorMap* xmap, const int32_t* gptr,
+                         const int32_t* gcol, const float* gval, int64_t nrows, int b,
+                         const float* X, const double* sx, double shift, float* Y,
+                         const float* Z, const double* zc, const double* zs, int epi,
+                         double* partials, int32_t* error, int64_t nnz, int64_t xrows,
+                         int* grid_out)
+{
+    const double bytes = nnz * 8.0 + (nrows + 1) * 4.0 + double(xrows) * b * 4.0 +
+                         double(nrows) * b * 4.0 * (Z ? 2.0 : 1.0);
+    ProfScope prof(SLQ_K_SPMM, bytes, L.st);
+    constexpr int STAGE = RGT_ROWS * (LV * 32 * 4) + RGT_ROWS * G * 4;
+    constexpr size_t smem = 1024 + RGT_WARPS * 256 * 8 +
+                            static_cast<size_t>(RGT_WARPS) * RGT_STAGES * STAGE;
+    static bool attr = false;
+    if (!attr)
+    {
+        SLQ_CK(cudaFuncSetAttribute(k_spmm_rgt<LV, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+        attr = true;
+    }
+    const int64_t ng = (nrows + G - 1) / G;
+    const int grid = static_cast<int>(
+        std::max<int64_t>(1, std::min<int64_t>((ng + RGT_WARPS - 1) / RGT_WARPS, L.sms)));
+    k_spmm_rgt<LV, G><<<grid, RGT_WARPS * 32, smem, L.st>>>(
+        *xmap, gptr, gcol, gval, nrows, ng, b, X, sx, shift, Y, Z, zc, zs, epi, partials, error);
+    SLQ_LAUNCH_CK();
+    ++L.launches;
+    *grid_out = grid;
+    return SLQ_OK;
+}
+
 // Operator product on a block: row-group SpMM where the operator has the
 // format and the width suits it (32 <= b <= 256; FP64 b <= 128), else CSR.
 // *grid_out receives the number of partial rows the launch writes.
@@ -842,11 +905,26 @@ slq_status spmm_rg_inst(Launcher& L, const int32_t* gptr, const int32_t* gcol, c
 template <typename VT>
 slq_status op_spmm(Launcher& L, const slq_op* op, int transpose, int b, const VT* X,
                    const double* sx, double shift, VT* Y, const VT* Z, const double* zc,
-                   const double* zs, int epi, double* partials, int* grid_out)
+                   const double* zs, int epi, double* partials, int* grid_out,
+                   const CUtensorMap* xmap = nullptr, int32_t* error = nullptr)
 {
     const int64_t rows = transpose ? op->ncols : op->nrows;
     const int64_t xrows = transpose ? op->nrows : op->ncols;
     const int32_t* gptr = transpose ? op->t_gptr : op->a_gptr;
+    if constexpr (sizeof(VT) == 4)
+    {
+        if (xmap && error && op->group_rows == 8 && gptr && (b == 128 || b == 256))
+        {
+            const int32_t* gcol = transpose ? op->t_gcol : op->a_gcol;
+            const float* gval = static_cast<const float*>(transpose ? op->t_gval : op->a_gval);
+            if (b == 256)
+                return spmm_rgt_inst<8, 8>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y,
+                                           Z, zc, zs, epi, partials, error, op->nnz, xrows,
+                                           grid_out);
+            return spmm_rgt_inst<4, 8>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y, Z,
+                                       zc, zs, epi, partials, error, op->nnz, xrows, grid_out);
+        }
+    }
     const int bmax_rg = (sizeof(VT) == 8) ? 64 : 256;
     if (op->group_rows && gptr && b >= 32 && b <= bmax_rg)
     {
@@ -1120,6 +1198,32 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
     auto Vs = [&](int vec) { return V + static_cast<int64_t>(((vec % bs) + bs) % bs) * vslot; };
     auto Us = [&](int vec) { return U + static_cast<int64_t>(((vec % bs) + bs) % bs) * uslot; };
 
+    // TMA row-gather SpMM: one tensor map per basis slot
+    std::vector<CUtensorMap> vmaps, umaps;
+    bool use_tma = false;
+    if constexpr (sizeof(VT) == 4)
+    {
+        if (op->group_rows == 8 && (b == 128 || b == 256))
+        {
+            use_tma = true;
+            vmaps.resize(bs);
+            for (int sl = 0; sl < bs; ++sl)
+                SLQ_TRY(row_map(&vmaps[sl], V + static_cast<int64_t>(sl) * vslot, r.nv, b));
+            if (r.gram)
+            {
+                umaps.resize(bs);
+                for (int sl = 0; sl < bs; ++sl)
+                    SLQ_TRY(row_map(&umaps[sl], U + static_cast<int64_t>(sl) * uslot, r.nu, b));
+            }
+        }
+    }
+    auto vmap_of = [&](int vec) -> const CUtensorMap* {
+        return use_tma ? &vmaps[((vec % bs) + bs) % bs] : nullptr;
+    };
+    auto umap_of = [&](int vec) -> const CUtensorMap* {
+        return (use_tma && r.gram) ? &umaps[((vec % bs) + bs) % bs] : nullptr;
+    };
+
     // dots + finalize(COEF) + reorth over chunks of MAX_J basis vectors;
     // returns the number of partial rows of the norm partials in *nparts.
     auto reorthogonalize = [&](int64_t n, VT* w_in_first, VT* w_work, VT* w_out, int do_update,
@@ -1162,7 +1266,7 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
             VT* vj = Vs(j);
             int sg = 0;
             SLQ_TRY(op_spmm<VT>(L, op, 0, b, vj, sv_of(j), shift, W, nullptr, nullptr, nullptr, 1,
-                                B.partials, &sg));
+                                B.partials, &sg, vmap_of(j), B.error));
             double* aj = B.alpha + static_cast<int64_t>(j) * b;
             SLQ_TRY(finalize<VT>(L, B.partials, sg, b, FIN_STORE, aj, nullptr, nullptr, b, bs, 0,
                                  nullptr, nullptr, nullptr, 0, 0.0, j));
@@ -1203,7 +1307,7 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
                                 (j > 0) ? Us(j - 1) : nullptr,
                                 (j > 0) ? B.beta + static_cast<int64_t>(j - 1) * b : nullptr,
                                 (j > 0) ? su_of(j - 1) : nullptr, Ju > 0 ? 0 : 2, B.partials,
-                                &sgu));
+                                &sgu, vmap_of(j), B.error));
             int nparts = sgu;
             if (Ju > 0)
                 SLQ_TRY(reorthogonalize(r.nu, uj, uj, uj, 0, nullptr, nullptr, nullptr, nullptr,
@@ -1217,7 +1321,7 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
             VT* vn = Vs(j + 1);
             int sgv = 0;
             SLQ_TRY(op_spmm<VT>(L, op, 1, b, uj, su_of(j), shift, vn, Vs(j), aj, sv_of(j),
-                                Jv > 0 ? 0 : 2, B.partials, &sgv));
+                                Jv > 0 ? 0 : 2, B.partials, &sgv, umap_of(j), B.error));
             nparts = sgv;
             if (Jv > 0)
                 SLQ_TRY(reorthogonalize(r.nv, vn, vn, vn, 0, nullptr, nullptr, nullptr, nullptr,

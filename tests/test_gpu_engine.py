@@ -381,3 +381,25 @@ def test_row_group_estimator_matches_oracle(cuda, gram):
         want["num_samples_used"][0]
     assert rel(info["convergence"]["samples"], want["samples"][:, 0]) < \
         RTOL_FP64
+
+
+@pytest.mark.parametrize("gram", [False, True])
+@pytest.mark.parametrize("block_size", [128, 256])
+def test_tma_row_group_spmm_bit_identical_in_estimator(cuda, gram, block_size):
+    # FP32 row-group operators with 128/256-wide blocks take the TMA
+    # gather4 SpMM; its sums run in the CSR order, so samples are bitwise
+    # equal to the CSR run
+    A = ib.correlation_matrix(6000, scale=0.02, threshold=0.05, shift=0.2,
+                              seed=3, dtype=np.float32)
+    kw = dict(min_num_samples=block_size, max_num_samples=block_size,
+              error_rtol=0.0, lanczos_degree=12, orthogonalize=-1, seed=4)
+    out = []
+    for g in (0, 8):
+        M = ib.Matrix(A, reorder=True, group_rows=g)
+        tr, info = _run("log", M, gram=gram, block_size=block_size,
+                        coefficients=True, **kw)
+        assert M.get_device_operator(need_transpose=gram).group_rows == g
+        out.append(info)
+    assert np.array_equal(out[0]["convergence"]["samples"],
+                          out[1]["convergence"]["samples"])
+    assert np.array_equal(out[0]["engine"]["alpha"], out[1]["engine"]["alpha"])
