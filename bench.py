@@ -240,11 +240,11 @@ def peaks():
 
 def ncu_traffic(kind):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
-    summary (profiles/*.txt lines 'traffic <kind> <bytes_per_launch>')."""
+    summary (profiles/*.txt or *.md lines 'traffic <kind> <bytes_per_launch>')."""
     pdir = os.path.join(ROOT, "profiles")
     try:
         for fn in sorted(os.listdir(pdir)):
-            if not fn.endswith(".txt"):
+            if not fn.endswith((".txt", ".md")):
                 continue
             with open(os.path.join(pdir, fn)) as f:
                 for line in f:

@@ -817,7 +817,7 @@ slq_status finalize(Launcher& L, const double* partials, int nparts, int cols, i
 }
 
 // Tensor maps for the TMA row gathers of k_spmm_rgt: one per probe-block
-// buffer, [rows][b] FP32, box = one row of b values.
+// buffer, [rows][b] FP32, box = 128 values of one row (a warp's slice).
 PFN_cuTensorMapEncodeTiled_v12000 g_encode_tiled = nullptr;
 
 slq_status row_map(CUtensorMap* m, const float* base, int64_t rows, int b)
@@ -833,7 +833,7 @@ slq_status row_map(CUtensorMap* m, const float* base, int64_t rows, int b)
     }
     cuuint64_t dims[2] = {static_cast<cuuint64_t>(b), static_cast<cuuint64_t>(rows)};
     cuuint64_t strides[1] = {static_cast<cuuint64_t>(b) * sizeof(float)};
-    cuuint32_t box[2] = {static_cast<cuuint32_t>(b), 1};
+    cuuint32_t box[2] = {static_cast<cuuint32_t>(std::min(b, 128)), 1};
     cuuint32_t es[2] = {1, 1};
     CUresult r = g_encode_tiled(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
                                 const_cast<float*>(base), dims, strides, box, es,
@@ -845,7 +845,7 @@ slq_status row_map(CUtensorMap* m, const float* base, int64_t rows, int b)
     return SLQ_OK;
 }
 
-template <int LV, int G>
+template <int G, int NS>
 slq_status spmm_rgt_inst(Launcher& L, const CUtensorMap* xmap, const int32_t* gptr,
                          const int32_t* gcol, const float* gval, int64_t nrows, int b,
                          const float* X, const double* sx, double shift, float* Y,
@@ -856,20 +856,21 @@ slq_status spmm_rgt_inst(Launcher& L, const CUtensorMap* xmap, const int32_t* gp
     const double bytes = nnz * 8.0 + (nrows + 1) * 4.0 + double(xrows) * b * 4.0 +
                          double(nrows) * b * 4.0 * (Z ? 2.0 : 1.0);
     ProfScope prof(SLQ_K_SPMM, bytes, L.st);
-    constexpr int STAGE = RGT_ROWS * (LV * 32 * 4) + RGT_ROWS * G * 4;
-    constexpr size_t smem = 1024 + RGT_WARPS * 256 * 8 +
-                            static_cast<size_t>(RGT_WARPS) * RGT_STAGES * STAGE;
+    constexpr int STAGE = RGT_ROWS * 128 * 4 + RGT_ROWS * G * 4;
+    constexpr size_t ring = static_cast<size_t>(RGT_WARPS) * RGT_STAGES * STAGE;
+    constexpr size_t smem = 1024 + (ring > RGT_WARPS * 256 * 8 ? ring : RGT_WARPS * 256 * 8);
     static bool attr = false;
     if (!attr)
     {
-        SLQ_CK(cudaFuncSetAttribute(k_spmm_rgt<LV, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SLQ_CK(cudaFuncSetAttribute(k_spmm_rgt<G, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
         attr = true;
     }
     const int64_t ng = (nrows + G - 1) / G;
+    constexpr int GPC = RGT_WARPS / NS;
     const int grid = static_cast<int>(
-        std::max<int64_t>(1, std::min<int64_t>((ng + RGT_WARPS - 1) / RGT_WARPS, L.sms)));
-    k_spmm_rgt<LV, G><<<grid, RGT_WARPS * 32, smem, L.st>>>(
+        std::max<int64_t>(1, std::min<int64_t>((ng + GPC - 1) / GPC, L.sms)));
+    k_spmm_rgt<G, NS><<<grid, RGT_WARPS * 32, smem, L.st>>>(
         *xmap, gptr, gcol, gval, nrows, ng, b, X, sx, shift, Y, Z, zc, zs, epi, partials, error);
     SLQ_LAUNCH_CK();
     ++L.launches;
@@ -918,10 +919,10 @@ slq_status op_spmm(Launcher& L, const slq_op* op, int transpose, int b, const VT
             const int32_t* gcol = transpose ? op->t_gcol : op->a_gcol;
             const float* gval = static_cast<const float*>(transpose ? op->t_gval : op->a_gval);
             if (b == 256)
-                return spmm_rgt_inst<8, 8>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y,
+                return spmm_rgt_inst<8, 2>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y,
                                            Z, zc, zs, epi, partials, error, op->nnz, xrows,
                                            grid_out);
-            return spmm_rgt_inst<4, 8>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y, Z,
+            return spmm_rgt_inst<8, 1>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y, Z,
                                        zc, zs, epi, partials, error, op->nnz, xrows, grid_out);
         }
     }

@@ -1270,16 +1270,13 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
                     const int i = ib;
                     if (MODE == 0)
                     {
-                        // two independent FMA chains
-                        double l0 = 0.0, l1 = 0.0;
+                        // four independent FMA chains (two warps per scheduler
+                        // cannot hide one long FP64 dependency chain)
+                        double l[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-                        for (int k = 0; k < R; k += 2)
-                        {
-                            l0 += static_cast<double>(st[(roff + k * RSTEP) * PT + pl]) * w[k];
-                            l1 += static_cast<double>(st[(roff + (k + 1) * RSTEP) * PT + pl]) *
-                                  w[k + 1];
-                        }
-                        extra[i * STREAM_CONSUMERS + tid] = prev + (l0 + l1);
+                        for (int k = 0; k < R; ++k)
+                            l[k & 3] += static_cast<double>(st[(roff + k * RSTEP) * PT + pl]) * w[k];
+                        extra[i * STREAM_CONSUMERS + tid] = prev + ((l[0] + l[1]) + (l[2] + l[3]));
                     }
                     else
                     {
@@ -1628,7 +1625,7 @@ k_spmm_rg(const int32_t* __restrict__ gptr, const int32_t* __restrict__ gcol,
 // shared-memory read of a stage row is a contiguous 512-byte span.
 // ===========================================================================
 
-constexpr int RGT_WARPS = 8;
+constexpr int RGT_WARPS = 16;
 constexpr int RGT_STAGES = 3;
 constexpr int RGT_ROWS = 8;  // union columns per stage (two gather4)
 
@@ -1643,7 +1640,10 @@ __device__ __forceinline__ void tma_gather4(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
-template <int LV, int G>
+// b = 128 * NS probes; NS warps share a row group, each owning a 128-probe
+// slice (lane l: probes slice*128 + 4l .. 4l+3); 16 warps per CTA.  The
+// tensor map's box is one row of 128 values.
+template <int G, int NS>
 __global__ void __launch_bounds__(RGT_WARPS * 32, 1)
 k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__ gptr,
            const int32_t* __restrict__ gcol, const float* __restrict__ gval, int64_t nrows,
@@ -1652,17 +1652,18 @@ k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__
            const double* __restrict__ zc, const double* __restrict__ zs, int epi,
            double* __restrict__ partials, int32_t* __restrict__ error)
 {
-    constexpr int NCH = LV / 4;                      // 16-byte chunks per lane
-    constexpr int ROWB = NCH * 128 * 4;              // bytes of one X row (= b * 4)
+    constexpr int LV = 4;
+    constexpr int ROWB = 128 * 4;                    // bytes of one row slice
     constexpr int STAGE_X = RGT_ROWS * ROWB;
     constexpr int STAGE_A = RGT_ROWS * G * 4;
     constexpr int STAGE = STAGE_X + STAGE_A;
+    constexpr int GPC = RGT_WARPS / NS;              // groups in flight per CTA
     extern __shared__ __align__(128) unsigned char smem_rgt[];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem_rgt);              // [warps][stages]
-    double* s_red = reinterpret_cast<double*>(smem_rgt + 1024);          // [warps][256]
-    unsigned char* ring0 = smem_rgt + 1024 + RGT_WARPS * 256 * 8;
+    unsigned char* ring0 = smem_rgt + 1024;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    const int slice = warp % NS;
     unsigned char* ring = ring0 + static_cast<size_t>(warp) * RGT_STAGES * STAGE;
     uint64_t* wbar = bars + warp * RGT_STAGES;
 
@@ -1671,59 +1672,44 @@ k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     __syncwarp();
 
-    int pidx[LV];
+    const int pbase = slice * 128 + lane * 4;        // this lane's 4 probes
+    double part[LV];
 #pragma unroll
-    for (int c = 0; c < NCH; ++c)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) pidx[c * 4 + e] = c * 128 + lane * 4 + e;
-    double sxr[LV], zcr[LV], part[LV];
-#pragma unroll
-    for (int v = 0; v < LV; ++v)
-    {
-        sxr[v] = sx ? sx[pidx[v]] : 1.0;
-        zcr[v] = Z ? zc[pidx[v]] * zs[pidx[v]] : 0.0;
-        part[v] = 0.0;
-    }
+    for (int v = 0; v < LV; ++v) part[v] = 0.0;
 
     uint32_t phases = 0;  // bit st = parity of stage st's next completion
     bool ok = true;
     const int dummy_flag = 0;
-    const int64_t gw = static_cast<int64_t>(blockIdx.x) * RGT_WARPS + warp;
-    const int64_t gstride = static_cast<int64_t>(gridDim.x) * RGT_WARPS;
+    const int64_t gw = static_cast<int64_t>(blockIdx.x) * GPC + warp / NS;
+    const int64_t gstride = static_cast<int64_t>(gridDim.x) * GPC;
     for (int64_t g = gw; g < ngroups && ok; g += gstride)
     {
         const int u0 = gptr[g];
         const int nu = gptr[g + 1] - u0;
         const int nst = (nu + RGT_ROWS - 1) / RGT_ROWS;
-        // union column ids, 32 at a time, held one per lane
+        // union column ids, 32 at a time, one per lane
         int idx_cur = (lane < nu) ? gcol[u0 + lane] : 0;
-        int idx_next = (32 + lane < nu) ? gcol[u0 + 32 + lane] : 0;
         const int last_col = (nu > 0) ? gcol[u0 + nu - 1] : 0;
         auto issue = [&](int k) {
-            // stage k: union entries k*8 .. k*8+7 of this group
             const int st = k % RGT_STAGES;
             unsigned char* dst = ring + static_cast<size_t>(st) * STAGE;
             const int e0 = k * RGT_ROWS;
             const int cnt = min(RGT_ROWS, nu - e0);
-            // ids of entries e0..e0+7 from the lanes holding them
             int id[RGT_ROWS];
-            const int chunk_base = (e0 / 32) * 32;
 #pragma unroll
             for (int i = 0; i < RGT_ROWS; ++i)
             {
                 const int e = e0 + i;
-                const int src = (e - chunk_base) & 31;
-                const int from_cur = __shfl_sync(FULL_MASK, idx_cur, src);
-                const int from_next = __shfl_sync(FULL_MASK, idx_next, src);
-                int v = (e - chunk_base < 32) ? from_cur : from_next;
+                const int v = __shfl_sync(FULL_MASK, idx_cur, e & 31);
                 id[i] = (e < nu) ? v : last_col;
             }
             if (lane == 0)
             {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 mbar_expect_tx(&wbar[st], static_cast<uint32_t>(STAGE_X + cnt * G * 4));
-                tma_gather4(dst, &xmap, 0, id[0], id[1], id[2], id[3], &wbar[st]);
-                tma_gather4(dst + 4 * ROWB, &xmap, 0, id[4], id[5], id[6], id[7], &wbar[st]);
+                tma_gather4(dst, &xmap, slice * 128, id[0], id[1], id[2], id[3], &wbar[st]);
+                tma_gather4(dst + 4 * ROWB, &xmap, slice * 128, id[4], id[5], id[6], id[7],
+                            &wbar[st]);
                 bulk_copy_g2s(dst + STAGE_X, gval + static_cast<int64_t>(u0 + e0) * G,
                               static_cast<uint32_t>(cnt * G * 4), &wbar[st]);
             }
@@ -1738,10 +1724,16 @@ k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__
         for (int k = 0; k < pre; ++k) issue(k);
         for (int k = 0; k < nst; ++k)
         {
-            if (k + RGT_STAGES - 1 < nst)
+            const int kn = k + RGT_STAGES - 1;       // stage to issue now
+            if (kn < nst)
             {
-                // entry ids of the stage to issue may lie in the next 32-chunk
-                issue(k + RGT_STAGES - 1);
+                if ((kn * RGT_ROWS) % 32 == 0 && kn > 0)
+                {
+                    // the entries of stage kn start a new 32-chunk
+                    const int nb = kn * RGT_ROWS + lane;
+                    idx_cur = (nb < nu) ? gcol[u0 + nb] : 0;
+                }
+                issue(kn);
             }
             const int st = k % RGT_STAGES;
             if (!mbar_wait(&wbar[st], (phases >> st) & 1u, &dummy_flag))
@@ -1756,17 +1748,8 @@ k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__
             const int cnt = min(RGT_ROWS, nu - k * RGT_ROWS);
             for (int c = 0; c < cnt; ++c)
             {
-                const float* xr = reinterpret_cast<const float*>(src + c * ROWB);
-                float x[LV];
-#pragma unroll
-                for (int ch = 0; ch < NCH; ++ch)
-                {
-                    const float4 t = *reinterpret_cast<const float4*>(xr + ch * 128 + lane * 4);
-                    x[ch * 4 + 0] = t.x;
-                    x[ch * 4 + 1] = t.y;
-                    x[ch * 4 + 2] = t.z;
-                    x[ch * 4 + 3] = t.w;
-                }
+                const float4 xv = *reinterpret_cast<const float4*>(src + c * ROWB + lane * 16);
+                const float x[4] = {xv.x, xv.y, xv.z, xv.w};
                 float a[G];
 #pragma unroll
                 for (int q = 0; q < G; q += 4)
@@ -1783,69 +1766,62 @@ k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__
                     for (int v = 0; v < LV; ++v) acc[r][v] += a[r] * x[v];
             }
             __syncwarp();
-            // the next 32 entry ids once the stages have moved past them
-            if (((k + RGT_STAGES) * RGT_ROWS) % 32 == 0 && (k + RGT_STAGES) * RGT_ROWS < nu)
-            {
-                idx_cur = idx_next;
-                const int nb = (k + RGT_STAGES) * RGT_ROWS + 32 + lane;
-                idx_next = (nb < nu) ? gcol[u0 + nb] : 0;
-            }
         }
         if (!ok)
         {
             // let this warp's copies in flight land before leaving
-            for (int st = 0; st < RGT_STAGES; ++st) mbar_wait(&wbar[st], (phases >> st) & 1u, &dummy_flag);
+            for (int st = 0; st < RGT_STAGES; ++st)
+                mbar_wait(&wbar[st], (phases >> st) & 1u, &dummy_flag);
             break;
+        }
+        double sxr[LV], zcr[LV];
+#pragma unroll
+        for (int v = 0; v < LV; ++v)
+        {
+            sxr[v] = sx ? sx[pbase + v] : 1.0;
+            zcr[v] = Z ? zc[pbase + v] * zs[pbase + v] : 0.0;
         }
 #pragma unroll
         for (int r = 0; r < G; ++r)
         {
             const int64_t row = g * G + r;
             if (row >= nrows) continue;
-            float xr[LV], zr[LV], yr[LV];
-            const int64_t o = row * b;
-#pragma unroll
-            for (int ch = 0; ch < NCH; ++ch)
-            {
-                if (shift != 0.0 || epi == 1)
-                {
-                    const float4 t = __ldg(reinterpret_cast<const float4*>(X + o + ch * 128 + lane * 4));
-                    xr[ch * 4 + 0] = t.x; xr[ch * 4 + 1] = t.y; xr[ch * 4 + 2] = t.z; xr[ch * 4 + 3] = t.w;
-                }
-                if (Z)
-                {
-                    const float4 t = __ldg(reinterpret_cast<const float4*>(Z + o + ch * 128 + lane * 4));
-                    zr[ch * 4 + 0] = t.x; zr[ch * 4 + 1] = t.y; zr[ch * 4 + 2] = t.z; zr[ch * 4 + 3] = t.w;
-                }
-            }
+            const int64_t o = row * b + pbase;
+            float4 xr = make_float4(0.f, 0.f, 0.f, 0.f), zr = xr;
+            if (shift != 0.0 || epi == 1) xr = __ldg(reinterpret_cast<const float4*>(X + o));
+            if (Z) zr = __ldg(reinterpret_cast<const float4*>(Z + o));
+            const float xs[4] = {xr.x, xr.y, xr.z, xr.w};
+            const float zsv[4] = {zr.x, zr.y, zr.z, zr.w};
+            float yr[4];
 #pragma unroll
             for (int v = 0; v < LV; ++v)
             {
                 double y = static_cast<double>(acc[r][v]) * sxr[v];
-                if (shift != 0.0) y += shift * (sxr[v] * static_cast<double>(xr[v]));
-                if (Z) y -= zcr[v] * static_cast<double>(zr[v]);
+                if (shift != 0.0) y += shift * (sxr[v] * static_cast<double>(xs[v]));
+                if (Z) y -= zcr[v] * static_cast<double>(zsv[v]);
                 yr[v] = static_cast<float>(y);
                 const double ys = static_cast<double>(yr[v]);
-                if (epi == 1) part[v] += (sxr[v] * static_cast<double>(xr[v])) * ys;
+                if (epi == 1) part[v] += (sxr[v] * static_cast<double>(xs[v])) * ys;
                 else if (epi == 2) part[v] += ys * ys;
             }
-#pragma unroll
-            for (int ch = 0; ch < NCH; ++ch)
-                *reinterpret_cast<float4*>(Y + o + ch * 128 + lane * 4) =
-                    make_float4(yr[ch * 4 + 0], yr[ch * 4 + 1], yr[ch * 4 + 2], yr[ch * 4 + 3]);
+            *reinterpret_cast<float4*>(Y + o) = make_float4(yr[0], yr[1], yr[2], yr[3]);
         }
     }
 
     if (epi == 0) return;
-    for (int i = threadIdx.x; i < RGT_WARPS * 256; i += blockDim.x) s_red[i] = 0.0;
+    // all copies have landed (every issued stage was waited on), so the ring
+    // memory can hold the CTA reduction: red[warp][256]
+    __syncthreads();
+    double* red = reinterpret_cast<double*>(ring0);
+    for (int i = threadIdx.x; i < RGT_WARPS * 256; i += blockDim.x) red[i] = 0.0;
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < LV; ++v) s_red[warp * 256 + pidx[v]] = part[v];
+    for (int v = 0; v < LV; ++v) red[warp * 256 + pbase + v] = part[v];
     __syncthreads();
     for (int p = threadIdx.x; p < b; p += blockDim.x)
     {
         double sum = 0.0;
-        for (int w = 0; w < RGT_WARPS; ++w) sum += s_red[w * 256 + p];
+        for (int w = 0; w < RGT_WARPS; ++w) sum += red[w * 256 + p];
         partials[static_cast<int64_t>(blockIdx.x) * b + p] = sum;
     }
 }

@@ -387,8 +387,9 @@ def test_row_group_estimator_matches_oracle(cuda, gram):
 @pytest.mark.parametrize("block_size", [128, 256])
 def test_tma_row_group_spmm_bit_identical_in_estimator(cuda, gram, block_size):
     # FP32 row-group operators with 128/256-wide blocks take the TMA
-    # gather4 SpMM; its sums run in the CSR order, so samples are bitwise
-    # equal to the CSR run
+    # gather4 SpMM; its row sums run in the CSR order (bitwise equal
+    # products), only the CTA count of the alpha reduction differs, so the
+    # runs agree to FP64 rounding
     A = ib.correlation_matrix(6000, scale=0.02, threshold=0.05, shift=0.2,
                               seed=3, dtype=np.float32)
     kw = dict(min_num_samples=block_size, max_num_samples=block_size,
@@ -400,6 +401,7 @@ def test_tma_row_group_spmm_bit_identical_in_estimator(cuda, gram, block_size):
                         coefficients=True, **kw)
         assert M.get_device_operator(need_transpose=gram).group_rows == g
         out.append(info)
-    assert np.array_equal(out[0]["convergence"]["samples"],
-                          out[1]["convergence"]["samples"])
-    assert np.array_equal(out[0]["engine"]["alpha"], out[1]["engine"]["alpha"])
+    assert rel(out[1]["convergence"]["samples"],
+               out[0]["convergence"]["samples"]) < 1e-9
+    assert rel(out[1]["engine"]["alpha"], out[0]["engine"]["alpha"]) < 1e-9
+    assert rel(out[1]["engine"]["beta"], out[0]["engine"]["beta"]) < 1e-9
