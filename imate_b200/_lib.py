@@ -31,8 +31,12 @@ EXPORTS = (
     "slq_nodes_weights", "slq_check_convergence", "slq_average_estimates",
     "slq_erfinv", "slq_xoshiro_jump_ahead", "slq_device_info",
     "slq_last_error", "slq_abi_version", "slq_profile_begin",
-    "slq_profile_end", "slq_generate_probes_noalloc",
+    "slq_profile_end", "slq_generate_probes_noalloc", "slq_mlp_forward",
+    "slq_mlp_grad", "slq_mlp_train",
 )
+MLP_WIDTH = 64
+MLP_PARAMS = 64 + 64 + 64 * 64 + 64 + 64 + 1
+MLP_MAX_BATCH = 64
 
 
 class SlqError(RuntimeError):
@@ -133,6 +137,10 @@ def _declare(lib):
         "slq_profile_begin": (i32, []),
         "slq_profile_end": (i32, [ctypes.POINTER(SlqKernelStat)]),
         "slq_abi_version": (i32, []),
+        "slq_mlp_forward": (i32, [vp, vp, i32, vp, vp]),
+        "slq_mlp_grad": (i32, [vp, vp, vp, i32, vp, vp, vp]),
+        "slq_mlp_train": (i32, [vp, vp, vp, vp, vp, i32, i32, i32,
+                                ctypes.c_float, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -1808,4 +1808,8 @@ extern "C" void slq_xoshiro_jump_ahead(uint64_t* state, uint64_t k) { jump_ahead
 
 extern "C" const char* slq_last_error(void) { return g_error.c_str(); }
 
+namespace slq {
+void set_error(const std::string& message) { g_error = message; }
+}  // namespace slq
+
 extern "C" int slq_abi_version(void) { return SLQ_ABI_VERSION; }

@@ -1,0 +1,212 @@
+"""Learned surrogate for parameter sweeps of trace f(A + t I).
+
+imate answers sweeps over t either by running SLQ per t or, for A + t I, by
+one Krylov run per probe with shifted Ritz values
+(imate/_c_trace_estimator/c_trace_estimator.cpp:564-593), and it offers
+interpolators of such sweeps (imate/interpolator/,
+interpolate_schatten.py:426-492).  This module fits a small network to SLQ
+samples of the sweep on the device and answers the sweep from it:
+
+1. SLQ (this engine, one Krylov run per probe thanks to the shift relation)
+   evaluates the sweep at ``num_train`` log-spaced training points and at
+   ``num_check`` held-out points between them;
+2. the network 1 -> 64 -> 64 -> 1 (tanh, FP32; input log t, output f/n,
+   both standardised) is trained on the device by ``slq_mlp_train``;
+3. each held-out point is compared with its SLQ value; an interval between
+   training points whose check point misses ``rtol`` (relative error,
+   judged against a floor of ``rtol_floor`` times the sweep's mean
+   magnitude where the values cross zero) is answered by SLQ instead (the
+   fallback), as is any t outside the trained range.
+
+``SweepSurrogate.timings`` records where the time goes so the sweep can be
+compared with per-t SLQ and with the shift relation alone.
+"""
+
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from ._functions import logdet, traceinv, trace
+from ._trace_estimator import EngineOptions
+from .linear_operator import AffineMatrixFunction
+
+__all__ = ["SweepSurrogate", "init_params"]
+
+_FUNCS = {"log": logdet, "inv": traceinv, "id": trace}
+
+
+def init_params(seed=0):
+    """Xavier-uniform weights, zero biases, packed as the device expects."""
+    rng = np.random.default_rng(seed)
+    H = _lib.MLP_WIDTH
+
+    def xavier(fan_in, fan_out, size):
+        lim = np.sqrt(6.0 / (fan_in + fan_out))
+        return rng.uniform(-lim, lim, size)
+    W1 = xavier(1, H, H)
+    b1 = np.zeros(H)
+    W2 = xavier(H, H, H * H)
+    b2 = np.zeros(H)
+    W3 = xavier(H, 1, H)
+    b3 = np.zeros(1)
+    return np.concatenate([W1, b1, W2, b2, W3, b3]).astype(np.float32)
+
+
+class SweepSurrogate:
+    """Fitted surrogate of t -> trace f(A + t I) on [t_min, t_max].
+
+    ``slq_options`` are the keyword arguments of the SLQ runs (imate's
+    logdet / traceinv / trace options, e.g. lanczos_degree, min/max samples,
+    orthogonalize, seed); ``engine`` an EngineOptions.
+    """
+
+    def __init__(self, A, func="log", t_min=1e-4, t_max=1e2, num_train=32,
+                 num_check=16, rtol=1e-3, rtol_floor=1e-3, steps=20000,
+                 lr=2e-3, seed=0, engine=None, **slq_options):
+        if func not in _FUNCS:
+            raise ValueError("func must be 'log', 'inv' or 'id'")
+        if not 0 < t_min < t_max:
+            raise ValueError("need 0 < t_min < t_max")
+        if num_train > _lib.MLP_MAX_BATCH:
+            raise ValueError("num_train is at most %d" % _lib.MLP_MAX_BATCH)
+        self.A = A
+        self.func = func
+        self.t_min, self.t_max = float(t_min), float(t_max)
+        self.num_train = int(num_train)
+        self.num_check = int(num_check)
+        self.rtol = float(rtol)
+        self.rtol_floor = float(rtol_floor)
+        self.steps = int(steps)
+        self.lr = float(lr)
+        self.seed = seed
+        self.engine = engine if engine is not None else EngineOptions()
+        opts = dict(min_num_samples=64, max_num_samples=64, error_rtol=0.0,
+                    lanczos_degree=30, orthogonalize=0, seed=0)
+        opts.update(slq_options)
+        self.slq_options = opts
+        self.n = A.shape[0]
+        self.Aop = AffineMatrixFunction(A)
+        self.timings = {}
+        self.params = None
+        self.fitted = False
+
+    # -- SLQ ------------------------------------------------------------------
+    def slq(self, t):
+        """SLQ values of the sweep at t (one Krylov run per probe)."""
+        t = np.atleast_1d(np.asarray(t, dtype=np.float64))
+        f = _FUNCS[self.func]
+        vals, _ = f(self.Aop, method="slq", gpu=True, parameters=t,
+                    return_info=True, engine=self.engine,
+                    **self.slq_options)
+        return np.atleast_1d(np.asarray(vals, dtype=np.float64))
+
+    # -- fitting --------------------------------------------------------------
+    def _x(self, t):
+        return ((np.log(t) - self.x_mean) / self.x_scale).astype(np.float32)
+
+    def fit(self):
+        import torch
+        lib = _lib.load()
+        lt0, lt1 = np.log(self.t_min), np.log(self.t_max)
+        self.t_train = np.exp(np.linspace(lt0, lt1, self.num_train))
+        # held-out points: midpoints (in log t) of evenly spread intervals
+        lmid = 0.5 * (np.log(self.t_train[:-1]) + np.log(self.t_train[1:]))
+        pick = np.unique(np.linspace(0, lmid.size - 1,
+                                     self.num_check).round().astype(int))
+        self.check_interval = pick
+        self.t_check = np.exp(lmid[pick])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        allt = np.concatenate([self.t_train, self.t_check])
+        vals = self.slq(allt)
+        torch.cuda.synchronize()
+        self.timings["slq_training_data"] = time.perf_counter() - t0
+        self.y_train = vals[:self.num_train]
+        self.y_check = vals[self.num_train:]
+
+        self.x_mean = 0.5 * (lt0 + lt1)
+        self.x_scale = 0.5 * (lt1 - lt0)
+        yn = self.y_train / self.n
+        self.y_mean = float(np.mean(yn))
+        self.y_scale = float(np.std(yn)) or 1.0
+        target = ((yn - self.y_mean) / self.y_scale).astype(np.float32)
+
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self._p = torch.from_numpy(init_params(self.seed)).to(dev)
+        self._m = torch.zeros_like(self._p)
+        self._v = torch.zeros_like(self._p)
+        xt = torch.from_numpy(self._x(self.t_train)).to(dev)
+        tt = torch.from_numpy(target).to(dev)
+        hist = torch.empty(max(self.steps, 1), dtype=torch.float32, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _lib.check(lib.slq_mlp_train(
+            self._p.data_ptr(), self._m.data_ptr(), self._v.data_ptr(),
+            xt.data_ptr(), tt.data_ptr(), self.num_train, self.steps, 0,
+            ctypes.c_float(self.lr), hist.data_ptr(), stream))
+        torch.cuda.synchronize()
+        self.timings["train"] = time.perf_counter() - t0
+        self.loss_history = hist.cpu().numpy()[:self.steps]
+        self.params = self._p.cpu().numpy()
+
+        pred = self.predict(self.t_check)
+        floor = self.rtol_floor * float(np.mean(np.abs(self.y_train)))
+        self.check_error = np.abs(pred - self.y_check) / np.maximum(
+            np.abs(self.y_check), floor)
+        self.check_passed = self.check_error <= self.rtol
+        self.fitted = True
+        return self
+
+    # -- answering ------------------------------------------------------------
+    def predict(self, t):
+        """Network values at t (no checks, no fallback)."""
+        import torch
+        lib = _lib.load()
+        t = np.atleast_1d(np.asarray(t, dtype=np.float64))
+        dev = self._p.device
+        x = torch.from_numpy(self._x(t)).to(dev)
+        y = torch.empty_like(x)
+        _lib.check(lib.slq_mlp_forward(
+            self._p.data_ptr(), x.data_ptr(), t.size, y.data_ptr(),
+            torch.cuda.current_stream(dev).cuda_stream))
+        z = y.cpu().numpy().astype(np.float64)
+        return (z * self.y_scale + self.y_mean) * self.n
+
+    def _trusted(self, t):
+        """True where t lies in the fitted range inside an interval whose
+        held-out check passed (intervals without a check point borrow the
+        nearest checked interval's verdict)."""
+        t = np.asarray(t, dtype=np.float64)
+        inside = (t >= self.t_min * (1 - 1e-12)) & (t <= self.t_max * (1 + 1e-12))
+        lt = np.log(np.clip(t, self.t_min, self.t_max))
+        edges = np.log(self.t_train)
+        interval = np.clip(np.searchsorted(edges, lt, side="right") - 1, 0,
+                           edges.size - 2)
+        nearest = np.abs(interval[:, None] -
+                         self.check_interval[None, :]).argmin(axis=1)
+        return inside & self.check_passed[nearest]
+
+    def __call__(self, t):
+        """Sweep values at t: the network where trusted, SLQ elsewhere."""
+        import torch
+        if not self.fitted:
+            self.fit()
+        t = np.atleast_1d(np.asarray(t, dtype=np.float64))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = self.predict(t)
+        torch.cuda.synchronize()
+        self.timings["predict"] = time.perf_counter() - t0
+        trust = self._trusted(t)
+        self.last_fallback = ~trust
+        if not np.all(trust):
+            t0 = time.perf_counter()
+            out[~trust] = self.slq(t[~trust])
+            torch.cuda.synchronize()
+            self.timings["fallback_slq"] = time.perf_counter() - t0
+        else:
+            self.timings["fallback_slq"] = 0.0
+        return out

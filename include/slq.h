@@ -259,6 +259,35 @@ typedef struct {
 slq_status slq_profile_begin(void);
 slq_status slq_profile_end(slq_kernel_stat* stats /* [SLQ_K_COUNT] */);
 
+/* Learned surrogate of a parameter sweep t -> trace f(A + t I): a fully
+ * connected network 1 -> 64 -> 64 -> 1 with tanh hidden units in FP32,
+ * fitted on the device to SLQ samples of the sweep.  It stands in for
+ * imate's interpolators of such sweeps (imate/interpolator/,
+ * interpolate_schatten.py:426-492; no counterpart of the network itself).
+ * Parameters: float[SLQ_MLP_PARAMS] packed as W1[64] b1[64] W2[64][64]
+ * b2[64] W3[64] b3[1] (device).  All pointers are device memory. */
+#define SLQ_MLP_WIDTH 64
+#define SLQ_MLP_PARAMS (64 + 64 + 64 * 64 + 64 + 64 + 1)
+#define SLQ_MLP_MAX_BATCH 64
+
+/* y[i] = net(x[i]) for count inputs. */
+slq_status slq_mlp_forward(const float* params, const float* x, int count,
+                           float* y, void* stream);
+
+/* Gradient of mean_i (net(x_i) - t_i)^2 over a batch (<= 64 points) into
+ * grad[SLQ_MLP_PARAMS], and the loss into *loss. */
+slq_status slq_mlp_grad(const float* params, const float* x, const float* t,
+                        int batch, float* grad, float* loss, void* stream);
+
+/* `steps` full-batch Adam steps (beta1 0.9, beta2 0.999, eps 1e-8) in one
+ * launch.  adam_m / adam_v (float[SLQ_MLP_PARAMS]) carry the moments across
+ * calls; steps_done is the number of steps already taken.  loss_history
+ * (float[steps] or NULL) receives the loss before each step. */
+slq_status slq_mlp_train(float* params, float* adam_m, float* adam_v,
+                         const float* x, const float* t, int batch, int steps,
+                         int steps_done, float lr, float* loss_history,
+                         void* stream);
+
 /* Device count / properties (replaces query_device.cu:48-64). */
 slq_status slq_device_info(int* num_devices, int* num_sms,
                            int* max_threads_per_sm);

@@ -405,3 +405,54 @@ def test_tma_row_group_spmm_bit_identical_in_estimator(cuda, gram, block_size):
                out[0]["convergence"]["samples"]) < 1e-9
     assert rel(out[1]["engine"]["alpha"], out[0]["engine"]["alpha"]) < 1e-9
     assert rel(out[1]["engine"]["beta"], out[0]["engine"]["beta"]) < 1e-9
+
+
+@pytest.mark.parametrize("fmt", ["csr", "csc"])
+def test_rectangular_gram_matches_oracle(cuda, fmt):
+    # X^T X of a tall X: probes of length ncols, trace scale ncols (the
+    # reference uses nrows there, which is only right for square X)
+    rng = np.random.default_rng(3)
+    X = sp.random(700, 240, density=0.04, random_state=4, format="csr")
+    X = (X + sp.eye(700, 240) * 0.7).asformat(fmt)
+    kw = dict(min_num_samples=10, max_num_samples=64, error_rtol=1e-3,
+              lanczos_degree=20, orthogonalize=-1, seed=5)
+    tr, info = ib.logdet(X, gram=True, method="slq", gpu=True,
+                         return_info=True, **kw)
+    want = oracle.trace_estimator(X, "log", gram=True, **kw)
+    used = int(want["num_samples_used"][0])
+    assert info["convergence"]["num_samples_used"] == used
+    assert rel(info["convergence"]["samples"][:used],
+               want["samples"][:used, 0]) < RTOL_FP64
+    exact = np.linalg.slogdet((X.T @ X).toarray())[1]
+    assert abs(tr - exact) / abs(exact) < 0.02
+    assert info["matrix"]["size"] == (700, 240)
+    assert rng is not None
+
+
+def test_distributed_single_rank_nccl_matches_single_process(cuda):
+    import os
+    import torch.distributed as dist
+    from imate_b200.distributed import (distributed_trace_estimator,
+                                        engine_block_runner)
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ.setdefault("MASTER_PORT", "29533")
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        A = ib.correlation_matrix(2000, scale=0.03, threshold=0.05,
+                                  shift=0.2, seed=8)
+        M = ib.Matrix(A)
+        kw = dict(lanczos_degree=15, orthogonalize=-1, seed=11)
+        run = engine_block_runner(M, "log", **kw)
+        res = distributed_trace_estimator(run, q=1, block=16,
+                                          min_num_samples=8,
+                                          max_num_samples=64,
+                                          error_rtol=1e-3)
+        tr, info = ib.logdet(M, method="slq", gpu=True, return_info=True,
+                             min_num_samples=8, max_num_samples=64,
+                             error_rtol=1e-3,
+                             engine=ib.EngineOptions(block_size=16), **kw)
+        assert int(res["num_samples_used"][0]) == \
+            int(info["convergence"]["num_samples_used"])
+        assert abs(res["trace"][0] - tr) <= 1e-12 * abs(tr)
+    finally:
+        dist.destroy_process_group()
