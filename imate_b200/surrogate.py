@@ -10,8 +10,14 @@ samples of the sweep on the device and answers the sweep from it:
 1. SLQ (this engine, one Krylov run per probe thanks to the shift relation)
    evaluates the sweep at ``num_train`` log-spaced training points and at
    ``num_check`` held-out points between them;
-2. the network 1 -> 64 -> 64 -> 1 (tanh, FP32; input log t, output f/n,
-   both standardised) is trained on the device by ``slq_mlp_train``;
+2. the network 1 -> 64 -> 64 -> 1 (tanh, FP32; input log t standardised)
+   is trained on the device by ``slq_mlp_train`` on the standardised
+   residual of a one-parameter base curve with the sweep's limits, tau
+   matched to the value at t_min, so the network only carries the shape of
+   the spectrum, a small correction: r = f/n - log(t + tau) for logdet,
+   r = log(f/n) + log(t + tau) for traceinv (f/n ~ 1/(t + tau); in log space
+   an absolute error of the network is a relative error of f), and
+   r = f/n - (t + tau) for trace;
 3. each held-out point is compared with its SLQ value; an interval between
    training points whose check point misses ``rtol`` (relative error,
    judged against a floor of ``rtol_floor`` times the sweep's mean
@@ -129,9 +135,16 @@ class SweepSurrogate:
         self.x_mean = 0.5 * (lt0 + lt1)
         self.x_scale = 0.5 * (lt1 - lt0)
         yn = self.y_train / self.n
-        self.y_mean = float(np.mean(yn))
-        self.y_scale = float(np.std(yn)) or 1.0
-        target = ((yn - self.y_mean) / self.y_scale).astype(np.float32)
+        self._fit_base(yn[0])
+        resid = self._to_resid(self.t_train, yn)
+        if not np.all(np.isfinite(resid)):
+            resid = np.nan_to_num(resid)
+            self._usable = False
+        else:
+            self._usable = True
+        self.y_mean = float(np.mean(resid))
+        self.y_scale = float(np.std(resid)) or 1.0
+        target = ((resid - self.y_mean) / self.y_scale).astype(np.float32)
 
         dev = torch.device("cuda", torch.cuda.current_device())
         self._p = torch.from_numpy(init_params(self.seed)).to(dev)
@@ -156,9 +169,37 @@ class SweepSurrogate:
         floor = self.rtol_floor * float(np.mean(np.abs(self.y_train)))
         self.check_error = np.abs(pred - self.y_check) / np.maximum(
             np.abs(self.y_check), floor)
-        self.check_passed = self.check_error <= self.rtol
+        self.check_passed = (self.check_error <= self.rtol) & self._usable
         self.fitted = True
         return self
+
+    def _fit_base(self, y0):
+        # base curve through (t_min, y0) with the sweep's large-t behaviour
+        t0 = self.t_min
+        tiny = 1e-300
+        if self.func == "log":
+            self.tau = max(float(np.exp(y0)) - t0, tiny)
+        elif self.func == "inv":
+            self.tau = max(1.0 / y0 - t0, tiny) if y0 > 0 else 1.0
+        else:
+            self.tau = float(y0) - t0
+
+    def _to_resid(self, t, yn):
+        t = np.asarray(t, dtype=np.float64)
+        if self.func == "log":
+            return yn - np.log(t + self.tau)
+        if self.func == "inv":
+            with np.errstate(divide="ignore", invalid="ignore"):
+                return np.log(yn) + np.log(t + self.tau)
+        return yn - (t + self.tau)
+
+    def _from_resid(self, t, r):
+        t = np.asarray(t, dtype=np.float64)
+        if self.func == "log":
+            return r + np.log(t + self.tau)
+        if self.func == "inv":
+            return np.exp(r) / (t + self.tau)
+        return r + t + self.tau
 
     # -- answering ------------------------------------------------------------
     def predict(self, t):
@@ -173,7 +214,7 @@ class SweepSurrogate:
             self._p.data_ptr(), x.data_ptr(), t.size, y.data_ptr(),
             torch.cuda.current_stream(dev).cuda_stream))
         z = y.cpu().numpy().astype(np.float64)
-        return (z * self.y_scale + self.y_mean) * self.n
+        return self._from_resid(t, z * self.y_scale + self.y_mean) * self.n
 
     def _trusted(self, t):
         """True where t lies in the fitted range inside an interval whose

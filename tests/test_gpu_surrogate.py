@@ -50,9 +50,12 @@ def test_gradient_matches_numpy(cuda, batch):
     t = np.cos(3 * x).astype(np.float32)
     G = torch.empty(mlp_oracle.P, dtype=torch.float32, device="cuda")
     L = torch.empty(1, dtype=torch.float32, device="cuda")
-    _lib.check(cuda.slq_mlp_grad(_dev(p).data_ptr(), _dev(x).data_ptr(),
-                                 _dev(t).data_ptr(), batch, G.data_ptr(),
-                                 L.data_ptr(), _stream()))
+    # keep the device copies alive until the kernel has run
+    Pd, Xd, Td = _dev(p), _dev(x), _dev(t)
+    _lib.check(cuda.slq_mlp_grad(Pd.data_ptr(), Xd.data_ptr(), Td.data_ptr(),
+                                 batch, G.data_ptr(), L.data_ptr(),
+                                 _stream()))
+    torch.cuda.synchronize()
     loss, g = mlp_oracle.loss_grad(p.astype(np.float64), x, t)
     got = G.cpu().numpy()
     assert np.max(np.abs(got - g)) <= 1e-3 * np.max(np.abs(g))
@@ -68,10 +71,12 @@ def test_training_follows_numpy_adam(cuda):
     M = torch.zeros_like(P)
     V = torch.zeros_like(P)
     hist = torch.empty(400, dtype=torch.float32, device="cuda")
+    Xd, Td = _dev(x), _dev(t)
     _lib.check(cuda.slq_mlp_train(P.data_ptr(), M.data_ptr(), V.data_ptr(),
-                                  _dev(x).data_ptr(), _dev(t).data_ptr(), 32,
-                                  400, 0, np.float32(3e-3), hist.data_ptr(),
+                                  Xd.data_ptr(), Td.data_ptr(), 32, 400, 0,
+                                  np.float32(3e-3), hist.data_ptr(),
                                   _stream()))
+    torch.cuda.synchronize()
     losses = hist.cpu().numpy()
     _, _, _, want = mlp_oracle.adam(p0.astype(np.float64), x, t, 400, 3e-3)
     # same trajectory up to FP32 rounding
@@ -80,7 +85,7 @@ def test_training_follows_numpy_adam(cuda):
     assert abs(losses[-1] - want[-1]) <= 0.1 * want[-1] + 1e-6
 
 
-@pytest.mark.parametrize("func", ["log", "inv"])
+@pytest.mark.parametrize("func", ["log", "inv", "id"])
 def test_surrogate_sweep_against_slq(cuda, func):
     import torch
     A = ib.correlation_matrix(20000, scale=0.01, threshold=0.05, shift=0.1,
@@ -96,12 +101,14 @@ def test_surrogate_sweep_against_slq(cuda, func):
     trusted = ~sur.last_fallback
     floor = sur.rtol_floor * float(np.mean(np.abs(sur.y_train)))
     err = np.abs(got - want) / np.maximum(np.abs(want), floor)
-    assert np.all(err[~trusted] < 1e-12)          # fallback is SLQ itself
-    assert np.mean(trusted) >= 0.5
+    # fallback is SLQ itself (same probes; its Krylov run is shifted to the
+    # first fallback t, so FP32 rounding differs slightly)
+    assert np.all(err[~trusted] < 1e-5)
+    assert np.mean(trusted) >= 0.75
     assert np.max(err[trusted]) < 5e-3
     # what the network gains: a per-t SLQ run versus the whole sweep from the
     # network (training data and training included, amortised or not)
-    f = {"log": ib.logdet, "inv": ib.traceinv}[func]
+    f = {"log": ib.logdet, "inv": ib.traceinv, "id": ib.trace}[func]
     M = ib.Matrix(A)
     f(M, method="slq", gpu=True, **opts)
     torch.cuda.synchronize()
