@@ -12,11 +12,12 @@ buffers.
 from .__version__ import __version__
 from ._functions import logdet, traceinv, trace, schatten
 from ._trace_estimator import EngineOptions
-from .linear_operator import LinearOperator, Matrix, AffineMatrixFunction
+from .linear_operator import (LinearOperator, Matrix, AffineMatrixFunction,
+                              GramAffineMatrixFunction)
 from .sample_matrices import (toeplitz, toeplitz_logdet, toeplitz_trace,
                               toeplitz_traceinv, correlation_matrix)
 
 __all__ = ["__version__", "logdet", "traceinv", "trace", "schatten",
            "EngineOptions", "LinearOperator", "Matrix",
-           "AffineMatrixFunction", "toeplitz", "toeplitz_logdet",
+           "AffineMatrixFunction", "GramAffineMatrixFunction", "toeplitz", "toeplitz_logdet",
            "toeplitz_trace", "toeplitz_traceinv", "correlation_matrix"]

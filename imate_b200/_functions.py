@@ -89,7 +89,7 @@ def schatten(A, gram=False, p=2.0, return_info=False, method="eigenvalue",
     (traceinv(A^|p|)/n)^(1/p)."""
     if not isinstance(p, (int, np.integer, float)):
         raise ValueError('"p" should be float or integer.')
-    n = A.shape[0]
+    n = A.get_num_rows() if hasattr(A, "get_num_rows") else A.shape[0]
     if p == 0:
         out = logdet(A, gram=gram, p=1.0, return_info=return_info,
                      method=method, **options)

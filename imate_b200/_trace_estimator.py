@@ -289,6 +289,10 @@ def trace_estimator(A, parameters, func, gram, exponent, min_num_samples,
     init_proc = time.process_time()
 
     affine = Aop.get_num_parameters() > 0
+    normal = bool(getattr(Aop, "normal_equations", False))
+    if normal and gram:
+        raise ValueError('GramAffineMatrixFunction is already a Gram '
+                         'operator: call with "gram=False".')
     if affine:
         t_values = np.atleast_1d(np.asarray(parameters, dtype=np.float64))
     else:
@@ -320,12 +324,13 @@ def trace_estimator(A, parameters, func, gram, exponent, min_num_samples,
     engine = dict(block_size=None, rng=options.rng, num_blocks=0,
                   num_probes_computed=0, gpu_launches=0)
 
-    dev_op = Aop.get_device_operator(need_transpose=bool(gram))
+    dev_op = Aop.get_device_operator(need_transpose=bool(gram) or normal)
+    gram_mode = 2 if normal else int(bool(gram))
     stream = torch.cuda.current_stream(dev_op.device)
     for gi, group in enumerate(groups):
         gq = len(group)
         prm = _lib.SlqParams(
-            func=_lib.FUNC_IDS[func], gram=int(bool(gram)),
+            func=_lib.FUNC_IDS[func], gram=gram_mode,
             exponent=float(exponent), orthogonalize=int(orthogonalize),
             seed=seed_used, lanczos_degree=m, lanczos_tol=float(lanczos_tol),
             min_num_samples=int(min_num_samples),

@@ -483,8 +483,6 @@ extern "C" slq_status slq_operator_create(const void* data, const int32_t* indic
         return fail(SLQ_ERR_BAD_ARG, "operator_create: sizes out of range (int32 indices)");
     if (!indptr || (nnz > 0 && (!indices || !data)))
         return fail(SLQ_ERR_BAD_ARG, "operator_create: NULL array");
-    if (affine && num_rows != num_cols)
-        return fail(SLQ_ERR_BAD_ARG, "operator_create: A + tI needs a square matrix");
     size_t need = 0;
     SLQ_TRY(slq_operator_workspace_bytes(num_rows, num_cols, nnz, dtype, format,
                                          need_transpose, perm != nullptr, group_rows, &need));
@@ -1044,6 +1042,8 @@ struct RunBufs {
     void* U;
     void* W;
     void* W2;
+    void* T;              // normal-equations runs: A v, [nu][b]
+    double* negshift;     // normal-equations runs: -t per probe
     double* scale_v;
     double* scale_u;
     double* alpha;
@@ -1089,21 +1089,23 @@ slq_status make_plan(const slq_op* op, const slq_params* p, int q, RunPlan* r)
     if (q < 1) return fail(SLQ_ERR_BAD_ARG, "num_inquiries must be >= 1");
     if (q > 1 && !op->affine)
         return fail(SLQ_ERR_BAD_ARG, "several inquiries need an affine operator");
-    if (q > 1 && p->gram)
+    if (p->gram < 0 || p->gram > 2)
+        return fail(SLQ_ERR_BAD_ARG, "gram must be 0, 1 or 2");
+    if (q > 1 && p->gram == 1)
         return fail(SLQ_ERR_UNSUPPORTED,
-                    "eigenvalue shift across inquiries is not valid for gram operators");
-    if (!p->gram && op->nrows != op->ncols)
-        return fail(SLQ_ERR_BAD_ARG, "non-gram runs need a square matrix");
+                    "eigenvalue shift across inquiries is not valid for Golub-Kahn runs");
+    if (p->gram != 2 && op->nrows != op->ncols && (p->gram == 0 || op->affine))
+        return fail(SLQ_ERR_BAD_ARG, "this run needs a square matrix");
     if (p->gram && !op->t_ptr)
         return fail(SLQ_ERR_BAD_ARG, "gram runs need an operator created with need_transpose");
     if (p->orthogonalize > p->lanczos_degree)
         return fail(SLQ_ERR_BAD_ARG, "orthogonalize must be at most lanczos_degree");
     if (p->rng != SLQ_RNG_PARITY && p->rng != SLQ_RNG_FAST)
         return fail(SLQ_ERR_BAD_ARG, "unknown rng mode");
-    r->gram = p->gram ? 1 : 0;
+    r->gram = p->gram;
     r->orth = p->orthogonalize;
     r->m = p->lanczos_degree;
-    r->bs = buffer_size(r->gram, r->orth, r->m);
+    r->bs = buffer_size(r->gram == 1, r->orth, r->m);
     r->q = q;
     r->nv = r->gram ? op->ncols : op->nrows;
     r->nu = r->gram ? op->nrows : 0;
@@ -1135,9 +1137,11 @@ void carve(Carver& c, const RunPlan& r, int sms, RunBufs* B)
     const int64_t vslot = slot_stride<VT>(r.nv, r.b);
     const int64_t uslot = slot_stride<VT>(r.nu, r.b);
     B->V = c.take<VT>(static_cast<size_t>(r.bs) * vslot);
-    B->U = r.gram ? c.take<VT>(static_cast<size_t>(r.bs) * uslot) : nullptr;
-    B->W = r.gram ? nullptr : c.take<VT>(vslot);
-    B->W2 = (!r.gram && r.orth != 0) ? c.take<VT>(vslot) : nullptr;
+    B->U = (r.gram == 1) ? c.take<VT>(static_cast<size_t>(r.bs) * uslot) : nullptr;
+    B->W = (r.gram == 1) ? nullptr : c.take<VT>(vslot);
+    B->W2 = (r.gram != 1 && r.orth != 0) ? c.take<VT>(vslot) : nullptr;
+    B->T = (r.gram == 2) ? c.take<VT>(static_cast<size_t>(r.nu) * r.b) : nullptr;
+    B->negshift = c.take<double>(r.b);
     B->scale_v = c.take<double>(static_cast<size_t>(r.bs) * r.b);
     B->scale_u = c.take<double>(static_cast<size_t>(r.bs) * r.b);
     B->alpha = c.take<double>(static_cast<size_t>(r.m) * r.b);
@@ -1260,14 +1264,28 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
         return SLQ_OK;
     };
 
-    if (!r.gram)
+    if (r.gram != 1)
     {
+        VT* T = static_cast<VT*>(B.T);
         for (int j = 0; j < m; ++j)
         {
             VT* vj = Vs(j);
             int sg = 0;
-            SLQ_TRY(op_spmm<VT>(L, op, 0, b, vj, sv_of(j), shift, W, nullptr, nullptr, nullptr, 1,
-                                B.partials, &sg, vmap_of(j), B.error));
+            if (r.gram == 0)
+            {
+                SLQ_TRY(op_spmm<VT>(L, op, 0, b, vj, sv_of(j), shift, W, nullptr, nullptr,
+                                    nullptr, 1, B.partials, &sg, vmap_of(j), B.error));
+            }
+            else
+            {
+                // normal equations: T = s_j A v_j, W = A^T T + t s_j v_j,
+                // alpha partials against s_j v_j
+                int sg1 = 0;
+                SLQ_TRY(op_spmm<VT>(L, op, 0, b, vj, sv_of(j), 0.0, T, nullptr, nullptr,
+                                    nullptr, 0, B.partials, &sg1, vmap_of(j), B.error));
+                SLQ_TRY(op_spmm<VT>(L, op, 1, b, T, nullptr, 0.0, W, vj, B.negshift, sv_of(j),
+                                    3, B.partials, &sg));
+            }
             double* aj = B.alpha + static_cast<int64_t>(j) * b;
             SLQ_TRY(finalize<VT>(L, B.partials, sg, b, FIN_STORE, aj, nullptr, nullptr, b, bs, 0,
                                  nullptr, nullptr, nullptr, 0, 0.0, j));
@@ -1360,6 +1378,8 @@ slq_status run_typed(slq_op* op, const slq_params* p, const double* parameters, 
     const double shift = op->affine ? params[0] : 0.0;
     SLQ_CK(cudaMemcpyAsync(B.params, params.data(), sizeof(double) * q, cudaMemcpyHostToDevice, st));
     SLQ_CK(cudaMemsetAsync(B.error, 0, sizeof(int32_t), st));
+    k_fill_f64<<<(b + 255) / 256, 256, 0, st>>>(B.negshift, b, -shift);
+    SLQ_LAUNCH_CK();
     int32_t herr = 0;
 
     // parity stream set-up on the host: state of probe 0 and the per-chunk
@@ -1453,7 +1473,7 @@ slq_status run_typed(slq_op* op, const slq_params* p, const double* parameters, 
         {
         ProfScope prof(SLQ_K_EIG, double(m) * b * 16.0 + double(count) * q * 8.0, st);
         k_eig_quad<<<(count + 127) / 128, 128, 0, st>>>(
-            count, b, m, B.alpha, B.beta, B.size, r.gram, p->func, p->exponent, B.params, q,
+            count, b, m, B.alpha, B.beta, B.size, r.gram == 1, p->func, p->exponent, B.params, q,
             static_cast<double>(r.nv), B.samples, nullptr, nullptr, B.status);
         SLQ_LAUNCH_CK();
         ++L.launches;

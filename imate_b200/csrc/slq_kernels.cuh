@@ -153,7 +153,9 @@ __device__ __forceinline__ int ring_slot(int vec, int bs)
 // epilogue applies the per-probe scale and the Krylov recurrence's axpy and
 // accumulates the FP64 partial of alpha (Lanczos) or of the squared norm.
 //
-// epi: 0 store only, 1 alpha partial <sx X[r], Y[r]>, 2 norm partial |Y[r]|^2
+// epi: 0 store only, 1 alpha partial <sx X[r], Y[r]>, 2 norm partial
+// |Y[r]|^2, 3 alpha partial <zs Z[r], Y[r]> (normal-equations Lanczos, where
+// the Krylov vector is Z and X is the intermediate A v)
 // ---------------------------------------------------------------------------
 
 template <typename VT, int LV, int KS>
@@ -266,6 +268,8 @@ k_spmm(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
                     part[v] += (sxr[v] * static_cast<double>(xr[v])) * ys;
                 else if (epi == 2)
                     part[v] += ys * ys;
+                else if (epi == 3)
+                    part[v] += (zs[p0 + v] * static_cast<double>(zr[v])) * ys;
             }
             store_n<VT, LV>(Y + o, yr);
         }
@@ -1479,7 +1483,8 @@ __device__ __forceinline__ void spmm_row_epilogue(int64_t row, int b, int p0, co
                                                   const double (&sxr)[LV],
                                                   const double (&zcr)[LV], double shift,
                                                   const VT* __restrict__ X, VT* __restrict__ Y,
-                                                  const VT* __restrict__ Z, int epi,
+                                                  const VT* __restrict__ Z,
+                                                  const double* __restrict__ zs, int epi,
                                                   double (&part)[LV])
 {
     const int64_t o = row * b + p0;
@@ -1498,6 +1503,8 @@ __device__ __forceinline__ void spmm_row_epilogue(int64_t row, int b, int p0, co
             part[v] += (sxr[v] * static_cast<double>(xr[v])) * ys;
         else if (epi == 2)
             part[v] += ys * ys;
+        else if (epi == 3)
+            part[v] += (zs[p0 + v] * static_cast<double>(zr[v])) * ys;
     }
     store_n<VT, LV>(Y + o, yr);
 }
@@ -1592,7 +1599,8 @@ k_spmm_rg(const int32_t* __restrict__ gptr, const int32_t* __restrict__ gcol,
         {
             const int64_t row = g * G + r;
             if (row < nrows)
-                spmm_row_epilogue<VT, LV>(row, b, p0, acc[r], sxr, zcr, shift, X, Y, Z, epi, part);
+                spmm_row_epilogue<VT, LV>(row, b, p0, acc[r], sxr, zcr, shift, X, Y, Z, zs, epi,
+                                          part);
         }
     }
 
@@ -1803,6 +1811,8 @@ k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__
                 const double ys = static_cast<double>(yr[v]);
                 if (epi == 1) part[v] += (sxr[v] * static_cast<double>(xs[v])) * ys;
                 else if (epi == 2) part[v] += ys * ys;
+                else if (epi == 3)
+                    part[v] += (zs[pbase + v] * static_cast<double>(zsv[v])) * ys;
             }
             *reinterpret_cast<float4*>(Y + o) = make_float4(yr[0], yr[1], yr[2], yr[3]);
         }

@@ -17,7 +17,8 @@ import scipy.sparse as sp
 
 from . import _lib
 
-__all__ = ["LinearOperator", "Matrix", "AffineMatrixFunction"]
+__all__ = ["LinearOperator", "Matrix", "AffineMatrixFunction",
+           "GramAffineMatrixFunction"]
 
 
 def _dtype_code(dtype):
@@ -323,3 +324,39 @@ class AffineMatrixFunction(LinearOperator):
 
     def _affine(self):
         return True
+
+
+class GramAffineMatrixFunction(LinearOperator):
+    """A^T A + t I for a sparse (possibly rectangular) A.
+
+    imate can form the Gram matrix of A (``gram=True``) but not shift it:
+    its AffineMatrixFunction with ``gram=True`` means (A + t I)^T (A + t I).
+    This operator is the shifted Gram matrix itself, an n x n SPD operator
+    (n = columns of A) used with ``gram=False``; the engine runs Lanczos on
+    it as x -> A^T (A x) + t x (normal-equations mode).  Its eigenvalues
+    shift with t, so one Krylov run per probe serves a sweep of t.
+    """
+
+    def __init__(self, A):
+        super().__init__()
+        if not sp.issparse(A):
+            A = sp.csr_matrix(A)
+        self.A = A
+        self.num_parameters = 1
+        self.normal_equations = True
+        self.reorder = False
+        self.group_rows = 0
+        self.set_data_type_name(A)
+
+    def _affine(self):
+        return True
+
+    def get_num_rows(self):
+        return self.A.shape[1]
+
+    def get_num_columns(self):
+        return self.A.shape[1]
+
+    def get_density(self):
+        n = self.A.shape[1]
+        return self.A.nnz / float(n * n)

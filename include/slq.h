@@ -63,7 +63,8 @@ slq_status slq_operator_workspace_bytes(int64_t num_rows, int64_t num_cols,
  * pointer of length num_rows+1 for CSR / num_cols+1 for CSC) as an operator.
  * need_transpose requests A^T as well (gram / Golub-Kahn runs).  affine marks
  * the operator as A + t I (imate.AffineMatrixFunction with B = I; the
- * eigenvalue shift relation of c_affine_matrix_function.cpp:98-113 holds).
+ * eigenvalue shift relation of c_affine_matrix_function.cpp:98-113 holds),
+ * or, in normal-equations runs (slq_params.gram = 2), as A^T A + t I.
  * check_indices != 0 validates indptr monotonicity and index range on the
  * device first (SLQ_ERR_BAD_CSR on failure).
  *
@@ -117,7 +118,12 @@ slq_status slq_operator_dot(slq_op* op, int transpose, double t,
  * engine's own block width and probe-generator choice. */
 typedef struct {
     int func;                      /* slq_func                               */
-    int gram;                      /* Golub-Kahn on A (A^T A) if != 0        */
+    int gram;                      /* 0 Lanczos on A; 1 Golub-Kahn on A      */
+                                   /* (spectrum of A^T A); 2 Lanczos on the  */
+                                   /* normal operator A^T A (+ t I if the    */
+                                   /* operator is affine; no counterpart in  */
+                                   /* the reference: imate cannot shift a    */
+                                   /* Gram matrix)                           */
     double exponent;               /* p in f(A^p)                            */
     int orthogonalize;             /* 0 none, <0 full, k last-k              */
     int64_t seed;                  /* >= 0 (the host maps None to a clock seed) */

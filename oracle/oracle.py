@@ -136,7 +136,9 @@ def trace_estimator(A, func, gram=False, exponent=1.0, parameters=None,
                     error_rtol=1e-2, confidence_level=0.95,
                     outlier_significance_level=0.001, lanczos_degree=20,
                     lanczos_tol=None, orthogonalize=0, seed=0):
-    """Single-thread restatement of the reference estimator (FP64)."""
+    """Single-thread restatement of the reference estimator (FP64).
+    gram: False/0 Lanczos on A, True/1 Golub-Kahn on A, 2 Lanczos on
+    A^T A (+ t I with parameters)."""
     lib = load()
     A, fmt, data, indices, indptr = _csr_parts(A)
     affine = parameters is not None

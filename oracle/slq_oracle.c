@@ -21,7 +21,10 @@
  *     eigenvectors are the right singular vectors;
  *   - for gram=1 on a rectangular matrix the probe length and the trace scale
  *     are the number of columns (the reference uses the number of rows,
- *     c_trace_estimator.cpp:220,620, which is only right for square A).
+ *     c_trace_estimator.cpp:220,620, which is only right for square A);
+ *   - gram=2 (no counterpart in the reference) runs Lanczos on A^T A (+ t I
+ *     for affine operators), the operator of the engine's normal-equations
+ *     mode.
  * The first two are pinned against the reference's LAPACK results by the
  * tests; the third only changes rectangular inputs, which the reference
  * cannot run.
@@ -149,11 +152,26 @@ typedef struct {
     int fmt;        /* 0 CSR, 1 CSC */
     int affine;     /* adds t * x */
     double t;
+    int normal;     /* operator is A^T A (+ t I): x -> A^T (A x) + t x */
+    double* tmp;    /* nrows scratch for the normal operator */
 } op_t;
 
-/* y = A x (+ t x) */
+static void op_tdot(const op_t* A, const double* x, double* y);
+
+/* y = A x (+ t x); for the normal operator y = A^T (A x) + t x */
 static void op_dot(const op_t* A, const double* x, double* y)
 {
+    if (A->normal)
+    {
+        op_t B = *A;
+        B.normal = 0;
+        B.affine = 0;
+        op_dot(&B, x, A->tmp);
+        op_tdot(&B, A->tmp, y);
+        if (A->affine && A->t != 0.0)
+            for (int64_t c = 0; c < A->ncols; ++c) y[c] += A->t * x[c];
+        return;
+    }
     if (A->fmt == 0)
     {
         for (int64_t r = 0; r < A->nrows; ++r)
@@ -595,13 +613,22 @@ void oracle_stream_words(int64_t seed, int64_t count, uint64_t* out)
     for (int64_t i = 0; i < count; ++i) out[i] = xoshiro_next(&x);
 }
 
+/* gram: 0 Lanczos on A, 1 Golub-Kahn on A, 2 Lanczos on A^T A (+ t I). */
 int oracle_krylov(const double* data, const int* indices, const int* indptr,
                   int64_t nrows, int64_t ncols, int fmt, int affine, double t,
                   int gram, const double* v, int m, double tol,
                   int orthogonalize, double* alpha, double* beta)
 {
-    op_t A = {data, indices, indptr, nrows, ncols, fmt, affine, t};
-    if (gram) return golub_kahn(&A, v, m, tol, orthogonalize, alpha, beta);
+    op_t A = {data, indices, indptr, nrows, ncols, fmt, affine, t, 0, NULL};
+    if (gram == 1) return golub_kahn(&A, v, m, tol, orthogonalize, alpha, beta);
+    if (gram == 2)
+    {
+        A.normal = 1;
+        A.tmp = (double*)malloc(sizeof(double) * nrows);
+        int k = lanczos(&A, v, ncols, m, tol, orthogonalize, alpha, beta);
+        free(A.tmp);
+        return k;
+    }
     return lanczos(&A, v, nrows, m, tol, orthogonalize, alpha, beta);
 }
 
@@ -648,7 +675,8 @@ int oracle_trace_estimator(
 {
     int64_t n = gram ? ncols : nrows;
     op_t A = {data, indices, indptr, nrows, ncols, fmt, affine,
-              affine ? params[0] : 0.0};
+              affine ? params[0] : 0.0, gram == 2, NULL};
+    if (gram == 2) A.tmp = (double*)malloc(sizeof(double) * nrows);
     xoshiro_t x;
     stream_init(&x, seed);
     double* v = (double*)malloc(sizeof(double) * n);
@@ -668,12 +696,12 @@ int oracle_trace_estimator(
     {
         rademacher_fill(&x, v, n);
         int k;
-        if (gram) k = golub_kahn(&A, v, m, tol, orthogonalize, alpha, beta);
+        if (gram == 1) k = golub_kahn(&A, v, m, tol, orthogonalize, alpha, beta);
         else k = lanczos(&A, v, n, m, tol, orthogonalize, alpha, beta);
         if (lanczos_sizes) lanczos_sizes[s] = k;
         if (alphas) memcpy(alphas + (int64_t)s * m, alpha, sizeof(double) * k);
         if (betas) memcpy(betas + (int64_t)s * m, beta, sizeof(double) * k);
-        if (nodes_weights(alpha, beta, k, gram, theta, tau) != 0) status = 2;
+        if (nodes_weights(alpha, beta, k, gram == 1, theta, tau) != 0) status = 2;
         if (affine && q > 1)
             for (int j = 0; j < q; ++j) converged[j] = 0;
         for (int j = 0; j < q; ++j)
@@ -694,6 +722,7 @@ int oracle_trace_estimator(
     }
     average_estimates(conf, outlier_sig, q, max_s, used, order, samples,
                       num_outliers, trace, error);
+    free(A.tmp);
     free(v);
     free(alpha);
     free(beta);

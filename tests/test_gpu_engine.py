@@ -456,3 +456,47 @@ def test_distributed_single_rank_nccl_matches_single_process(cuda):
         assert abs(res["trace"][0] - tr) <= 1e-12 * abs(tr)
     finally:
         dist.destroy_process_group()
+
+
+def _tall_sparse(m, n, per_col, seed, dtype=np.float64):
+    # per_col distinct rows per column, N(0,1) values, CSC (the large
+    # Gram-form workload's construction, scaled down)
+    rng = np.random.default_rng(seed)
+    rows = np.concatenate([rng.choice(m, per_col, replace=False)
+                           for _ in range(n)])
+    cols = np.repeat(np.arange(n), per_col)
+    vals = rng.standard_normal(rows.size)
+    return sp.csc_matrix((vals, (rows, cols)), shape=(m, n)).astype(dtype)
+
+
+@pytest.mark.parametrize("orth", [0, -1])
+def test_normal_equations_mode_matches_oracle(cuda, orth):
+    X = _tall_sparse(2000, 500, 16, 4)
+    lam = 1e-2
+    kw = dict(min_num_samples=8, max_num_samples=40, error_rtol=1e-3,
+              lanczos_degree=24, orthogonalize=orth, seed=9)
+    G = ib.GramAffineMatrixFunction(X)
+    tr, info = ib.logdet(G, method="slq", gpu=True, parameters=lam,
+                         return_info=True, **kw)
+    want = oracle.trace_estimator(X, "log", gram=2, parameters=[lam], **kw)
+    used = int(want["num_samples_used"][0])
+    assert int(info["convergence"]["num_samples_used"]) == used
+    assert rel(info["convergence"]["samples"][:used],
+               want["samples"][:used, 0]) < 1e-9
+    exact = np.linalg.slogdet((X.T @ X).toarray() + lam * np.eye(500))[1]
+    assert abs(tr - exact) / abs(exact) < 0.02
+
+
+def test_normal_equations_sweep_and_fp32(cuda):
+    X = _tall_sparse(3000, 800, 16, 5, dtype=np.float32)
+    lams = [1e-2, 1e-1, 1.0]
+    G = ib.GramAffineMatrixFunction(X)
+    tr, info = ib.logdet(G, method="slq", gpu=True, parameters=lams,
+                         return_info=True, min_num_samples=128,
+                         max_num_samples=128, error_rtol=0.0,
+                         lanczos_degree=40, orthogonalize=0, seed=1,
+                         engine=ib.EngineOptions(block_size=128))
+    XtX = (X.T @ X).toarray().astype(np.float64)
+    for i, lam in enumerate(lams):
+        exact = np.linalg.slogdet(XtX + lam * np.eye(800))[1]
+        assert abs(tr[i] - exact) / abs(exact) < 0.02
