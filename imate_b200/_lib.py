@@ -32,8 +32,13 @@ EXPORTS = (
     "slq_erfinv", "slq_xoshiro_jump_ahead", "slq_device_info",
     "slq_last_error", "slq_abi_version", "slq_profile_begin",
     "slq_profile_end", "slq_generate_probes_noalloc", "slq_mlp_forward",
-    "slq_mlp_grad", "slq_mlp_train",
+    "slq_mlp_grad", "slq_mlp_train", "slq_operator_tune_workspace_bytes",
+    "slq_operator_tune", "slq_operator_set_variant",
+    "slq_batch_workspace_bytes", "slq_batch_create", "slq_batch_run",
+    "slq_batch_info", "slq_batch_destroy",
 )
+TUNE_MAX_CANDIDATES = 16
+SPMM_KINDS = ("csr", "row-group", "row-group-tma")
 MLP_WIDTH = 64
 MLP_PARAMS = 64 + 64 + 64 * 64 + 64 + 64 + 1
 MLP_MAX_BATCH = 64
@@ -100,6 +105,20 @@ class SlqResult(ctypes.Structure):
     ]
 
 
+class SlqTuneResult(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_int32),
+        ("transpose", ctypes.c_int32),
+        ("num_candidates", ctypes.c_int32),
+        ("chosen", ctypes.c_int32),
+        ("kind", ctypes.c_int32 * 16),
+        ("group_rows", ctypes.c_int32 * 16),
+        ("lanes_vec", ctypes.c_int32 * 16),
+        ("slices", ctypes.c_int32 * 16),
+        ("milliseconds", ctypes.c_double * 16),
+    ]
+
+
 _lib = None
 
 
@@ -141,6 +160,17 @@ def _declare(lib):
         "slq_mlp_grad": (i32, [vp, vp, vp, i32, vp, vp, vp]),
         "slq_mlp_train": (i32, [vp, vp, vp, vp, vp, i32, i32, i32,
                                 ctypes.c_float, vp, vp]),
+        "slq_operator_tune_workspace_bytes": (i32, [vp, i32, psz]),
+        "slq_operator_tune": (i32, [vp, i32, i32, i32, vp, sz, vp,
+                                    ctypes.POINTER(SlqTuneResult)]),
+        "slq_operator_set_variant": (i32, [vp, i32, i32, i32]),
+        "slq_batch_workspace_bytes": (i32, [i32, vp, vp, vp, psz]),
+        "slq_batch_create": (i32, [i32, vp, vp, vp, vp, vp, sz, vp,
+                                   ctypes.POINTER(vp)]),
+        "slq_batch_run": (i32, [vp, vp, vp]),
+        "slq_batch_info": (i32, [vp, ctypes.POINTER(i64),
+                                 ctypes.POINTER(i64)]),
+        "slq_batch_destroy": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

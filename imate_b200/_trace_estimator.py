@@ -234,15 +234,21 @@ def _clock_seed():
     return int(time.perf_counter_ns() & 0x7FFFFFFF)
 
 
-def trace_estimator(A, parameters, func, gram, exponent, min_num_samples,
-                    max_num_samples, error_atol, error_rtol,
-                    confidence_level, outlier_significance_level,
-                    lanczos_degree, lanczos_tol, orthogonalize, seed,
-                    num_threads, num_gpu_devices, verbose, plot, gpu,
-                    options=None):
-    """SLQ estimate of trace(f(A^p)) (or of f((A^T A)^p) with gram) on the
-    GPU.  ``func`` is 'log', 'inv' or 'id'.  Returns (trace, info) like
-    ``trace_estimator.pyx``."""
+class _Job:
+    """One estimator call prepared for the engine: the checked arguments,
+    the device operator, one ``SlqParams`` per run and the output arrays the
+    runs fill in."""
+
+
+def prepare(A, parameters, func, gram, exponent, min_num_samples,
+            max_num_samples, error_atol, error_rtol, confidence_level,
+            outlier_significance_level, lanczos_degree, lanczos_tol,
+            orthogonalize, seed, num_threads, num_gpu_devices, verbose, plot,
+            gpu, options=None):
+    """Argument checks and set-up of one estimate (the part of
+    ``trace_estimator.pyx:38-260`` before the sample loop).  Returns a job
+    whose ``runs`` (one per group of inquiries) are executed by ``slq_run``
+    or by a batch plan, then ``collect``-ed and ``finish``-ed."""
     import torch
 
     if options is None:
@@ -281,12 +287,13 @@ def trace_estimator(A, parameters, func, gram, exponent, min_num_samples,
         import os
         num_threads = os.cpu_count() or 1
 
-    lib = _lib.load()
+    _lib.load()
     if not torch.cuda.is_available():
         raise RuntimeError("no CUDA device is available for the SLQ engine")
 
-    init_wall = time.perf_counter()
-    init_proc = time.process_time()
+    J = _Job()
+    J.init_wall = time.perf_counter()
+    J.init_proc = time.process_time()
 
     affine = Aop.get_num_parameters() > 0
     normal = bool(getattr(Aop, "normal_equations", False))
@@ -305,31 +312,15 @@ def trace_estimator(A, parameters, func, gram, exponent, min_num_samples,
     else:
         groups = [list(range(num_inquiries))]
 
-    q = num_inquiries
     m = int(lanczos_degree)
-    trace = np.full(q, np.nan)
-    error = np.full(q, np.nan)
-    samples = np.full((max_num_samples, q), np.nan)
-    processed = np.zeros(max_num_samples, dtype=np.int32)
-    num_samples_used = np.zeros(q, dtype=np.int32)
-    num_outliers = np.zeros(q, dtype=np.int32)
-    converged = np.zeros(q, dtype=np.int32)
-    lanczos_size = np.zeros((max_num_samples, len(groups)), dtype=np.int32)
-    alphas = betas = None
-    if options.return_coefficients:
-        alphas = np.full((len(groups), max_num_samples, m), np.nan)
-        betas = np.full((len(groups), max_num_samples, m), np.nan)
-    all_converged = True
-    alg_wall_time = 0.0
-    engine = dict(block_size=None, rng=options.rng, num_blocks=0,
-                  num_probes_computed=0, gpu_launches=0)
-
-    dev_op = Aop.get_device_operator(need_transpose=bool(gram) or normal)
+    J.Aop = Aop
+    J.dev_op = Aop.get_device_operator(need_transpose=bool(gram) or normal)
     gram_mode = 2 if normal else int(bool(gram))
-    stream = torch.cuda.current_stream(dev_op.device)
-    for gi, group in enumerate(groups):
-        gq = len(group)
-        prm = _lib.SlqParams(
+    J.groups = groups
+    J.params = []
+    J.t_groups = []
+    for group in groups:
+        J.params.append(_lib.SlqParams(
             func=_lib.FUNC_IDS[func], gram=gram_mode,
             exponent=float(exponent), orthogonalize=int(orthogonalize),
             seed=seed_used, lanczos_degree=m, lanczos_tol=float(lanczos_tol),
@@ -339,116 +330,195 @@ def trace_estimator(A, parameters, func, gram, exponent, min_num_samples,
             confidence_level=float(confidence_level),
             outlier_significance_level=float(outlier_significance_level),
             block_size=options.block_size, rng=_lib.RNG_IDS[options.rng],
-            first_probe=options.first_probe)
+            first_probe=options.first_probe))
+        J.t_groups.append(np.ascontiguousarray(t_values[group],
+                                               dtype=np.float64))
+    J.options = options
+    J.dtype_str = dtype_str
+    J.data_type_name = data_type_name
+    J.gram = gram
+    J.exponent = exponent
+    J.parameters = parameters
+    J.num_inquiries = num_inquiries
+    J.error_atol, J.error_rtol = error_atol, error_rtol
+    J.confidence_level = confidence_level
+    J.outlier_significance_level = outlier_significance_level
+    J.min_num_samples, J.max_num_samples = min_num_samples, max_num_samples
+    J.lanczos_degree, J.lanczos_tol = lanczos_degree, lanczos_tol
+    J.orthogonalize, J.seed, J.seed_used = orthogonalize, seed, seed_used
+    J.num_threads = num_threads
+    J.verbose, J.plot = verbose, plot
+    reset_outputs(J)
+    return J
+
+
+def reset_outputs(J):
+    """Fresh output arrays and counters for job J (before its runs)."""
+    q = J.num_inquiries
+    mx = J.max_num_samples
+    m = int(J.lanczos_degree)
+    ng = len(J.groups)
+    J.trace = np.full(q, np.nan)
+    J.error = np.full(q, np.nan)
+    J.samples = np.full((mx, q), np.nan)
+    J.processed = np.zeros(mx, dtype=np.int32)
+    J.num_samples_used = np.zeros(q, dtype=np.int32)
+    J.num_outliers = np.zeros(q, dtype=np.int32)
+    J.converged = np.zeros(q, dtype=np.int32)
+    J.lanczos_size = np.zeros((mx, ng), dtype=np.int32)
+    J.alphas = J.betas = None
+    if J.options.return_coefficients:
+        J.alphas = np.full((ng, mx, m), np.nan)
+        J.betas = np.full((ng, mx, m), np.nan)
+    J.all_converged = True
+    J.alg_wall_time = 0.0
+    J.engine = dict(block_size=None, rng=J.options.rng, num_blocks=0,
+                    num_probes_computed=0, gpu_launches=0)
+
+
+def run_outputs(J, gi):
+    """Host arrays for run ``gi`` of job J and the SlqResult pointing at
+    them."""
+    gq = len(J.groups[gi])
+    mx = J.max_num_samples
+    m = int(J.lanczos_degree)
+    a = dict(
+        trace=np.zeros(gq), error=np.zeros(gq), samples=np.zeros((mx, gq)),
+        order=np.zeros(mx, dtype=np.int32),
+        used=np.zeros(gq, dtype=np.int32), out=np.zeros(gq, dtype=np.int32),
+        conv=np.zeros(gq, dtype=np.int32), size=np.zeros(mx, dtype=np.int32),
+        alpha=np.zeros((mx, m)) if J.alphas is not None else None,
+        beta=np.zeros((mx, m)) if J.betas is not None else None)
+
+    def ptr(x):
+        return x.ctypes.data if x is not None else None
+    res = _lib.SlqResult(
+        trace=ptr(a["trace"]), error=ptr(a["error"]),
+        samples=ptr(a["samples"]), processed_samples_indices=ptr(a["order"]),
+        num_samples_used=ptr(a["used"]), num_outliers=ptr(a["out"]),
+        converged=ptr(a["conv"]), lanczos_size=ptr(a["size"]),
+        alpha=ptr(a["alpha"]), beta=ptr(a["beta"]))
+    return res, a
+
+
+def collect(J, gi, res, a, status):
+    """Put run ``gi``'s outputs into the job (raising on engine errors; an
+    eigen-solve failure is reported as a warning, as the samples it affects
+    are NaN)."""
+    lib = _lib.load()
+    if status == 6:
+        import warnings
+        warnings.warn("SLQ: " + lib.slq_last_error().decode())
+    elif status != _lib.SLQ_OK:
+        _lib.check(status)
+    for k, j in enumerate(J.groups[gi]):
+        J.trace[j] = a["trace"][k]
+        J.error[j] = a["error"][k]
+        J.samples[:, j] = a["samples"][:, k]
+        J.num_samples_used[j] = a["used"][k]
+        J.num_outliers[j] = a["out"][k]
+        J.converged[j] = a["conv"][k]
+    if gi == 0:
+        J.processed = a["order"]
+    J.lanczos_size[:, gi] = a["size"]
+    if J.alphas is not None:
+        J.alphas[gi] = a["alpha"]
+        J.betas[gi] = a["beta"]
+    J.all_converged = J.all_converged and bool(res.all_converged)
+    J.alg_wall_time += float(res.alg_wall_time)
+    J.engine["num_blocks"] += int(res.num_blocks)
+    J.engine["num_probes_computed"] += int(res.num_probes_computed)
+    J.engine["gpu_launches"] += int(res.gpu_launches)
+
+
+def run_job(J):
+    """Run every group of J with slq_run on the current stream."""
+    import torch
+    lib = _lib.load()
+    dev_op = J.dev_op
+    stream = torch.cuda.current_stream(dev_op.device)
+    for gi, prm in enumerate(J.params):
+        gq = len(J.groups[gi])
         ws_bytes = ctypes.c_size_t(0)
         _lib.check(lib.slq_run_workspace_bytes(dev_op.handle,
                                                ctypes.byref(prm), gq,
                                                ctypes.byref(ws_bytes)))
         workspace = torch.empty(int(ws_bytes.value), dtype=torch.uint8,
                                 device=dev_op.device)
-        g_trace = np.zeros(gq)
-        g_error = np.zeros(gq)
-        g_samples = np.zeros((max_num_samples, gq))
-        g_order = np.zeros(max_num_samples, dtype=np.int32)
-        g_used = np.zeros(gq, dtype=np.int32)
-        g_out = np.zeros(gq, dtype=np.int32)
-        g_conv = np.zeros(gq, dtype=np.int32)
-        g_size = np.zeros(max_num_samples, dtype=np.int32)
-        g_alpha = np.zeros((max_num_samples, m)) if alphas is not None \
-            else None
-        g_beta = np.zeros((max_num_samples, m)) if betas is not None \
-            else None
-        ptr = (lambda a: a.ctypes.data if a is not None else None)
-        res = _lib.SlqResult(
-            trace=ptr(g_trace), error=ptr(g_error), samples=ptr(g_samples),
-            processed_samples_indices=ptr(g_order),
-            num_samples_used=ptr(g_used), num_outliers=ptr(g_out),
-            converged=ptr(g_conv), lanczos_size=ptr(g_size),
-            alpha=ptr(g_alpha), beta=ptr(g_beta))
-        t_g = np.ascontiguousarray(t_values[group], dtype=np.float64)
+        res, a = run_outputs(J, gi)
+        t_g = J.t_groups[gi]
         status = lib.slq_run(dev_op.handle, ctypes.byref(prm),
                              t_g.ctypes.data, gq, workspace.data_ptr(),
                              workspace.numel(), stream.cuda_stream,
                              ctypes.byref(res))
         del workspace
-        if status == 6:  # eigen-solve failure: report, do not hide
-            import warnings
-            warnings.warn("SLQ: " + lib.slq_last_error().decode())
-        elif status != _lib.SLQ_OK:
-            _lib.check(status)
-        for k, j in enumerate(group):
-            trace[j] = g_trace[k]
-            error[j] = g_error[k]
-            samples[:, j] = g_samples[:, k]
-            num_samples_used[j] = g_used[k]
-            num_outliers[j] = g_out[k]
-            converged[j] = g_conv[k]
-        processed = g_order if gi == 0 else processed
-        lanczos_size[:, gi] = g_size
-        if alphas is not None:
-            alphas[gi] = g_alpha
-            betas[gi] = g_beta
-        all_converged = all_converged and bool(res.all_converged)
-        alg_wall_time += float(res.alg_wall_time)
-        engine["num_blocks"] += int(res.num_blocks)
-        engine["num_probes_computed"] += int(res.num_probes_computed)
-        engine["gpu_launches"] += int(res.gpu_launches)
+        collect(J, gi, res, a, status)
 
-    b = options.block_size
+
+def block_width(max_num_samples, block_size, dtype_str):
+    """The engine's block width for these settings (make_plan's rule)."""
+    b = block_size
     if b <= 0:
         b = min(256, 1 << max(0, (max_num_samples - 1).bit_length()))
     bmax = 512 if dtype_str == "float64" else 1024
-    b = min(1 << max(0, (b - 1).bit_length()), bmax,
-            1 << max(0, (max_num_samples - 1).bit_length()))
-    engine["block_size"] = b
+    return min(1 << max(0, (b - 1).bit_length()), bmax,
+               1 << max(0, (max_num_samples - 1).bit_length()))
 
-    tot_wall_time = time.perf_counter() - init_wall
-    cpu_proc_time = time.process_time() - init_proc
 
-    props = torch.cuda.get_device_properties(dev_op.device)
-    out_dtype = np.dtype(dtype_str)
-    trace_out = trace.astype(out_dtype)
-    error_out = error.astype(out_dtype)
-    samples_out = samples.astype(out_dtype)
+def finish(J):
+    """(trace, info) of a completed job, as ``trace_estimator.pyx:260-390``
+    returns them."""
+    import torch
+    J.engine["block_size"] = block_width(J.max_num_samples,
+                                         J.params[0].block_size, J.dtype_str)
+    tot_wall_time = time.perf_counter() - J.init_wall
+    cpu_proc_time = time.process_time() - J.init_proc
+    Aop = J.Aop
+    props = torch.cuda.get_device_properties(J.dev_op.device)
+    out_dtype = np.dtype(J.dtype_str)
+    trace_out = J.trace.astype(out_dtype)
+    error_out = J.error.astype(out_dtype)
+    samples_out = J.samples.astype(out_dtype)
+    ngroups = len(J.groups)
     info = {
         "matrix": {
-            "data_type": data_type_name,
-            "gram": gram,
-            "exponent": exponent,
+            "data_type": J.data_type_name,
+            "gram": J.gram,
+            "exponent": J.exponent,
             "size": (Aop.get_num_rows(), Aop.get_num_columns()),
             "sparse": Aop.is_sparse(),
             "nnz": Aop.get_nnz(),
             "density": Aop.get_density(),
-            "num_inquiries": num_inquiries,
+            "num_inquiries": J.num_inquiries,
             "num_operator_parameters": Aop.get_num_parameters(),
-            "parameters": parameters,
+            "parameters": J.parameters,
         },
         "error": {
             "absolute_error": None,
             "relative_error": None,
-            "error_atol": error_atol,
-            "error_rtol": error_rtol,
-            "confidence_level": confidence_level,
-            "outlier_significance_level": outlier_significance_level,
+            "error_atol": J.error_atol,
+            "error_rtol": J.error_rtol,
+            "confidence_level": J.confidence_level,
+            "outlier_significance_level": J.outlier_significance_level,
         },
         "convergence": {
             "converged": None,
-            "all_converged": bool(all_converged),
-            "min_num_samples": min_num_samples,
-            "max_num_samples": max_num_samples,
+            "all_converged": bool(J.all_converged),
+            "min_num_samples": J.min_num_samples,
+            "max_num_samples": J.max_num_samples,
             "num_samples_used": None,
             "num_outliers": None,
             "samples": None,
             "samples_mean": None,
-            "samples_processed_order": processed,
+            "samples_processed_order": J.processed,
         },
         "time": {
             "tot_wall_time": tot_wall_time,
-            "alg_wall_time": alg_wall_time,
+            "alg_wall_time": J.alg_wall_time,
             "cpu_proc_time": cpu_proc_time,
         },
         "device": {
-            "num_cpu_threads": num_threads,
+            "num_cpu_threads": J.num_threads,
             "num_gpu_devices": 1,
             "num_gpu_multiprocessors": props.multi_processor_count,
             "num_gpu_threads_per_multiprocessor":
@@ -456,42 +526,43 @@ def trace_estimator(A, parameters, func, gram, exponent, min_num_samples,
         },
         "solver": {
             "version": __version__,
-            "lanczos_degree": lanczos_degree,
-            "lanczos_tol": lanczos_tol,
-            "orthogonalize": orthogonalize,
-            "seed": seed_used if seed is not None and seed >= 0 else -1,
+            "lanczos_degree": J.lanczos_degree,
+            "lanczos_tol": J.lanczos_tol,
+            "orthogonalize": J.orthogonalize,
+            "seed": J.seed_used if J.seed is not None and J.seed >= 0
+            else -1,
             "method": "slq",
         },
-        "engine": dict(engine, lanczos_size=lanczos_size[:, 0]
-                       if len(groups) == 1 else lanczos_size),
+        "engine": dict(J.engine, lanczos_size=J.lanczos_size[:, 0]
+                       if ngroups == 1 else J.lanczos_size),
     }
-    if alphas is not None:
-        info["engine"]["alpha"] = alphas[0] if len(groups) == 1 else alphas
-        info["engine"]["beta"] = betas[0] if len(groups) == 1 else betas
+    if J.alphas is not None:
+        info["engine"]["alpha"] = J.alphas[0] if ngroups == 1 else J.alphas
+        info["engine"]["beta"] = J.betas[0] if ngroups == 1 else J.betas
 
-    output_is_array = not (parameters is None or np.isscalar(parameters))
+    output_is_array = not (J.parameters is None or np.isscalar(J.parameters))
     eps = np.finfo(float).eps
     if output_is_array:
         info["error"]["absolute_error"] = error_out
         info["error"]["relative_error"] = error_out / (np.abs(trace_out) + eps)
-        info["convergence"]["converged"] = converged.astype(bool)
-        info["convergence"]["num_samples_used"] = num_samples_used
-        info["convergence"]["num_outliers"] = num_outliers
+        info["convergence"]["converged"] = J.converged.astype(bool)
+        info["convergence"]["num_samples_used"] = J.num_samples_used
+        info["convergence"]["num_outliers"] = J.num_outliers
         info["convergence"]["samples"] = samples_out
         info["convergence"]["samples_mean"] = trace_out
     else:
         info["error"]["absolute_error"] = error_out[0]
         info["error"]["relative_error"] = \
             error_out[0] / (np.abs(trace_out[0]) + eps)
-        info["convergence"]["converged"] = bool(converged[0])
-        info["convergence"]["num_samples_used"] = num_samples_used[0]
-        info["convergence"]["num_outliers"] = num_outliers[0]
+        info["convergence"]["converged"] = bool(J.converged[0])
+        info["convergence"]["num_samples_used"] = J.num_samples_used[0]
+        info["convergence"]["num_outliers"] = J.num_outliers[0]
         info["convergence"]["samples"] = samples_out[:, 0]
         info["convergence"]["samples_mean"] = trace_out[0]
 
-    if verbose:
+    if J.verbose:
         print_summary(info)
-    if plot:
+    if J.plot:
         import warnings
         warnings.warn("plot=True: convergence plots are not produced by the "
                       "B200 engine (no plotting stack)")
@@ -499,6 +570,24 @@ def trace_estimator(A, parameters, func, gram, exponent, min_num_samples,
     if output_is_array:
         return trace_out, info
     return trace_out[0], info
+
+
+def trace_estimator(A, parameters, func, gram, exponent, min_num_samples,
+                    max_num_samples, error_atol, error_rtol,
+                    confidence_level, outlier_significance_level,
+                    lanczos_degree, lanczos_tol, orthogonalize, seed,
+                    num_threads, num_gpu_devices, verbose, plot, gpu,
+                    options=None):
+    """SLQ estimate of trace(f(A^p)) (or of f((A^T A)^p) with gram) on the
+    GPU.  ``func`` is 'log', 'inv' or 'id'.  Returns (trace, info) like
+    ``trace_estimator.pyx``."""
+    J = prepare(A, parameters, func, gram, exponent, min_num_samples,
+                max_num_samples, error_atol, error_rtol, confidence_level,
+                outlier_significance_level, lanczos_degree, lanczos_tol,
+                orthogonalize, seed, num_threads, num_gpu_devices, verbose,
+                plot, gpu, options)
+    run_job(J)
+    return finish(J)
 
 
 def print_summary(info):

@@ -1,0 +1,269 @@
+"""Batched SLQ: many independent estimates in one CUDA graph launch.
+
+imate estimates one matrix per call (``trace_estimator.pyx:38-390``; its GPU
+sample loop ``cu_trace_estimator.cu:197-315`` keeps one matrix per device).
+A batch plan records every probe block of every estimate into one CUDA graph
+(``slq_batch_create``), each estimate on its own graph branch so that
+estimates of small matrices overlap on the device, launches the graph once
+and applies imate's stopping rule to each estimate on the host
+(``slq_batch_run``).  Each estimate equals what ``logdet`` / ``traceinv`` /
+``trace`` return for the same arguments and the same SpMM choice.
+
+``autotune`` picks, per operator, the SpMM storage format and tile (row-group
+rows, probes per lane, warps per row group) and the probe block width: every
+candidate the operator supports is timed at each width
+(``slq_operator_tune``) and the width with the least SpMM time per probe
+becomes the estimate's block size.
+"""
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._functions import _SLQ_DEFAULTS
+from ._trace_estimator import (EngineOptions, prepare, run_outputs, collect,
+                               finish, reset_outputs)
+
+__all__ = ["BatchPlan", "autotune", "tune_operator", "logdet_batch",
+           "traceinv_batch", "trace_batch"]
+
+_FUNC_OF = {"logdet": "log", "traceinv": "inv", "trace": "id"}
+
+
+def tune_operator(dev_op, width, transpose=False, reps=5):
+    """Time every SpMM candidate of a device operator at one block width;
+    the fastest becomes the operator's choice at that width.  Returns a list
+    of candidate dicts and the chosen index."""
+    import torch
+    lib = _lib.load()
+    nbytes = ctypes.c_size_t(0)
+    _lib.check(lib.slq_operator_tune_workspace_bytes(
+        dev_op.handle, int(width), ctypes.byref(nbytes)))
+    ws = torch.empty(int(nbytes.value), dtype=torch.uint8,
+                     device=dev_op.device)
+    res = _lib.SlqTuneResult()
+    stream = torch.cuda.current_stream(dev_op.device)
+    _lib.check(lib.slq_operator_tune(
+        dev_op.handle, int(width), int(bool(transpose)), int(reps),
+        ws.data_ptr(), ws.numel(), stream.cuda_stream, ctypes.byref(res)))
+    cands = [dict(kind=_lib.SPMM_KINDS[res.kind[i]],
+                  group_rows=int(res.group_rows[i]),
+                  lanes_vec=int(res.lanes_vec[i]), slices=int(res.slices[i]),
+                  ms=float(res.milliseconds[i]))
+             for i in range(res.num_candidates)]
+    return cands, int(res.chosen)
+
+
+def set_variant(dev_op, width, candidate, transpose=False):
+    """Force SpMM candidate ``candidate`` (index from tune_operator) at this
+    width; -1 restores the built-in choice."""
+    _lib.check(_lib.load().slq_operator_set_variant(
+        dev_op.handle, int(width), int(bool(transpose)), int(candidate)))
+
+
+def autotune(dev_op, max_num_samples, directions=(False,), widths=None,
+             reps=5, per_step_ms=0.01):
+    """Tune the operator's SpMM at every candidate block width and return
+    the width with the least estimated time per probe-step,
+
+        ceil(S / w) * (sum over directions of the fastest SpMM at w
+                       + per_step_ms) / S,
+
+    S = max_num_samples (``per_step_ms`` stands for the launches of a step
+    that do not scale with the width).  Returns (width, report) with the
+    report listing every width's candidates."""
+    bmax = 512 if dev_op.dtype_code == _lib.SLQ_F64 else 1024
+    top = min(bmax, 1 << max(0, (int(max_num_samples) - 1).bit_length()))
+    if widths is None:
+        widths = [w for w in (32, 64, 128, 256, 512, 1024) if w <= top] or \
+            [top]
+    report = {}
+    best = None
+    for w in widths:
+        t = 0.0
+        report[w] = {}
+        for tr in directions:
+            cands, chosen = tune_operator(dev_op, w, transpose=tr, reps=reps)
+            report[w]["transpose" if tr else "direct"] = dict(
+                candidates=cands, chosen=chosen)
+            t += cands[chosen]["ms"]
+        blocks = -(-int(max_num_samples) // w)
+        cost = blocks * (t + per_step_ms)
+        report[w]["cost_ms_per_step"] = cost
+        if best is None or cost < best[1]:
+            best = (w, cost)
+    return best[0], report
+
+
+class BatchPlan:
+    """Many SLQ estimates recorded into one CUDA graph.
+
+    ``estimates`` is a list of dicts, one per estimate, with keys ``func``
+    ('logdet', 'traceinv' or 'trace'), ``A`` (matrix or operator), optional
+    ``gram`` and ``p``, any of imate's SLQ keyword arguments, and optionally
+    ``engine`` (EngineOptions).  ``autotune=True`` tunes each operator's SpMM
+    and block width first (and overrides the estimate's block size);
+    otherwise every operator keeps its current choice.  ``gpu=True`` is
+    implied.
+    """
+
+    def __init__(self, estimates, autotune=True, tune_reps=5):
+        import torch
+        lib = _lib.load()
+        self.jobs = []
+        self.tuning = []
+        tuned = {}
+        for est in estimates:
+            est = dict(est)
+            func = _FUNC_OF[est.pop("func")]
+            A = est.pop("A")
+            gram = bool(est.pop("gram", False))
+            p = est.pop("p", 1.0)
+            engine = est.pop("engine", None) or EngineOptions()
+            kw = dict(_SLQ_DEFAULTS)
+            kw["gpu"] = True
+            unknown = set(est) - set(kw)
+            if unknown:
+                raise TypeError("unexpected keyword argument(s): %s"
+                                % ", ".join(sorted(unknown)))
+            kw.update(est)
+            J = prepare(A, kw["parameters"], func, gram, p,
+                        kw["min_num_samples"], kw["max_num_samples"],
+                        kw["error_atol"], kw["error_rtol"],
+                        kw["confidence_level"],
+                        kw["outlier_significance_level"],
+                        kw["lanczos_degree"], kw["lanczos_tol"],
+                        kw["orthogonalize"], kw["seed"], kw["num_threads"],
+                        kw["num_gpu_devices"], kw["verbose"], kw["plot"],
+                        kw["gpu"], engine)
+            if autotune:
+                key = (id(J.dev_op), J.params[0].gram, J.max_num_samples)
+                if key not in tuned:
+                    dirs = (False,) if J.params[0].gram == 0 else \
+                        (False, True)
+                    tuned[key] = autotune_fn(J.dev_op, J.max_num_samples,
+                                             directions=dirs, reps=tune_reps)
+                width, report = tuned[key]
+                for prm in J.params:
+                    prm.block_size = width
+                self.tuning.append(dict(width=width, report=report))
+            else:
+                self.tuning.append(None)
+            self.jobs.append(J)
+        self.runs = [(J, gi) for J in self.jobs for gi in range(len(J.params))]
+        R = len(self.runs)
+        if R == 0:
+            raise ValueError("a batch needs at least one estimate")
+        devs = {J.dev_op.device for J in self.jobs}
+        if len(devs) != 1:
+            raise ValueError("all estimates of a batch must be on one device")
+        self.device = devs.pop()
+        self._ops = (ctypes.c_void_p * R)(
+            *[J.dev_op.handle.value for J, _ in self.runs])
+        self._prms = (_lib.SlqParams * R)(*[J.params[gi]
+                                            for J, gi in self.runs])
+        self._tps = (ctypes.c_void_p * R)(
+            *[J.t_groups[gi].ctypes.data for J, gi in self.runs])
+        self._nq = (ctypes.c_int * R)(*[len(J.groups[gi])
+                                        for J, gi in self.runs])
+        nbytes = ctypes.c_size_t(0)
+        _lib.check(lib.slq_batch_workspace_bytes(
+            R, self._ops, self._prms, self._nq, ctypes.byref(nbytes)))
+        self.workspace = torch.empty(int(nbytes.value), dtype=torch.uint8,
+                                     device=self.device)
+        self.handle = ctypes.c_void_p(None)
+        stream = torch.cuda.current_stream(self.device)
+        _lib.check(lib.slq_batch_create(
+            R, self._ops, self._prms, self._tps, self._nq,
+            self.workspace.data_ptr(), self.workspace.numel(),
+            stream.cuda_stream, ctypes.byref(self.handle)))
+        k = ctypes.c_int64(0)
+        nn = ctypes.c_int64(0)
+        _lib.check(lib.slq_batch_info(self.handle, ctypes.byref(k),
+                                      ctypes.byref(nn)))
+        self.graph_kernels = int(k.value)
+        self.graph_nodes = int(nn.value)
+        self._lib = lib
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            self._lib.slq_batch_destroy(h)
+            self.handle = ctypes.c_void_p(None)
+
+    def launch(self):
+        """One graph launch plus the host stopping rule; returns the
+        per-run (SlqResult, arrays) pairs and the batch status."""
+        import torch
+        R = len(self.runs)
+        outs = [run_outputs(J, gi) for J, gi in self.runs]
+        results = (_lib.SlqResult * R)(*[o[0] for o in outs])
+        stream = torch.cuda.current_stream(self.device)
+        status = self._lib.slq_batch_run(self.handle, stream.cuda_stream,
+                                         results)
+        return results, outs, status
+
+    def run(self):
+        """Run the batch; returns [(trace, info), ...] in estimate order."""
+        results, outs, status = self.launch()
+        if status not in (_lib.SLQ_OK, 6):
+            _lib.check(status)
+        for J in self.jobs:
+            reset_outputs(J)
+        for k, (J, gi) in enumerate(self.runs):
+            collect(J, gi, results[k], outs[k][1],
+                    status if status == 6 else _lib.SLQ_OK)
+        out = []
+        for J in self.jobs:
+            tr, info = finish(J)
+            info["engine"]["batch"] = dict(
+                estimates=len(self.jobs), runs=len(self.runs),
+                graph_kernels=self.graph_kernels,
+                graph_nodes=self.graph_nodes)
+            out.append((tr, info))
+        return out
+
+
+autotune_fn = autotune
+
+
+def _batch(name, matrices, gram, p, return_info, autotune, options):
+    if not isinstance(return_info, bool):
+        raise TypeError('"return_info" should be boolean.')
+    per = options.pop("per_matrix", None)
+    ests = []
+    for i, A in enumerate(matrices):
+        e = dict(options)
+        if per is not None:
+            e.update(per[i])
+        e.update(func=name, A=A, gram=gram, p=p)
+        ests.append(e)
+    plan = BatchPlan(ests, autotune=autotune)
+    res = plan.run()
+    if return_info:
+        return res
+    return [tr for tr, _ in res]
+
+
+def logdet_batch(matrices, gram=False, p=1.0, return_info=False,
+                 autotune=True, **options):
+    """logdet of every matrix by SLQ in one batched graph launch.  Keyword
+    arguments are imate's SLQ options shared by all matrices; ``per_matrix``
+    (a list of dicts) overrides them per matrix."""
+    return _batch("logdet", matrices, gram, p, return_info, autotune,
+                  options)
+
+
+def traceinv_batch(matrices, gram=False, p=1, return_info=False,
+                   autotune=True, **options):
+    """trace of the inverse of every matrix, batched (see logdet_batch)."""
+    return _batch("traceinv", matrices, gram, p, return_info, autotune,
+                  options)
+
+
+def trace_batch(matrices, gram=False, p=1.0, return_info=False,
+                autotune=True, **options):
+    """trace of every matrix, batched (see logdet_batch)."""
+    return _batch("trace", matrices, gram, p, return_info, autotune,
+                  options)

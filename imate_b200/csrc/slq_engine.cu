@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -220,6 +221,13 @@ struct slq_op {
     const int32_t* t_gptr = nullptr;
     const int32_t* t_gcol = nullptr;
     const void* t_gval = nullptr;
+    // autotuned SpMM candidate per direction and log2(block width); -1 = built-in
+    int8_t tuned[2][11];
+    slq_op()
+    {
+        for (auto& d : tuned)
+            for (auto& v : d) v = -1;
+    }
 };
 
 namespace {
@@ -901,52 +909,90 @@ slq_status spmm_rg_inst(Launcher& L, const int32_t* gptr, const int32_t* gcol, c
     return SLQ_OK;
 }
 
+// ---------------------------------------------------------------------------
+// SpMM candidates: storage format x tile.  A row-group candidate is the tile
+// of LV probes per lane and NS warps sharing one row group (b = 32 LV NS);
+// the TMA candidate gathers X rows with tile::gather4 into shared memory.
+// The built-in choice (op_spmm without a tuned entry) is the first of: TMA
+// (FP32, G = 8, b = 128 or 256), row-group with the widest LV <= 4, CSR.
+// ---------------------------------------------------------------------------
+
+enum { CAND_CSR = 0, CAND_RG = 1, CAND_TMA = 2 };
+
+struct SpmmCand {
+    int kind, g, lv, ns;
+};
+
 template <typename VT>
-slq_status op_spmm(Launcher& L, const slq_op* op, int transpose, int b, const VT* X,
-                   const double* sx, double shift, VT* Y, const VT* Z, const double* zc,
-                   const double* zs, int epi, double* partials, int* grid_out,
-                   const CUtensorMap* xmap = nullptr, int32_t* error = nullptr)
+int spmm_candidates(const slq_op* op, int transpose, int b, SpmmCand* out)
+{
+    int n = 0;
+    out[n++] = {CAND_CSR, 0, 0, 0};
+    const int32_t* gptr = transpose ? op->t_gptr : op->a_gptr;
+    const int G = op->group_rows;
+    if (!G || !gptr) return n;
+    const int bmax = (sizeof(VT) == 8) ? 64 : 256;
+    if (b >= 32 && b <= bmax)
+        for (int lv = 1; lv <= ((sizeof(VT) == 8) ? 2 : 4); lv *= 2)
+        {
+            const int ns = b / (32 * lv);
+            if (ns >= 1 && ns <= 8 && 32 * lv * ns == b) out[n++] = {CAND_RG, G, lv, ns};
+        }
+    if (sizeof(VT) == 4 && G == 8 && (b == 128 || b == 256)) out[n++] = {CAND_TMA, 8, 4, b / 128};
+    return n;
+}
+
+template <typename VT>
+slq_status spmm_cand(Launcher& L, const slq_op* op, int transpose, const SpmmCand& c, int b,
+                     const VT* X, const double* sx, double shift, VT* Y, const VT* Z,
+                     const double* zc, const double* zs, int epi, double* partials,
+                     int* grid_out, const CUtensorMap* xmap, int32_t* error)
 {
     const int64_t rows = transpose ? op->ncols : op->nrows;
     const int64_t xrows = transpose ? op->nrows : op->ncols;
     const int32_t* gptr = transpose ? op->t_gptr : op->a_gptr;
-    if constexpr (sizeof(VT) == 4)
+    const int32_t* gcol = transpose ? op->t_gcol : op->a_gcol;
+    if (c.kind == CAND_TMA)
     {
-        if (xmap && error && op->group_rows == 8 && gptr && (b == 128 || b == 256))
+        if constexpr (sizeof(VT) == 4)
         {
-            const int32_t* gcol = transpose ? op->t_gcol : op->a_gcol;
+            if (!xmap || !error) return fail(SLQ_ERR_BAD_ARG, "TMA SpMM needs a tensor map");
             const float* gval = static_cast<const float*>(transpose ? op->t_gval : op->a_gval);
-            if (b == 256)
+            if (c.ns == 2)
                 return spmm_rgt_inst<8, 2>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y,
                                            Z, zc, zs, epi, partials, error, op->nnz, xrows,
                                            grid_out);
             return spmm_rgt_inst<8, 1>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y, Z,
                                        zc, zs, epi, partials, error, op->nnz, xrows, grid_out);
         }
+        return fail(SLQ_ERR_BAD_ARG, "TMA SpMM is FP32 only");
     }
-    const int bmax_rg = (sizeof(VT) == 8) ? 64 : 256;
-    if (op->group_rows && gptr && b >= 32 && b <= bmax_rg)
+    if (c.kind == CAND_RG)
     {
-        const int32_t* gcol = transpose ? op->t_gcol : op->a_gcol;
         const VT* gval = static_cast<const VT*>(transpose ? op->t_gval : op->a_gval);
-#define SLQ_RG(BB, LVV, NSS)                                                                   \
-    if (b == BB)                                                                               \
-    {                                                                                          \
-        if (op->group_rows == 8)                                                               \
-            return spmm_rg_inst<VT, LVV, 8, NSS>(L, gptr, gcol, gval, rows, b, X, sx, shift,   \
-                                                 Y, Z, zc, zs, epi, partials, op->nnz, xrows,  \
-                                                 grid_out);                                    \
-        return spmm_rg_inst<VT, LVV, 4, NSS>(L, gptr, gcol, gval, rows, b, X, sx, shift, Y, Z, \
-                                             zc, zs, epi, partials, op->nnz, xrows, grid_out); \
+#define SLQ_RG_CASE(GG, LVV, NSS)                                                            \
+    if (c.g == GG && c.lv == LVV && c.ns == NSS)                                           \
+        return spmm_rg_inst<VT, LVV, GG, NSS>(L, gptr, gcol, gval, rows, b, X, sx, shift, Y, \
+                                              Z, zc, zs, epi, partials, op->nnz, xrows,     \
+                                              grid_out);
+#define SLQ_RG_ALL(GG)         \
+    SLQ_RG_CASE(GG, 1, 1)      \
+    SLQ_RG_CASE(GG, 1, 2)      \
+    SLQ_RG_CASE(GG, 2, 1)      \
+    if constexpr (sizeof(VT) == 4) \
+    {                          \
+        SLQ_RG_CASE(GG, 1, 4)  \
+        SLQ_RG_CASE(GG, 2, 2)  \
+        SLQ_RG_CASE(GG, 4, 1)  \
+        SLQ_RG_CASE(GG, 1, 8)  \
+        SLQ_RG_CASE(GG, 2, 4)  \
+        SLQ_RG_CASE(GG, 4, 2)  \
     }
-        SLQ_RG(32, 1, 1)
-        SLQ_RG(64, 2, 1)
-        SLQ_RG(128, 4, 1)
-        if constexpr (sizeof(VT) == 4)
-        {
-            SLQ_RG(256, 4, 2)
-        }
-#undef SLQ_RG
+        SLQ_RG_ALL(8)
+        SLQ_RG_ALL(4)
+#undef SLQ_RG_ALL
+#undef SLQ_RG_CASE
+        return fail(SLQ_ERR_BAD_ARG, "row-group SpMM: unsupported tile");
     }
     const int32_t* ptr = transpose ? op->t_ptr : op->a_ptr;
     const int32_t* ind = transpose ? op->t_ind : op->a_ind;
@@ -955,6 +1001,48 @@ slq_status op_spmm(Launcher& L, const slq_op* op, int transpose, int b, const VT
     *grid_out = grid;
     return spmm<VT>(L, grid, ptr, ind, val, rows, b, X, sx, shift, Y, Z, zc, zs, epi, partials,
                     op->nnz, xrows);
+}
+
+int log2_width(int b)
+{
+    int lg = 0;
+    while ((1 << lg) < b) ++lg;
+    return lg;
+}
+
+// Operator product on a block.  An autotuned choice (slq_operator_tune /
+// slq_operator_set_variant) for this width and direction is used where one
+// is set; the built-in choice otherwise (and for a tuned TMA candidate when
+// the caller has no tensor map).  *grid_out receives the number of partial
+// rows the launch writes.
+template <typename VT>
+slq_status op_spmm(Launcher& L, const slq_op* op, int transpose, int b, const VT* X,
+                   const double* sx, double shift, VT* Y, const VT* Z, const double* zc,
+                   const double* zs, int epi, double* partials, int* grid_out,
+                   const CUtensorMap* xmap = nullptr, int32_t* error = nullptr)
+{
+    SpmmCand cands[SLQ_TUNE_MAX_CANDIDATES];
+    const int nc = spmm_candidates<VT>(op, transpose, b, cands);
+    const int lg = log2_width(b);
+    const int ti = (lg <= 10) ? op->tuned[transpose ? 1 : 0][lg] : -1;
+    if (ti >= 0 && ti < nc && (cands[ti].kind != CAND_TMA || (xmap && error)))
+        return spmm_cand<VT>(L, op, transpose, cands[ti], b, X, sx, shift, Y, Z, zc, zs, epi,
+                             partials, grid_out, xmap, error);
+    // built-in choice: TMA, then the row-group tile with the widest LV, then CSR
+    int pick = 0;
+    for (int i = 0; i < nc; ++i)
+    {
+        if (cands[i].kind == CAND_TMA && !(xmap && error)) continue;
+        if (cands[i].kind == CAND_TMA)
+        {
+            pick = i;
+            break;
+        }
+        if (cands[i].kind == CAND_RG && (cands[pick].kind != CAND_RG || cands[i].lv > cands[pick].lv))
+            pick = i;
+    }
+    return spmm_cand<VT>(L, op, transpose, cands[pick], b, X, sx, shift, Y, Z, zc, zs, epi,
+                         partials, grid_out, xmap, error);
 }
 
 // TMA-streamed pass (k_stream): MODE 0 = update + inner products,
@@ -1353,6 +1441,26 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
     return SLQ_OK;
 }
 
+// Parity stream set-up of a run: start state of its probe 0, the advance
+// polynomial between consecutive probes and the per-chunk polynomials.
+slq_status parity_setup(const slq_params* p, const RunPlan& r, uint64_t* cur, Poly256* advance,
+                        std::vector<uint64_t>* polys)
+{
+    if (!self_check()) return fail(SLQ_ERR_CUDA, "xoshiro256 jump polynomial self-check failed");
+    stream_state(p->seed, cur);
+    jump_ahead(cur, static_cast<uint64_t>(p->first_probe) * static_cast<uint64_t>(r.wpp));
+    *advance = jump_poly(static_cast<uint64_t>(r.wpp));
+    polys->assign(static_cast<size_t>(r.nchunks) * 4, 0);
+    const Poly256 step = jump_poly(static_cast<uint64_t>(r.cw));
+    Poly256 acc = {{1, 0, 0, 0}};
+    for (int cidx = 0; cidx < r.nchunks; ++cidx)
+    {
+        for (int k = 0; k < 4; ++k) (*polys)[static_cast<size_t>(cidx) * 4 + k] = acc.w[k];
+        acc = poly_mulmod(acc, step);
+    }
+    return SLQ_OK;
+}
+
 template <typename VT>
 slq_status run_typed(slq_op* op, const slq_params* p, const double* parameters, int q,
                      void* workspace, size_t workspace_bytes, cudaStream_t st, slq_result* res)
@@ -1386,21 +1494,10 @@ slq_status run_typed(slq_op* op, const slq_params* p, const double* parameters, 
     // advance polynomials
     uint64_t cur[4] = {0, 0, 0, 0};
     Poly256 advance = {{1, 0, 0, 0}};
+    std::vector<uint64_t> polys;
     if (p->rng == SLQ_RNG_PARITY)
     {
-        if (!self_check())
-            return fail(SLQ_ERR_CUDA, "xoshiro256 jump polynomial self-check failed");
-        stream_state(p->seed, cur);
-        jump_ahead(cur, static_cast<uint64_t>(p->first_probe) * static_cast<uint64_t>(r.wpp));
-        advance = jump_poly(static_cast<uint64_t>(r.wpp));
-        std::vector<uint64_t> polys(static_cast<size_t>(r.nchunks) * 4);
-        Poly256 step = jump_poly(static_cast<uint64_t>(r.cw));
-        Poly256 acc = {{1, 0, 0, 0}};
-        for (int cidx = 0; cidx < r.nchunks; ++cidx)
-        {
-            for (int k = 0; k < 4; ++k) polys[static_cast<size_t>(cidx) * 4 + k] = acc.w[k];
-            acc = poly_mulmod(acc, step);
-        }
+        SLQ_TRY(parity_setup(p, r, cur, &advance, &polys));
         SLQ_CK(cudaMemcpyAsync(B.chunk_polys, polys.data(), polys.size() * sizeof(uint64_t),
                                cudaMemcpyHostToDevice, st));
     }
@@ -1577,6 +1674,601 @@ extern "C" slq_status slq_run(slq_op* op, const slq_params* p, const double* par
                                  result);
     return run_typed<float>(op, p, parameters, num_inquiries, workspace, workspace_bytes, st,
                             result);
+}
+
+// ---------------------------------------------------------------------------
+// SpMM autotuner
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~EventPair()
+    {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
+struct TuneBufs {
+    void* X;
+    void* Y;
+    double* sx;
+    double* partials;
+    int32_t* error;
+};
+
+void tune_layout(Carver& c, const slq_op* op, int width, int sms, TuneBufs* t)
+{
+    const size_t s = (op->dtype == SLQ_F64) ? 8 : 4;
+    const size_t len = static_cast<size_t>(std::max(op->nrows, op->ncols));
+    t->X = c.take<char>(len * width * s);
+    t->Y = c.take<char>(len * width * s);
+    t->sx = c.take<double>(width);
+    t->partials = c.take<double>(static_cast<size_t>(sms) * 4 * width);
+    t->error = c.take<int32_t>(1);
+}
+
+template <typename VT>
+slq_status tune_typed(slq_op* op, int width, int transpose, int reps, const TuneBufs& t,
+                      cudaStream_t st, slq_tune_result* res)
+{
+    Launcher L;
+    L.st = st;
+    SLQ_TRY(device_sms(&L.sms));
+    SpmmCand c[SLQ_TUNE_MAX_CANDIDATES];
+    const int nc = spmm_candidates<VT>(op, transpose, width, c);
+    const int64_t xrows = transpose ? op->nrows : op->ncols;
+    SLQ_CK(cudaMemsetAsync(t.X, 0, static_cast<size_t>(xrows) * width * sizeof(VT), st));
+    SLQ_CK(cudaMemsetAsync(t.error, 0, sizeof(int32_t), st));
+    k_fill_f64<<<(width + 255) / 256, 256, 0, st>>>(t.sx, width, 1.0);
+    SLQ_LAUNCH_CK();
+    CUtensorMap map;
+    bool have_map = false;
+    if constexpr (sizeof(VT) == 4)
+    {
+        if (width == 128 || width == 256)
+        {
+            SLQ_TRY(row_map(&map, static_cast<const float*>(t.X), xrows, width));
+            have_map = true;
+        }
+    }
+    EventPair ev;
+    SLQ_CK(cudaEventCreate(&ev.a));
+    SLQ_CK(cudaEventCreate(&ev.b));
+    res->width = width;
+    res->transpose = transpose;
+    res->num_candidates = nc;
+    res->chosen = 0;
+    for (int i = 0; i < SLQ_TUNE_MAX_CANDIDATES; ++i)
+    {
+        res->kind[i] = res->group_rows[i] = res->lanes_vec[i] = res->slices[i] = 0;
+        res->milliseconds[i] = 0.0;
+    }
+    for (int i = 0; i < nc; ++i)
+    {
+        int grid = 0;
+        auto launch = [&]() {
+            return spmm_cand<VT>(L, op, transpose, c[i], width, static_cast<const VT*>(t.X), t.sx,
+                                 0.0, static_cast<VT*>(t.Y), nullptr, nullptr, nullptr, 1,
+                                 t.partials, &grid, have_map ? &map : nullptr, t.error);
+        };
+        SLQ_TRY(launch());
+        SLQ_CK(cudaEventRecord(ev.a, st));
+        for (int r = 0; r < reps; ++r) SLQ_TRY(launch());
+        SLQ_CK(cudaEventRecord(ev.b, st));
+        SLQ_CK(cudaEventSynchronize(ev.b));
+        float ms = 0.0f;
+        SLQ_CK(cudaEventElapsedTime(&ms, ev.a, ev.b));
+        res->kind[i] = c[i].kind;
+        res->group_rows[i] = c[i].g;
+        res->lanes_vec[i] = c[i].lv;
+        res->slices[i] = c[i].ns;
+        res->milliseconds[i] = static_cast<double>(ms) / reps;
+        if (res->milliseconds[i] < res->milliseconds[res->chosen]) res->chosen = i;
+    }
+    int32_t herr = 0;
+    SLQ_CK(cudaMemcpy(&herr, t.error, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (herr) return fail(SLQ_ERR_TIMEOUT, "tune: a TMA SpMM gave up waiting for its copies");
+    op->tuned[transpose ? 1 : 0][log2_width(width)] = static_cast<int8_t>(res->chosen);
+    return SLQ_OK;
+}
+
+slq_status check_width(const slq_op* op, int width)
+{
+    if (!op) return fail(SLQ_ERR_BAD_ARG, "operator is NULL");
+    if (!is_pow2(width) || width > ((op->dtype == SLQ_F64) ? 512 : 1024))
+        return fail(SLQ_ERR_BAD_ARG, "width must be a power of two <= 1024 (512 for float64)");
+    return SLQ_OK;
+}
+
+}  // namespace
+
+extern "C" slq_status slq_operator_tune_workspace_bytes(const slq_op* op, int width,
+                                                        size_t* bytes)
+{
+    SLQ_TRY(check_width(op, width));
+    if (!bytes) return fail(SLQ_ERR_BAD_ARG, "bytes is NULL");
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
+    Carver c(nullptr, 0);
+    TuneBufs t;
+    tune_layout(c, op, width, sms, &t);
+    *bytes = c.off + 256;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_operator_tune(slq_op* op, int width, int transpose, int reps,
+                                        void* workspace, size_t workspace_bytes, void* stream,
+                                        slq_tune_result* result)
+{
+    SLQ_TRY(check_width(op, width));
+    if (!result) return fail(SLQ_ERR_BAD_ARG, "tune: result is NULL");
+    if (transpose && !op->t_ptr) return fail(SLQ_ERR_BAD_ARG, "tune: operator has no transpose");
+    if (reps < 1) return fail(SLQ_ERR_BAD_ARG, "tune: reps must be positive");
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
+    Carver c(workspace, workspace_bytes);
+    TuneBufs t;
+    tune_layout(c, op, width, sms, &t);
+    if (!workspace || !c.fits()) return fail(SLQ_ERR_WORKSPACE, "tune: workspace too small");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (op->dtype == SLQ_F64) return tune_typed<double>(op, width, transpose, reps, t, st, result);
+    return tune_typed<float>(op, width, transpose, reps, t, st, result);
+}
+
+extern "C" slq_status slq_operator_set_variant(slq_op* op, int width, int transpose,
+                                               int candidate)
+{
+    SLQ_TRY(check_width(op, width));
+    if (candidate < -1 || candidate >= SLQ_TUNE_MAX_CANDIDATES)
+        return fail(SLQ_ERR_BAD_ARG, "set_variant: candidate out of range");
+    if (candidate >= 0)
+    {
+        SpmmCand c[SLQ_TUNE_MAX_CANDIDATES];
+        const int nc = (op->dtype == SLQ_F64)
+                           ? spmm_candidates<double>(op, transpose, width, c)
+                           : spmm_candidates<float>(op, transpose, width, c);
+        if (candidate >= nc)
+            return fail(SLQ_ERR_BAD_ARG, "set_variant: no such candidate for this operator");
+    }
+    op->tuned[transpose ? 1 : 0][log2_width(width)] = static_cast<int8_t>(candidate);
+    return SLQ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched estimator: every probe block of every run recorded into one CUDA
+// graph, one branch per run, then the host stopping rule per run.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct BatchRun {
+    slq_op* op = nullptr;
+    slq_params p{};
+    RunPlan r{};
+    std::vector<double> params;
+    double shift = 0.0;
+    int nblocks = 0;
+    RunBufs B{};
+    // outputs (device, inside the batch's contiguous output region)
+    double* samples = nullptr;  // [max][q]
+    int32_t* size = nullptr;    // [max]
+    int32_t* status = nullptr;  // [max]
+    double* alpha = nullptr;    // [nblocks][m][b]
+    double* beta = nullptr;
+    int32_t* error = nullptr;
+    uint64_t* starts = nullptr;  // [nblocks][b][4]
+    int64_t launches = 0;
+};
+
+// Outputs of all runs first (one device-to-host copy brings them back), then
+// each run's working buffers.
+void batch_layout(Carver& c, std::vector<BatchRun>& runs, int sms, size_t* out_bytes)
+{
+    for (auto& R : runs)
+    {
+        const size_t mx = static_cast<size_t>(R.p.max_num_samples);
+        R.samples = c.take<double>(mx * R.r.q);
+        R.size = c.take<int32_t>(mx);
+        R.status = c.take<int32_t>(mx);
+        R.alpha = c.take<double>(static_cast<size_t>(R.nblocks) * R.r.m * R.r.b);
+        R.beta = c.take<double>(static_cast<size_t>(R.nblocks) * R.r.m * R.r.b);
+        R.error = c.take<int32_t>(1);
+    }
+    *out_bytes = (c.off + 255) & ~static_cast<size_t>(255);
+    for (auto& R : runs)
+    {
+        if (R.op->dtype == SLQ_F64) carve<double>(c, R.r, sms, &R.B);
+        else carve<float>(c, R.r, sms, &R.B);
+        R.B.error = R.error;
+        R.starts = c.take<uint64_t>(static_cast<size_t>(R.nblocks) * R.r.b * 4);
+    }
+}
+
+template <typename VT>
+slq_status batch_upload(BatchRun& R, cudaStream_t st)
+{
+    const RunPlan& r = R.r;
+    RunBufs& B = R.B;
+    SLQ_CK(cudaMemcpyAsync(B.params, R.params.data(), sizeof(double) * r.q,
+                           cudaMemcpyHostToDevice, st));
+    k_fill_f64<<<(r.b + 255) / 256, 256, 0, st>>>(B.negshift, r.b, -R.shift);
+    SLQ_LAUNCH_CK();
+    if (R.p.rng == SLQ_RNG_PARITY)
+    {
+        uint64_t cur[4];
+        Poly256 advance;
+        std::vector<uint64_t> polys;
+        SLQ_TRY(parity_setup(&R.p, r, cur, &advance, &polys));
+        SLQ_CK(cudaMemcpyAsync(B.chunk_polys, polys.data(), polys.size() * sizeof(uint64_t),
+                               cudaMemcpyHostToDevice, st));
+        std::vector<uint64_t> hs(static_cast<size_t>(R.nblocks) * r.b * 4, 0);
+        for (int s = 0; s < R.p.max_num_samples; ++s)
+        {
+            for (int k = 0; k < 4; ++k) hs[static_cast<size_t>(s) * 4 + k] = cur[k];
+            apply_poly(advance, cur);
+        }
+        SLQ_CK(cudaMemcpyAsync(R.starts, hs.data(), hs.size() * sizeof(uint64_t),
+                               cudaMemcpyHostToDevice, st));
+        // the copy reads a host vector that goes out of scope here
+        SLQ_CK(cudaStreamSynchronize(st));
+    }
+    return SLQ_OK;
+}
+
+// All probe blocks of one run on stream st (recorded into the graph).
+template <typename VT>
+slq_status batch_enqueue(BatchRun& R, cudaStream_t st, int sms)
+{
+    Launcher L;
+    L.st = st;
+    L.sms = sms;
+    const RunPlan& r = R.r;
+    const slq_params* p = &R.p;
+    const int max_s = p->max_num_samples;
+    const double s0 = 1.0 / std::sqrt(static_cast<double>(r.nv));
+    RunBufs B = R.B;
+    SLQ_CK(cudaMemsetAsync(R.error, 0, sizeof(int32_t), st));
+    for (int blk = 0; blk < R.nblocks; ++blk)
+    {
+        const int g = blk * r.b;
+        const int count = std::min(r.b, max_s - g);
+        B.starts = R.starts + static_cast<size_t>(blk) * r.b * 4;
+        SLQ_TRY(launch_probes<VT>(L, r, p->rng, p->seed, p->first_probe + g, count, B,
+                                  R.op->inv, static_cast<VT*>(B.V)));
+        k_init_block<<<(r.b + 127) / 128, 128, 0, st>>>(count, r.b, r.m, s0, B.scale_v, B.active,
+                                                        B.size);
+        SLQ_LAUNCH_CK();
+        ++L.launches;
+        SLQ_TRY(krylov_block<VT>(L, R.op, p, r, B, count, R.shift));
+        k_eig_quad<<<(count + 127) / 128, 128, 0, st>>>(
+            count, r.b, r.m, B.alpha, B.beta, B.size, r.gram == 1, p->func, p->exponent,
+            B.params, r.q, static_cast<double>(r.nv), R.samples + static_cast<size_t>(g) * r.q,
+            nullptr, nullptr, R.status + g);
+        SLQ_LAUNCH_CK();
+        ++L.launches;
+        const size_t ab = static_cast<size_t>(r.m) * r.b;
+        SLQ_CK(cudaMemcpyAsync(R.size + g, B.size, sizeof(int32_t) * count,
+                               cudaMemcpyDeviceToDevice, st));
+        SLQ_CK(cudaMemcpyAsync(R.alpha + blk * ab, B.alpha, sizeof(double) * ab,
+                               cudaMemcpyDeviceToDevice, st));
+        SLQ_CK(cudaMemcpyAsync(R.beta + blk * ab, B.beta, sizeof(double) * ab,
+                               cudaMemcpyDeviceToDevice, st));
+    }
+    R.launches = L.launches;
+    return SLQ_OK;
+}
+
+slq_status batch_plan(int count, slq_op* const* ops, const slq_params* params,
+                      const double* const* parameters, const int* num_inquiries,
+                      std::vector<BatchRun>* runs)
+{
+    if (count < 1 || !ops || !params || !num_inquiries)
+        return fail(SLQ_ERR_BAD_ARG, "batch: count, ops, params and num_inquiries are required");
+    runs->resize(count);
+    for (int i = 0; i < count; ++i)
+    {
+        BatchRun& R = (*runs)[i];
+        if (!ops[i]) return fail(SLQ_ERR_BAD_ARG, "batch: operator " + std::to_string(i) + " is NULL");
+        R.op = ops[i];
+        R.p = params[i];
+        const int q = num_inquiries[i];
+        SLQ_TRY(make_plan(R.op, &R.p, q, &R.r));
+        R.params.assign(q, 0.0);
+        if (R.op->affine && parameters && parameters[i])
+            for (int j = 0; j < q; ++j) R.params[j] = parameters[i][j];
+        R.shift = R.op->affine ? R.params[0] : 0.0;
+        R.nblocks = (R.p.max_num_samples + R.r.b - 1) / R.r.b;
+    }
+    return SLQ_OK;
+}
+
+// Reference stopping rule over a run's samples, in probe order, into res
+// (the same bookkeeping as run_typed's sample loop).
+slq_status batch_replay(const BatchRun& R, const char* host, const char* dev_base, float ms,
+                        slq_result* res)
+{
+    auto hp = [&](const void* d) { return host + (static_cast<const char*>(d) - dev_base); };
+    const double* hs = reinterpret_cast<const double*>(hp(R.samples));
+    const int32_t* hsize = reinterpret_cast<const int32_t*>(hp(R.size));
+    const int32_t* hstat = reinterpret_cast<const int32_t*>(hp(R.status));
+    const double* ha = reinterpret_cast<const double*>(hp(R.alpha));
+    const double* hb = reinterpret_cast<const double*>(hp(R.beta));
+    const int32_t herr = *reinterpret_cast<const int32_t*>(hp(R.error));
+    const slq_params* p = &R.p;
+    const int max_s = p->max_num_samples;
+    const int q = R.r.q;
+    const int m = R.r.m;
+    const int b = R.r.b;
+    if (!res->trace || !res->error || !res->samples || !res->processed_samples_indices ||
+        !res->num_samples_used || !res->num_outliers || !res->converged)
+        return fail(SLQ_ERR_BAD_ARG, "batch: result arrays missing");
+    for (int64_t i = 0; i < static_cast<int64_t>(max_s) * q; ++i) res->samples[i] = NAN;
+    for (int i = 0; i < max_s; ++i)
+    {
+        res->processed_samples_indices[i] = 0;
+        if (res->lanczos_size) res->lanczos_size[i] = 0;
+    }
+    for (int j = 0; j < q; ++j)
+    {
+        res->converged[j] = 0;
+        res->num_samples_used[j] = 0;
+        res->num_outliers[j] = 0;
+        res->trace[j] = NAN;
+        res->error[j] = NAN;
+    }
+    if (res->alpha)
+        for (int64_t i = 0; i < static_cast<int64_t>(max_s) * m; ++i) res->alpha[i] = NAN;
+    if (res->beta)
+        for (int64_t i = 0; i < static_cast<int64_t>(max_s) * m; ++i) res->beta[i] = NAN;
+    res->num_blocks = R.nblocks;
+    res->num_probes_computed = max_s;
+    res->gpu_launches = R.launches;
+    res->alg_wall_time = ms * 1e-3f;
+    res->all_converged = 0;
+    if (herr) return fail(SLQ_ERR_TIMEOUT, "a streaming kernel gave up waiting for its copies");
+
+    int nproc = 0;
+    int all = 0;
+    bool eig_failed = false;
+    for (int s = 0; s < max_s && !all; ++s)
+    {
+        const int blk = s / b;
+        const int pi = s % b;
+        for (int j = 0; j < q; ++j)
+            res->samples[static_cast<int64_t>(s) * q + j] = hs[static_cast<size_t>(s) * q + j];
+        if (res->lanczos_size) res->lanczos_size[s] = hsize[s];
+        if (hstat[s] == 2) eig_failed = true;
+        const size_t base = static_cast<size_t>(blk) * m * b;
+        for (int i = 0; i < m; ++i)
+        {
+            if (res->alpha)
+                res->alpha[static_cast<int64_t>(s) * m + i] =
+                    (i < hsize[s]) ? ha[base + static_cast<size_t>(i) * b + pi] : NAN;
+            if (res->beta)
+                res->beta[static_cast<int64_t>(s) * m + i] =
+                    (i < hsize[s]) ? hb[base + static_cast<size_t>(i) * b + pi] : NAN;
+        }
+        if (R.op->affine && q > 1)
+            for (int j = 0; j < q; ++j) res->converged[j] = 0;
+        res->processed_samples_indices[nproc++] = s;
+        all = slq_check_convergence(res->samples, q, p->min_num_samples,
+                                    res->processed_samples_indices, nproc, p->confidence_level,
+                                    p->error_atol, p->error_rtol, res->error,
+                                    res->num_samples_used, res->converged);
+    }
+    slq_average_estimates(p->confidence_level, p->outlier_significance_level, q, max_s,
+                          res->num_samples_used, res->processed_samples_indices, res->samples,
+                          res->num_outliers, res->trace, res->error);
+    res->all_converged = all;
+    if (eig_failed) return fail(SLQ_ERR_EIGEN, "tridiagonal eigen-solve did not converge");
+    return SLQ_OK;
+}
+
+}  // namespace
+
+struct slq_batch {
+    std::vector<BatchRun> runs;
+    char* out_dev = nullptr;
+    size_t out_bytes = 0;
+    std::vector<char> out_host;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t kernels = 0;
+    int64_t nodes = 0;
+    ~slq_batch()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+namespace {
+
+// Streams and events of one capture, released on every path.
+struct CaptureRes {
+    cudaStream_t origin = nullptr;
+    std::vector<cudaStream_t> br;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    ~CaptureRes()
+    {
+        for (auto e : join)
+            if (e) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        for (auto s : br)
+            if (s) cudaStreamDestroy(s);
+        if (origin) cudaStreamDestroy(origin);
+    }
+};
+
+slq_status batch_capture(slq_batch* bt, int sms)
+{
+    const int count = static_cast<int>(bt->runs.size());
+    const int nbr = std::min(count, 64);
+    CaptureRes cr;
+    SLQ_CK(cudaStreamCreateWithFlags(&cr.origin, cudaStreamNonBlocking));
+    cr.br.assign(nbr, nullptr);
+    cr.join.assign(nbr, nullptr);
+    for (int k = 0; k < nbr; ++k)
+    {
+        SLQ_CK(cudaStreamCreateWithFlags(&cr.br[k], cudaStreamNonBlocking));
+        SLQ_CK(cudaEventCreateWithFlags(&cr.join[k], cudaEventDisableTiming));
+    }
+    SLQ_CK(cudaEventCreateWithFlags(&cr.fork, cudaEventDisableTiming));
+
+    const bool prof = g_prof.on;
+    g_prof.on = false;  // no timing events inside the graph
+    SLQ_CK(cudaStreamBeginCapture(cr.origin, cudaStreamCaptureModeRelaxed));
+    slq_status st = SLQ_OK;
+    if (cudaEventRecord(cr.fork, cr.origin) != cudaSuccess)
+        st = fail(SLQ_ERR_CUDA, "batch: capture fork failed");
+    for (int k = 0; k < nbr && st == SLQ_OK; ++k)
+        if (cudaStreamWaitEvent(cr.br[k], cr.fork, 0) != cudaSuccess)
+            st = fail(SLQ_ERR_CUDA, "batch: capture fork failed");
+    // longest runs first so that each branch's queue is balanced
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) order[i] = i;
+    std::vector<double> cost(count);
+    for (int i = 0; i < count; ++i)
+    {
+        const BatchRun& R = bt->runs[i];
+        cost[i] = double(R.op->nnz + R.r.nv) * R.p.max_num_samples * R.r.m;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<double> load(nbr, 0.0);
+    for (int oi = 0; oi < count && st == SLQ_OK; ++oi)
+    {
+        const int i = order[oi];
+        const int k = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+        load[k] += cost[i];
+        BatchRun& R = bt->runs[i];
+        st = (R.op->dtype == SLQ_F64) ? batch_enqueue<double>(R, cr.br[k], sms)
+                                      : batch_enqueue<float>(R, cr.br[k], sms);
+    }
+    // join every branch (also after an error, so that the capture ends cleanly)
+    for (int k = 0; k < nbr; ++k)
+    {
+        cudaEventRecord(cr.join[k], cr.br[k]);
+        cudaStreamWaitEvent(cr.origin, cr.join[k], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(cr.origin, &graph);
+    g_prof.on = prof;
+    if (st != SLQ_OK)
+    {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return st;
+    }
+    if (ee != cudaSuccess || !graph)
+    {
+        if (graph) cudaGraphDestroy(graph);
+        return fail(SLQ_ERR_CUDA, std::string("batch: stream capture failed: ") +
+                                      cudaGetErrorString(ee));
+    }
+    bt->graph = graph;
+    size_t nn = 0;
+    SLQ_CK(cudaGraphGetNodes(graph, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    SLQ_CK(cudaGraphGetNodes(graph, nodes.data(), &nn));
+    int64_t kn = 0;
+    for (auto nd : nodes)
+    {
+        cudaGraphNodeType ty;
+        SLQ_CK(cudaGraphNodeGetType(nd, &ty));
+        if (ty == cudaGraphNodeTypeKernel) ++kn;
+    }
+    bt->nodes = static_cast<int64_t>(nn);
+    bt->kernels = kn;
+    SLQ_CK(cudaGraphInstantiate(&bt->exec, graph, 0));
+    return SLQ_OK;
+}
+
+}  // namespace
+
+extern "C" slq_status slq_batch_workspace_bytes(int count, slq_op* const* ops,
+                                                const slq_params* params,
+                                                const int* num_inquiries, size_t* bytes)
+{
+    if (!bytes) return fail(SLQ_ERR_BAD_ARG, "bytes is NULL");
+    std::vector<BatchRun> runs;
+    SLQ_TRY(batch_plan(count, ops, params, nullptr, num_inquiries, &runs));
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
+    Carver c(nullptr, 0);
+    size_t ob = 0;
+    batch_layout(c, runs, sms, &ob);
+    *bytes = c.off + 256;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_batch_create(int count, slq_op* const* ops, const slq_params* params,
+                                       const double* const* parameters,
+                                       const int* num_inquiries, void* workspace,
+                                       size_t workspace_bytes, void* stream, slq_batch** out)
+{
+    if (!out) return fail(SLQ_ERR_BAD_ARG, "batch: out is NULL");
+    *out = nullptr;
+    std::unique_ptr<slq_batch> bt(new slq_batch());
+    SLQ_TRY(batch_plan(count, ops, params, parameters, num_inquiries, &bt->runs));
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
+    Carver c(workspace, workspace_bytes);
+    batch_layout(c, bt->runs, sms, &bt->out_bytes);
+    if (!workspace || !c.fits())
+        return fail(SLQ_ERR_WORKSPACE, "batch: workspace too small (need " +
+                                           std::to_string(c.off) + " bytes)");
+    bt->out_dev = static_cast<char*>(workspace);
+    bt->out_host.resize(bt->out_bytes);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    for (auto& R : bt->runs)
+        SLQ_TRY((R.op->dtype == SLQ_F64) ? batch_upload<double>(R, st) : batch_upload<float>(R, st));
+    SLQ_CK(cudaStreamSynchronize(st));
+    SLQ_TRY(batch_capture(bt.get(), sms));
+    *out = bt.release();
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_batch_run(slq_batch* bt, void* stream, slq_result* results)
+{
+    if (!bt || !results) return fail(SLQ_ERR_BAD_ARG, "batch_run: NULL argument");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    EventPair ev;
+    SLQ_CK(cudaEventCreate(&ev.a));
+    SLQ_CK(cudaEventCreate(&ev.b));
+    SLQ_CK(cudaEventRecord(ev.a, st));
+    SLQ_CK(cudaGraphLaunch(bt->exec, st));
+    SLQ_CK(cudaEventRecord(ev.b, st));
+    SLQ_CK(cudaMemcpyAsync(bt->out_host.data(), bt->out_dev, bt->out_bytes,
+                           cudaMemcpyDeviceToHost, st));
+    SLQ_CK(cudaStreamSynchronize(st));
+    float ms = 0.0f;
+    SLQ_CK(cudaEventElapsedTime(&ms, ev.a, ev.b));
+    slq_status worst = SLQ_OK;
+    for (size_t i = 0; i < bt->runs.size(); ++i)
+    {
+        const slq_status s =
+            batch_replay(bt->runs[i], bt->out_host.data(), bt->out_dev, ms, &results[i]);
+        if (s != SLQ_OK && (worst == SLQ_OK || worst == SLQ_ERR_EIGEN)) worst = s;
+    }
+    return worst;
+}
+
+extern "C" slq_status slq_batch_info(const slq_batch* bt, int64_t* kernels, int64_t* nodes)
+{
+    if (!bt) return fail(SLQ_ERR_BAD_ARG, "batch_info: batch is NULL");
+    if (kernels) *kernels = bt->kernels;
+    if (nodes) *nodes = bt->nodes;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_batch_destroy(slq_batch* bt)
+{
+    delete bt;
+    return SLQ_OK;
 }
 
 // ---------------------------------------------------------------------------

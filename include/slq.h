@@ -182,6 +182,79 @@ slq_status slq_run(slq_op* op, const slq_params* p, const double* parameters,
                    int num_inquiries, void* workspace, size_t workspace_bytes,
                    void* stream, slq_result* result);
 
+/* SpMM autotuner (no counterpart in the reference, whose products are one
+ * cusparseSpMV per probe, cusparse_interface.cu:243).  The candidates for a
+ * block width are the storage formats the operator holds crossed with their
+ * tiles: CSR warp per row; row-group (the operator's group_rows rows sharing
+ * a union of columns) with LV probes per lane and NS warps per row group,
+ * b = 32 LV NS; and, in FP32 with 8-row groups at b = 128 or 256, the
+ * row-group kernel whose X rows arrive by TMA gathers.  slq_operator_tune
+ * times every candidate (reps launches each, CUDA events, after one untimed
+ * launch) on workspace blocks and makes the fastest the operator's choice
+ * for that width and direction; every later product the operator takes at
+ * that width (slq_run, slq_batch_*, slq_operator_dot) uses it.  Results of
+ * different candidates agree to rounding, not bitwise (their partial-sum
+ * orders differ). */
+#define SLQ_TUNE_MAX_CANDIDATES 16
+
+typedef struct {
+    int32_t width;
+    int32_t transpose;
+    int32_t num_candidates;
+    int32_t chosen;                                /* fastest candidate      */
+    int32_t kind[SLQ_TUNE_MAX_CANDIDATES];         /* 0 CSR, 1 row-group,    */
+                                                   /* 2 row-group + TMA      */
+    int32_t group_rows[SLQ_TUNE_MAX_CANDIDATES];
+    int32_t lanes_vec[SLQ_TUNE_MAX_CANDIDATES];    /* LV probes per lane     */
+    int32_t slices[SLQ_TUNE_MAX_CANDIDATES];       /* NS warps per row group */
+    double milliseconds[SLQ_TUNE_MAX_CANDIDATES];  /* mean per launch        */
+} slq_tune_result;
+
+slq_status slq_operator_tune_workspace_bytes(const slq_op* op, int width,
+                                             size_t* bytes);
+slq_status slq_operator_tune(slq_op* op, int width, int transpose, int reps,
+                             void* workspace, size_t workspace_bytes,
+                             void* stream, slq_tune_result* result);
+/* Force candidate `candidate` (an index as reported by slq_operator_tune) for
+ * this width and direction; -1 restores the built-in choice. */
+slq_status slq_operator_set_variant(slq_op* op, int width, int transpose,
+                                    int candidate);
+
+/* Batched estimator (no counterpart in the reference, which runs one matrix
+ * per call).  A batch plan holds `count` independent estimator runs -- any
+ * mix of operators, sizes, dtypes, functions and settings -- and records
+ * every probe block of every run into one CUDA graph, each run on its own
+ * branch so that runs of small matrices overlap on the device.  A run
+ * computes all max_num_samples probes (there is no host decision inside the
+ * graph) and the host then applies the reference's sequential stopping rule
+ * to them, so each slq_result equals that of slq_run with the same operator,
+ * settings and SpMM choice: the samples it would have used, its estimate,
+ * error, sample counts and outliers.  Differences from slq_run's result:
+ * num_blocks and num_probes_computed count every block, alg_wall_time is the
+ * time of the whole graph, and gpu_launches counts the run's kernels in the
+ * graph.  parameters[i] (host, num_inquiries[i] values) are run i's t values
+ * (NULL for a non-affine operator).  The plan keeps pointers into the
+ * workspace and the operators; both must outlive it.  slq_batch_create
+ * synchronizes `stream` (it uploads the probe start states). */
+typedef struct slq_batch slq_batch;
+
+slq_status slq_batch_workspace_bytes(int count, slq_op* const* ops,
+                                     const slq_params* params,
+                                     const int* num_inquiries, size_t* bytes);
+slq_status slq_batch_create(int count, slq_op* const* ops,
+                            const slq_params* params,
+                            const double* const* parameters,
+                            const int* num_inquiries, void* workspace,
+                            size_t workspace_bytes, void* stream,
+                            slq_batch** out);
+/* One launch of the plan's graph on `stream`, then the host stopping rule
+ * into results[0..count). */
+slq_status slq_batch_run(slq_batch* batch, void* stream, slq_result* results);
+/* Kernel nodes in the plan's graph. */
+slq_status slq_batch_info(const slq_batch* batch, int64_t* kernels,
+                          int64_t* nodes);
+slq_status slq_batch_destroy(slq_batch* batch);
+
 /* Probe generator alone: writes probes [first, first+count) of the stream for
  * (seed, rng) as a row-major block [len][width] of +-1 in the given dtype
  * (columns >= count are zero).  Replaces

@@ -190,3 +190,18 @@ def test_correlation_matrix_matches_brute_force():
     K[K < 0.05] = 0.0
     K += 1e-3 * np.eye(300)
     np.testing.assert_allclose(A, K, rtol=1e-14, atol=1e-15)
+
+
+def test_batch_and_tuner_reject_bad_arguments_without_a_gpu(lib):
+    nb = ctypes.c_size_t(0)
+    # argument checks come before any CUDA call
+    assert lib.slq_batch_workspace_bytes(0, None, None, None,
+                                         ctypes.byref(nb)) == 1
+    assert lib.slq_batch_create(0, None, None, None, None, None, 0, None,
+                                None) == 1
+    assert lib.slq_batch_run(None, None, None) == 1
+    assert lib.slq_batch_info(None, None, None) == 1
+    assert lib.slq_batch_destroy(None) == 0
+    assert lib.slq_operator_set_variant(None, 64, 0, 0) == 1
+    assert lib.slq_operator_tune_workspace_bytes(None, 64,
+                                                 ctypes.byref(nb)) == 1
