@@ -10,7 +10,8 @@ buffers.
 """
 
 from .__version__ import __version__
-from ._functions import logdet, traceinv, trace, schatten
+from ._functions import (logdet, traceinv, trace, schatten, trexp,
+                         trlinfrac, eigencount, density)
 from ._trace_estimator import EngineOptions
 from .linear_operator import (LinearOperator, Matrix, AffineMatrixFunction,
                               GramAffineMatrixFunction)
@@ -18,6 +19,7 @@ from .sample_matrices import (toeplitz, toeplitz_logdet, toeplitz_trace,
                               toeplitz_traceinv, correlation_matrix)
 
 __all__ = ["__version__", "logdet", "traceinv", "trace", "schatten",
+           "trexp", "trlinfrac", "eigencount", "density",
            "EngineOptions", "LinearOperator", "Matrix",
            "AffineMatrixFunction", "GramAffineMatrixFunction", "toeplitz", "toeplitz_logdet",
            "toeplitz_trace", "toeplitz_traceinv", "correlation_matrix"]

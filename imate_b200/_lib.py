@@ -19,7 +19,8 @@ STATUS_NAMES = {
 }
 SLQ_F32, SLQ_F64 = 0, 1
 SLQ_CSR, SLQ_CSC = 0, 1
-FUNC_IDS = {"log": 0, "inv": 1, "id": 2}
+FUNC_IDS = {"log": 0, "inv": 1, "id": 2, "exp": 3, "linfrac": 4,
+            "indicator": 5, "gaussian": 6, "smoothstep": 7}
 RNG_IDS = {"parity": 0, "fast": 1}
 MAX_DEGREE = 256
 
@@ -71,6 +72,7 @@ class SlqParams(ctypes.Structure):
         ("block_size", ctypes.c_int),
         ("rng", ctypes.c_int),
         ("first_probe", ctypes.c_int64),
+        ("func_coeff", ctypes.c_double * 4),
     ]
 
 

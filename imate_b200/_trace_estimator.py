@@ -244,7 +244,7 @@ def prepare(A, parameters, func, gram, exponent, min_num_samples,
             max_num_samples, error_atol, error_rtol, confidence_level,
             outlier_significance_level, lanczos_degree, lanczos_tol,
             orthogonalize, seed, num_threads, num_gpu_devices, verbose, plot,
-            gpu, options=None):
+            gpu, options=None, func_coeff=None):
     """Argument checks and set-up of one estimate (the part of
     ``trace_estimator.pyx:38-260`` before the sample loop).  Returns a job
     whose ``runs`` (one per group of inquiries) are executed by ``slq_run``
@@ -313,6 +313,9 @@ def prepare(A, parameters, func, gram, exponent, min_num_samples,
         groups = [list(range(num_inquiries))]
 
     m = int(lanczos_degree)
+    coeff = [0.0] * 4
+    if func_coeff is not None:
+        coeff[:len(func_coeff)] = [float(c) for c in func_coeff]
     J.Aop = Aop
     J.dev_op = Aop.get_device_operator(need_transpose=bool(gram) or normal)
     gram_mode = 2 if normal else int(bool(gram))
@@ -330,7 +333,8 @@ def prepare(A, parameters, func, gram, exponent, min_num_samples,
             confidence_level=float(confidence_level),
             outlier_significance_level=float(outlier_significance_level),
             block_size=options.block_size, rng=_lib.RNG_IDS[options.rng],
-            first_probe=options.first_probe))
+            first_probe=options.first_probe,
+            func_coeff=(ctypes.c_double * 4)(*coeff)))
         J.t_groups.append(np.ascontiguousarray(t_values[group],
                                                dtype=np.float64))
     J.options = options
@@ -577,15 +581,16 @@ def trace_estimator(A, parameters, func, gram, exponent, min_num_samples,
                     confidence_level, outlier_significance_level,
                     lanczos_degree, lanczos_tol, orthogonalize, seed,
                     num_threads, num_gpu_devices, verbose, plot, gpu,
-                    options=None):
+                    options=None, func_coeff=None):
     """SLQ estimate of trace(f(A^p)) (or of f((A^T A)^p) with gram) on the
-    GPU.  ``func`` is 'log', 'inv' or 'id'.  Returns (trace, info) like
-    ``trace_estimator.pyx``."""
+    GPU.  ``func`` is a key of ``_lib.FUNC_IDS`` ('log', 'inv', 'id', 'exp',
+    'linfrac', 'indicator', 'gaussian', 'smoothstep') with its coefficients
+    in ``func_coeff``.  Returns (trace, info) like ``trace_estimator.pyx``."""
     J = prepare(A, parameters, func, gram, exponent, min_num_samples,
                 max_num_samples, error_atol, error_rtol, confidence_level,
                 outlier_significance_level, lanczos_degree, lanczos_tol,
                 orthogonalize, seed, num_threads, num_gpu_devices, verbose,
-                plot, gpu, options)
+                plot, gpu, options, func_coeff)
     run_job(J)
     return finish(J)
 

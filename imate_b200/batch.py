@@ -28,7 +28,9 @@ from ._trace_estimator import (EngineOptions, prepare, run_outputs, collect,
 __all__ = ["BatchPlan", "autotune", "tune_operator", "logdet_batch",
            "traceinv_batch", "trace_batch"]
 
-_FUNC_OF = {"logdet": "log", "traceinv": "inv", "trace": "id"}
+_FUNC_OF = {"logdet": "log", "traceinv": "inv", "trace": "id",
+            "trexp": "exp", "trlinfrac": "linfrac", "eigencount": "indicator",
+            "density": "gaussian"}
 
 
 def tune_operator(dev_op, width, transpose=False, reps=5):
@@ -100,12 +102,14 @@ class BatchPlan:
     """Many SLQ estimates recorded into one CUDA graph.
 
     ``estimates`` is a list of dicts, one per estimate, with keys ``func``
-    ('logdet', 'traceinv' or 'trace'), ``A`` (matrix or operator), optional
-    ``gram`` and ``p``, any of imate's SLQ keyword arguments, and optionally
-    ``engine`` (EngineOptions).  ``autotune=True`` tunes each operator's SpMM
-    and block width first (and overrides the estimate's block size);
-    otherwise every operator keeps its current choice.  ``gpu=True`` is
-    implied.
+    ('logdet', 'traceinv', 'trace', 'trexp', 'trlinfrac', 'eigencount' or
+    'density'), ``A`` (matrix or operator), optional ``gram``, ``p`` and
+    ``func_coeff`` (the function's coefficients: trexp [c], trlinfrac
+    [a, b, c, d], eigencount [lo, hi], density [mu, sigma]), any of imate's
+    SLQ keyword arguments, and optionally ``engine`` (EngineOptions).
+    ``autotune=True`` tunes each operator's SpMM and block width first (and
+    overrides the estimate's block size); otherwise every operator keeps its
+    current choice.  ``gpu=True`` is implied.
     """
 
     def __init__(self, estimates, autotune=True, tune_reps=5):
@@ -121,6 +125,7 @@ class BatchPlan:
             gram = bool(est.pop("gram", False))
             p = est.pop("p", 1.0)
             engine = est.pop("engine", None) or EngineOptions()
+            coeff = est.pop("func_coeff", None)
             kw = dict(_SLQ_DEFAULTS)
             kw["gpu"] = True
             unknown = set(est) - set(kw)
@@ -136,7 +141,7 @@ class BatchPlan:
                         kw["lanczos_degree"], kw["lanczos_tol"],
                         kw["orthogonalize"], kw["seed"], kw["num_threads"],
                         kw["num_gpu_devices"], kw["verbose"], kw["plot"],
-                        kw["gpu"], engine)
+                        kw["gpu"], engine, coeff)
             if autotune:
                 key = (id(J.dev_op), J.params[0].gram, J.max_num_samples)
                 if key not in tuned:

@@ -1170,7 +1170,7 @@ slq_status make_plan(const slq_op* op, const slq_params* p, int q, RunPlan* r)
     if (p->min_num_samples < 1 || p->max_num_samples < 1 ||
         p->min_num_samples > p->max_num_samples)
         return fail(SLQ_ERR_BAD_ARG, "need 1 <= min_num_samples <= max_num_samples");
-    if (p->func < SLQ_FUNC_LOG || p->func > SLQ_FUNC_ID)
+    if (p->func < SLQ_FUNC_LOG || p->func > SLQ_FUNC_SMOOTHSTEP)
         return fail(SLQ_ERR_BAD_ARG, "unknown matrix function");
     if (p->seed < 0) return fail(SLQ_ERR_BAD_ARG, "seed must be >= 0");
     if (p->first_probe < 0) return fail(SLQ_ERR_BAD_ARG, "first_probe must be >= 0");
@@ -1247,6 +1247,11 @@ void carve(Carver& c, const RunPlan& r, int sms, RunBufs* B)
     B->params = c.take<double>(r.q);
     B->starts = c.take<uint64_t>(static_cast<size_t>(r.b) * 4);
     B->chunk_polys = c.take<uint64_t>(static_cast<size_t>(r.nchunks) * 4);
+}
+
+double4 func_coeff(const slq_params* p)
+{
+    return make_double4(p->func_coeff[0], p->func_coeff[1], p->func_coeff[2], p->func_coeff[3]);
 }
 
 template <typename VT>
@@ -1570,8 +1575,9 @@ slq_status run_typed(slq_op* op, const slq_params* p, const double* parameters, 
         {
         ProfScope prof(SLQ_K_EIG, double(m) * b * 16.0 + double(count) * q * 8.0, st);
         k_eig_quad<<<(count + 127) / 128, 128, 0, st>>>(
-            count, b, m, B.alpha, B.beta, B.size, r.gram == 1, p->func, p->exponent, B.params, q,
-            static_cast<double>(r.nv), B.samples, nullptr, nullptr, B.status);
+            count, b, m, B.alpha, B.beta, B.size, r.gram == 1, p->func, func_coeff(p),
+            p->exponent, B.params, q, static_cast<double>(r.nv), B.samples, nullptr, nullptr,
+            B.status);
         SLQ_LAUNCH_CK();
         ++L.launches;
         }
@@ -1944,8 +1950,8 @@ slq_status batch_enqueue(BatchRun& R, cudaStream_t st, int sms)
         ++L.launches;
         SLQ_TRY(krylov_block<VT>(L, R.op, p, r, B, count, R.shift));
         k_eig_quad<<<(count + 127) / 128, 128, 0, st>>>(
-            count, r.b, r.m, B.alpha, B.beta, B.size, r.gram == 1, p->func, p->exponent,
-            B.params, r.q, static_cast<double>(r.nv), R.samples + static_cast<size_t>(g) * r.q,
+            count, r.b, r.m, B.alpha, B.beta, B.size, r.gram == 1, p->func, func_coeff(p),
+            p->exponent, B.params, r.q, static_cast<double>(r.nv), R.samples + static_cast<size_t>(g) * r.q,
             nullptr, nullptr, R.status + g);
         SLQ_LAUNCH_CK();
         ++L.launches;
@@ -2493,8 +2499,8 @@ extern "C" slq_status slq_nodes_weights(const double* alpha, const double* beta,
         return fail(SLQ_ERR_BAD_ARG, "nodes_weights: bad argument");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     k_eig_quad<<<(count + 127) / 128, 128, 0, st>>>(count, count, m, alpha, beta, sizes, gram, 0,
-                                                   1.0, nullptr, 0, 1.0, nullptr, theta, tau,
-                                                   status);
+                                                   make_double4(0.0, 0.0, 0.0, 0.0), 1.0, nullptr,
+                                                   0, 1.0, nullptr, theta, tau, status);
     SLQ_LAUNCH_CK();
     return SLQ_OK;
 }

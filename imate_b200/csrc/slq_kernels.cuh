@@ -601,11 +601,26 @@ k_finalize(const double* __restrict__ partials, int nparts, int cols, int mode,
 
 constexpr int EIG_MAX = 256;
 
-__device__ __forceinline__ double apply_func(int func, double x)
+// f at a node (imate/functions/*.cpp; coefficients c as in slq_func)
+__device__ __forceinline__ double apply_func(int func, double x, const double4& c)
 {
-    if (func == 0) return log(x);
-    if (func == 1) return 1.0 / x;
-    return x;
+    switch (func)
+    {
+        case 0: return log(x);
+        case 1: return 1.0 / x;
+        case 3: return exp(x * c.x);
+        case 4: return (c.x * x + c.y) / (c.z * x + c.w);
+        case 5: return (x < c.x || x > c.y) ? 0.0 : 1.0;
+        case 6:
+        {
+            // 0.5 * M_SQRT1_2 * M_2_SQRTPI / sigma = 1 / (sigma sqrt(2 pi))
+            const double u = (x - c.x) / c.y;
+            return (0.5 * 0.70710678118654752440 * 1.12837916709551257390 / c.y) *
+                   exp(-0.5 * u * u);
+        }
+        case 7: return 0.5 * (1.0 + tanh(c.x * x));
+        default: return x;
+    }
 }
 
 __device__ int ql_first_row(double* d, double* e, double* z, int k)
@@ -668,7 +683,7 @@ __device__ int ql_first_row(double* d, double* e, double* z, int k)
 __global__ void __launch_bounds__(128)
 k_eig_quad(int count, int b, int m, const double* __restrict__ alpha,
            const double* __restrict__ beta, const int32_t* __restrict__ size,
-           int gram, int func, double exponent,
+           int gram, int func, double4 fc, double exponent,
            const double* __restrict__ params, int q, double nscale,
            double* __restrict__ samples, double* __restrict__ theta_out,
            double* __restrict__ tau_out, int32_t* __restrict__ status)
@@ -710,7 +725,7 @@ k_eig_quad(int count, int b, int m, const double* __restrict__ alpha,
         for (int i = 0; i < k; ++i)
         {
             const double th = (j > 0) ? d[i] - t0 + params[j] : d[i];
-            acc += z[i] * z[i] * apply_func(func, pow(th, exponent));
+            acc += z[i] * z[i] * apply_func(func, pow(th, exponent), fc);
         }
         samples[static_cast<int64_t>(p) * q + j] = nscale * acc;
     }

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define SLQ_ABI_VERSION 1
+#define SLQ_ABI_VERSION 2
 
 typedef enum {
     SLQ_OK = 0,
@@ -41,7 +41,18 @@ typedef enum {
 
 typedef enum { SLQ_F32 = 0, SLQ_F64 = 1 } slq_dtype;
 typedef enum { SLQ_CSR = 0, SLQ_CSC = 1 } slq_format;
-typedef enum { SLQ_FUNC_LOG = 0, SLQ_FUNC_INV = 1, SLQ_FUNC_ID = 2 } slq_func;
+/* Matrix functions f applied at the quadrature nodes as f(theta^p), with
+ * their coefficients in slq_params.func_coeff: log (logdet,
+ * imate/functions/logarithm.cpp), 1/x (traceinv, inverse.cpp), x (trace,
+ * identity.cpp), exp(c0 x) (trexp, exponential.cpp), (c0 x + c1) /
+ * (c2 x + c3) (trlinfrac, homographic.cpp), 1 on [c0, c1] else 0
+ * (eigencount, indicator.cpp), exp(-((x - c0) / c1)^2 / 2) / (c1 sqrt(2 pi))
+ * (density, gaussian.cpp) and (1 + tanh(c0 x)) / 2 (smoothstep.cpp). */
+typedef enum {
+    SLQ_FUNC_LOG = 0, SLQ_FUNC_INV = 1, SLQ_FUNC_ID = 2, SLQ_FUNC_EXP = 3,
+    SLQ_FUNC_LINFRAC = 4, SLQ_FUNC_INDICATOR = 5, SLQ_FUNC_GAUSSIAN = 6,
+    SLQ_FUNC_SMOOTHSTEP = 7
+} slq_func;
 typedef enum { SLQ_RNG_PARITY = 0, SLQ_RNG_FAST = 1 } slq_rng;
 
 /* Opaque operator: a sparse matrix A (or A + t I when affine != 0) resident
@@ -138,6 +149,7 @@ typedef struct {
     int block_size;                /* probes advanced together; 0 = auto     */
     int rng;                       /* slq_rng                                */
     int64_t first_probe;           /* global index of sample 0 (probe shards) */
+    double func_coeff[4];          /* coefficients of func (see slq_func)    */
 } slq_params;
 
 #define SLQ_MAX_DEGREE 256

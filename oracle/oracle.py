@@ -15,6 +15,8 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(_HERE, "_build", "libslq_oracle.so")
+FUNC_IDS = {"log": 0, "inv": 1, "id": 2, "exp": 3, "linfrac": 4,
+            "indicator": 5, "gaussian": 6, "smoothstep": 7}
 
 _lib = None
 
@@ -135,10 +137,12 @@ def trace_estimator(A, func, gram=False, exponent=1.0, parameters=None,
                     min_num_samples=10, max_num_samples=50, error_atol=0.0,
                     error_rtol=1e-2, confidence_level=0.95,
                     outlier_significance_level=0.001, lanczos_degree=20,
-                    lanczos_tol=None, orthogonalize=0, seed=0):
+                    lanczos_tol=None, orthogonalize=0, seed=0, coeff=None):
     """Single-thread restatement of the reference estimator (FP64).
     gram: False/0 Lanczos on A, True/1 Golub-Kahn on A, 2 Lanczos on
-    A^T A (+ t I with parameters)."""
+    A^T A (+ t I with parameters).  func: 'log', 'inv', 'id', 'exp',
+    'linfrac', 'indicator', 'gaussian', 'smoothstep' with coefficients
+    ``coeff`` (imate/functions/*.cpp)."""
     lib = load()
     A, fmt, data, indices, indptr = _csr_parts(A)
     affine = parameters is not None
@@ -158,16 +162,20 @@ def trace_estimator(A, func, gram=False, exponent=1.0, parameters=None,
     sizes = np.zeros(max_num_samples, np.int32)
     alphas = np.zeros((max_num_samples, m))
     betas = np.zeros((max_num_samples, m))
-    fid = {"log": 0, "inv": 1, "id": 2}[func]
+    fid = FUNC_IDS[func]
+    fc = np.zeros(4)
+    if coeff is not None:
+        fc[:len(coeff)] = coeff
     fn = lib.oracle_trace_estimator
     fn.restype = ctypes.c_int
     vp, i32, i64, d = (ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
                        ctypes.c_double)
-    fn.argtypes = [vp, vp, vp, i64, i64, i32, i32, vp, i32, i32, i32, d, i32,
-                   i64, i32, d, i32, i32, d, d, d, d, vp, vp, vp, vp, vp, vp,
-                   vp, vp, vp, vp]
+    fn.argtypes = [vp, vp, vp, i64, i64, i32, i32, vp, i32, i32, vp, i32, d,
+                   i32, i64, i32, d, i32, i32, d, d, d, d, vp, vp, vp, vp, vp,
+                   vp, vp, vp, vp, vp]
     st = fn(_p(data), _p(indices), _p(indptr), A.shape[0], A.shape[1], fmt,
-            int(affine), _p(params), q, fid, int(gram), float(exponent),
+            int(affine), _p(params), q, fid, _p(fc), int(gram),
+            float(exponent),
             orthogonalize, seed, m, lanczos_tol, min_num_samples,
             max_num_samples, error_atol, error_rtol, confidence_level,
             outlier_significance_level, _p(trace), _p(error), _p(samples),

@@ -77,8 +77,11 @@ def trace_estimator(A, func, gram=False, exponent=1.0, parameters=None,
                     min_num_samples=10, max_num_samples=50, error_atol=0.0,
                     error_rtol=1e-2, confidence_level=0.95,
                     outlier_significance_level=0.001, lanczos_degree=20,
-                    lanczos_tol=None, orthogonalize=0, seed=0, num_threads=1):
-    """Run the reference estimator.  ``func`` in {'log', 'inv', 'id'}.
+                    lanczos_tol=None, orthogonalize=0, seed=0, num_threads=1,
+                    coeff=None):
+    """Run the reference estimator.  ``func`` in {'log', 'inv', 'id', 'exp',
+    'linfrac', 'indicator', 'gaussian', 'smoothstep'} with the function's
+    coefficients ``coeff`` (functions/*.cpp).
 
     ``parameters`` (None or a 1-D array) selects an ``A + t I`` operator as
     ``imate.AffineMatrixFunction(A)`` does.  Returns a dict with the same
@@ -102,18 +105,23 @@ def trace_estimator(A, func, gram=False, exponent=1.0, parameters=None,
     outl = np.zeros(q, np.int32)
     conv = np.zeros(q, np.int32)
     wall = ctypes.c_float(0.0)
-    fid = {"log": 0, "inv": 1, "id": 2}[func]
+    fid = {"log": 0, "inv": 1, "id": 2, "exp": 3, "linfrac": 4,
+           "indicator": 5, "gaussian": 6, "smoothstep": 7}[func]
+    fc = np.zeros(4)
+    if coeff is not None:
+        fc[:len(coeff)] = coeff
     if dt == np.float64:
         fn, real = lib.ref_trace_estimator_f64, ctypes.c_double
     else:
         fn, real = lib.ref_trace_estimator_f32, ctypes.c_float
     fn.restype = ctypes.c_int
     vp, i32, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64
-    fn.argtypes = [vp, vp, vp, i64, i64, i32, i32, vp, i32, i32, i32, real,
+    fn.argtypes = [vp, vp, vp, i64, i64, i32, i32, vp, i32, i32, vp, i32,
+                   real,
                    i32, i64, i32, real, i32, i32, real, real, real, real, i32,
                    vp, vp, vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_float)]
     allc = fn(_p(data), _p(indices), _p(indptr), A.shape[0], A.shape[1], fmt,
-              int(affine), _p(params), q, fid, int(gram), exponent,
+              int(affine), _p(params), q, fid, _p(fc), int(gram), exponent,
               orthogonalize, seed, lanczos_degree, lanczos_tol,
               min_num_samples, max_num_samples, error_atol, error_rtol,
               confidence_level, outlier_significance_level, num_threads,

@@ -32,6 +32,11 @@
 #include "functions/logarithm.h"
 #include "functions/inverse.h"
 #include "functions/identity.h"
+#include "functions/exponential.h"
+#include "functions/homographic.h"
+#include "functions/indicator.h"
+#include "functions/gaussian.h"
+#include "functions/smoothstep.h"
 
 // ---------------------------------------------------------------------------
 // LAPACK trampolines (signatures of lapack_api.h)
@@ -115,12 +120,18 @@ static cLinearOperator<T>* make_operator(
     return new cCSCMatrix<T>(data, ind, ptr, num_rows, num_cols);
 }
 
-static Function* make_function(int func_id)
+// The reference's function objects (functions/*.cpp) with coefficients c.
+static Function* make_function(int func_id, const double* c)
 {
     switch (func_id)
     {
         case 0: return new Logarithm();
         case 1: return new Inverse();
+        case 3: return new Exponential(c[0]);
+        case 4: return new Homographic(c[0], c[1], c[2], c[3]);
+        case 5: return new Indicator(c[0], c[1]);
+        case 6: return new Gaussian(c[0], c[1]);
+        case 7: return new SmoothStep(c[0]);
         default: return new Identity();
     }
 }
@@ -129,7 +140,8 @@ template <typename T>
 static int run_trace_estimator(
         const T* data, const int* indices, const int* indptr,
         int64_t num_rows, int64_t num_cols, int fmt, int affine,
-        T* parameters, int num_inquiries, int func_id, int gram, T exponent,
+        T* parameters, int num_inquiries, int func_id, const double* coeff,
+        int gram, T exponent,
         int orthogonalize, int64_t seed, int lanczos_degree, T lanczos_tol,
         int min_num_samples, int max_num_samples, T error_atol, T error_rtol,
         T confidence_level, T outlier_significance_level, int num_threads,
@@ -139,7 +151,7 @@ static int run_trace_estimator(
 {
     cLinearOperator<T>* A = make_operator<T>(data, indices, indptr, num_rows,
                                              num_cols, fmt, affine);
-    Function* f = make_function(func_id);
+    Function* f = make_function(func_id, coeff);
     T** rows = new T*[max_num_samples];
     for (int i = 0; i < max_num_samples * num_inquiries; ++i)
         samples[i] = NAN;
@@ -173,8 +185,9 @@ extern "C" {
 int ref_trace_estimator_f64(
         const double* data, const int* indices, const int* indptr,
         int64_t num_rows, int64_t num_cols, int fmt, int affine,
-        double* parameters, int num_inquiries, int func_id, int gram,
-        double exponent, int orthogonalize, int64_t seed, int lanczos_degree,
+        double* parameters, int num_inquiries, int func_id, const double* coeff,
+        int gram, double exponent, int orthogonalize, int64_t seed,
+        int lanczos_degree,
         double lanczos_tol, int min_num_samples, int max_num_samples,
         double error_atol, double error_rtol, double confidence_level,
         double outlier_significance_level, int num_threads, double* trace,
@@ -184,7 +197,8 @@ int ref_trace_estimator_f64(
 {
     return run_trace_estimator<double>(
             data, indices, indptr, num_rows, num_cols, fmt, affine,
-            parameters, num_inquiries, func_id, gram, exponent, orthogonalize,
+            parameters, num_inquiries, func_id, coeff, gram, exponent,
+            orthogonalize,
             seed, lanczos_degree, lanczos_tol, min_num_samples,
             max_num_samples, error_atol, error_rtol, confidence_level,
             outlier_significance_level, num_threads, trace, error, samples,
@@ -195,8 +209,9 @@ int ref_trace_estimator_f64(
 int ref_trace_estimator_f32(
         const float* data, const int* indices, const int* indptr,
         int64_t num_rows, int64_t num_cols, int fmt, int affine,
-        float* parameters, int num_inquiries, int func_id, int gram,
-        float exponent, int orthogonalize, int64_t seed, int lanczos_degree,
+        float* parameters, int num_inquiries, int func_id, const double* coeff,
+        int gram, float exponent, int orthogonalize, int64_t seed,
+        int lanczos_degree,
         float lanczos_tol, int min_num_samples, int max_num_samples,
         float error_atol, float error_rtol, float confidence_level,
         float outlier_significance_level, int num_threads, float* trace,
@@ -206,7 +221,8 @@ int ref_trace_estimator_f32(
 {
     return run_trace_estimator<float>(
             data, indices, indptr, num_rows, num_cols, fmt, affine,
-            parameters, num_inquiries, func_id, gram, exponent, orthogonalize,
+            parameters, num_inquiries, func_id, coeff, gram, exponent,
+            orthogonalize,
             seed, lanczos_degree, lanczos_tol, min_num_samples,
             max_num_samples, error_atol, error_rtol, confidence_level,
             outlier_significance_level, num_threads, trace, error, samples,

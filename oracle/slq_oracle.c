@@ -583,12 +583,25 @@ static void average_estimates(double conf, double outlier_sig, int q,
     free(out);
 }
 
-static double apply_function(int func_id, double x)
-{   /* functions/logarithm.cpp, inverse.cpp:41, identity.cpp:41 */
+static double apply_function(int func_id, double x, const double* c)
+{   /* functions/logarithm.cpp, inverse.cpp:41, identity.cpp:41,
+     * exponential.cpp:55-58, homographic.cpp:63-75, indicator.cpp:62-72,
+     * gaussian.cpp:65-69, smoothstep.cpp:55-58 */
     switch (func_id)
     {
         case 0: return log(x);
         case 1: return 1.0 / x;
+        case 3: return exp(x * c[0]);
+        case 4: return (c[0] * x + c[1]) / (c[2] * x + c[3]);
+        case 5: return (x < c[0] || x > c[1]) ? 0.0 : 1.0;
+        case 6:
+        {
+            double u = (x - c[0]) / c[1];
+            /* 0.5 * M_SQRT1_2 * M_2_SQRTPI / sigma = 1 / (sigma sqrt(2 pi)) */
+            return (0.5 * 0.70710678118654752440 * 1.12837916709551257390 /
+                    c[1]) * exp(-0.5 * u * u);
+        }
+        case 7: return 0.5 * (1.0 + tanh(c[0] * x));
         default: return x;
     }
 }
@@ -666,8 +679,9 @@ void oracle_average_estimates(double conf, double outlier_sig, int q,
 int oracle_trace_estimator(
         const double* data, const int* indices, const int* indptr,
         int64_t nrows, int64_t ncols, int fmt, int affine,
-        const double* params, int q, int func_id, int gram, double exponent,
-        int orthogonalize, int64_t seed, int m, double tol, int min_s,
+        const double* params, int q, int func_id, const double* func_coeff,
+        int gram, double exponent, int orthogonalize, int64_t seed, int m,
+        double tol, int min_s,
         int max_s, double atol, double rtol, double conf, double outlier_sig,
         double* trace, double* error, double* samples, int* order, int* used,
         int* num_outliers, int* converged, int* lanczos_sizes,
@@ -712,7 +726,8 @@ int oracle_trace_estimator(
             {
                 double th = (affine && j > 0) ? theta[i] - params[0] + params[j]
                                               : theta[i];
-                acc += tau[i] * tau[i] * apply_function(func_id, pow(th, exponent));
+                acc += tau[i] * tau[i] *
+                       apply_function(func_id, pow(th, exponent), func_coeff);
             }
             samples[(int64_t)s * q + j] = (double)n * acc;
         }

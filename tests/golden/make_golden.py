@@ -14,6 +14,10 @@ seeded inputs and stores what it returns:
   estimator.npz  full estimator outputs (c_trace_estimator.cpp:192-307,
                  num_threads=1): samples, processed order, num_samples_used,
                  outliers, trace, error
+  functions.npz  the same for the other matrix functions of imate's SLQ
+                 consumers (functions/exponential.cpp, homographic.cpp,
+                 indicator.cpp, gaussian.cpp, smoothstep.cpp) with their
+                 coefficients, settings in FUNC_SETTINGS
 
 Usage (needs the reference tree and oracle/_ref built):
     python tests/golden/make_golden.py
@@ -27,8 +31,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
 
 from oracle import ref  # noqa: E402
+from golden_cases import FUNC_CASES, FUNC_SETTINGS  # noqa: E402
 from imate_b200.sample_matrices import toeplitz, correlation_matrix  # noqa
 
 
@@ -131,9 +137,20 @@ def make_estimator():
     np.savez_compressed(os.path.join(HERE, "estimator.npz"), **out)
 
 
+def make_functions():
+    out = {}
+    C = small_correlation()
+    for name, func, coeff, gram, params in FUNC_CASES:
+        r = ref.trace_estimator(C, func, gram=gram, parameters=params,
+                                coeff=coeff, num_threads=1, **FUNC_SETTINGS)
+        _store(out, "fn_" + name, r)
+    np.savez_compressed(os.path.join(HERE, "functions.npz"), **out)
+
+
 if __name__ == "__main__":
     make_rng()
     make_krylov()
     make_estimator()
-    for f in ("rng.npz", "krylov.npz", "estimator.npz"):
+    make_functions()
+    for f in ("rng.npz", "krylov.npz", "estimator.npz", "functions.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")

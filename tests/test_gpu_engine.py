@@ -12,6 +12,7 @@ import scipy.sparse as sp
 
 import imate_b200 as ib
 from imate_b200 import _lib
+from golden_cases import FUNC_CASES, FUNC_SETTINGS
 from oracle import oracle
 
 pytestmark = pytest.mark.gpu
@@ -500,3 +501,51 @@ def test_normal_equations_sweep_and_fp32(cuda):
     for i, lam in enumerate(lams):
         exact = np.linalg.slogdet(XtX + lam * np.eye(800))[1]
         assert abs(tr[i] - exact) / abs(exact) < 0.02
+
+
+def _consumer_call(A, func, coeff, gram, params, kw):
+    # the public wrapper of imate's SLQ consumer that uses this function
+    if params is not None:
+        A = ib.AffineMatrixFunction(A)
+        kw = dict(kw, parameters=params)
+    common = dict(method="slq", gpu=True, return_info=True, gram=gram, **kw)
+    if func == "exp":
+        return ib.trexp(A, coeff=coeff[0], **common)
+    if func == "linfrac":
+        return ib.trlinfrac(A, coeff=coeff, **common)
+    if func == "indicator":
+        return ib.eigencount(A, interval=coeff, **common)
+    if func == "gaussian":
+        return ib.density(A, mu=coeff[0], sigma=coeff[1], **common)
+    from imate_b200._trace_estimator import trace_estimator
+    d = dict(ib._functions._SLQ_DEFAULTS)
+    d.update(kw, gpu=True)
+    return trace_estimator(
+        A, d["parameters"], func, gram, 1.0, d["min_num_samples"],
+        d["max_num_samples"], d["error_atol"], d["error_rtol"],
+        d["confidence_level"], d["outlier_significance_level"],
+        d["lanczos_degree"], d["lanczos_tol"], d["orthogonalize"], d["seed"],
+        d["num_threads"], d["num_gpu_devices"], False, False, True,
+        func_coeff=coeff)
+
+
+@pytest.mark.parametrize("case", FUNC_CASES, ids=[c[0] for c in FUNC_CASES])
+def test_other_functions_match_reference(cuda, golden, corr_small, case):
+    # trexp / trlinfrac / eigencount / density (and smoothstep) against the
+    # reference's own outputs on the same probes
+    name, func, coeff, gram, params = case
+    g = golden("functions.npz")
+    key = "fn_" + name
+    tr, info = _consumer_call(corr_small, func, coeff, gram, params,
+                              dict(FUNC_SETTINGS))
+    conv = info["convergence"]
+    used = np.atleast_1d(conv["num_samples_used"])
+    assert np.array_equal(used, g[key + "_num_samples_used"])
+    order = g[key + "_processed_samples_indices"][:int(used[0])]
+    assert np.array_equal(conv["samples_processed_order"][:order.size],
+                          order)
+    samples = np.asarray(conv["samples"]).reshape(FUNC_SETTINGS[
+        "max_num_samples"], -1)
+    assert rel(samples[order], g[key + "_samples"][order]) < RTOL_FP64
+    assert rel(np.atleast_1d(tr), g[key + "_trace"]) < RTOL_FP64
+

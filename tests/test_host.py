@@ -39,7 +39,7 @@ def test_library_exports_every_declared_symbol(lib):
     for n in names:
         assert hasattr(lib, n), n
     assert set(names) == set(_lib.EXPORTS)
-    assert lib.slq_abi_version() == 1
+    assert lib.slq_abi_version() == 2
 
 
 def test_erfinv_matches_oracle(lib):
@@ -205,3 +205,17 @@ def test_batch_and_tuner_reject_bad_arguments_without_a_gpu(lib):
     assert lib.slq_operator_set_variant(None, 64, 0, 0) == 1
     assert lib.slq_operator_tune_workspace_bytes(None, 64,
                                                  ctypes.byref(nb)) == 1
+
+
+def test_consumer_argument_checks(corr_small):
+    # imate's checks of trlinfrac / eigencount / density arguments
+    # (*/_slq_method.pyx check_arguments) run before any device work
+    with pytest.raises(ValueError):
+        ib.trlinfrac(corr_small, coeff=[1.0, 2.0, 2.0, 4.0], method="slq",
+                     gpu=True)
+    with pytest.raises(ValueError):
+        ib.eigencount(corr_small, interval=[0.0], method="slq", gpu=True)
+    with pytest.raises(ValueError):
+        ib.density(corr_small, sigma=0.0, method="slq", gpu=True)
+    with pytest.raises(NotImplementedError):
+        ib.trexp(corr_small, method="eigenvalue")

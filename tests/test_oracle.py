@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from imate_b200.sample_matrices import toeplitz
+from golden_cases import FUNC_CASES, FUNC_SETTINGS
 from oracle import oracle, ref
 
 
@@ -146,6 +147,17 @@ def test_estimator_gram_affine_exponent(golden, corr_small):
                                error_rtol=1e-2, lanczos_degree=10,
                                orthogonalize=3, seed=2)
     _check_estimator(r, g, "corr_log_p2")
+
+
+@pytest.mark.parametrize("case", FUNC_CASES, ids=[c[0] for c in FUNC_CASES])
+def test_estimator_other_functions(golden, corr_small, case):
+    # trexp / trlinfrac / eigencount / density functions (and smoothstep)
+    # against the reference's own outputs
+    name, func, coeff, gram, params = case
+    g = golden("functions.npz")
+    r = oracle.trace_estimator(corr_small, func, gram=gram, parameters=params,
+                               coeff=coeff, **FUNC_SETTINGS)
+    _check_estimator(r, g, "fn_" + name)
 
 
 def test_toeplitz_estimate_vs_exact(golden):
