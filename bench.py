@@ -64,6 +64,14 @@ def parse():
     ap.add_argument("--fp64-probes", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="c2prime",
+                    choices=["c2prime", "batched", "sweep", "gram-large"],
+                    help="c2prime: the headline line (default); batched: 64 "
+                         "correlation matrices in one graph; sweep: 512-point "
+                         "t-sweep by the surrogate; gram-large: logdet(X^T X "
+                         "+ lambda I) of an 8388608 x 2097152 sparse X")
+    ap.add_argument("--batch-count", type=int, default=64)
+    ap.add_argument("--block", type=int, default=256)
     return ap.parse_args()
 
 
@@ -434,8 +442,302 @@ def run_engine_arm(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# other workloads (one JSON line each; not the headline line)
+# ---------------------------------------------------------------------------
+
+def _timed(fn, steps):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    out = [fn(i) for i in range(steps)]
+    e1.record()
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1) * 1e-3
+
+
+def run_batched(args):
+    """64 sparse SPD correlation matrices (sizes log-uniform 2^10..2^17 and
+    length scales U(0.002, 0.05) from PCG64 seed 2; points from seed 1000+i;
+    kernel cut 0.05; diagonal shift --shift), built on the device, FP32;
+    512 probes each, lanczos_degree 40, no reorthogonalisation; one batch
+    plan (one CUDA graph, autotuned SpMM and block width per matrix).  A
+    step is one launch of the plan over all matrices."""
+    import torch
+    import imate_b200 as ib
+    from imate_b200.batch import BatchPlan
+    from imate_b200.sample_matrices import (correlation_matrix_device,
+                                            batched_correlation_sizes)
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    probes = 512 if args.probes == 256 else args.probes
+    degree = 40 if args.degree == 50 else args.degree
+    sizes, scales = batched_correlation_sizes(args.batch_count, seed=2)
+    mats, mats64, nnz = [], [], []
+    t0 = time.perf_counter()
+    for i, (n, sc) in enumerate(zip(sizes, scales)):
+        ip, ind, dat, _ = correlation_matrix_device(
+            int(n), scale=float(sc), threshold=0.05, shift=args.shift,
+            seed=1000 + i, dtype="float32")
+        mats.append(ib.DeviceMatrix(ip, ind, dat, (int(n), int(n))))
+        nnz.append(int(ind.numel()))
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    ests = [dict(func="logdet", A=M, min_num_samples=probes,
+                 max_num_samples=probes, error_rtol=0.0,
+                 lanczos_degree=degree, orthogonalize=0, seed=i)
+            for i, M in enumerate(mats)]
+    t0 = time.perf_counter()
+    plan = BatchPlan(ests, autotune=True)
+    plan_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        plan.run()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    outs, elapsed = _timed(lambda i: plan.run(), args.steps)
+    clk = clocks.stop()
+    ps = sum(int(np.sum(info["engine"]["lanczos_size"])) for res in outs
+             for _, info in res)
+    value = ps / elapsed
+    widths = [t["width"] for t in plan.tuning]
+    # algorithmic bytes of the whole graph per step: per matrix and
+    # Lanczos step, the SpMM of every block plus the update pass
+    by = 0.0
+    flops = 0.0
+    for n, z, w in zip(sizes, nnz, widths):
+        blocks = -(-probes // w)
+        spmm = z * 8.0 + (n + 1) * 4.0 + 2.0 * n * w * 4.0
+        upd = 4.0 * n * w * 4.0
+        by += degree * blocks * (spmm + upd)
+        flops += degree * 2.0 * z * probes
+    achieved = by * args.steps / elapsed / 1e9
+    peak, peak_kind = peaks()
+    # plain FP64 per-probe path (block width 1) on three of the matrices
+    order = np.argsort(sizes)
+    pick = [int(order[len(order) // 4]), int(order[len(order) // 2]),
+            int(order[-1])]
+    ps64, t64 = 0, 0.0
+    for i in pick:
+        ip, ind, dat, _ = correlation_matrix_device(
+            int(sizes[i]), scale=float(scales[i]), threshold=0.05,
+            shift=args.shift, seed=1000 + i, dtype="float64")
+        M64 = ib.DeviceMatrix(ip, ind, dat, (int(sizes[i]),) * 2,
+                              group_rows=0)
+        kw64 = dict(method="slq", gpu=True, return_info=True,
+                    min_num_samples=4, max_num_samples=4, error_rtol=0.0,
+                    lanczos_degree=degree, orthogonalize=0, seed=i,
+                    engine=ib.EngineOptions(block_size=1))
+        ib.logdet(M64, **dict(kw64, min_num_samples=1, max_num_samples=1))
+        (res,), t = _timed(lambda k: ib.logdet(M64, **kw64), 1)
+        ps64 += int(np.sum(res[1]["engine"]["lanczos_size"]))
+        t64 += t
+        del M64
+    v64 = ps64 / t64
+    line = {
+        "workload_kind": "batched", "metric": "batched SLQ logdet "
+        "probe*steps/s (64 matrices, one graph launch)", "value": value,
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "%d sparse SPD correlation matrices, one "
+                               "batch plan" % len(mats),
+                   "total_rows": int(np.sum(sizes)), "total_nnz": int(sum(nnz)),
+                   "max_nnz_per_row": float(max(z / n for z, n in
+                                                zip(nnz, sizes))),
+                   "probes_per_matrix": probes, "lanczos_degree": degree,
+                   "orthogonalize": 0, "diag_shift": args.shift,
+                   "l2": "inputs larger than L2 (matrices %.1f GB)"
+                         % (sum(nnz) * 8 / 1e9)},
+        "graph": {"kernels": plan.graph_kernels, "nodes": plan.graph_nodes,
+                  "build_s": build_s, "plan_s": plan_s,
+                  "widths": {str(w): widths.count(w) for w in sorted(
+                      set(widths))}},
+        "roofline": {"bound": "hbm", "kernel": "whole graph (SpMM + update "
+                     "passes)", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_kind,
+                     "spmm_fp32_tflops": flops * args.steps / elapsed / 1e12},
+        "gpu_launches": plan.graph_kernels * args.steps, "clocks": clk,
+        "fp64_plain": {"value": v64, "unit": UNIT, "probes": 4 * len(pick),
+                       "block_size": 1, "matrices": [int(sizes[i])
+                                                     for i in pick],
+                       "speedup_mixed_batched": value / v64},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_sweep(args):
+    """t-sweep of logdet(A + tI) and traceinv(A + tI) over 512 log-spaced t
+    in [1e-4, 1e2] on the benchmark matrix (FP32): the surrogate (trained
+    on 32 SLQ points, gated on 16 held-out points, SLQ fallback) against
+    per-t SLQ and against one shift-relation SLQ run over all 512 t."""
+    import torch
+    import imate_b200 as ib
+    from imate_b200.surrogate import SweepSurrogate
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    A32 = build_matrix(args, "float32")
+    t_grid = np.logspace(-4, 2, 512)
+    opts = dict(min_num_samples=args.probes, max_num_samples=args.probes,
+                error_rtol=0.0, lanczos_degree=args.degree,
+                orthogonalize=args.orthogonalize, seed=0)
+    funcs = {"log": ib.logdet, "inv": ib.traceinv}
+    Aop = ib.AffineMatrixFunction(A32)
+    Aop.get_device_operator()
+    out = {}
+    for func, f in funcs.items():
+        S = SweepSurrogate(A32, func=func, t_min=1e-4, t_max=1e2,
+                           num_train=32, num_check=16, rtol=1e-3, **opts)
+        S.Aop = Aop  # share the resident operator
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        S.fit()
+        torch.cuda.synchronize()
+        fit_s = time.perf_counter() - t0
+        vals = None
+        reps = max(3, args.steps)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            vals = S(t_grid)
+        torch.cuda.synchronize()
+        answer_s = (time.perf_counter() - t0) / reps
+        fallback = int(np.sum(S.last_fallback))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        shift_vals = f(Aop, method="slq", gpu=True, parameters=t_grid, **opts)
+        torch.cuda.synchronize()
+        shift_s = time.perf_counter() - t0
+        k = 3
+        t0 = time.perf_counter()
+        for t in t_grid[::len(t_grid) // k][:k]:
+            f(Aop, method="slq", gpu=True, parameters=float(t), **opts)
+        torch.cuda.synchronize()
+        per_t_s = (time.perf_counter() - t0) / k
+        # relative error judged as the held-out gate judges it: against
+        # max(|value|, rtol_floor * mean |value|), since logdet(A + tI)
+        # crosses zero inside the sweep
+        floor = S.rtol_floor * float(np.mean(np.abs(shift_vals)))
+        err = np.abs(vals - shift_vals) / np.maximum(np.abs(shift_vals),
+                                                     floor)
+        out[func] = {
+            "fit_s": fit_s, "answer_512_s": answer_s,
+            "per_t_slq_s": per_t_s, "per_t_slq_512_s": 512 * per_t_s,
+            "shift_relation_slq_512_s": shift_s,
+            "speedup_vs_per_t": 512 * per_t_s / answer_s,
+            "speedup_vs_per_t_incl_fit": 512 * per_t_s / (answer_s + fit_s),
+            "speedup_vs_shift_relation": shift_s / answer_s,
+            "fallback_points": fallback,
+            "held_out_max_rel_err": float(np.max(S.check_error)),
+            "max_rel_diff_vs_shift_relation_slq": float(np.max(err)),
+            "points_over_1e-3_vs_shift_relation_slq": int(np.sum(err >
+                                                                 1e-3)),
+            "train_timings": dict(S.timings),
+        }
+    line = {
+        "workload_kind": "sweep", "metric": "512-point t-sweep answer time, "
+        "surrogate vs per-t SLQ", "value": out["log"]["speedup_vs_per_t"],
+        "unit": "x faster than per-t SLQ (logdet)", "n_gpus": 1,
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": dict(workload_config(args, A32.nnz),
+                       sweep="512 t log-spaced over [1e-4, 1e2]",
+                       per_t_note="per-t SLQ time = mean of 3 single-t "
+                                  "runs x 512"),
+        "sweeps": out,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gram_large(args):
+    """logdet(X^T X + lambda I), lambda = 1e-2, X 8388608 x 2097152 sparse
+    (16 nonzeros per column at uniform rows, N(0,1) values, PCG64 seed 4),
+    FP32 CSC; Lanczos on the normal operator, lanczos_degree 60, 1024
+    probes in blocks of --block, no reorthogonalisation."""
+    import torch
+    import imate_b200 as ib
+    from imate_b200.sample_matrices import sparse_gram_design
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    t0 = time.perf_counter()
+    X = sparse_gram_design(8388608, 2097152, 16, seed=4)
+    build_s = time.perf_counter() - t0
+    probes = 1024 if args.probes == 256 else args.probes
+    degree = 60 if args.degree == 50 else args.degree
+    G = ib.GramAffineMatrixFunction(X)
+    G.get_device_operator(need_transpose=True)
+    kw = dict(method="slq", gpu=True, return_info=True, parameters=1e-2,
+              min_num_samples=probes, max_num_samples=probes,
+              error_rtol=0.0, lanczos_degree=degree, orthogonalize=0, seed=0)
+    eng = ib.EngineOptions(block_size=args.block)
+    for _ in range(args.warmup):
+        ib.logdet(G, engine=eng, **kw)
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    from imate_b200 import _lib
+    _lib.profile_begin()
+    outs, elapsed = _timed(lambda i: ib.logdet(G, engine=eng, **kw),
+                           args.steps)
+    kstats = _lib.profile_end()
+    clk = clocks.stop()
+    ps = sum(int(np.sum(info["engine"]["lanczos_size"])) for _, info in outs)
+    value = ps / elapsed
+    nl, ms, by = kstats["spmm"]
+    achieved = (by / nl) / (ms / nl * 1e-3) / 1e9 if nl else 0.0
+    peak, peak_kind = peaks()
+    # plain FP64 per-probe path on 4 probes, and the same probes mixed
+    G64 = ib.GramAffineMatrixFunction(X.astype(np.float64))
+    kw64 = dict(kw, min_num_samples=4, max_num_samples=4)
+    ib.logdet(G64, engine=ib.EngineOptions(block_size=1),
+              **dict(kw64, min_num_samples=1, max_num_samples=1))
+    (r64,), t64 = _timed(lambda i: ib.logdet(
+        G64, engine=ib.EngineOptions(block_size=1), **kw64), 1)
+    r32 = ib.logdet(G, engine=ib.EngineOptions(block_size=4), **kw64)
+    s64 = np.asarray(r64[1]["convergence"]["samples"][:4], float)
+    s32 = np.asarray(r32[1]["convergence"]["samples"][:4], float)
+    v64 = int(np.sum(r64[1]["engine"]["lanczos_size"])) / t64
+    est = float(np.mean([tr for tr, _ in outs]))
+    line = {
+        "workload_kind": "gram-large", "metric": "Gram-form SLQ logdet "
+        "probe*steps/s (normal operator X^T X + lambda I)", "value": value,
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "logdet(X^T X + 1e-2 I), X 8388608 x 2097152,"
+                               " 16 nnz/col, CSC FP32", "nnz": int(X.nnz),
+                   "probes": probes, "block_size": args.block,
+                   "lanczos_degree": degree, "orthogonalize": 0,
+                   "host_build_s": build_s,
+                   "l2": "inputs larger than L2 (basis blocks > 2 GB)"},
+        "roofline": {"bound": "hbm", "kernel": "spmm", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_kind,
+                     "note": "algorithmic bytes count each X value once; the "
+                             "random rows make every nonzero gather a "
+                             "b-wide row of the other operand"},
+        "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in
+                    kstats.items() if v[0]},
+        "estimate": est, "estimate_error": float(np.mean(
+            [info["error"]["absolute_error"] for _, info in outs])),
+        "clocks": clk,
+        "fp64_plain": {"value": v64, "unit": UNIT, "probes": 4,
+                       "block_size": 1, "speedup_mixed_batched": value / v64,
+                       "rel_diff_same_probes": float(np.max(
+                           np.abs(s32 - s64) / np.abs(s64)))},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload != "c2prime":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference CPU path is timed on the "
+                              "headline workload only"}), flush=True)
+            return
+        {"batched": run_batched, "sweep": run_sweep,
+         "gram-large": run_gram_large}[args.workload](args)
+        return
     if args.impl == "reference":
         run_reference_arm(args)
     else:

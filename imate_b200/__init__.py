@@ -14,12 +14,13 @@ from ._functions import (logdet, traceinv, trace, schatten, trexp,
                          trlinfrac, eigencount, density)
 from ._trace_estimator import EngineOptions
 from .linear_operator import (LinearOperator, Matrix, AffineMatrixFunction,
-                              GramAffineMatrixFunction)
+                              GramAffineMatrixFunction, DeviceMatrix)
 from .sample_matrices import (toeplitz, toeplitz_logdet, toeplitz_trace,
                               toeplitz_traceinv, correlation_matrix)
 
 __all__ = ["__version__", "logdet", "traceinv", "trace", "schatten",
            "trexp", "trlinfrac", "eigencount", "density",
            "EngineOptions", "LinearOperator", "Matrix",
-           "AffineMatrixFunction", "GramAffineMatrixFunction", "toeplitz", "toeplitz_logdet",
-           "toeplitz_trace", "toeplitz_traceinv", "correlation_matrix"]
+           "AffineMatrixFunction", "GramAffineMatrixFunction", "DeviceMatrix",
+           "toeplitz", "toeplitz_logdet", "toeplitz_trace",
+           "toeplitz_traceinv", "correlation_matrix"]

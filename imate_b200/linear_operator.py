@@ -111,11 +111,12 @@ class _DeviceOperator:
     def __init__(self, A, affine, need_transpose, check_indices=True,
                  reorder="auto", group_rows="auto"):
         import torch
-        lib = _lib.load()
         if not torch.cuda.is_available():
             raise RuntimeError("no CUDA device is available for the SLQ "
                                "engine (it has no CPU path)")
         self.device = torch.device("cuda", torch.cuda.current_device())
+        if A is None:
+            return  # from_device fills the fields
         perm = locality_order(A, reorder)
         self.group_rows = group_rows_for(A, perm, group_rows)
         if perm is not None and A.format != "csr":
@@ -147,10 +148,42 @@ class _DeviceOperator:
             self.inv = torch.empty_like(self.perm)
             self.inv[self.perm.long()] = torch.arange(
                 perm.size, dtype=torch.int32, device=dev)
+        self._create(fmt, affine, need_transpose, check_indices)
+
+    @classmethod
+    def from_device(cls, indptr, indices, data, shape, affine=False,
+                    need_transpose=False, group_rows=8, fmt=_lib.SLQ_CSR,
+                    check_indices=True):
+        """Operator over CSR (or CSC) arrays already on the device (torch
+        int32 indptr / indices, float32 or float64 data), without copies."""
+        import torch
+        self = cls(None, affine, need_transpose)
+        self.data = data.contiguous()
+        self.indices = indices.contiguous()
+        self.indptr = indptr.contiguous()
+        self.device = self.data.device
+        if self.data.dtype == torch.float32:
+            self.dtype_code, self.np_dtype = _lib.SLQ_F32, np.dtype(np.float32)
+        elif self.data.dtype == torch.float64:
+            self.dtype_code, self.np_dtype = _lib.SLQ_F64, np.dtype(np.float64)
+        else:
+            raise TypeError("data must be float32 or float64")
+        self.shape = tuple(int(x) for x in shape)
+        self.nnz = int(self.indices.numel())
+        self.group_rows = int(group_rows)
+        self.perm = None
+        self.inv = None
+        self._create(fmt, affine, need_transpose, check_indices)
+        return self
+
+    def _create(self, fmt, affine, need_transpose, check_indices):
+        import torch
+        lib = _lib.load()
+        dev = self.device
         nbytes = ctypes.c_size_t(0)
         _lib.check(lib.slq_operator_workspace_bytes(
-            A.shape[0], A.shape[1], self.nnz, self.dtype_code, fmt,
-            int(need_transpose), int(perm is not None), self.group_rows,
+            self.shape[0], self.shape[1], self.nnz, self.dtype_code, fmt,
+            int(need_transpose), int(self.perm is not None), self.group_rows,
             ctypes.byref(nbytes)))
         self.workspace = torch.empty(max(int(nbytes.value), 256),
                                      dtype=torch.uint8, device=dev)
@@ -158,7 +191,7 @@ class _DeviceOperator:
         stream = torch.cuda.current_stream(dev)
         _lib.check(lib.slq_operator_create(
             self.data.data_ptr(), self.indices.data_ptr(),
-            self.indptr.data_ptr(), A.shape[0], A.shape[1], self.nnz,
+            self.indptr.data_ptr(), self.shape[0], self.shape[1], self.nnz,
             self.dtype_code, fmt, int(affine), int(need_transpose),
             int(check_indices),
             self.perm.data_ptr() if self.perm is not None else None,
@@ -324,6 +357,51 @@ class AffineMatrixFunction(LinearOperator):
 
     def _affine(self):
         return True
+
+
+class DeviceMatrix(LinearOperator):
+    """A sparse matrix whose CSR arrays are already on the GPU (torch
+    tensors: int32 indptr and indices, float32 or float64 data), e.g. from
+    ``sample_matrices.correlation_matrix_device``.  No host copy is made;
+    rows must list their columns in increasing order.  ``group_rows`` (0, 4
+    or 8) adds the row-group format on the device (the autotuner then picks
+    between it and CSR)."""
+
+    def __init__(self, indptr, indices, data, shape, group_rows=8):
+        super().__init__()
+        self.indptr, self.indices, self.data = indptr, indices, data
+        self.shape = tuple(int(x) for x in shape)
+        self.group_rows = int(group_rows)
+        self.num_parameters = 0
+        self.data_type_name = str(data.dtype).replace("torch.", "").encode()
+
+    def get_num_rows(self):
+        return self.shape[0]
+
+    def get_num_columns(self):
+        return self.shape[1]
+
+    def is_sparse(self):
+        return True
+
+    def get_nnz(self):
+        return int(self.indices.numel())
+
+    def get_density(self):
+        return self.get_nnz() / float(self.shape[0] * self.shape[1])
+
+    def get_device_operator(self, need_transpose=False):
+        key = (self.data.device.index, bool(need_transpose))
+        op = self._device_ops.get(key)
+        if op is None and not need_transpose:
+            op = self._device_ops.get((self.data.device.index, True))
+        if op is None:
+            op = _DeviceOperator.from_device(
+                self.indptr, self.indices, self.data, self.shape,
+                affine=self._affine(), need_transpose=need_transpose,
+                group_rows=self.group_rows)
+            self._device_ops[key] = op
+        return op
 
 
 class GramAffineMatrixFunction(LinearOperator):

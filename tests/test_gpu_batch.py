@@ -248,3 +248,34 @@ def test_batch_argument_errors(cuda):
     assert st == 3 and not h.value  # SLQ_ERR_WORKSPACE
     assert lib.slq_operator_set_variant(op.handle, 64, 0, 15) == 1
     assert lib.slq_operator_set_variant(op.handle, 48, 0, 0) == 1
+
+
+def test_device_built_correlation_matrix(cuda):
+    # the device builder gives the host builder's matrix in cell order
+    from imate_b200.sample_matrices import (correlation_matrix,
+                                            correlation_matrix_device,
+                                            correlation_points)
+    pts = correlation_points(6000, 2, 17)
+    A = correlation_matrix(points=pts, scale=0.03, threshold=0.05, shift=0.1)
+    ip, ind, dat, perm = correlation_matrix_device(
+        points=pts, scale=0.03, threshold=0.05, shift=0.1, dtype="float64",
+        max_candidates=200000)
+    B = sp.csr_matrix((dat.cpu().numpy(), ind.cpu().numpy(),
+                       ip.cpu().numpy()), shape=A.shape)
+    p = perm.cpu().numpy()
+    Ap = A[p][:, p].tocsr()
+    Ap.sort_indices()
+    assert np.array_equal(Ap.indptr, B.indptr)
+    assert np.array_equal(Ap.indices, B.indices)
+    assert np.max(np.abs(Ap.data - B.data)) < 1e-15
+    # an operator over the device arrays equals one uploaded from the host
+    D = ib.DeviceMatrix(ip, ind, dat, A.shape, group_rows=8)
+    H = ib.Matrix(B, reorder=False, group_rows=8)
+    kw = dict(method="slq", gpu=True, return_info=True, min_num_samples=64,
+              max_num_samples=64, error_rtol=0.0, lanczos_degree=20,
+              orthogonalize=-1, seed=3)
+    td, idv = ib.logdet(D, **kw)
+    th, ih = ib.logdet(H, **kw)
+    assert np.array_equal(idv["convergence"]["samples"],
+                          ih["convergence"]["samples"])
+    assert td == th
