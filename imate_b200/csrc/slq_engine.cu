@@ -692,121 +692,6 @@ slq_status spmm(Launcher& L, int grid, const int32_t* ptr, const int32_t* ind, c
 }
 
 template <typename VT>
-constexpr int vec_of(int b)
-{
-    return (sizeof(VT) == 4) ? (b >= 4 ? 4 : 1) : (b >= 2 ? 2 : 1);
-}
-
-// Geometry shared by k_update_dots and k_reorth.
-struct StreamGeom {
-    int VEC, PT, P;
-};
-
-template <typename VT>
-StreamGeom stream_geom(int b)
-{
-    StreamGeom g;
-    g.VEC = vec_of<VT>(b);
-    g.PT = std::min(b, 64 * g.VEC);
-    g.P = g.PT / g.VEC;
-    return g;
-}
-
-template <typename VT>
-int dots_grid(const Launcher& L, int64_t n, int b, int J)
-{
-    const StreamGeom g = stream_geom<VT>(b);
-    const int G = std::max(1, (J + DOT_K - 1) / DOT_K);
-    const int RS = std::max(1, 256 / (g.P * G));
-    const int64_t gx = (n + RS - 1) / RS;
-    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(gx, int64_t(L.sms) * 2)));
-}
-
-template <typename VT>
-int reorth_grid(const Launcher& L, int64_t n, int b)
-{
-    const StreamGeom g = stream_geom<VT>(b);
-    const int RS = std::max(1, 512 / g.P);
-    const int64_t gx = (n + RS - 1) / RS;
-    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(gx, int64_t(L.sms) * 2)));
-}
-
-template <typename VT>
-slq_status update_dots(Launcher& L, int grid, int64_t n, int b, const VT* W, VT* Wout,
-                       int do_update, const VT* Vj, const double* sj, const double* aj,
-                       const VT* Vm, const double* sm, const double* bm, const VT* basis,
-                       int64_t slot_elems, int bs, int last, int J, double* partials)
-{
-    const StreamGeom g = stream_geom<VT>(b);
-    const int G = std::max(1, (J + DOT_K - 1) / DOT_K);
-    const int RS = std::max(1, 256 / (g.P * G));
-    const int threads = g.P * G * RS;
-    const size_t smem = (RS > 1) ? static_cast<size_t>(RS) * J * g.PT * sizeof(double) : 0;
-    dim3 grd(grid, b / g.PT);
-    const double vb = double(n) * b * sizeof(VT);
-    ProfScope prof(SLQ_K_DOTS, vb * (1 + J + (do_update ? (Vm ? 3 : 2) : 0)), L.st);
-#define SLQ_DOTS(VECV)                                                                    \
-    {                                                                                     \
-        static bool attr = false;                                                         \
-        if (!attr)                                                                        \
-        {                                                                                 \
-            SLQ_CK(cudaFuncSetAttribute(k_update_dots<VT, VECV>,                          \
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,      \
-                                        200 * 1024));                                     \
-            attr = true;                                                                  \
-        }                                                                                 \
-        k_update_dots<VT, VECV><<<grd, threads, smem, L.st>>>(                            \
-            n, b, g.PT, G, RS, W, Wout, do_update, Vj, sj, aj, Vm, sm, bm, basis,         \
-            slot_elems, bs, last, J, partials);                                           \
-    }
-    if (g.VEC == 4) SLQ_DOTS(4)
-    else if (g.VEC == 2) SLQ_DOTS(2)
-    else SLQ_DOTS(1)
-#undef SLQ_DOTS
-    SLQ_LAUNCH_CK();
-    ++L.launches;
-    return SLQ_OK;
-}
-
-template <typename VT>
-slq_status reorth(Launcher& L, int grid, int64_t n, int b, const VT* Win, VT* Wout,
-                  int do_update, const VT* Vj, const double* sj, const double* aj,
-                  const VT* Vm, const double* sm, const double* bm, const VT* basis,
-                  int64_t slot_elems, int bs, int last, int J, const VT* coef,
-                  int want_norm, double* partials)
-{
-    const StreamGeom g = stream_geom<VT>(b);
-    const int RS = std::max(1, 512 / g.P);
-    const int threads = g.P * RS;
-    const size_t smem = ((static_cast<size_t>(J) * g.PT * sizeof(VT) + 15) / 16) * 16 +
-                        static_cast<size_t>(RS) * g.PT * sizeof(double);
-    dim3 grd(grid, b / g.PT);
-    const double vb = double(n) * b * sizeof(VT);
-    ProfScope prof(SLQ_K_REORTH, vb * (2 + J + (do_update ? (Vm ? 2 : 1) : 0)), L.st);
-#define SLQ_REORTH(VECV)                                                                  \
-    {                                                                                     \
-        static bool attr = false;                                                         \
-        if (!attr)                                                                        \
-        {                                                                                 \
-            SLQ_CK(cudaFuncSetAttribute(k_reorth<VT, VECV>,                               \
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,      \
-                                        200 * 1024));                                     \
-            attr = true;                                                                  \
-        }                                                                                 \
-        k_reorth<VT, VECV><<<grd, threads, smem, L.st>>>(                                 \
-            n, b, g.PT, RS, Win, Wout, do_update, Vj, sj, aj, Vm, sm, bm, basis,          \
-            slot_elems, bs, last, J, coef, want_norm, partials);                          \
-    }
-    if (g.VEC == 4) SLQ_REORTH(4)
-    else if (g.VEC == 2) SLQ_REORTH(2)
-    else SLQ_REORTH(1)
-#undef SLQ_REORTH
-    SLQ_LAUNCH_CK();
-    ++L.launches;
-    return SLQ_OK;
-}
-
-template <typename VT>
 slq_status finalize(Launcher& L, const double* partials, int nparts, int cols, int mode,
                     double* out, VT* coef, const double* scales, int b, int bs, int last,
                     double* next_scale, int32_t* active, int32_t* size, int check_break,

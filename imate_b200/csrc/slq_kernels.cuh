@@ -29,9 +29,7 @@
 namespace slq {
 
 constexpr unsigned FULL_MASK = 0xffffffffu;
-constexpr int DOT_K = 8;        // basis vectors per thread in k_update_dots
-constexpr int DOT_GMAX = 8;     // basis-vector groups per CTA
-constexpr int MAX_J = DOT_K * DOT_GMAX;  // basis vectors per launch
+constexpr int MAX_J = 64;  // basis vectors per streaming-pass launch
 
 // ---------------------------------------------------------------------------
 // small helpers
@@ -286,242 +284,6 @@ k_spmm(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
         double s = 0.0;
         for (int w = 0; w < nwarps; ++w) s += smem_spmm[w * b + p];
         partials[static_cast<int64_t>(blockIdx.x) * b + p] = s;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Fused Lanczos three-term update and reorthogonalisation inner products.
-//
-// w = W - alpha_j (s_j v_j) - beta_{j-1} (s_{j-1} v_{j-1})  (if do_update;
-// written to Wout, a buffer no thread of the launch reads) and, for the J
-// basis vectors last, last-1, ..., partial sums of <v_i, w> (unscaled;
-// k_finalize applies s_i).
-//
-// CTA = probe tile of PT = P*VEC probes (blockIdx.y) x G basis-vector groups
-// x RS row lanes.  A thread owns VEC probes and the basis vectors
-// g, g+G, ..., so it keeps DOT_K x VEC FP64 accumulators and no intra-CTA
-// reduction is needed across basis vectors; only the RS row lanes are summed
-// through shared memory at the end.
-// ---------------------------------------------------------------------------
-
-template <typename VT, int VEC>
-__global__ void __launch_bounds__(512)
-k_update_dots(int64_t n, int b, int PT, int G, int RS, const VT* W,
-              VT* __restrict__ Wout, int do_update,
-              const VT* Vj, const double* __restrict__ sj,
-              const double* __restrict__ aj, const VT* Vm,
-              const double* __restrict__ sm, const double* __restrict__ bm,
-              const VT* basis, int64_t slot_elems, int bs, int last, int J,
-              double* __restrict__ partials)
-{
-    extern __shared__ double smem_dots[];
-    const int P = PT / VEC;
-    const int tid = threadIdx.x;
-    const int pv = tid % P;
-    const int t2 = tid / P;
-    const int rs = t2 % RS;
-    const int g = t2 / RS;
-    const int pl = pv * VEC;                       // probe within tile
-    const int p0 = blockIdx.y * PT + pl;           // probe within block
-
-    double acc[DOT_K][VEC];
-#pragma unroll
-    for (int k = 0; k < DOT_K; ++k)
-#pragma unroll
-        for (int e = 0; e < VEC; ++e) acc[k][e] = 0.0;
-
-    double cj[VEC], cm[VEC];
-#pragma unroll
-    for (int e = 0; e < VEC; ++e)
-    {
-        cj[e] = do_update ? aj[p0 + e] * sj[p0 + e] : 0.0;
-        cm[e] = (do_update && Vm) ? bm[p0 + e] * sm[p0 + e] : 0.0;
-    }
-    const VT* vptr[DOT_K];
-#pragma unroll
-    for (int k = 0; k < DOT_K; ++k)
-    {
-        const int i = g + k * G;
-        vptr[k] = (i < J) ? basis + static_cast<int64_t>(ring_slot(last - i, bs)) * slot_elems
-                          : nullptr;
-    }
-
-    for (int64_t r = static_cast<int64_t>(blockIdx.x) * RS + rs; r < n;
-         r += static_cast<int64_t>(gridDim.x) * RS)
-    {
-        const int64_t o = r * b + p0;
-        VT wv[VEC];
-        load_n<VT, VEC>(W + o, wv);
-        double w[VEC];
-        if (do_update)
-        {
-            VT a[VEC], m[VEC];
-            load_n<VT, VEC>(Vj + o, a);
-            if (Vm) load_n<VT, VEC>(Vm + o, m);
-#pragma unroll
-            for (int e = 0; e < VEC; ++e)
-            {
-                double t = static_cast<double>(wv[e]) - cj[e] * static_cast<double>(a[e]);
-                if (Vm) t -= cm[e] * static_cast<double>(m[e]);
-                wv[e] = static_cast<VT>(t);
-            }
-            if (g == 0) store_n<VT, VEC>(Wout + o, wv);
-        }
-#pragma unroll
-        for (int e = 0; e < VEC; ++e) w[e] = static_cast<double>(wv[e]);
-#pragma unroll
-        for (int k = 0; k < DOT_K; ++k)
-        {
-            if (vptr[k])
-            {
-                VT v[VEC];
-                load_n<VT, VEC>(vptr[k] + o, v);
-#pragma unroll
-                for (int e = 0; e < VEC; ++e) acc[k][e] += static_cast<double>(v[e]) * w[e];
-            }
-        }
-    }
-
-    // reduce the RS row lanes; layout red[rs][i][pl + e]
-    if (RS > 1)
-    {
-#pragma unroll
-        for (int k = 0; k < DOT_K; ++k)
-        {
-            const int i = g + k * G;
-            if (i < J)
-#pragma unroll
-                for (int e = 0; e < VEC; ++e)
-                    smem_dots[(static_cast<int64_t>(rs) * J + i) * PT + pl + e] = acc[k][e];
-        }
-        __syncthreads();
-        const int nthreads = blockDim.x;
-        for (int idx = tid; idx < J * PT; idx += nthreads)
-        {
-            double s = 0.0;
-            for (int q = 0; q < RS; ++q) s += smem_dots[static_cast<int64_t>(q) * J * PT + idx];
-            const int i = idx / PT;
-            const int pp = idx % PT;
-            partials[(static_cast<int64_t>(blockIdx.x) * J + i) * b + blockIdx.y * PT + pp] = s;
-        }
-    }
-    else
-    {
-#pragma unroll
-        for (int k = 0; k < DOT_K; ++k)
-        {
-            const int i = g + k * G;
-            if (i < J)
-#pragma unroll
-                for (int e = 0; e < VEC; ++e)
-                    partials[(static_cast<int64_t>(blockIdx.x) * J + i) * b + p0 + e] = acc[k][e];
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Reorthogonalisation update (and the plain three-term update):
-// w = Win [- alpha_j s_j v_j - beta_{j-1} s_{j-1} v_{j-1}] - sum_i c_i v_i,
-// written to Wout (may alias Win or a basis slot: every element is read
-// before the same thread writes it), with FP64 partials of |w|^2.
-// c_i = h_i s_i, [J][b] in VT, staged in shared memory per probe tile.
-// ---------------------------------------------------------------------------
-
-template <typename VT, int VEC>
-__global__ void __launch_bounds__(512)
-k_reorth(int64_t n, int b, int PT, int RS, const VT* Win, VT* Wout,
-         int do_update, const VT* Vj, const double* __restrict__ sj,
-         const double* __restrict__ aj, const VT* Vm,
-         const double* __restrict__ sm, const double* __restrict__ bm,
-         const VT* basis, int64_t slot_elems, int bs, int last, int J,
-         const VT* __restrict__ coef, int want_norm,
-         double* __restrict__ partials)
-{
-    extern __shared__ unsigned char smem_raw[];
-    VT* cs = reinterpret_cast<VT*>(smem_raw);                 // [J][PT]
-    double* red = reinterpret_cast<double*>(smem_raw + ((J * PT * sizeof(VT) + 15) / 16) * 16);
-    const int P = PT / VEC;
-    const int tid = threadIdx.x;
-    const int pv = tid % P;
-    const int rs = tid / P;
-    const int pl = pv * VEC;
-    const int p0 = blockIdx.y * PT + pl;
-
-    for (int idx = tid; idx < J * PT; idx += blockDim.x)
-        cs[idx] = coef[static_cast<int64_t>(idx / PT) * b + blockIdx.y * PT + idx % PT];
-    __syncthreads();
-
-    double cj[VEC], cm[VEC], nacc[VEC];
-#pragma unroll
-    for (int e = 0; e < VEC; ++e)
-    {
-        cj[e] = do_update ? aj[p0 + e] * sj[p0 + e] : 0.0;
-        cm[e] = (do_update && Vm) ? bm[p0 + e] * sm[p0 + e] : 0.0;
-        nacc[e] = 0.0;
-    }
-
-    for (int64_t r = static_cast<int64_t>(blockIdx.x) * RS + rs; r < n;
-         r += static_cast<int64_t>(gridDim.x) * RS)
-    {
-        const int64_t o = r * b + p0;
-        VT wv[VEC];
-        load_n<VT, VEC>(Win + o, wv);
-        double w[VEC];
-#pragma unroll
-        for (int e = 0; e < VEC; ++e) w[e] = static_cast<double>(wv[e]);
-        if (do_update)
-        {
-            VT a[VEC], m[VEC];
-            load_n<VT, VEC>(Vj + o, a);
-            if (Vm) load_n<VT, VEC>(Vm + o, m);
-#pragma unroll
-            for (int e = 0; e < VEC; ++e)
-            {
-                w[e] -= cj[e] * static_cast<double>(a[e]);
-                if (Vm) w[e] -= cm[e] * static_cast<double>(m[e]);
-            }
-        }
-        int i = 0;
-        for (; i + 4 <= J; i += 4)
-        {
-            VT v[4][VEC];
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                load_n<VT, VEC>(basis + static_cast<int64_t>(ring_slot(last - i - u, bs)) * slot_elems + o, v[u]);
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int e = 0; e < VEC; ++e)
-                    w[e] -= static_cast<double>(cs[(i + u) * PT + pl + e]) * static_cast<double>(v[u][e]);
-        }
-        for (; i < J; ++i)
-        {
-            VT v[VEC];
-            load_n<VT, VEC>(basis + static_cast<int64_t>(ring_slot(last - i, bs)) * slot_elems + o, v);
-#pragma unroll
-            for (int e = 0; e < VEC; ++e)
-                w[e] -= static_cast<double>(cs[i * PT + pl + e]) * static_cast<double>(v[e]);
-        }
-#pragma unroll
-        for (int e = 0; e < VEC; ++e)
-        {
-            wv[e] = static_cast<VT>(w[e]);
-            const double d = static_cast<double>(wv[e]);
-            nacc[e] += d * d;
-        }
-        store_n<VT, VEC>(Wout + o, wv);
-    }
-
-    if (!want_norm) return;
-    const int RSn = blockDim.x / P;
-#pragma unroll
-    for (int e = 0; e < VEC; ++e) red[rs * PT + pl + e] = nacc[e];
-    __syncthreads();
-    for (int pp = tid; pp < PT; pp += blockDim.x)
-    {
-        double s = 0.0;
-        for (int q = 0; q < RSn; ++q) s += red[q * PT + pp];
-        partials[static_cast<int64_t>(blockIdx.x) * b + blockIdx.y * PT + pp] = s;
     }
 }
 
