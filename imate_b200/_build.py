@@ -14,7 +14,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libslq_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["slq_engine.cu", "slq_mlp.cu", "slq_rng.cpp", "slq_stats.cpp"]
+SOURCES = ["slq_engine.cu", "slq_mlp.cu", "slq_rng.cpp", "slq_stats.cpp",
+           "slq_order.cpp"]
 HEADERS = ["slq_kernels.cuh", "slq_rng.h"]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -36,7 +36,7 @@ EXPORTS = (
     "slq_mlp_grad", "slq_mlp_train", "slq_operator_tune_workspace_bytes",
     "slq_operator_tune", "slq_operator_set_variant",
     "slq_batch_workspace_bytes", "slq_batch_create", "slq_batch_run",
-    "slq_batch_info", "slq_batch_destroy",
+    "slq_batch_info", "slq_batch_destroy", "slq_group_order",
 )
 TUNE_MAX_CANDIDATES = 16
 SPMM_KINDS = ("csr", "row-group", "row-group-tma")
@@ -173,6 +173,7 @@ def _declare(lib):
         "slq_batch_info": (i32, [vp, ctypes.POINTER(i64),
                                  ctypes.POINTER(i64)]),
         "slq_batch_destroy": (i32, [vp]),
+        "slq_group_order": (i32, [i64, vp, vp, vp, i32, i32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

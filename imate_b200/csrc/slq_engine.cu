@@ -443,8 +443,8 @@ extern "C" slq_status slq_operator_workspace_bytes(int64_t num_rows, int64_t num
                                                    int need_transpose, int has_perm,
                                                    int group_rows, size_t* bytes)
 {
-    if (group_rows != 0 && group_rows != 4 && group_rows != 8)
-        return fail(SLQ_ERR_BAD_ARG, "group_rows must be 0, 4 or 8");
+    if (group_rows != 0 && group_rows != 4 && group_rows != 8 && group_rows != 16)
+        return fail(SLQ_ERR_BAD_ARG, "group_rows must be 0, 4, 8 or 16");
     if (!bytes || num_rows < 0 || num_cols < 0 || nnz < 0)
         return fail(SLQ_ERR_BAD_ARG, "operator_workspace_bytes: bad argument");
     if (has_perm && (format != SLQ_CSR || num_rows != num_cols))
@@ -816,14 +816,18 @@ int spmm_candidates(const slq_op* op, int transpose, int b, SpmmCand* out)
     const int32_t* gptr = transpose ? op->t_gptr : op->a_gptr;
     const int G = op->group_rows;
     if (!G || !gptr) return n;
+    // FP64 row groups: b <= 64, LV <= 2, G <= 8 (shared-memory staging);
+    // 16-row groups keep LV <= 2 (16 x LV accumulators per lane)
     const int bmax = (sizeof(VT) == 8) ? 64 : 256;
-    if (b >= 32 && b <= bmax)
-        for (int lv = 1; lv <= ((sizeof(VT) == 8) ? 2 : 4); lv *= 2)
+    const int lvmax = (sizeof(VT) == 8 || G == 16) ? 2 : 4;
+    if (b >= 32 && b <= bmax && (sizeof(VT) == 4 || G <= 8))
+        for (int lv = 1; lv <= lvmax; lv *= 2)
         {
             const int ns = b / (32 * lv);
             if (ns >= 1 && ns <= 8 && 32 * lv * ns == b) out[n++] = {CAND_RG, G, lv, ns};
         }
-    if (sizeof(VT) == 4 && G == 8 && (b == 128 || b == 256)) out[n++] = {CAND_TMA, 8, 4, b / 128};
+    if (sizeof(VT) == 4 && (G == 8 || G == 16) && (b == 128 || b == 256))
+        out[n++] = {CAND_TMA, G, 4, b / 128};
     return n;
 }
 
@@ -843,12 +847,16 @@ slq_status spmm_cand(Launcher& L, const slq_op* op, int transpose, const SpmmCan
         {
             if (!xmap || !error) return fail(SLQ_ERR_BAD_ARG, "TMA SpMM needs a tensor map");
             const float* gval = static_cast<const float*>(transpose ? op->t_gval : op->a_gval);
-            if (c.ns == 2)
-                return spmm_rgt_inst<8, 2>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y,
-                                           Z, zc, zs, epi, partials, error, op->nnz, xrows,
-                                           grid_out);
-            return spmm_rgt_inst<8, 1>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y, Z,
-                                       zc, zs, epi, partials, error, op->nnz, xrows, grid_out);
+#define SLQ_RGT_CASE(GG, NSS)                                                                  \
+    if (c.g == GG && c.ns == NSS)                                                              \
+        return spmm_rgt_inst<GG, NSS>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y, Z, \
+                                      zc, zs, epi, partials, error, op->nnz, xrows, grid_out);
+            SLQ_RGT_CASE(8, 1)
+            SLQ_RGT_CASE(8, 2)
+            SLQ_RGT_CASE(16, 1)
+            SLQ_RGT_CASE(16, 2)
+#undef SLQ_RGT_CASE
+            return fail(SLQ_ERR_BAD_ARG, "TMA SpMM: unsupported tile");
         }
         return fail(SLQ_ERR_BAD_ARG, "TMA SpMM is FP32 only");
     }
@@ -875,6 +883,16 @@ slq_status spmm_cand(Launcher& L, const slq_op* op, int transpose, const SpmmCan
     }
         SLQ_RG_ALL(8)
         SLQ_RG_ALL(4)
+        if constexpr (sizeof(VT) == 4)
+        {
+            SLQ_RG_CASE(16, 1, 1)
+            SLQ_RG_CASE(16, 1, 2)
+            SLQ_RG_CASE(16, 2, 1)
+            SLQ_RG_CASE(16, 1, 4)
+            SLQ_RG_CASE(16, 2, 2)
+            SLQ_RG_CASE(16, 1, 8)
+            SLQ_RG_CASE(16, 2, 4)
+        }
 #undef SLQ_RG_ALL
 #undef SLQ_RG_CASE
         return fail(SLQ_ERR_BAD_ARG, "row-group SpMM: unsupported tile");
@@ -1186,7 +1204,7 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
     bool use_tma = false;
     if constexpr (sizeof(VT) == 4)
     {
-        if (op->group_rows == 8 && (b == 128 || b == 256))
+        if ((op->group_rows == 8 || op->group_rows == 16) && (b == 128 || b == 256))
         {
             use_tma = true;
             vmaps.resize(bs);

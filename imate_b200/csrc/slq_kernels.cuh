@@ -1005,7 +1005,8 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
         for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
         {
             const int64_t row0 = tile * a.T;
-            double w[R], vj[R], vm[R];
+            // 9 warps put 3 on one scheduler: at most 168 registers/thread
+            double w[R], vj[R];
             for (int item = 0; item < nitems; ++item)
             {
                 if (*reinterpret_cast<volatile int*>(abort_flag)) { ok = false; break; }
@@ -1041,23 +1042,22 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
                 {
 #pragma unroll
                     for (int k = 0; k < R; ++k)
-                    {
-                        vm[k] = static_cast<double>(st[(roff + k * RSTEP) * PT + pl]);
-                        w[k] -= cm * vm[k];
-                    }
+                        w[k] -= cm * static_cast<double>(st[(roff + k * RSTEP) * PT + pl]);
                 }
                 else
                 {
                     const int i = ib;
                     if (MODE == 0)
                     {
-                        // four independent FMA chains (two warps per scheduler
-                        // cannot hide one long FP64 dependency chain)
-                        double l[4] = {0.0, 0.0, 0.0, 0.0};
+                        // eight independent FMA chains: the pass is bound by
+                        // the latency of this reduction (two warps per
+                        // scheduler), not by FP64 throughput
+                        double l[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
                         for (int k = 0; k < R; ++k)
-                            l[k & 3] += static_cast<double>(st[(roff + k * RSTEP) * PT + pl]) * w[k];
-                        extra[i * STREAM_CONSUMERS + tid] = prev + ((l[0] + l[1]) + (l[2] + l[3]));
+                            l[k & 7] += static_cast<double>(st[(roff + k * RSTEP) * PT + pl]) * w[k];
+                        extra[i * STREAM_CONSUMERS + tid] =
+                            prev + (((l[0] + l[1]) + (l[2] + l[3])) + ((l[4] + l[5]) + (l[6] + l[7])));
                     }
                     else
                     {
@@ -1067,12 +1067,11 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
                             w[k] -= c * static_cast<double>(st[(roff + k * RSTEP) * PT + pl]);
                     }
                 }
-                release(s);
-                if (++s == a.S) { s = 0; phase ^= 1; }
                 if (MODE == 0 && upd && item == npre - 1)
                 {
                     // updated w: round to storage, store, and serve the
-                    // products with v_j, v_{j-1} from registers
+                    // products with v_j (registers) and v_{j-1} (still in
+                    // this item's stage) without reading them again
                     double lj = 0.0, lm = 0.0;
 #pragma unroll
                     for (int k = 0; k < R; ++k)
@@ -1081,11 +1080,14 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
                         w[k] = static_cast<double>(wr);
                         a.Wout[(row0 + roff + k * RSTEP) * b + p0 + pl] = wr;
                         lj += vj[k] * w[k];
-                        if (a.Vm) lm += vm[k] * w[k];
+                        if (a.Vm)
+                            lm += static_cast<double>(st[(roff + k * RSTEP) * PT + pl]) * w[k];
                     }
                     if (J > 0) extra[0 * STREAM_CONSUMERS + tid] += lj;
                     if (a.Vm && J > 1) extra[1 * STREAM_CONSUMERS + tid] += lm;
                 }
+                release(s);
+                if (++s == a.S) { s = 0; phase ^= 1; }
             }
             if (MODE == 1 && ok)
             {

@@ -88,11 +88,12 @@ slq_status slq_operator_workspace_bytes(int64_t num_rows, int64_t num_cols,
  * window inside L2.  slq_operator_dot on such an operator acts on permuted
  * vectors (y' = B x').
  *
- * group_rows (0, 4 or 8) additionally stores A (and A^T) in a row-group
+ * group_rows (0, 4, 8 or 16) additionally stores A (and A^T) in a row-group
  * format: per group of consecutive rows, the sorted union of their column
  * indices with a dense value per (union column, row), zero where absent.
  * One gathered row of a probe block then feeds group_rows rows of FMAs, which
  * cuts the SpMM's L1/L2 gather traffic for wide blocks (32 <= b <= 256).
+ * slq_group_order makes the groups of consecutive rows overlap well.
  * Results are bit-identical to the CSR kernel (same summation order; the
  * padding adds exact zeros).
  *
@@ -107,6 +108,21 @@ slq_status slq_operator_create(const void* data, const int32_t* indices,
                                int group_rows, void* workspace,
                                size_t workspace_bytes, void* stream,
                                slq_op** out);
+
+/* Row-group aggregation order (host; no counterpart in the reference).
+ * For a square CSR pattern (host arrays; data of dtype or NULL), visits the
+ * rows in base_order (NULL = identity) and makes each row not yet placed the
+ * seed of a group of group_rows rows: the seed, its not-yet-placed
+ * neighbours by decreasing |a_ij|, their neighbours, and, when the
+ * neighbourhood runs out, the next unplaced rows of the base order.
+ * order[k] receives the row at position k; every group but the last has
+ * exactly group_rows rows, so passing order as slq_operator_create's perm
+ * lines the groups up with the row-group format's, whose cost falls with
+ * the overlap of the rows' column sets. */
+slq_status slq_group_order(int64_t n, const int32_t* indptr,
+                           const int32_t* indices, const void* data,
+                           int dtype, int group_rows,
+                           const int32_t* base_order, int32_t* order);
 
 /* Release the host-side operator record (device arrays stay with their
  * owners).  Replaces the cuLinearOperator destructors

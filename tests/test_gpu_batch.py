@@ -270,7 +270,7 @@ def test_device_built_correlation_matrix(cuda):
     assert np.max(np.abs(Ap.data - B.data)) < 1e-15
     # an operator over the device arrays equals one uploaded from the host
     D = ib.DeviceMatrix(ip, ind, dat, A.shape, group_rows=8)
-    H = ib.Matrix(B, reorder=False, group_rows=8)
+    H = ib.Matrix(B, reorder=False, group_rows=8, aggregate=False)
     kw = dict(method="slq", gpu=True, return_info=True, min_num_samples=64,
               max_num_samples=64, error_rtol=0.0, lanczos_degree=20,
               orthogonalize=-1, seed=3)

@@ -347,13 +347,16 @@ def test_reordered_gram_matches_oracle(cuda, corr_small):
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("width", [32, 64, 128, 256])
-@pytest.mark.parametrize("group", [4, 8])
+@pytest.mark.parametrize("group", [4, 8, 16])
 def test_row_group_products_bit_identical_to_csr(cuda, dtype, width, group):
+    if group == 16 and dtype == np.float64:
+        pytest.skip("16-row groups are served by the FP32 kernels only")
     A = ib.correlation_matrix(5000, scale=0.02, threshold=0.05, shift=0.1,
                               seed=7, dtype=dtype)
     x = np.random.default_rng(1).standard_normal((5000, width)).astype(dtype)
+    # same row order for both (aggregation would change the summation order)
     plain = ib.Matrix(A, reorder=True, group_rows=0)
-    grouped = ib.Matrix(A, reorder=True, group_rows=group)
+    grouped = ib.Matrix(A, reorder=True, group_rows=group, aggregate=False)
     op0 = plain.get_device_operator(need_transpose=True)
     op1 = grouped.get_device_operator(need_transpose=True)
     assert op1.group_rows == group
@@ -396,16 +399,17 @@ def test_tma_row_group_spmm_bit_identical_in_estimator(cuda, gram, block_size):
     kw = dict(min_num_samples=block_size, max_num_samples=block_size,
               error_rtol=0.0, lanczos_degree=12, orthogonalize=-1, seed=4)
     out = []
-    for g in (0, 8):
-        M = ib.Matrix(A, reorder=True, group_rows=g)
+    for g in (0, 8, 16):
+        M = ib.Matrix(A, reorder=True, group_rows=g, aggregate=False)
         tr, info = _run("log", M, gram=gram, block_size=block_size,
                         coefficients=True, **kw)
         assert M.get_device_operator(need_transpose=gram).group_rows == g
         out.append(info)
-    assert rel(out[1]["convergence"]["samples"],
-               out[0]["convergence"]["samples"]) < 1e-9
-    assert rel(out[1]["engine"]["alpha"], out[0]["engine"]["alpha"]) < 1e-9
-    assert rel(out[1]["engine"]["beta"], out[0]["engine"]["beta"]) < 1e-9
+    for o in out[1:]:
+        assert rel(o["convergence"]["samples"],
+                   out[0]["convergence"]["samples"]) < 1e-9
+        assert rel(o["engine"]["alpha"], out[0]["engine"]["alpha"]) < 1e-9
+        assert rel(o["engine"]["beta"], out[0]["engine"]["beta"]) < 1e-9
 
 
 @pytest.mark.parametrize("fmt", ["csr", "csc"])
@@ -549,3 +553,28 @@ def test_other_functions_match_reference(cuda, golden, corr_small, case):
     assert rel(samples[order], g[key + "_samples"][order]) < RTOL_FP64
     assert rel(np.atleast_1d(tr), g[key + "_trace"]) < RTOL_FP64
 
+
+
+@pytest.mark.parametrize("group", [8, 16])
+def test_aggregated_groups_match_oracle(cuda, group):
+    # neighbour-aggregated row order (a symmetric permutation): FP64 samples
+    # within 1e-10 of the oracle (8-row groups; 16-row groups are FP32-only,
+    # compared with the FP64 run on identical probes)
+    A = ib.correlation_matrix(20000, scale=0.01, threshold=0.05, shift=0.2,
+                              seed=6)
+    kw = dict(min_num_samples=4, max_num_samples=16, error_rtol=1e-9,
+              lanczos_degree=12, orthogonalize=-1, seed=8)
+    M64 = ib.Matrix(A, reorder=True, group_rows=8, aggregate=True)
+    tr64, info64 = _run("log", M64, gram=False, block_size=16,
+                        coefficients=False, **kw)
+    want = oracle.trace_estimator(A, "log", **kw)
+    assert rel(info64["convergence"]["samples"], want["samples"][:, 0]) < \
+        RTOL_FP64
+    M32 = ib.Matrix(A.astype(np.float32), reorder=True, group_rows=group,
+                    aggregate=True)
+    op = M32.get_device_operator()
+    assert op.group_rows == group and op.perm is not None
+    tr32, info32 = _run("log", M32, gram=False, block_size=16,
+                        coefficients=False, **kw)
+    assert rel(info32["convergence"]["samples"],
+               info64["convergence"]["samples"]) < 1e-5

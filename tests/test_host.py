@@ -219,3 +219,39 @@ def test_consumer_argument_checks(corr_small):
         ib.density(corr_small, sigma=0.0, method="slq", gpu=True)
     with pytest.raises(NotImplementedError):
         ib.trexp(corr_small, method="eigenvalue")
+
+
+def test_group_order_is_an_aligned_permutation_that_raises_fill(lib):
+    from imate_b200.linear_operator import (group_order, _group_fill,
+                                            locality_order)
+    A = ib.correlation_matrix(20000, scale=0.01, threshold=0.05, shift=0.1,
+                              seed=4)
+    base = locality_order(A, True)
+    for G in (8, 16):
+        order = group_order(A, base, G)
+        assert np.array_equal(np.sort(order), np.arange(A.shape[0]))
+        # groups are seeds with their neighbours: every group's rows are
+        # adjacent to the seed or reached through it
+        assert _group_fill(A, order, G) > 1.3 * _group_fill(A, base, G)
+        assert np.array_equal(order, group_order(A, base, G))  # deterministic
+    # identity base order
+    order = group_order(A, None, 8)
+    assert np.array_equal(np.sort(order), np.arange(A.shape[0]))
+
+
+def test_group_order_rejects_bad_input(lib):
+    n = 4
+    ip = np.array([0, 1, 2, 3, 4], np.int32)
+    ind = np.array([0, 1, 2, 5], np.int32)
+    out = np.empty(n, np.int32)
+    st = lib.slq_group_order(n, ip.ctypes.data, ind.ctypes.data, None, 0, 2,
+                             None, out.ctypes.data)
+    assert st == 2  # index out of range
+    ind = np.array([0, 1, 2, 3], np.int32)
+    bad = np.array([0, 0, 1, 2], np.int32)
+    st = lib.slq_group_order(n, ip.ctypes.data, ind.ctypes.data, None, 0, 2,
+                             bad.ctypes.data, out.ctypes.data)
+    assert st == 1  # base order not a permutation
+    st = lib.slq_group_order(n, ip.ctypes.data, ind.ctypes.data, None, 0, 2,
+                             None, out.ctypes.data)
+    assert st == 0 and sorted(out) == [0, 1, 2, 3]
