@@ -37,6 +37,7 @@ EXPORTS = (
     "slq_operator_tune", "slq_operator_set_variant",
     "slq_batch_workspace_bytes", "slq_batch_create", "slq_batch_run",
     "slq_batch_info", "slq_batch_destroy", "slq_group_order",
+    "slq_rcm_order",
 )
 TUNE_MAX_CANDIDATES = 16
 SPMM_KINDS = ("csr", "row-group", "row-group-tma")
@@ -174,6 +175,7 @@ def _declare(lib):
                                  ctypes.POINTER(i64)]),
         "slq_batch_destroy": (i32, [vp]),
         "slq_group_order": (i32, [i64, vp, vp, vp, i32, i32, vp, vp]),
+        "slq_rcm_order": (i32, [i64, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

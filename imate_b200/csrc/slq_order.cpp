@@ -1,5 +1,7 @@
-// Row-group aggregation order (host).
+// Host-side row orders of square sparse matrices: reverse Cuthill-McKee
+// (slq_rcm_order) and row-group aggregation (slq_group_order).
 //
+// Row-group aggregation:
 // The row-group SpMM formats store, per group of G consecutive rows, the
 // union of their columns with a dense value per (union column, row); their
 // cost grows with the union, i.e. with how little the G rows' column sets
@@ -110,7 +112,79 @@ void aggregate(int64_t n, const int32_t* indptr, const int32_t* indices, const V
     }
 }
 
+// Breadth-first search from `start` over the unvisited rows of its
+// component, the children of a row in increasing degree (Cuthill-McKee);
+// appends the visit order to `out`.
+void cm_bfs(int32_t start, const int32_t* indptr, const int32_t* indices, const int32_t* degree,
+            std::vector<uint8_t>& visited, std::vector<int32_t>& out,
+            std::vector<std::pair<int32_t, int32_t>>& kids)
+{
+    size_t head = out.size();
+    out.push_back(start);
+    visited[start] = 1;
+    while (head < out.size())
+    {
+        const int32_t r = out[head++];
+        kids.clear();
+        for (int32_t e = indptr[r]; e < indptr[r + 1]; ++e)
+        {
+            const int32_t c = indices[e];
+            if (!visited[c])
+            {
+                visited[c] = 1;
+                kids.emplace_back(degree[c], c);
+            }
+        }
+        std::sort(kids.begin(), kids.end());
+        for (const auto& k : kids) out.push_back(k.second);
+    }
+}
+
 }  // namespace
+
+extern "C" slq_status slq_rcm_order(int64_t n, const int32_t* indptr, const int32_t* indices,
+                                    int32_t* order)
+{
+    if (n < 0 || !indptr || !indices || !order)
+    {
+        slq::set_error("rcm_order: bad arguments");
+        return SLQ_ERR_BAD_ARG;
+    }
+    for (int64_t r = 0; r < n; ++r)
+        if (indptr[r + 1] < indptr[r])
+        {
+            slq::set_error("rcm_order: indptr is not monotone");
+            return SLQ_ERR_BAD_CSR;
+        }
+    for (int64_t e = 0; e < indptr[n]; ++e)
+        if (indices[e] < 0 || indices[e] >= n)
+        {
+            slq::set_error("rcm_order: column index out of range");
+            return SLQ_ERR_BAD_CSR;
+        }
+    std::vector<int32_t> degree(static_cast<size_t>(n));
+    for (int64_t r = 0; r < n; ++r) degree[r] = indptr[r + 1] - indptr[r];
+    // rows by increasing degree: component start candidates
+    std::vector<int32_t> by_degree(static_cast<size_t>(n));
+    for (int64_t r = 0; r < n; ++r) by_degree[r] = static_cast<int32_t>(r);
+    std::stable_sort(by_degree.begin(), by_degree.end(),
+                     [&](int32_t a, int32_t b) { return degree[a] < degree[b]; });
+    std::vector<uint8_t> visited(static_cast<size_t>(n), 0);
+    std::vector<int32_t> out;
+    std::vector<std::pair<int32_t, int32_t>> kids;
+    out.reserve(static_cast<size_t>(n));
+    for (int32_t seed : by_degree)
+    {
+        if (visited[seed]) continue;
+        // each component starts at its lowest-degree row (as scipy's
+        // reverse_cuthill_mckee does)
+        const int32_t start = seed;
+        cm_bfs(start, indptr, indices, degree.data(), visited, out, kids);
+    }
+    // reverse Cuthill-McKee
+    for (int64_t k = 0; k < n; ++k) order[k] = out[static_cast<size_t>(n - 1 - k)];
+    return SLQ_OK;
+}
 
 extern "C" slq_status slq_group_order(int64_t n, const int32_t* indptr, const int32_t* indices,
                                       const void* data, int dtype, int group_rows,

@@ -32,7 +32,8 @@ def _dtype_code(dtype):
 
 
 def locality_order(A, reorder="auto"):
-    """Reverse Cuthill-McKee order of a square sparse matrix, or None.
+    """Reverse Cuthill-McKee order (``rcm_order``) of a square sparse
+    matrix, or None.
 
     'auto' reorders square matrices of order >= 16384 whose nonzeros lie far
     from the diagonal (mean |i - j| > 256) when RCM shrinks that distance at
@@ -41,7 +42,6 @@ def locality_order(A, reorder="auto"):
     """
     if reorder is False or A.shape[0] != A.shape[1]:
         return None
-    from scipy.sparse.csgraph import reverse_cuthill_mckee
     A = sp.csr_matrix(A)
     n = A.shape[0]
     if reorder == "auto":
@@ -49,22 +49,34 @@ def locality_order(A, reorder="auto"):
             return None
         # mean |i - j| over the nonzeros of a sample of rows
         rows = np.unique(np.linspace(0, n - 1, min(n, 20000)).astype(np.int64))
-        counts = np.diff(A.indptr)[rows]
-        idx = np.concatenate([np.arange(A.indptr[r], A.indptr[r + 1])
-                              for r in rows])
-        ri = np.repeat(rows, counts)
-        spread = float(np.mean(np.abs(A.indices[idx] - ri))) if idx.size \
-            else 0.0
+        S = A[rows]
+        ri = np.repeat(rows, np.diff(S.indptr))
+        cols = S.indices.astype(np.int64)
+        spread = float(np.mean(np.abs(cols - ri))) if cols.size else 0.0
         if spread <= 256.0:
             return None
-    perm = reverse_cuthill_mckee(A, symmetric_mode=True)
+    perm = rcm_order(A)
     if reorder == "auto":
         inv = np.empty_like(perm)
         inv[perm] = np.arange(n, dtype=perm.dtype)
-        new_spread = float(np.mean(np.abs(inv[A.indices[idx]] - inv[ri])))
+        new_spread = float(np.mean(np.abs(inv[cols] - inv[ri])))
         if new_spread * 4.0 > spread:
             return None
     return np.ascontiguousarray(perm, dtype=np.int32)
+
+
+def rcm_order(A):
+    """Reverse Cuthill-McKee order of a square sparse pattern, taken as
+    symmetric (``slq_rcm_order``; the order scipy's reverse_cuthill_mckee
+    with symmetric_mode=True gives)."""
+    A = sp.csr_matrix(A)
+    n = A.shape[0]
+    ip = np.ascontiguousarray(A.indptr, dtype=np.int32)
+    ind = np.ascontiguousarray(A.indices, dtype=np.int32)
+    order = np.empty(n, dtype=np.int32)
+    _lib.check(_lib.load().slq_rcm_order(n, ip.ctypes.data, ind.ctypes.data,
+                                         order.ctypes.data))
+    return order
 
 
 def _group_fill(A, order, G, sample=256):
@@ -74,15 +86,19 @@ def _group_fill(A, order, G, sample=256):
     ngroups = n // G
     if ngroups == 0:
         return 0.0
-    picks = np.linspace(0, ngroups - 1, min(sample, ngroups)).astype(np.int64)
-    fills = []
-    for g in picks:
-        rows = order[g * G:(g + 1) * G]
-        cols = np.concatenate([A.indices[A.indptr[r]:A.indptr[r + 1]]
-                               for r in rows])
-        if cols.size:
-            fills.append(cols.size / (G * np.unique(cols).size))
-    return float(np.mean(fills)) if fills else 0.0
+    picks = np.unique(np.linspace(0, ngroups - 1,
+                                  min(sample, ngroups)).astype(np.int64))
+    rows = np.asarray(order)[(picks[:, None] * G +
+                              np.arange(G)[None, :]).ravel()]
+    S = A[rows]
+    grp = np.repeat(np.repeat(np.arange(picks.size), G), np.diff(S.indptr))
+    if grp.size == 0:
+        return 0.0
+    keys = grp.astype(np.int64) * A.shape[1] + S.indices
+    union = np.bincount(np.unique(keys) // A.shape[1], minlength=picks.size)
+    nnz = np.bincount(grp, minlength=picks.size)
+    ok = union > 0
+    return float(np.mean(nnz[ok] / (G * union[ok]))) if ok.any() else 0.0
 
 
 def group_order(A, base_perm, G):
@@ -182,9 +198,10 @@ class _DeviceOperator:
         if A.format not in ("csr", "csc"):
             A = A.tocsr()
             fmt = _lib.SLQ_CSR
-        A = A.copy()
-        A.sort_indices()
-        A.sum_duplicates()
+        if not (A.has_sorted_indices and A.has_canonical_format):
+            A = A.copy()
+            A.sort_indices()
+            A.sum_duplicates()
         self.dtype_code = _dtype_code(A.dtype)
         self.np_dtype = A.dtype
         self.shape = A.shape

@@ -109,6 +109,16 @@ slq_status slq_operator_create(const void* data, const int32_t* indices,
                                size_t workspace_bytes, void* stream,
                                slq_op** out);
 
+/* Reverse Cuthill-McKee order of a square CSR pattern (host arrays; the
+ * pattern is taken as symmetric).  Each connected component starts at its
+ * lowest-degree row and is visited breadth-first with the children of a row
+ * in increasing degree;
+ * order[k] receives the row at position k of the reversed visit order.  A
+ * bandwidth-reducing order for the locality of the SpMM gathers (no
+ * counterpart in the reference). */
+slq_status slq_rcm_order(int64_t n, const int32_t* indptr,
+                         const int32_t* indices, int32_t* order);
+
 /* Row-group aggregation order (host; no counterpart in the reference).
  * For a square CSR pattern (host arrays; data of dtype or NULL), visits the
  * rows in base_order (NULL = identity) and makes each row not yet placed the
