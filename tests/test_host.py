@@ -255,3 +255,27 @@ def test_group_order_rejects_bad_input(lib):
     st = lib.slq_group_order(n, ip.ctypes.data, ind.ctypes.data, None, 0, 2,
                              None, out.ctypes.data)
     assert st == 0 and sorted(out) == [0, 1, 2, 3]
+
+
+def test_rcm_order_is_a_bandwidth_reducing_permutation(lib):
+    from imate_b200.linear_operator import rcm_order
+    from scipy.sparse.csgraph import reverse_cuthill_mckee
+
+    def spread(A, perm):
+        inv = np.empty(A.shape[0], np.int64)
+        inv[perm] = np.arange(A.shape[0])
+        ri = np.repeat(np.arange(A.shape[0]), np.diff(A.indptr))
+        return float(np.mean(np.abs(inv[A.indices] - inv[ri])))
+
+    R = sp.random(4000, 4000, density=0.001, random_state=5, format="csr")
+    cases = [ib.correlation_matrix(20000, scale=0.01, shift=0.1, seed=2),
+             ib.correlation_matrix(3000, scale=0.02, shift=0.1, seed=1),
+             sp.csr_matrix(R + R.T + sp.eye(4000))]
+    for A in cases:
+        perm = rcm_order(A)
+        assert np.array_equal(np.sort(perm), np.arange(A.shape[0]))
+        ident = np.arange(A.shape[0])
+        ours = spread(A, perm)
+        assert ours < spread(A, ident)
+        ref = spread(A, reverse_cuthill_mckee(A, symmetric_mode=True))
+        assert ours <= 1.1 * ref
