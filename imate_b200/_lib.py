@@ -37,10 +37,10 @@ EXPORTS = (
     "slq_operator_tune", "slq_operator_set_variant",
     "slq_batch_workspace_bytes", "slq_batch_create", "slq_batch_run",
     "slq_batch_info", "slq_batch_destroy", "slq_group_order",
-    "slq_rcm_order",
+    "slq_rcm_order", "slq_tc_selftest",
 )
 TUNE_MAX_CANDIDATES = 16
-SPMM_KINDS = ("csr", "row-group", "row-group-tma")
+SPMM_KINDS = ("csr", "row-group", "row-group-tma", "row-group-tc")
 MLP_WIDTH = 64
 MLP_PARAMS = 64 + 64 + 64 * 64 + 64 + 64 + 1
 MLP_MAX_BATCH = 64
@@ -176,6 +176,7 @@ def _declare(lib):
         "slq_batch_destroy": (i32, [vp]),
         "slq_group_order": (i32, [i64, vp, vp, vp, i32, i32, vp, vp]),
         "slq_rcm_order": (i32, [i64, vp, vp, vp]),
+        "slq_tc_selftest": (i32, [vp, vp, vp, i32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -794,6 +794,37 @@ slq_status spmm_rg_inst(Launcher& L, const int32_t* gptr, const int32_t* gcol, c
     return SLQ_OK;
 }
 
+// Tensor-core row-group SpMM (k_spmm_tc): 16-row groups, b = 128 NS, two
+// CTAs per SM; X rows by TMA gathers (xmap as for k_spmm_rgt).
+template <int NS>
+slq_status spmm_tc_inst(Launcher& L, const CUtensorMap* xmap, const int32_t* gptr,
+                        const int32_t* gcol, const float* gval, int64_t nrows, int b,
+                        const float* X, const double* sx, double shift, float* Y, const float* Z,
+                        const double* zc, const double* zs, int epi, double* partials,
+                        int32_t* error, int64_t nnz, int64_t xrows, int* grid_out)
+{
+    const double bytes = nnz * 8.0 + (nrows + 1) * 4.0 + double(xrows) * b * 4.0 +
+                         double(nrows) * b * 4.0 * (Z ? 2.0 : 1.0);
+    ProfScope prof(SLQ_K_SPMM, bytes, L.st);
+    const int64_t ng = (nrows + 15) / 16;
+    const int grid = static_cast<int>(
+        std::max<int64_t>(1, std::min<int64_t>(ng * NS, int64_t(L.sms) * 2)));
+    static bool attr = false;
+    if (!attr)
+    {
+        SLQ_CK(cudaFuncSetAttribute(k_spmm_tc<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(TC_DYN_SMEM)));
+        attr = true;
+    }
+    k_spmm_tc<NS><<<grid, TC_THREADS, TC_DYN_SMEM, L.st>>>(*xmap, gptr, gcol, gval, nrows, ng, b,
+                                                          X, sx, shift, Y, Z, zc, zs, epi,
+                                                          partials, error);
+    SLQ_LAUNCH_CK();
+    ++L.launches;
+    *grid_out = grid;
+    return SLQ_OK;
+}
+
 // ---------------------------------------------------------------------------
 // SpMM candidates: storage format x tile.  A row-group candidate is the tile
 // of LV probes per lane and NS warps sharing one row group (b = 32 LV NS);
@@ -802,7 +833,7 @@ slq_status spmm_rg_inst(Launcher& L, const int32_t* gptr, const int32_t* gcol, c
 // (FP32, G = 8, b = 128 or 256), row-group with the widest LV <= 4, CSR.
 // ---------------------------------------------------------------------------
 
-enum { CAND_CSR = 0, CAND_RG = 1, CAND_TMA = 2 };
+enum { CAND_CSR = 0, CAND_RG = 1, CAND_TMA = 2, CAND_TC = 3 };
 
 struct SpmmCand {
     int kind, g, lv, ns;
@@ -828,6 +859,8 @@ int spmm_candidates(const slq_op* op, int transpose, int b, SpmmCand* out)
         }
     if (sizeof(VT) == 4 && (G == 8 || G == 16) && (b == 128 || b == 256))
         out[n++] = {CAND_TMA, G, 4, b / 128};
+    if (sizeof(VT) == 4 && G == 16 && (b == 128 || b == 256))
+        out[n++] = {CAND_TC, 16, 1, b / 128};
     return n;
 }
 
@@ -859,6 +892,21 @@ slq_status spmm_cand(Launcher& L, const slq_op* op, int transpose, const SpmmCan
             return fail(SLQ_ERR_BAD_ARG, "TMA SpMM: unsupported tile");
         }
         return fail(SLQ_ERR_BAD_ARG, "TMA SpMM is FP32 only");
+    }
+    if (c.kind == CAND_TC)
+    {
+        if constexpr (sizeof(VT) == 4)
+        {
+            if (!xmap || !error)
+                return fail(SLQ_ERR_BAD_ARG, "tensor-core SpMM needs a tensor map and error word");
+            const float* gval = static_cast<const float*>(transpose ? op->t_gval : op->a_gval);
+            if (c.ns == 2)
+                return spmm_tc_inst<2>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y, Z, zc,
+                                       zs, epi, partials, error, op->nnz, xrows, grid_out);
+            return spmm_tc_inst<1>(L, xmap, gptr, gcol, gval, rows, b, X, sx, shift, Y, Z, zc, zs,
+                                   epi, partials, error, op->nnz, xrows, grid_out);
+        }
+        return fail(SLQ_ERR_BAD_ARG, "tensor-core SpMM is FP32 only");
     }
     if (c.kind == CAND_RG)
     {
@@ -928,13 +976,16 @@ slq_status op_spmm(Launcher& L, const slq_op* op, int transpose, int b, const VT
     const int nc = spmm_candidates<VT>(op, transpose, b, cands);
     const int lg = log2_width(b);
     const int ti = (lg <= 10) ? op->tuned[transpose ? 1 : 0][lg] : -1;
-    if (ti >= 0 && ti < nc && (cands[ti].kind != CAND_TMA || (xmap && error)))
+    const bool needs_map = cands[ti >= 0 && ti < nc ? ti : 0].kind == CAND_TMA ||
+                           cands[ti >= 0 && ti < nc ? ti : 0].kind == CAND_TC;
+    if (ti >= 0 && ti < nc && (!needs_map || (xmap && error)))
         return spmm_cand<VT>(L, op, transpose, cands[ti], b, X, sx, shift, Y, Z, zc, zs, epi,
                              partials, grid_out, xmap, error);
     // built-in choice: TMA, then the row-group tile with the widest LV, then CSR
     int pick = 0;
     for (int i = 0; i < nc; ++i)
     {
+        if (cands[i].kind == CAND_TC) continue;  // chosen by the tuner only
         if (cands[i].kind == CAND_TMA && !(xmap && error)) continue;
         if (cands[i].kind == CAND_TMA)
         {
@@ -2432,5 +2483,21 @@ extern "C" const char* slq_last_error(void) { return g_error.c_str(); }
 namespace slq {
 void set_error(const std::string& message) { g_error = message; }
 }  // namespace slq
+
+extern "C" slq_status slq_tc_selftest(const float* a, const float* b, float* d, int mode,
+                                      int32_t* error, void* stream)
+{
+    if (!a || !b || !d || !error) return fail(SLQ_ERR_BAD_ARG, "tc_selftest: NULL argument");
+    if (mode < 0 || mode > 3) return fail(SLQ_ERR_BAD_ARG, "tc_selftest: mode must be 0..3");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    SLQ_CK(cudaMemsetAsync(error, 0, sizeof(int32_t), st));
+    k_tc_selftest<<<1, 128, 0, st>>>(a, b, d, mode, error);
+    SLQ_LAUNCH_CK();
+    int32_t herr = 0;
+    SLQ_CK(cudaMemcpyAsync(&herr, error, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    SLQ_CK(cudaStreamSynchronize(st));
+    if (herr) return fail(SLQ_ERR_TIMEOUT, "tc_selftest: the MMA did not complete");
+    return SLQ_OK;
+}
 
 extern "C" int slq_abi_version(void) { return SLQ_ABI_VERSION; }

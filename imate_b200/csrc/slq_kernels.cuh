@@ -26,6 +26,8 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include "slq_tc.cuh"
+
 namespace slq {
 
 constexpr unsigned FULL_MASK = 0xffffffffu;
@@ -1613,6 +1615,465 @@ k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__
         for (int w = 0; w < RGT_WARPS; ++w) sum += red[w * 256 + p];
         partials[static_cast<int64_t>(blockIdx.x) * b + p] = sum;
     }
+}
+
+
+// ===========================================================================
+// Tensor-core row-group SpMM (FP32, 16-row groups, b = 128 NS probes).
+//
+// Per work item (row group g, 128-probe slice) and K step of 8 union columns
+// the tile D[128 probes][16 rows] += X^T[128][8] A_g^T[8][16] runs on the
+// tensor cores as three kind::tf32 MMAs on TF32 hi/lo splits (slq_tc.cuh):
+//   warp 9     copy producer: the step's 8 X rows (two TMA tile::gather4
+//              of 128 probes) and the group's 8 x 16 values (bulk copy)
+//              into a 20-stage shared-memory ring, the union column ids
+//              read 32 at a time across the warp, one chunk ahead;
+//   warps 0-3  converters (thread = probe): read their X values and one
+//              group value each from the ring, free the ring stage, split
+//              into TF32 hi/lo, store A to a tensor-memory stage (their own
+//              lane quarter) and B as K-major tiles in shared memory;
+//   warp 8     MMA issuer (one thread) and tensor-memory owner;
+//   warps 4-7  epilogue: read the finished accumulator (16 rows of their
+//              lane quarter's probes), apply the SpMM epilogue (scale, shift,
+//              three-term subtraction, alpha / norm partials) and store Y.
+// Barriers: ring (sfull / sempty), tensor-memory stages (tfull / tempty, 4
+// stages), accumulator double buffer (acc_full / acc_empty).  Tensor memory
+// per CTA: stage s A hi at column 16 s, A lo at 16 s + 8, accumulator i at
+// 64 + 16 i (128 columns allocated).  Every wait is bounded; a wait that
+// runs out sets *error and the abort flag and every role leaves; the copy
+// thread waits (bounded) for its copies in flight and the MMA thread drains
+// its MMAs before the tensor memory is freed.  Each probe's partial sum
+// belongs to one epilogue thread, so partials[block][p] is written without a
+// CTA reduction.  Sums run in the tensor core's order, so results agree with
+// the CUDA-core kernels to FP32 rounding, not bitwise.
+// ===========================================================================
+
+constexpr int TC_XSTAGES = 20;
+constexpr size_t TC_DYN_SMEM = TC_XSTAGES * (8 * 128 + 8 * 16) * sizeof(float);
+constexpr int TC_TSTAGES = 4;
+constexpr int TC_THREADS = 320;
+constexpr uint32_t TC_COLS = 128;
+
+template <int NS>
+__global__ void __launch_bounds__(TC_THREADS, 2)
+k_spmm_tc(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__ gptr,
+          const int32_t* __restrict__ gcol, const float* __restrict__ gval, int64_t nrows,
+          int64_t ngroups, int b, const float* __restrict__ X, const double* __restrict__ sx,
+          double shift, float* __restrict__ Y, const float* __restrict__ Z,
+          const double* __restrict__ zc, const double* __restrict__ zs, int epi,
+          double* __restrict__ partials, int32_t* __restrict__ error)
+{
+    // dynamic shared memory: X rows of a step [TC_XSTAGES][8 * 128], group
+    // values of a step [TC_XSTAGES][8 * 16]; static: B tiles
+    extern __shared__ __align__(1024) unsigned char smem_tc[];
+    float (*xst)[8 * 128] = reinterpret_cast<float (*)[8 * 128]>(smem_tc);
+    float (*vst)[8 * 16] =
+        reinterpret_cast<float (*)[8 * 16]>(smem_tc + TC_XSTAGES * 8 * 128 * sizeof(float));
+    __shared__ __align__(1024) unsigned char bst[TC_TSTAGES][2][512];  // B hi / lo, K-major
+    __shared__ __align__(8) uint64_t sfull[TC_XSTAGES];
+    __shared__ __align__(8) uint64_t sempty[TC_XSTAGES];
+    __shared__ __align__(8) uint64_t tfull[TC_TSTAGES];
+    __shared__ __align__(8) uint64_t tempty[TC_TSTAGES];
+    __shared__ __align__(8) uint64_t acc_full[2];
+    __shared__ __align__(8) uint64_t acc_empty[2];
+    __shared__ __align__(8) uint64_t drain;
+    __shared__ uint32_t tbase;
+    __shared__ int abort_flag[2];  // [1] stays 0: bounded waits on the way out
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
+    const int64_t nitems = ngroups * NS;
+
+    if (warp == 8)
+    {
+        tc::tmem_alloc(&tbase, TC_COLS);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0)
+    {
+        for (int s = 0; s < TC_XSTAGES; ++s)
+        {
+            mbar_init(&sfull[s], 1);
+            mbar_init(&sempty[s], 4);
+        }
+        for (int s = 0; s < TC_TSTAGES; ++s)
+        {
+            mbar_init(&tfull[s], 4);
+            mbar_init(&tempty[s], 1);
+        }
+        for (int i = 0; i < 2; ++i)
+        {
+            mbar_init(&acc_full[i], 1);
+            mbar_init(&acc_empty[i], 4);
+        }
+        mbar_init(&drain, 1);
+        abort_flag[0] = 0;
+        abort_flag[1] = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tb = tbase;
+    auto give_up = [&]() {
+        *reinterpret_cast<volatile int*>(abort_flag) = 1;
+        atomicExch(error, 1);
+    };
+
+    if (warp == 9)
+    {
+        // copy producer: the whole warp walks the steps (lane l holds union
+        // column id l of the current 32-entry chunk, the next chunk is
+        // loaded one chunk ahead); lane 0 issues the copies
+        int64_t kstep = 0;
+        bool ok = true;
+        for (int64_t item = blockIdx.x; item < nitems && ok; item += gridDim.x)
+        {
+            const int64_t g = item / NS;
+            const int sl = static_cast<int>(item % NS);
+            const int u0 = gptr[g];
+            const int nu = gptr[g + 1] - u0;
+            const int T = max(1, (nu + 7) / 8);
+            const int last = (nu > 0) ? gcol[u0 + nu - 1] : 0;
+            int cur = (lane < nu) ? gcol[u0 + lane] : last;
+            int nxt = (32 + lane < nu) ? gcol[u0 + 32 + lane] : last;
+            for (int t = 0; t < T; ++t, ++kstep)
+            {
+                const int e0 = t * 8;
+                if (t > 0 && (e0 & 31) == 0)
+                {
+                    cur = nxt;
+                    const int e = e0 + 32 + lane;
+                    nxt = (e < nu) ? gcol[u0 + e] : last;
+                }
+                const int s = static_cast<int>(kstep % TC_XSTAGES);
+                const int64_t use = kstep / TC_XSTAGES;
+                const int cnt = min(8, nu - e0);  // <= 0 only for an empty group
+                int id[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                {
+                    const int v = __shfl_sync(FULL_MASK, cur, (e0 + k) & 31);
+                    id[k] = (k < cnt) ? v : last;
+                }
+                bool good = true;
+                if (lane == 0)
+                {
+                    good = *reinterpret_cast<volatile int*>(abort_flag) == 0;
+                    if (good && use > 0) good = mbar_wait(&sempty[s], (use - 1) & 1, abort_flag);
+                    if (!good)
+                    {
+                        give_up();
+                    }
+                    else
+                    {
+                        const uint32_t vbytes = cnt > 0 ? static_cast<uint32_t>(cnt * 64) : 0u;
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        mbar_expect_tx(&sfull[s], 8u * 512u + vbytes);
+                        tma_gather4(&xst[s][0], &xmap, sl * 128, id[0], id[1], id[2], id[3],
+                                    &sfull[s]);
+                        tma_gather4(&xst[s][4 * 128], &xmap, sl * 128, id[4], id[5], id[6],
+                                    id[7], &sfull[s]);
+                        if (vbytes)
+                            bulk_copy_g2s(&vst[s][0], gval + static_cast<int64_t>(u0 + e0) * 16,
+                                          vbytes, &sfull[s]);
+                    }
+                }
+                if (!__shfl_sync(FULL_MASK, good ? 1 : 0, 0))
+                {
+                    ok = false;
+                    break;
+                }
+            }
+        }
+        // the copies in flight land before the CTA leaves
+        if (lane == 0)
+            for (int64_t k = (kstep > TC_XSTAGES ? kstep - TC_XSTAGES : 0); k < kstep; ++k)
+                mbar_wait(&sfull[k % TC_XSTAGES], (k / TC_XSTAGES) & 1, abort_flag + 1);
+        __syncwarp();
+    }
+    else if (warp < 4)
+    {
+        // converters
+        const int cq = warp;
+        const uint32_t lanes = static_cast<uint32_t>(32 * cq) << 16;
+        const int kb = tid >> 4;  // this thread's group value: K row kb, group row nb
+        const int nb = tid & 15;
+        int64_t kstep = 0;
+        bool ok = true;
+        for (int64_t item = blockIdx.x; item < nitems && ok; item += gridDim.x)
+        {
+            const int64_t g = item / NS;
+            const int nu = gptr[g + 1] - gptr[g];
+            const int T = max(1, (nu + 7) / 8);
+            for (int t = 0; t < T; ++t, ++kstep)
+            {
+                const int s = static_cast<int>(kstep % TC_XSTAGES);
+                const int64_t use = kstep / TC_XSTAGES;
+                const int ts = static_cast<int>(kstep % TC_TSTAGES);
+                const int64_t tuse = kstep / TC_TSTAGES;
+                const int cnt = min(8, nu - t * 8);
+                if (!__all_sync(FULL_MASK, mbar_wait(&sfull[s], use & 1, abort_flag)))
+                {
+                    if (lane == 0) give_up();
+                    ok = false;
+                    break;
+                }
+                uint32_t hi[8], lo[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    tc::split_tf32(k < cnt ? xst[s][k * 128 + cq * 32 + lane] : 0.0f, hi[k],
+                                   lo[k]);
+                uint32_t bh, bl;
+                tc::split_tf32(kb < cnt ? vst[s][kb * 16 + nb] : 0.0f, bh, bl);
+                // the split consumed the ring values: the stage can be refilled
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&sempty[s]);
+                bool good = true;
+                if (tuse > 0) good = mbar_wait(&tempty[ts], (tuse - 1) & 1, abort_flag);
+                if (!__all_sync(FULL_MASK, good))
+                {
+                    if (lane == 0) give_up();
+                    ok = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                tc::st_x8(tb + lanes + 16 * ts, hi);
+                tc::st_x8(tb + lanes + 16 * ts + 8, lo);
+                *reinterpret_cast<uint32_t*>(bst[ts][0] + tc::kmajor_offset(nb, kb)) = bh;
+                *reinterpret_cast<uint32_t*>(bst[ts][1] + tc::kmajor_offset(nb, kb)) = bl;
+                tc::fence_proxy_async_smem();
+                tc::wait_st();
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tfull[ts]);
+            }
+        }
+    }
+    else if (warp == 8)
+    {
+        // MMA issuer
+        if (lane == 0)
+        {
+            int64_t kstep = 0;
+            int64_t it = 0;
+            bool ok = true;
+            for (int64_t item = blockIdx.x; item < nitems && ok; item += gridDim.x, ++it)
+            {
+                const int64_t g = item / NS;
+                const int nu = gptr[g + 1] - gptr[g];
+                const int T = max(1, (nu + 7) / 8);
+                const int db = static_cast<int>(it & 1);
+                const int64_t duse = it >> 1;
+                if (duse > 0 && !mbar_wait(&acc_empty[db], (duse - 1) & 1, abort_flag))
+                {
+                    give_up();
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t dcol = tb + 64 + 16 * db;
+                for (int t = 0; t < T; ++t, ++kstep)
+                {
+                    const int ts = static_cast<int>(kstep % TC_TSTAGES);
+                    const int64_t tuse = kstep / TC_TSTAGES;
+                    if (!mbar_wait(&tfull[ts], tuse & 1, abort_flag))
+                    {
+                        give_up();
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    const uint64_t bh = tc::smem_desc(bst[ts][0], 128, 256);
+                    const uint64_t bl = tc::smem_desc(bst[ts][1], 128, 256);
+                    const uint32_t ahi = tb + 16 * ts;
+                    const uint32_t alo = ahi + 8;
+                    tc::mma_tf32_ts(dcol, alo, bh, tc::IDESC_TF32_M128_N16, t > 0 ? 1u : 0u);
+                    tc::mma_tf32_ts(dcol, ahi, bl, tc::IDESC_TF32_M128_N16, 1u);
+                    tc::mma_tf32_ts(dcol, ahi, bh, tc::IDESC_TF32_M128_N16, 1u);
+                    tc::commit(&tempty[ts]);
+                }
+                if (ok) tc::commit(&acc_full[db]);
+            }
+            // every issued MMA completes before the tensor memory is freed
+            tc::commit(&drain);
+            mbar_wait(&drain, 0, abort_flag + 1);
+        }
+        __syncwarp();
+    }
+    else
+    {
+        // epilogue
+        const int q = warp - 4;
+        const uint32_t lanes = static_cast<uint32_t>(32 * q) << 16;
+        double part[NS];
+#pragma unroll
+        for (int i = 0; i < NS; ++i) part[i] = 0.0;
+        int64_t it = 0;
+        for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x, ++it)
+        {
+            const int64_t g = item / NS;
+            const int sl = static_cast<int>(item % NS);
+            const int db = static_cast<int>(it & 1);
+            const int64_t duse = it >> 1;
+            if (!__all_sync(FULL_MASK, mbar_wait(&acc_full[db], duse & 1, abort_flag)))
+            {
+                if (lane == 0) give_up();
+                break;
+            }
+            tc::fence_after_sync();
+            uint32_t v[16];
+            tc::ld_x16(tb + lanes + 64 + 16 * db, v);
+            tc::wait_ld();
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[db]);
+            const int p = sl * 128 + q * 32 + lane;
+            const double sxp = sx ? sx[p] : 1.0;
+            const double zcp = Z ? zc[p] * zs[p] : 0.0;
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+            {
+                const int64_t row = g * 16 + r;
+                if (row >= nrows) continue;
+                const int64_t o = row * b + p;
+                const float xr = (shift != 0.0 || epi == 1) ? __ldg(X + o) : 0.0f;
+                const float zr = Z ? __ldg(Z + o) : 0.0f;
+                double y = static_cast<double>(__uint_as_float(v[r])) * sxp;
+                if (shift != 0.0) y += shift * (sxp * static_cast<double>(xr));
+                if (Z) y -= zcp * static_cast<double>(zr);
+                const float yf = static_cast<float>(y);
+                Y[o] = yf;
+                const double ys = static_cast<double>(yf);
+                double add = 0.0;
+                if (epi == 1)
+                    add = (sxp * static_cast<double>(xr)) * ys;
+                else if (epi == 2)
+                    add = ys * ys;
+                else if (epi == 3)
+                    add = (zs[p] * static_cast<double>(zr)) * ys;
+#pragma unroll
+                for (int i = 0; i < NS; ++i)
+                    if (i == sl) part[i] += add;
+            }
+        }
+        if (epi != 0)
+        {
+#pragma unroll
+            for (int i = 0; i < NS; ++i)
+                partials[static_cast<int64_t>(blockIdx.x) * b + i * 128 + q * 32 + lane] = part[i];
+        }
+    }
+
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 8)
+    {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tb, TC_COLS);
+    }
+}
+
+// ===========================================================================
+// Tensor-core self-test: D[128][16] = A[128][8] B[8][16] for one tile
+// through tcgen05 (one CTA of 128 threads; thread m owns row m).  mode:
+//   0  A in tensor memory (written by its owning warps), B in shared
+//      memory, one kind::tf32 MMA (the tensor-core SpMM's form);
+//   1  as 0 with both operands split into TF32 hi/lo, three MMAs;
+//   2  tensor-memory round trip: D[m][0..7] / [8..15] = the stored A hi / lo;
+//   3  A and B in shared memory, one MMA.
+// ===========================================================================
+
+__global__ void __launch_bounds__(128, 1)
+k_tc_selftest(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ d,
+              int mode, int32_t* __restrict__ error)
+{
+    __shared__ __align__(1024) unsigned char atile[4096];
+    __shared__ __align__(1024) unsigned char btile[2][512];  // B hi, B lo
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tbase;
+    __shared__ int abort_none;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    if (warp == 0)
+    {
+        tc::tmem_alloc(&tbase, 64);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0)
+    {
+        mbar_init(&bar, 1);
+        abort_none = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t base = tbase;
+    const uint32_t lanes = static_cast<uint32_t>(32 * warp) << 16;
+    // tensor-memory columns: A hi 0..7, A lo 8..15, D 32..47
+    uint32_t hi[8], lo[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+    {
+        tc::split_tf32(a[tid * 8 + k], hi[k], lo[k]);
+        if (mode == 0 || mode == 3) lo[k] = 0u;
+        *reinterpret_cast<uint32_t*>(atile + tc::kmajor_offset(tid, k)) = hi[k];
+    }
+    tc::st_x8(base + lanes + 0, hi);
+    tc::st_x8(base + lanes + 8, lo);
+    {
+        const int k = tid >> 4;
+        const int n = tid & 15;
+        uint32_t h, l;
+        tc::split_tf32(b[k * 16 + n], h, l);
+        *reinterpret_cast<uint32_t*>(btile[0] + tc::kmajor_offset(n, k)) = h;
+        *reinterpret_cast<uint32_t*>(btile[1] + tc::kmajor_offset(n, k)) = (mode == 1) ? l : 0u;
+    }
+    tc::fence_proxy_async_smem();
+    tc::wait_st();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t dcol = (mode == 2) ? base : base + 32;
+    if (tid == 0)
+    {
+        const uint64_t bh = tc::smem_desc(btile[0], 128, 256);
+        const uint64_t bl = tc::smem_desc(btile[1], 128, 256);
+        if (mode == 1)
+        {
+            tc::mma_tf32_ts(dcol, base + 8, bh, tc::IDESC_TF32_M128_N16, 0);
+            tc::mma_tf32_ts(dcol, base + 0, bl, tc::IDESC_TF32_M128_N16, 1);
+            tc::mma_tf32_ts(dcol, base + 0, bh, tc::IDESC_TF32_M128_N16, 1);
+        }
+        else if (mode == 0)
+        {
+            tc::mma_tf32_ts(dcol, base + 0, bh, tc::IDESC_TF32_M128_N16, 0);
+        }
+        else if (mode == 3)
+        {
+            const uint64_t ad = tc::smem_desc(atile, 128, 256);
+            tc::mma_tf32_ss(dcol, ad, bh, tc::IDESC_TF32_M128_N16, 0);
+        }
+        tc::commit(&bar);  // with no MMA issued it arrives at once
+    }
+    const bool ok = __all_sync(FULL_MASK, mbar_wait(&bar, 0, &abort_none));
+    tc::fence_after_sync();
+    if (ok)
+    {
+        uint32_t v[16];
+        tc::ld_x16(dcol + lanes, v);
+        tc::wait_ld();
+#pragma unroll
+        for (int n = 0; n < 16; ++n) d[tid * 16 + n] = __uint_as_float(v[n]);
+    }
+    else if ((tid & 31) == 0)
+    {
+        atomicExch(error, 1);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(base, 64);
 }
 
 }  // namespace slq

@@ -225,14 +225,20 @@ slq_status slq_run(slq_op* op, const slq_params* p, const double* parameters,
  * block width are the storage formats the operator holds crossed with their
  * tiles: CSR warp per row; row-group (the operator's group_rows rows sharing
  * a union of columns) with LV probes per lane and NS warps per row group,
- * b = 32 LV NS; and, in FP32 with 8-row groups at b = 128 or 256, the
- * row-group kernel whose X rows arrive by TMA gathers.  slq_operator_tune
- * times every candidate (reps launches each, CUDA events, after one untimed
- * launch) on workspace blocks and makes the fastest the operator's choice
- * for that width and direction; every later product the operator takes at
- * that width (slq_run, slq_batch_*, slq_operator_dot) uses it.  Results of
- * different candidates agree to rounding, not bitwise (their partial-sum
- * orders differ). */
+ * b = 32 LV NS; in FP32 with 8- or 16-row groups at b = 128 or 256, the
+ * row-group kernel whose X rows arrive by TMA gathers; and in FP32 with
+ * 16-row groups at b = 128 or 256, the tensor-core row-group kernel
+ * (tcgen05 kind::tf32 on TF32 hi/lo splits of both operands, accumulators
+ * in tensor memory; FP32-level accuracy, chosen only by the tuner or
+ * slq_operator_set_variant).  slq_operator_tune times every candidate (reps
+ * launches each, CUDA events, after one untimed launch) on workspace blocks
+ * and makes the fastest the operator's choice for that width and
+ * direction; every later product the operator takes at that width
+ * (slq_run, slq_batch_*, slq_operator_dot) uses it, except that
+ * slq_operator_dot, which has no tensor map or error word, falls back to the
+ * built-in choice for the TMA and tensor-core kernels.  Results of different
+ * candidates agree to rounding, not bitwise (their partial-sum orders
+ * differ). */
 #define SLQ_TUNE_MAX_CANDIDATES 16
 
 typedef struct {
@@ -241,7 +247,9 @@ typedef struct {
     int32_t num_candidates;
     int32_t chosen;                                /* fastest candidate      */
     int32_t kind[SLQ_TUNE_MAX_CANDIDATES];         /* 0 CSR, 1 row-group,    */
-                                                   /* 2 row-group + TMA      */
+                                                   /* 2 row-group + TMA,     */
+                                                   /* 3 row-group, tensor    */
+                                                   /*   cores                */
     int32_t group_rows[SLQ_TUNE_MAX_CANDIDATES];
     int32_t lanes_vec[SLQ_TUNE_MAX_CANDIDATES];    /* LV probes per lane     */
     int32_t slices[SLQ_TUNE_MAX_CANDIDATES];       /* NS warps per row group */
@@ -292,6 +300,18 @@ slq_status slq_batch_run(slq_batch* batch, void* stream, slq_result* results);
 slq_status slq_batch_info(const slq_batch* batch, int64_t* kernels,
                           int64_t* nodes);
 slq_status slq_batch_destroy(slq_batch* batch);
+
+/* Tensor-core self-test (no counterpart in the reference): D = A B for one
+ * 128 x 8 by 8 x 16 FP32 tile (device arrays, row-major) through tcgen05,
+ * the building blocks of the tensor-core SpMM checked on one tile.  mode 0:
+ * A in tensor memory, B in shared memory, one kind::tf32 MMA; mode 1: as 0
+ * with both operands split into TF32 hi/lo parts, D = A_lo B_hi + A_hi B_lo
+ * + A_hi B_hi; mode 2: tensor-memory round trip (D[m][0..7] and [8..15]
+ * receive the stored TF32 hi and lo parts of A[m]); mode 3: A and B in
+ * shared memory, one MMA.  error: one device int32 of scratch (set when the
+ * MMA's completion wait runs out, SLQ_ERR_TIMEOUT). */
+slq_status slq_tc_selftest(const float* a, const float* b, float* d, int mode,
+                           int32_t* error, void* stream);
 
 /* Probe generator alone: writes probes [first, first+count) of the stream for
  * (seed, rng) as a row-major block [len][width] of +-1 in the given dtype
