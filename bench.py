@@ -501,6 +501,11 @@ def run_batched(args):
              for _, info in res)
     value = ps / elapsed
     widths = [t["width"] for t in plan.tuning]
+    kinds = {}
+    for t in plan.tuning:
+        rep = t["report"][t["width"]]["direct"]
+        k = rep["candidates"][rep["chosen"]]["kind"]
+        kinds[k] = kinds.get(k, 0) + 1
     # algorithmic bytes of the whole graph per step: per matrix and
     # Lanczos step, the SpMM of every block plus the update pass
     by = 0.0
@@ -553,7 +558,8 @@ def run_batched(args):
         "graph": {"kernels": plan.graph_kernels, "nodes": plan.graph_nodes,
                   "build_s": build_s, "plan_s": plan_s,
                   "widths": {str(w): widths.count(w) for w in sorted(
-                      set(widths))}},
+                      set(widths))},
+                  "spmm_kernels": kinds},
         "roofline": {"bound": "hbm", "kernel": "whole graph (SpMM + update "
                      "passes)", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,

@@ -441,14 +441,21 @@ class DeviceMatrix(LinearOperator):
     """A sparse matrix whose CSR arrays are already on the GPU (torch
     tensors: int32 indptr and indices, float32 or float64 data), e.g. from
     ``sample_matrices.correlation_matrix_device``.  No host copy is made;
-    rows must list their columns in increasing order.  ``group_rows`` (0, 4
-    or 8) adds the row-group format on the device (the autotuner then picks
-    between it and CSR)."""
+    rows must list their columns in increasing order.  ``group_rows``
+    ('auto' = 16 for float32 and 8 for float64, or 0, 4, 8, 16) adds the
+    row-group format on the device (the autotuner then picks between its
+    kernels and CSR); no reordering is done, so the rows should already be
+    in a local order (as the device builder's cell order is)."""
 
-    def __init__(self, indptr, indices, data, shape, group_rows=8):
+    def __init__(self, indptr, indices, data, shape, group_rows="auto"):
         super().__init__()
         self.indptr, self.indices, self.data = indptr, indices, data
         self.shape = tuple(int(x) for x in shape)
+        if group_rows == "auto":
+            # 16-row groups (FP32 kernels, including the tensor-core one),
+            # else 8
+            import torch
+            group_rows = 16 if data.dtype == torch.float32 else 8
         self.group_rows = int(group_rows)
         self.num_parameters = 0
         self.data_type_name = str(data.dtype).replace("torch.", "").encode()
