@@ -1012,6 +1012,46 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
             for (int item = 0; item < nitems; ++item)
             {
                 if (*reinterpret_cast<volatile int*>(abort_flag)) { ok = false; break; }
+                if (MODE == 0 && item >= npre && item + 1 < nitems)
+                {
+                    // dots: two basis tiles per turn, four FMA chains each, so
+                    // the two load -> convert -> FMA -> add-tree chains overlap
+                    // (two warps per scheduler leave little else to hide them)
+                    const int ib = skip + (item - npre);
+                    const double prev0 = extra[ib * STREAM_CONSUMERS + tid];
+                    const double prev1 = extra[(ib + 1) * STREAM_CONSUMERS + tid];
+                    int s1 = s + 1;
+                    uint32_t ph1 = phase;
+                    if (s1 == a.S) { s1 = 0; ph1 ^= 1; }
+                    if (!mbar_wait(&full[s], phase, abort_flag) ||
+                        !mbar_wait(&full[s1], ph1, abort_flag))
+                    {
+                        *abort_flag = 1;
+                        atomicExch(a.error, 1);
+                        ok = false;
+                        break;
+                    }
+                    const VT* t0 = stages + static_cast<size_t>(s) * (STREAM_TILE_BYTES / sizeof(VT));
+                    const VT* t1 = stages + static_cast<size_t>(s1) * (STREAM_TILE_BYTES / sizeof(VT));
+                    double l0[4] = {0.0, 0.0, 0.0, 0.0}, l1[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                    for (int k = 0; k < R; ++k)
+                    {
+                        const int e = (roff + k * RSTEP) * PT + pl;
+                        l0[k & 3] += static_cast<double>(t0[e]) * w[k];
+                        l1[k & 3] += static_cast<double>(t1[e]) * w[k];
+                    }
+                    extra[ib * STREAM_CONSUMERS + tid] = prev0 + ((l0[0] + l0[1]) + (l0[2] + l0[3]));
+                    extra[(ib + 1) * STREAM_CONSUMERS + tid] =
+                        prev1 + ((l1[0] + l1[1]) + (l1[2] + l1[3]));
+                    release(s);
+                    release(s1);
+                    s = s1 + 1;
+                    phase = ph1;
+                    if (s == a.S) { s = 0; phase ^= 1; }
+                    ++item;
+                    continue;
+                }
                 // dots: fetch this thread's running sum before the wait so the
                 // shared-memory latency overlaps it
                 const int ib = skip + (item - npre);
