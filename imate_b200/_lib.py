@@ -37,7 +37,8 @@ EXPORTS = (
     "slq_operator_tune", "slq_operator_set_variant",
     "slq_batch_workspace_bytes", "slq_batch_create", "slq_batch_run",
     "slq_batch_info", "slq_batch_destroy", "slq_group_order",
-    "slq_rcm_order", "slq_tc_selftest",
+    "slq_rcm_order", "slq_tc_selftest", "slq_order_spread", "slq_group_fill",
+    "slq_rcm_order_device_workspace_bytes", "slq_rcm_order_device",
 )
 TUNE_MAX_CANDIDATES = 16
 SPMM_KINDS = ("csr", "row-group", "row-group-tma", "row-group-tc")
@@ -176,6 +177,11 @@ def _declare(lib):
         "slq_batch_destroy": (i32, [vp]),
         "slq_group_order": (i32, [i64, vp, vp, vp, i32, i32, vp, vp]),
         "slq_rcm_order": (i32, [i64, vp, vp, vp]),
+        "slq_order_spread": (i32, [i64, vp, vp, vp, i64, vp]),
+        "slq_group_fill": (i32, [i64, vp, vp, vp, i32, i64, vp]),
+        "slq_rcm_order_device_workspace_bytes": (i32, [i64, vp]),
+        "slq_rcm_order_device": (i32, [i64, i64, vp, vp, i32, vp, vp, vp, sz,
+                                        vp]),
         "slq_tc_selftest": (i32, [vp, vp, vp, i32, vp, vp]),
     }
     for name, (res, args) in sig.items():

@@ -2257,6 +2257,187 @@ extern "C" slq_status slq_operator_dot(slq_op* op, int transpose, double t, cons
                           static_cast<float*>(y), nullptr, nullptr, nullptr, 0, nullptr, &grid);
 }
 
+// ---------------------------------------------------------------------------
+// reverse Cuthill-McKee order on the device
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct RcmBufs {
+    int32_t* flag;      // [4]: CSR check, level count, first unvisited, max degree
+    int32_t* degree;
+    int32_t* rows;
+    int32_t* deg_sorted;
+    int32_t* by_degree;
+    int32_t* pos;
+    int32_t* claim;
+    int32_t* out;
+    uint64_t* keys;
+    uint64_t* keys_alt;
+    void* temp;
+    size_t temp_bytes;
+};
+
+slq_status rcm_layout(Carver& c, int64_t n, RcmBufs* B)
+{
+    const int items = static_cast<int>(std::max<int64_t>(n, 1));
+    size_t t1 = 0, t2 = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(
+        nullptr, t1, static_cast<const int32_t*>(nullptr), static_cast<int32_t*>(nullptr),
+        static_cast<const int32_t*>(nullptr), static_cast<int32_t*>(nullptr), items);
+    if (e != cudaSuccess)
+        return fail(SLQ_ERR_CUDA, std::string("cub sort sizing: ") + cudaGetErrorString(e));
+    e = cub::DeviceRadixSort::SortKeys(nullptr, t2, static_cast<const uint64_t*>(nullptr),
+                                       static_cast<uint64_t*>(nullptr), items);
+    if (e != cudaSuccess)
+        return fail(SLQ_ERR_CUDA, std::string("cub sort sizing: ") + cudaGetErrorString(e));
+    B->flag = c.take<int32_t>(4);
+    B->degree = c.take<int32_t>(n);
+    B->rows = c.take<int32_t>(n);
+    B->deg_sorted = c.take<int32_t>(n);
+    B->by_degree = c.take<int32_t>(n);
+    B->pos = c.take<int32_t>(n);
+    B->claim = c.take<int32_t>(n);
+    B->out = c.take<int32_t>(n);
+    B->keys = c.take<uint64_t>(n);
+    B->keys_alt = c.take<uint64_t>(n);
+    B->temp_bytes = std::max(t1, t2);
+    B->temp = c.take<char>(B->temp_bytes);
+    return SLQ_OK;
+}
+
+int bits_for(int64_t v)  // bits to hold 0 .. v
+{
+    int b = 1;
+    while (b < 63 && (int64_t(1) << b) <= v) ++b;
+    return b;
+}
+
+}  // namespace
+
+extern "C" slq_status slq_rcm_order_device_workspace_bytes(int64_t n, size_t* bytes)
+{
+    if (!bytes || n < 0 || n > INT32_MAX) return fail(SLQ_ERR_BAD_ARG, "rcm_order_device: bad argument");
+    Carver c(nullptr, 0);
+    RcmBufs B;
+    SLQ_TRY(rcm_layout(c, n, &B));
+    *bytes = c.off + 256;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_rcm_order_device(int64_t n, int64_t nnz, const int32_t* indptr,
+                                           const int32_t* indices, int max_components,
+                                           int32_t* order, int* done, void* workspace,
+                                           size_t workspace_bytes, void* stream)
+{
+    if (!done || n < 0 || n > INT32_MAX || nnz < 0 || nnz > INT32_MAX || !indptr || !order ||
+        (nnz > 0 && !indices) || max_components < 1)
+        return fail(SLQ_ERR_BAD_ARG, "rcm_order_device: bad argument");
+    *done = 0;
+    size_t need = 0;
+    SLQ_TRY(slq_rcm_order_device_workspace_bytes(n, &need));
+    if (!workspace || workspace_bytes < need)
+        return fail(SLQ_ERR_WORKSPACE, "rcm_order_device: workspace too small (need " +
+                                           std::to_string(need) + " bytes)");
+    if (n == 0)
+    {
+        *done = 1;
+        return SLQ_OK;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Carver c(workspace, workspace_bytes);
+    RcmBufs B;
+    SLQ_TRY(rcm_layout(c, n, &B));
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
+    const int grid = sms * 4;
+
+    // the pattern must index inside [0, n) before any kernel follows it
+    SLQ_CK(cudaMemsetAsync(B.flag, 0, 4 * sizeof(int32_t), st));
+    k_check_csr<<<grid, 256, 0, st>>>(indptr, indices, n, n, nnz, B.flag);
+    SLQ_LAUNCH_CK();
+    k_rcm_init<<<grid, 256, 0, st>>>(indptr, n, B.degree, B.rows, B.pos, B.claim, B.flag + 3);
+    SLQ_LAUNCH_CK();
+    int32_t h[4] = {0, 0, 0, 0};
+    SLQ_CK(cudaMemcpyAsync(h, B.flag, sizeof(h), cudaMemcpyDeviceToHost, st));
+    SLQ_CK(cudaStreamSynchronize(st));
+    if (h[0] & 1) return fail(SLQ_ERR_BAD_CSR, "rcm_order_device: index pointer must start at 0 and end at nnz");
+    if (h[0] & 2) return fail(SLQ_ERR_BAD_CSR, "rcm_order_device: index pointer must be non-decreasing");
+    if (h[0] & 4) return fail(SLQ_ERR_BAD_CSR, "rcm_order_device: index out of range");
+    const int32_t maxdeg = h[3];
+    const int nb = bits_for(n - 1);
+    const int db = bits_for(maxdeg);
+    if (nb + db + 1 > 64) return SLQ_OK;  // keys do not fit: *done stays 0
+
+    // rows by increasing degree, ties by row (stable sort of (degree, row))
+    {
+        size_t tb = B.temp_bytes;
+        cudaError_t e = cub::DeviceRadixSort::SortPairs(
+            B.temp, tb, B.degree, B.deg_sorted, B.rows, B.by_degree, static_cast<int>(n), 0,
+            db, st);
+        if (e != cudaSuccess)
+            return fail(SLQ_ERR_CUDA, std::string("cub sort: ") + cudaGetErrorString(e));
+    }
+
+    const int32_t first_init = static_cast<int32_t>(n);
+    int64_t cnt = 0, cursor = 0;
+    int components = 0;
+    while (cnt < n)
+    {
+        if (++components > max_components) return SLQ_OK;  // *done stays 0
+        SLQ_CK(cudaMemcpyAsync(B.flag + 2, &first_init, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        k_rcm_first<<<grid, 256, 0, st>>>(B.by_degree, B.pos, cursor, n, B.flag + 2);
+        SLQ_LAUNCH_CK();
+        k_rcm_start<<<1, 1, 0, st>>>(B.by_degree, B.flag + 2, B.pos, B.out, cnt, n);
+        SLQ_LAUNCH_CK();
+        int32_t first = 0;
+        SLQ_CK(cudaMemcpyAsync(&first, B.flag + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        SLQ_CK(cudaStreamSynchronize(st));
+        if (first >= n) return fail(SLQ_ERR_CUDA, "rcm_order_device: lost track of the visited rows");
+        cursor = first + 1;
+        int64_t lb = cnt, le = cnt + 1;
+        cnt = le;
+        while (lb < le)
+        {
+            const int pb = bits_for(le - lb - 1);
+            if (pb + db + nb > 64) return SLQ_OK;  // *done stays 0
+            const int64_t warps = le - lb;
+            const int blocks = static_cast<int>(std::min<int64_t>((warps + 7) / 8, int64_t(sms) * 8));
+            k_rcm_claim<<<blocks, 256, 0, st>>>(B.out, lb, le, indptr, indices, B.pos, B.claim,
+                                                 B.flag + 1);
+            SLQ_LAUNCH_CK();
+            k_rcm_collect<<<blocks, 256, 0, st>>>(B.out, lb, le, indptr, indices, B.pos, B.degree,
+                                                   B.claim, nb, db, B.keys, B.flag + 1);
+            SLQ_LAUNCH_CK();
+            int32_t m = 0;
+            SLQ_CK(cudaMemcpyAsync(&m, B.flag + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            SLQ_CK(cudaStreamSynchronize(st));
+            if (m < 0 || cnt + m > n)
+                return fail(SLQ_ERR_CUDA, "rcm_order_device: level count out of range");
+            if (m > 0)
+            {
+                cub::DoubleBuffer<uint64_t> kb(B.keys, B.keys_alt);
+                size_t tb = B.temp_bytes;
+                cudaError_t e = cub::DeviceRadixSort::SortKeys(B.temp, tb, kb, static_cast<int>(m),
+                                                               0, pb + db + nb, st);
+                if (e != cudaSuccess)
+                    return fail(SLQ_ERR_CUDA, std::string("cub sort: ") + cudaGetErrorString(e));
+                const uint64_t rowmask = (uint64_t(1) << nb) - 1;
+                const int ab = static_cast<int>(std::min<int64_t>((m + 255) / 256, grid));
+                k_rcm_assign<<<ab, 256, 0, st>>>(kb.Current(), m, rowmask, cnt, B.out, B.pos);
+                SLQ_LAUNCH_CK();
+            }
+            lb = le;
+            le = cnt + m;
+            cnt = le;
+        }
+    }
+    k_rcm_reverse<<<grid, 256, 0, st>>>(B.out, n, order);
+    SLQ_LAUNCH_CK();
+    *done = 1;
+    return SLQ_OK;
+}
+
 extern "C" slq_status slq_generate_probes_workspace_bytes(int64_t len, int width,
                                                           size_t* bytes)
 {

@@ -732,6 +732,140 @@ __global__ void k_bounds64(const uint64_t* __restrict__ sorted_keys, int64_t nnz
     }
 }
 
+// ---------------------------------------------------------------------------
+// Cuthill-McKee order on the device, one breadth-first level per round.
+//
+// The serial order appends the not-yet-visited neighbours of each visited
+// row, sorted by (degree, row), in visit order; so a row of the next level
+// belongs to the earliest-visited row of the current level that lists it,
+// and the next level is its rows sorted by (that parent's position, degree,
+// row).  k_rcm_claim takes the parent as an atomic minimum of positions,
+// k_rcm_collect lists each claimed row once (packed key: parent offset,
+// degree, row), a radix sort orders the keys, k_rcm_assign places them.
+// pos[r] < 0 marks an unvisited row; claim[r] holds INT_MAX until claimed.
+// ---------------------------------------------------------------------------
+
+__global__ void k_rcm_init(const int32_t* __restrict__ indptr, int64_t n,
+                           int32_t* __restrict__ degree, int32_t* __restrict__ rows,
+                           int32_t* __restrict__ pos, int32_t* __restrict__ claim,
+                           int32_t* __restrict__ maxdeg)
+{
+    const int64_t i0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    int32_t m = 0;
+    for (int64_t r = i0; r < n; r += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        const int32_t d = indptr[r + 1] - indptr[r];
+        degree[r] = d;
+        rows[r] = static_cast<int32_t>(r);
+        pos[r] = -1;
+        claim[r] = INT_MAX;
+        m = max(m, d);
+    }
+    atomicMax(maxdeg, m);
+}
+
+// *result = the first index i >= from of by_degree whose row is unvisited
+// (n if none; *result must hold n before the launch)
+__global__ void k_rcm_first(const int32_t* __restrict__ by_degree,
+                            const int32_t* __restrict__ pos, int64_t from, int64_t n,
+                            int32_t* __restrict__ result)
+{
+    const int64_t i0 = from + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t i = i0; i < n; i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        if (pos[by_degree[i]] < 0)
+        {
+            atomicMin(result, static_cast<int32_t>(i));
+            return;
+        }
+}
+
+// the row at by_degree[*result] starts a component at position cnt
+__global__ void k_rcm_start(const int32_t* __restrict__ by_degree,
+                            const int32_t* __restrict__ result, int32_t* __restrict__ pos,
+                            int32_t* __restrict__ out, int64_t cnt, int64_t n)
+{
+    if (*result < 0 || *result >= n || cnt >= n) return;  // host reports it
+    const int32_t r = by_degree[*result];
+    pos[r] = static_cast<int32_t>(cnt);
+    out[cnt] = r;
+}
+
+// warp per frontier row k in [lb, le): claim[c] = min(claim[c], k) for its
+// unvisited neighbours c; also clears the level's row count
+__global__ void k_rcm_claim(const int32_t* __restrict__ out, int64_t lb, int64_t le,
+                            const int32_t* __restrict__ indptr,
+                            const int32_t* __restrict__ indices,
+                            const int32_t* __restrict__ pos, int32_t* __restrict__ claim,
+                            int32_t* __restrict__ count)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) *count = 0;
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t ws = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t k = lb + w0; k < le; k += ws)
+    {
+        const int32_t r = out[k];
+        const int32_t e1 = indptr[r + 1];
+        for (int32_t e = indptr[r] + lane; e < e1; e += 32)
+        {
+            const int32_t c = indices[e];
+            if (pos[c] < 0) atomicMin(&claim[c], static_cast<int32_t>(k));
+        }
+    }
+}
+
+// warp per frontier row k: each unvisited neighbour whose claim is k is
+// listed once, key = (k - lb) << (db + nb) | degree << nb | row
+__global__ void k_rcm_collect(const int32_t* __restrict__ out, int64_t lb, int64_t le,
+                              const int32_t* __restrict__ indptr,
+                              const int32_t* __restrict__ indices,
+                              const int32_t* __restrict__ pos,
+                              const int32_t* __restrict__ degree, int32_t* __restrict__ claim,
+                              int nb, int db, uint64_t* __restrict__ keys,
+                              int32_t* __restrict__ count)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t ws = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t k = lb + w0; k < le; k += ws)
+    {
+        const int32_t r = out[k];
+        const int32_t kk = static_cast<int32_t>(k);
+        const int32_t e1 = indptr[r + 1];
+        for (int32_t e = indptr[r] + lane; e < e1; e += 32)
+        {
+            const int32_t c = indices[e];
+            if (pos[c] >= 0 || claim[c] != kk) continue;
+            // once per row, also when r lists c twice
+            if (atomicCAS(&claim[c], kk, -1) != kk) continue;
+            const int32_t i = atomicAdd(count, 1);
+            keys[i] = (static_cast<uint64_t>(k - lb) << (db + nb)) |
+                      (static_cast<uint64_t>(degree[c]) << nb) | static_cast<uint64_t>(c);
+        }
+    }
+}
+
+// sorted keys -> positions cnt .. cnt + m - 1
+__global__ void k_rcm_assign(const uint64_t* __restrict__ keys, int64_t m, uint64_t rowmask,
+                             int64_t cnt, int32_t* __restrict__ out, int32_t* __restrict__ pos)
+{
+    const int64_t i0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t i = i0; i < m; i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        const int32_t c = static_cast<int32_t>(keys[i] & rowmask);
+        out[cnt + i] = c;
+        pos[c] = static_cast<int32_t>(cnt + i);
+    }
+}
+
+__global__ void k_rcm_reverse(const int32_t* __restrict__ out, int64_t n,
+                              int32_t* __restrict__ order)
+{
+    const int64_t i0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t k = i0; k < n; k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        order[k] = out[n - 1 - k];
+}
+
 __global__ void k_fill_f64(double* __restrict__ a, int64_t n, double v)
 {
     const int64_t i0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;

@@ -1,5 +1,13 @@
 // Host-side row orders of square sparse matrices: reverse Cuthill-McKee
-// (slq_rcm_order) and row-group aggregation (slq_group_order).
+// (slq_rcm_order), row-group aggregation (slq_group_order), and the sampled
+// statistics that decide whether to use them (slq_order_spread,
+// slq_group_fill).  Validation and aggregation run on a small pool of host
+// threads; every result is independent of the number of threads.
+//
+// Reverse Cuthill-McKee: breadth-first from the lowest-degree row of each
+// component, the not-yet-visited neighbours of each visited row appended in
+// increasing (degree, row), the visit order reversed.  The visited set is a
+// bit table (32 KB for 2^18 rows), which keeps the edge loop in L1.
 //
 // Row-group aggregation:
 // The row-group SpMM formats store, per group of G consecutive rows, the
@@ -14,12 +22,20 @@
 // not-yet-placed rows of the base order, so that every group except the
 // last has exactly G rows and lines up with the device format's groups.
 // Groups keep the base order's sequence, so the SpMM's gather window stays
-// as local as the base order made it.
+// as local as the base order made it.  The base order is cut into a fixed
+// number of chunks (a multiple of G rows each; the count depends on n only)
+// that are aggregated independently and in parallel, a group taking rows of
+// its own chunk only.
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstdint>
+#include <functional>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/slq.h"
@@ -29,6 +45,240 @@ void set_error(const std::string& message);  // slq_engine.cu
 }
 
 namespace {
+
+// Threads for the host orders: the machine's hardware threads, at most 16.
+int host_threads()
+{
+    const unsigned h = std::thread::hardware_concurrency();
+    return static_cast<int>(std::min(16u, std::max(1u, h)));
+}
+
+// A fixed set of threads that run one job at a time: run(f) calls f(t, n)
+// on threads t = 0..n-1 (the caller is thread 0) and returns when all are
+// done.  Idle workers spin briefly on the job counter before they block, so
+// back-to-back jobs start within microseconds.
+class Pool
+{
+  public:
+    explicit Pool(int n) : n_(std::max(1, n))
+    {
+        for (int i = 1; i < n_; ++i) workers_.emplace_back([this, i] { loop(i); });
+    }
+    ~Pool()
+    {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            stop_.store(true);
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+    Pool(const Pool&) = delete;
+    Pool& operator=(const Pool&) = delete;
+
+    int size() const { return n_; }
+
+    void run(const std::function<void(int, int)>& f)
+    {
+        if (n_ == 1)
+        {
+            f(0, 1);
+            return;
+        }
+        job_ = &f;
+        pending_.store(n_ - 1, std::memory_order_relaxed);
+        {
+            std::lock_guard<std::mutex> g(m_);
+            gen_.fetch_add(1, std::memory_order_release);
+        }
+        cv_.notify_all();
+        f(0, n_);
+        for (long spin = 0; pending_.load(std::memory_order_acquire) != 0; ++spin)
+            if (spin > 4096) std::this_thread::yield();
+        job_ = nullptr;
+    }
+
+  private:
+    void loop(int i)
+    {
+        uint64_t seen = 0;
+        for (;;)
+        {
+            long spin = 0;
+            while (gen_.load(std::memory_order_acquire) == seen && !stop_.load() && spin < 200000)
+                ++spin;
+            if (gen_.load(std::memory_order_acquire) == seen && !stop_.load())
+            {
+                std::unique_lock<std::mutex> l(m_);
+                cv_.wait(l, [&] { return stop_.load() || gen_.load() != seen; });
+            }
+            if (stop_.load()) return;
+            seen = gen_.load(std::memory_order_acquire);
+            (*job_)(i, n_);
+            pending_.fetch_sub(1, std::memory_order_acq_rel);
+        }
+    }
+
+    int n_;
+    std::vector<std::thread> workers_;
+    std::mutex m_;
+    std::condition_variable cv_;
+    const std::function<void(int, int)>* job_ = nullptr;
+    std::atomic<uint64_t> gen_{0};
+    std::atomic<int> pending_{0};
+    std::atomic<bool> stop_{false};
+};
+
+// [begin, end) of part t of n of a range of `total` items
+inline void part_range(int64_t total, int t, int n, int64_t& begin, int64_t& end)
+{
+    begin = total * t / n;
+    end = total * (t + 1) / n;
+}
+
+// indptr monotone from a non-negative start and every column index in
+// [0, n): the checks that make the host loops below safe
+bool valid_pattern(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices,
+                   const char* who)
+{
+    if (indptr[0] < 0)
+    {
+        slq::set_error(std::string(who) + ": indptr[0] is negative");
+        return false;
+    }
+    for (int64_t r = 0; r < n; ++r)
+        if (indptr[r + 1] < indptr[r])
+        {
+            slq::set_error(std::string(who) + ": indptr is not monotone");
+            return false;
+        }
+    const int64_t e0 = indptr[0], e1 = indptr[n];
+    std::atomic<bool> bad(false);
+    P.run([&](int t, int nt) {
+        int64_t b, e;
+        part_range(e1 - e0, t, nt, b, e);
+        for (int64_t k = e0 + b; k < e0 + e; ++k)
+            if (indices[k] < 0 || indices[k] >= n)
+            {
+                bad.store(true, std::memory_order_relaxed);
+                return;
+            }
+    });
+    if (bad.load())
+    {
+        slq::set_error(std::string(who) + ": column index out of range");
+        return false;
+    }
+    return true;
+}
+
+// inverse of a permutation, or false if perm is not one
+bool inverse_perm(int64_t n, const int32_t* perm, std::vector<int32_t>& inv)
+{
+    inv.assign(static_cast<size_t>(n), -1);
+    for (int64_t k = 0; k < n; ++k)
+    {
+        const int32_t r = perm[k];
+        if (r < 0 || r >= n || inv[r] >= 0) return false;
+        inv[r] = static_cast<int32_t>(k);
+    }
+    return true;
+}
+
+// The positions numpy's unique(linspace(0, last, count).astype(int64))
+// gives: k * (last / (count - 1)) truncated, the last one exactly `last`.
+std::vector<int64_t> sample_positions(int64_t last, int64_t count)
+{
+    std::vector<int64_t> out;
+    if (count <= 0) return out;
+    if (count == 1)
+    {
+        out.push_back(0);
+        return out;
+    }
+    const double step = static_cast<double>(last) / static_cast<double>(count - 1);
+    out.reserve(static_cast<size_t>(count));
+    for (int64_t k = 0; k < count; ++k)
+    {
+        const int64_t v =
+            (k == count - 1) ? last : static_cast<int64_t>(static_cast<double>(k) * step);
+        if (out.empty() || v != out.back()) out.push_back(v);
+    }
+    return out;
+}
+
+// ---------------------------------------------------------------------------
+// reverse Cuthill-McKee
+// ---------------------------------------------------------------------------
+
+// visited rows, one bit each
+struct Bits {
+    std::vector<uint64_t> w;
+    explicit Bits(int64_t n) : w(static_cast<size_t>((n + 63) / 64), 0) {}
+    bool get(int32_t r) const { return (w[static_cast<size_t>(r) >> 6] >> (r & 63)) & 1u; }
+    void set(int32_t r) { w[static_cast<size_t>(r) >> 6] |= uint64_t(1) << (r & 63); }
+};
+
+// Cuthill-McKee visit order of every component into out[0 .. n)
+void cm_order(int64_t n, const int32_t* indptr, const int32_t* indices, std::vector<int32_t>& out)
+{
+    std::vector<int32_t> degree(static_cast<size_t>(n));
+    int32_t maxdeg = 0;
+    for (int64_t r = 0; r < n; ++r)
+    {
+        degree[r] = indptr[r + 1] - indptr[r];
+        maxdeg = std::max(maxdeg, degree[r]);
+    }
+    // rows by increasing degree, ties by row (a stable counting sort):
+    // component start candidates
+    std::vector<int32_t> by_degree(static_cast<size_t>(n));
+    if (maxdeg <= 4 * n + 1024)
+    {
+        std::vector<int64_t> start(static_cast<size_t>(maxdeg) + 2, 0);
+        for (int64_t r = 0; r < n; ++r) ++start[degree[r] + 1];
+        for (size_t d = 1; d < start.size(); ++d) start[d] += start[d - 1];
+        for (int64_t r = 0; r < n; ++r) by_degree[start[degree[r]]++] = static_cast<int32_t>(r);
+    }
+    else
+    {
+        for (int64_t r = 0; r < n; ++r) by_degree[r] = static_cast<int32_t>(r);
+        std::stable_sort(by_degree.begin(), by_degree.end(),
+                         [&](int32_t a, int32_t b) { return degree[a] < degree[b]; });
+    }
+    Bits visited(n);
+    out.assign(static_cast<size_t>(n), 0);
+    int64_t cnt = 0;
+    std::vector<std::pair<int32_t, int32_t>> kids;
+    for (int32_t seed : by_degree)
+    {
+        if (visited.get(seed)) continue;
+        // each component starts at its lowest-degree row (as scipy's
+        // reverse_cuthill_mckee does)
+        int64_t head = cnt;
+        out[cnt++] = seed;
+        visited.set(seed);
+        while (head < cnt)
+        {
+            const int32_t r = out[head++];
+            kids.clear();
+            for (int32_t e = indptr[r]; e < indptr[r + 1]; ++e)
+            {
+                const int32_t c = indices[e];
+                if (!visited.get(c))
+                {
+                    visited.set(c);
+                    kids.emplace_back(degree[c], c);
+                }
+            }
+            std::sort(kids.begin(), kids.end());
+            for (const auto& k : kids) out[cnt++] = k.second;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// row-group aggregation
+// ---------------------------------------------------------------------------
 
 struct Cand {
     double w;
@@ -41,20 +291,36 @@ bool stronger(const Cand& a, const Cand& b)
     return a.w > b.w || (a.w == b.w && a.row < b.row);
 }
 
-template <typename VT>
-void aggregate(int64_t n, const int32_t* indptr, const int32_t* indices, const VT* data, int G,
-               const int32_t* base, int32_t* order)
+// chunks of the base order aggregated independently: a multiple of G rows
+// each, at least 16384 rows, at most 16 (the count depends on n only)
+void chunking(int64_t n, int G, int64_t& nchunks, int64_t& chunk)
 {
-    std::vector<uint8_t> placed(static_cast<size_t>(n), 0);
-    std::vector<int32_t> group;
-    std::vector<int32_t> frontier, next;
+    nchunks = std::max<int64_t>(1, std::min<int64_t>(16, n / 16384));
+    const int64_t groups = (n + G - 1) / G;
+    chunk = static_cast<int64_t>(G) * ((groups + nchunks - 1) / nchunks);
+    nchunks = std::max<int64_t>(1, (n + chunk - 1) / chunk);
+}
+
+// Aggregate the rows at base positions [k0, k1) into order[k0 .. k1).
+// Only rows of this chunk join its groups (owner test by base position).
+template <typename VT>
+void aggregate_chunk(const int32_t* indptr, const int32_t* indices, const VT* data, int G,
+                     const int32_t* base, const int32_t* base_pos, int64_t k0, int64_t k1,
+                     uint8_t* placed, int32_t* order)
+{
+    auto row_at = [&](int64_t k) { return base ? base[k] : static_cast<int32_t>(k); };
+    auto owned = [&](int32_t r) {
+        const int64_t p = base_pos ? base_pos[r] : r;
+        return p >= k0 && p < k1;
+    };
+    std::vector<int32_t> group, frontier, next;
     std::vector<Cand> best;
     group.reserve(G);
-    int64_t out = 0;
-    int64_t fill_cursor = 0;  // next base position for the fallback
-    for (int64_t k = 0; k < n; ++k)
+    int64_t out = k0;
+    int64_t fill_cursor = k0;  // next base position for the fallback
+    for (int64_t k = k0; k < k1; ++k)
     {
-        const int32_t seed = base ? base[k] : static_cast<int32_t>(k);
+        const int32_t seed = row_at(k);
         if (placed[seed]) continue;
         group.clear();
         group.push_back(seed);
@@ -73,7 +339,7 @@ void aggregate(int64_t n, const int32_t* indptr, const int32_t* indices, const V
                 for (int32_t e = indptr[f]; e < indptr[f + 1]; ++e)
                 {
                     const int32_t c = indices[e];
-                    if (placed[c]) continue;
+                    if (placed[c] || !owned(c)) continue;
                     const double w = data ? std::fabs(static_cast<double>(data[e])) : 1.0;
                     const Cand cand{w, c};
                     if (static_cast<int>(best.size()) < want)
@@ -91,6 +357,8 @@ void aggregate(int64_t n, const int32_t* indptr, const int32_t* indices, const V
                 std::sort(best.begin(), best.end(), stronger);
                 for (const Cand& bc : best)
                 {
+                    // a row that f lists twice joins once
+                    if (placed[bc.row]) continue;
                     placed[bc.row] = 1;
                     group.push_back(bc.row);
                     next.push_back(bc.row);
@@ -100,11 +368,9 @@ void aggregate(int64_t n, const int32_t* indptr, const int32_t* indices, const V
         }
         while (static_cast<int>(group.size()) < G)
         {
-            while (fill_cursor < n &&
-                   placed[base ? base[fill_cursor] : static_cast<int32_t>(fill_cursor)])
-                ++fill_cursor;
-            if (fill_cursor >= n) break;
-            const int32_t r = base ? base[fill_cursor] : static_cast<int32_t>(fill_cursor);
+            while (fill_cursor < k1 && placed[row_at(fill_cursor)]) ++fill_cursor;
+            if (fill_cursor >= k1) break;
+            const int32_t r = row_at(fill_cursor);
             placed[r] = 1;
             group.push_back(r);
         }
@@ -112,32 +378,24 @@ void aggregate(int64_t n, const int32_t* indptr, const int32_t* indices, const V
     }
 }
 
-// Breadth-first search from `start` over the unvisited rows of its
-// component, the children of a row in increasing degree (Cuthill-McKee);
-// appends the visit order to `out`.
-void cm_bfs(int32_t start, const int32_t* indptr, const int32_t* indices, const int32_t* degree,
-            std::vector<uint8_t>& visited, std::vector<int32_t>& out,
-            std::vector<std::pair<int32_t, int32_t>>& kids)
+template <typename VT>
+void aggregate(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices, const VT* data,
+               int G, const int32_t* base, const int32_t* base_pos, int32_t* order)
 {
-    size_t head = out.size();
-    out.push_back(start);
-    visited[start] = 1;
-    while (head < out.size())
-    {
-        const int32_t r = out[head++];
-        kids.clear();
-        for (int32_t e = indptr[r]; e < indptr[r + 1]; ++e)
+    std::vector<uint8_t> placed(static_cast<size_t>(n), 0);
+    int64_t nchunks, chunk;
+    chunking(n, G, nchunks, chunk);
+    std::atomic<int64_t> next_chunk(0);
+    P.run([&](int, int) {
+        for (;;)
         {
-            const int32_t c = indices[e];
-            if (!visited[c])
-            {
-                visited[c] = 1;
-                kids.emplace_back(degree[c], c);
-            }
+            const int64_t c = next_chunk.fetch_add(1);
+            if (c >= nchunks) return;
+            const int64_t k0 = c * chunk, k1 = std::min(n, k0 + chunk);
+            aggregate_chunk<VT>(indptr, indices, data, G, base, base_pos, k0, k1, placed.data(),
+                                order);
         }
-        std::sort(kids.begin(), kids.end());
-        for (const auto& k : kids) out.push_back(k.second);
-    }
+    });
 }
 
 }  // namespace
@@ -150,37 +408,10 @@ extern "C" slq_status slq_rcm_order(int64_t n, const int32_t* indptr, const int3
         slq::set_error("rcm_order: bad arguments");
         return SLQ_ERR_BAD_ARG;
     }
-    for (int64_t r = 0; r < n; ++r)
-        if (indptr[r + 1] < indptr[r])
-        {
-            slq::set_error("rcm_order: indptr is not monotone");
-            return SLQ_ERR_BAD_CSR;
-        }
-    for (int64_t e = 0; e < indptr[n]; ++e)
-        if (indices[e] < 0 || indices[e] >= n)
-        {
-            slq::set_error("rcm_order: column index out of range");
-            return SLQ_ERR_BAD_CSR;
-        }
-    std::vector<int32_t> degree(static_cast<size_t>(n));
-    for (int64_t r = 0; r < n; ++r) degree[r] = indptr[r + 1] - indptr[r];
-    // rows by increasing degree: component start candidates
-    std::vector<int32_t> by_degree(static_cast<size_t>(n));
-    for (int64_t r = 0; r < n; ++r) by_degree[r] = static_cast<int32_t>(r);
-    std::stable_sort(by_degree.begin(), by_degree.end(),
-                     [&](int32_t a, int32_t b) { return degree[a] < degree[b]; });
-    std::vector<uint8_t> visited(static_cast<size_t>(n), 0);
+    Pool P(host_threads());
+    if (!valid_pattern(P, n, indptr, indices, "rcm_order")) return SLQ_ERR_BAD_CSR;
     std::vector<int32_t> out;
-    std::vector<std::pair<int32_t, int32_t>> kids;
-    out.reserve(static_cast<size_t>(n));
-    for (int32_t seed : by_degree)
-    {
-        if (visited[seed]) continue;
-        // each component starts at its lowest-degree row (as scipy's
-        // reverse_cuthill_mckee does)
-        const int32_t start = seed;
-        cm_bfs(start, indptr, indices, degree.data(), visited, out, kids);
-    }
+    cm_order(n, indptr, indices, out);
     // reverse Cuthill-McKee
     for (int64_t k = 0; k < n; ++k) order[k] = out[static_cast<size_t>(n - 1 - k)];
     return SLQ_OK;
@@ -195,37 +426,102 @@ extern "C" slq_status slq_group_order(int64_t n, const int32_t* indptr, const in
         slq::set_error("group_order: bad arguments");
         return SLQ_ERR_BAD_ARG;
     }
-    for (int64_t r = 0; r < n; ++r)
-        if (indptr[r + 1] < indptr[r])
-        {
-            slq::set_error("group_order: indptr is not monotone");
-            return SLQ_ERR_BAD_CSR;
-        }
-    for (int64_t e = 0; e < indptr[n]; ++e)
-        if (indices[e] < 0 || indices[e] >= n)
-        {
-            slq::set_error("group_order: column index out of range");
-            return SLQ_ERR_BAD_CSR;
-        }
-    if (base_order)
+    Pool P(host_threads());
+    if (!valid_pattern(P, n, indptr, indices, "group_order")) return SLQ_ERR_BAD_CSR;
+    std::vector<int32_t> base_pos;
+    if (base_order && !inverse_perm(n, base_order, base_pos))
     {
-        std::vector<uint8_t> seen(static_cast<size_t>(n), 0);
-        for (int64_t k = 0; k < n; ++k)
+        slq::set_error("group_order: base_order is not a permutation");
+        return SLQ_ERR_BAD_ARG;
+    }
+    const int32_t* bp = base_order ? base_pos.data() : nullptr;
+    if (dtype == SLQ_F64)
+        aggregate<double>(P, n, indptr, indices, static_cast<const double*>(data), group_rows,
+                          base_order, bp, order);
+    else
+        aggregate<float>(P, n, indptr, indices, static_cast<const float*>(data), group_rows,
+                         base_order, bp, order);
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_order_spread(int64_t n, const int32_t* indptr, const int32_t* indices,
+                                       const int32_t* perm, int64_t sample_rows, double* spread)
+{
+    if (n < 0 || !indptr || !indices || !spread || sample_rows < 1)
+    {
+        slq::set_error("order_spread: bad arguments");
+        return SLQ_ERR_BAD_ARG;
+    }
+    Pool P(host_threads());
+    if (!valid_pattern(P, n, indptr, indices, "order_spread")) return SLQ_ERR_BAD_CSR;
+    std::vector<int32_t> inv;
+    if (perm && !inverse_perm(n, perm, inv))
+    {
+        slq::set_error("order_spread: perm is not a permutation");
+        return SLQ_ERR_BAD_ARG;
+    }
+    *spread = 0.0;
+    if (n == 0) return SLQ_OK;
+    const std::vector<int64_t> rows = sample_positions(n - 1, std::min(n, sample_rows));
+    double sum = 0.0;
+    int64_t count = 0;
+    for (int64_t r : rows)
+        for (int32_t e = indptr[r]; e < indptr[r + 1]; ++e)
         {
-            const int32_t r = base_order[k];
-            if (r < 0 || r >= n || seen[r])
-            {
-                slq::set_error("group_order: base_order is not a permutation");
-                return SLQ_ERR_BAD_ARG;
-            }
-            seen[r] = 1;
+            const int64_t c = indices[e];
+            const int64_t d = perm ? static_cast<int64_t>(inv[c]) - inv[r] : c - r;
+            sum += static_cast<double>(d < 0 ? -d : d);
+            ++count;
+        }
+    *spread = count ? sum / static_cast<double>(count) : 0.0;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_group_fill(int64_t n, const int32_t* indptr, const int32_t* indices,
+                                     const int32_t* order, int group_rows, int64_t sample_groups,
+                                     double* fill)
+{
+    if (n < 0 || !indptr || !indices || !fill || group_rows < 1 || sample_groups < 1)
+    {
+        slq::set_error("group_fill: bad arguments");
+        return SLQ_ERR_BAD_ARG;
+    }
+    Pool P(host_threads());
+    if (!valid_pattern(P, n, indptr, indices, "group_fill")) return SLQ_ERR_BAD_CSR;
+    if (order)
+    {
+        std::vector<int32_t> inv;
+        if (!inverse_perm(n, order, inv))
+        {
+            slq::set_error("group_fill: order is not a permutation");
+            return SLQ_ERR_BAD_ARG;
         }
     }
-    if (dtype == SLQ_F64)
-        aggregate<double>(n, indptr, indices, static_cast<const double*>(data), group_rows,
-                          base_order, order);
-    else
-        aggregate<float>(n, indptr, indices, static_cast<const float*>(data), group_rows,
-                         base_order, order);
+    const int G = group_rows;
+    const int64_t ngroups = n / G;
+    *fill = 0.0;
+    if (ngroups == 0) return SLQ_OK;
+    const std::vector<int64_t> picks =
+        sample_positions(ngroups - 1, std::min(sample_groups, ngroups));
+    double sum = 0.0;
+    int64_t ok = 0;
+    std::vector<int32_t> cols;
+    for (int64_t p : picks)
+    {
+        cols.clear();
+        for (int g = 0; g < G; ++g)
+        {
+            const int64_t k = p * G + g;
+            const int32_t r = order ? order[k] : static_cast<int32_t>(k);
+            cols.insert(cols.end(), indices + indptr[r], indices + indptr[r + 1]);
+        }
+        if (cols.empty()) continue;
+        const int64_t nnz = static_cast<int64_t>(cols.size());
+        std::sort(cols.begin(), cols.end());
+        const int64_t uni = std::unique(cols.begin(), cols.end()) - cols.begin();
+        sum += static_cast<double>(nnz) / (static_cast<double>(G) * static_cast<double>(uni));
+        ++ok;
+    }
+    *fill = ok ? sum / static_cast<double>(ok) : 0.0;
     return SLQ_OK;
 }

@@ -31,14 +31,39 @@ def _dtype_code(dtype):
                     'GPU; got "%s".' % dtype)
 
 
-def locality_order(A, reorder="auto"):
-    """Reverse Cuthill-McKee order (``rcm_order``) of a square sparse
-    matrix, or None.
+def _pattern(A):
+    """int32 indptr / indices of a CSR matrix, as the host orders take them."""
+    return (np.ascontiguousarray(A.indptr, dtype=np.int32),
+            np.ascontiguousarray(A.indices, dtype=np.int32))
+
+
+def order_spread(A, perm=None, sample_rows=20000):
+    """Mean |position(i) - position(j)| over the nonzeros of sampled rows of
+    a square sparse matrix (``slq_order_spread``; positions of ``perm``'s
+    inverse, or the identity)."""
+    A = sp.csr_matrix(A)
+    n = A.shape[0]
+    ip, ind = _pattern(A)
+    p = None if perm is None else np.ascontiguousarray(perm, dtype=np.int32)
+    out = ctypes.c_double(0.0)
+    _lib.check(_lib.load().slq_order_spread(
+        n, ip.ctypes.data, ind.ctypes.data,
+        None if p is None else p.ctypes.data, int(sample_rows),
+        ctypes.byref(out)))
+    return float(out.value)
+
+
+def locality_order(A, reorder="auto", device_pattern=None):
+    """Reverse Cuthill-McKee order (``rcm_order``) of a square sparse matrix,
+    or None.
 
     'auto' reorders square matrices of order >= 16384 whose nonzeros lie far
-    from the diagonal (mean |i - j| > 256) when RCM shrinks that distance at
-    least fourfold: the SpMM gathers of such matrices then stay inside a
-    window that fits L2.  True always reorders a square matrix, False never.
+    from the diagonal (mean |i - j| > 256 over sampled rows) when RCM
+    shrinks that distance at least fourfold: the SpMM gathers of such
+    matrices then stay inside a window that fits L2.  True always reorders a
+    square matrix, False never.  ``device_pattern`` = (indptr, indices), A's
+    CSR arrays as int32 CUDA tensors, computes the order on the device
+    (``rcm_order_device``; the host computes it when that declines).
     """
     if reorder is False or A.shape[0] != A.shape[1]:
         return None
@@ -47,21 +72,17 @@ def locality_order(A, reorder="auto"):
     if reorder == "auto":
         if n < 16384 or A.nnz == 0:
             return None
-        # mean |i - j| over the nonzeros of a sample of rows
-        rows = np.unique(np.linspace(0, n - 1, min(n, 20000)).astype(np.int64))
-        S = A[rows]
-        ri = np.repeat(rows, np.diff(S.indptr))
-        cols = S.indices.astype(np.int64)
-        spread = float(np.mean(np.abs(cols - ri))) if cols.size else 0.0
+        spread = order_spread(A)
         if spread <= 256.0:
             return None
-    perm = rcm_order(A)
-    if reorder == "auto":
-        inv = np.empty_like(perm)
-        inv[perm] = np.arange(n, dtype=perm.dtype)
-        new_spread = float(np.mean(np.abs(inv[cols] - inv[ri])))
-        if new_spread * 4.0 > spread:
-            return None
+    perm = None
+    if device_pattern is not None:
+        perm = rcm_order_device(device_pattern[0], device_pattern[1], n,
+                                A.nnz)
+    if perm is None:
+        perm = rcm_order(A)
+    if reorder == "auto" and order_spread(A, perm) * 4.0 > spread:
+        return None
     return np.ascontiguousarray(perm, dtype=np.int32)
 
 
@@ -71,34 +92,52 @@ def rcm_order(A):
     with symmetric_mode=True gives)."""
     A = sp.csr_matrix(A)
     n = A.shape[0]
-    ip = np.ascontiguousarray(A.indptr, dtype=np.int32)
-    ind = np.ascontiguousarray(A.indices, dtype=np.int32)
+    ip, ind = _pattern(A)
     order = np.empty(n, dtype=np.int32)
     _lib.check(_lib.load().slq_rcm_order(n, ip.ctypes.data, ind.ctypes.data,
                                          order.ctypes.data))
     return order
 
 
+def rcm_order_device(indptr, indices, n, nnz, max_components=64):
+    """``rcm_order`` of a square CSR pattern held on the device (int32 CUDA
+    tensors) by ``slq_rcm_order_device``, as a host array; None when the
+    pattern has more than ``max_components`` components (the host order is
+    then the faster one)."""
+    import torch
+    lib = _lib.load()
+    nbytes = ctypes.c_size_t(0)
+    _lib.check(lib.slq_rcm_order_device_workspace_bytes(int(n),
+                                                        ctypes.byref(nbytes)))
+    dev = indptr.device
+    ws = torch.empty(max(int(nbytes.value), 256), dtype=torch.uint8,
+                     device=dev)
+    order = torch.empty(max(int(n), 1), dtype=torch.int32, device=dev)
+    done = ctypes.c_int(0)
+    stream = torch.cuda.current_stream(dev)
+    _lib.check(lib.slq_rcm_order_device(
+        int(n), int(nnz), indptr.data_ptr(), indices.data_ptr(),
+        int(max_components), order.data_ptr(), ctypes.byref(done),
+        ws.data_ptr(), ws.numel(), stream.cuda_stream))
+    if not done.value:
+        return None
+    return order[:int(n)].cpu().numpy()
+
+
 def _group_fill(A, order, G, sample=256):
     """Mean fill of the dense union blocks of sampled groups of G
-    consecutive rows of ``order`` (nnz / (G x union size))."""
+    consecutive rows of ``order`` (nnz / (G x union size);
+    ``slq_group_fill``)."""
+    A = sp.csr_matrix(A)
     n = A.shape[0]
-    ngroups = n // G
-    if ngroups == 0:
-        return 0.0
-    picks = np.unique(np.linspace(0, ngroups - 1,
-                                  min(sample, ngroups)).astype(np.int64))
-    rows = np.asarray(order)[(picks[:, None] * G +
-                              np.arange(G)[None, :]).ravel()]
-    S = A[rows]
-    grp = np.repeat(np.repeat(np.arange(picks.size), G), np.diff(S.indptr))
-    if grp.size == 0:
-        return 0.0
-    keys = grp.astype(np.int64) * A.shape[1] + S.indices
-    union = np.bincount(np.unique(keys) // A.shape[1], minlength=picks.size)
-    nnz = np.bincount(grp, minlength=picks.size)
-    ok = union > 0
-    return float(np.mean(nnz[ok] / (G * union[ok]))) if ok.any() else 0.0
+    ip, ind = _pattern(A)
+    o = None if order is None else np.ascontiguousarray(order, dtype=np.int32)
+    out = ctypes.c_double(0.0)
+    _lib.check(_lib.load().slq_group_fill(
+        n, ip.ctypes.data, ind.ctypes.data,
+        None if o is None else o.ctypes.data, int(G), int(sample),
+        ctypes.byref(out)))
+    return float(out.value)
 
 
 def group_order(A, base_perm, G):
@@ -189,7 +228,21 @@ class _DeviceOperator:
         self.device = torch.device("cuda", torch.cuda.current_device())
         if A is None:
             return  # from_device fills the fields
-        base = locality_order(A, reorder)
+        dev = self.device
+        early = (A.format == "csr" and A.shape[0] == A.shape[1] and
+                 A.has_sorted_indices and A.has_canonical_format and
+                 max(A.shape) <= np.iinfo(np.int32).max and
+                 A.nnz <= np.iinfo(np.int32).max)
+        pattern = None
+        if early:
+            # canonical CSR goes to the device as it is: upload first, so
+            # that the locality order is computed there
+            self.indices = torch.from_numpy(
+                np.ascontiguousarray(A.indices, dtype=np.int32)).to(dev)
+            self.indptr = torch.from_numpy(
+                np.ascontiguousarray(A.indptr, dtype=np.int32)).to(dev)
+            pattern = (self.indptr, self.indices)
+        base = locality_order(A, reorder, device_pattern=pattern)
         self.group_rows, perm = group_rows_for(A, base, group_rows,
                                                aggregate=aggregate)
         if perm is not None and A.format != "csr":
@@ -209,12 +262,12 @@ class _DeviceOperator:
         if max(A.shape) > np.iinfo(np.int32).max or \
                 self.nnz > np.iinfo(np.int32).max:
             raise ValueError("matrix too large for 32-bit indices")
-        dev = self.device
         self.data = torch.from_numpy(np.ascontiguousarray(A.data)).to(dev)
-        self.indices = torch.from_numpy(
-            np.ascontiguousarray(A.indices, dtype=np.int32)).to(dev)
-        self.indptr = torch.from_numpy(
-            np.ascontiguousarray(A.indptr, dtype=np.int32)).to(dev)
+        if not early:
+            self.indices = torch.from_numpy(
+                np.ascontiguousarray(A.indices, dtype=np.int32)).to(dev)
+            self.indptr = torch.from_numpy(
+                np.ascontiguousarray(A.indptr, dtype=np.int32)).to(dev)
         self.perm = None
         self.inv = None
         if perm is not None:

@@ -124,7 +124,10 @@ slq_status slq_rcm_order(int64_t n, const int32_t* indptr,
  * rows in base_order (NULL = identity) and makes each row not yet placed the
  * seed of a group of group_rows rows: the seed, its not-yet-placed
  * neighbours by decreasing |a_ij|, their neighbours, and, when the
- * neighbourhood runs out, the next unplaced rows of the base order.
+ * neighbourhood runs out, the next unplaced rows of the base order.  The
+ * base order is cut into chunks of at least 16384 rows (at most 16, a
+ * multiple of group_rows each; the cut depends on n only) aggregated in
+ * parallel, each group from one chunk's rows.
  * order[k] receives the row at position k; every group but the last has
  * exactly group_rows rows, so passing order as slq_operator_create's perm
  * lines the groups up with the row-group format's, whose cost falls with
@@ -133,6 +136,44 @@ slq_status slq_group_order(int64_t n, const int32_t* indptr,
                            const int32_t* indices, const void* data,
                            int dtype, int group_rows,
                            const int32_t* base_order, int32_t* order);
+
+/* Workspace for slq_rcm_order_device (device bytes). */
+slq_status slq_rcm_order_device_workspace_bytes(int64_t n, size_t* bytes);
+
+/* slq_rcm_order on the device: the same order for a square CSR pattern of n
+ * rows and nnz entries in device memory (int32 indptr / indices, validated
+ * first), computed one breadth-first level at a time (one host
+ * synchronisation per level and per component); order (device, n entries)
+ * receives it.  *done = 1 on success; *done = 0, with SLQ_OK and order
+ * undefined, when the pattern has more than max_components connected
+ * components or its sort keys (level offset, degree, row) need more than 64
+ * bits -- the caller then uses slq_rcm_order.  No counterpart in the
+ * reference. */
+slq_status slq_rcm_order_device(int64_t n, int64_t nnz, const int32_t* indptr,
+                                const int32_t* indices, int max_components,
+                                int32_t* order, int* done, void* workspace,
+                                size_t workspace_bytes, void* stream);
+
+/* Mean |position(i) - position(j)| over the nonzeros (i, j) of sampled rows
+ * of a square CSR pattern (host arrays): the rows numpy's
+ * unique(linspace(0, n - 1, min(n, sample_rows)).astype(int64)) picks,
+ * positions the identity (perm NULL) or perm^-1 (perm[k] = row at position
+ * k).  Decides whether a locality order pays (no counterpart in the
+ * reference). */
+slq_status slq_order_spread(int64_t n, const int32_t* indptr,
+                            const int32_t* indices, const int32_t* perm,
+                            int64_t sample_rows, double* spread);
+
+/* Mean fill nnz / (group_rows x union size) of sampled groups of group_rows
+ * consecutive rows of `order` (NULL = identity) of a CSR pattern (host
+ * arrays): the groups numpy's unique(linspace(0, n / group_rows - 1,
+ * min(sample_groups, n / group_rows)).astype(int64)) picks, groups without
+ * entries left out.  Predicts the row-group format's padding (no
+ * counterpart in the reference). */
+slq_status slq_group_fill(int64_t n, const int32_t* indptr,
+                          const int32_t* indices, const int32_t* order,
+                          int group_rows, int64_t sample_groups,
+                          double* fill);
 
 /* Release the host-side operator record (device arrays stay with their
  * owners).  Replaces the cuLinearOperator destructors

@@ -578,3 +578,49 @@ def test_aggregated_groups_match_oracle(cuda, group):
                         coefficients=False, **kw)
     assert rel(info32["convergence"]["samples"],
                info64["convergence"]["samples"]) < 1e-5
+
+
+def _device_pattern(A):
+    import torch
+    A = sp.csr_matrix(A)
+    return (torch.from_numpy(A.indptr.astype(np.int32)).cuda(),
+            torch.from_numpy(A.indices.astype(np.int32)).cuda())
+
+
+def test_device_rcm_order_equals_host_order(cuda):
+    from imate_b200.linear_operator import rcm_order, rcm_order_device
+    R = sp.random(6000, 6000, density=0.0008, random_state=7, format="csr")
+    S = sp.random(6000, 6000, density=0.0003, random_state=7, format="csr")
+    N = sp.random(3000, 3000, density=0.002, random_state=8, format="csr")
+    cases = [ib.correlation_matrix(40000, scale=0.01, shift=0.1, seed=2),
+             sp.csr_matrix(R + R.T + sp.eye(6000)),   # connected
+             sp.csr_matrix(S + S.T + sp.eye(6000)),   # 176 components
+             sp.csr_matrix(S + S.T),                  # 169 empty rows
+             sp.csr_matrix(N + sp.eye(3000)),         # not symmetric
+             sp.csr_matrix((1, 1))]
+    for A in cases:
+        A = sp.csr_matrix(A)
+        A.sort_indices()
+        ip, ind = _device_pattern(A)
+        got = rcm_order_device(ip, ind, A.shape[0], A.nnz,
+                               max_components=A.shape[0])
+        assert got is not None
+        assert np.array_equal(got, rcm_order(A))
+
+
+def test_device_rcm_order_declines_many_components(cuda):
+    from imate_b200.linear_operator import rcm_order_device
+    A = sp.csr_matrix(sp.block_diag([sp.eye(3) + sp.eye(3, k=1)
+                                     for _ in range(100)]))
+    ip, ind = _device_pattern(A)
+    assert rcm_order_device(ip, ind, A.shape[0], A.nnz,
+                            max_components=10) is None
+
+
+def test_device_rcm_order_rejects_bad_pattern(cuda):
+    import torch
+    from imate_b200.linear_operator import rcm_order_device
+    ip = torch.tensor([0, 1, 2], dtype=torch.int32, device="cuda")
+    ind = torch.tensor([0, 5], dtype=torch.int32, device="cuda")
+    with pytest.raises(_lib.SlqError):
+        rcm_order_device(ip, ind, 2, 2)

@@ -279,3 +279,69 @@ def test_rcm_order_is_a_bandwidth_reducing_permutation(lib):
         assert ours < spread(A, ident)
         ref = spread(A, reverse_cuthill_mckee(A, symmetric_mode=True))
         assert ours <= 1.1 * ref
+
+
+def _np_group_fill(A, order, G, sample=256):
+    """numpy restatement of the sampled group fill (slq_group_fill)."""
+    n = A.shape[0]
+    ngroups = n // G
+    picks = np.unique(np.linspace(0, ngroups - 1,
+                                  min(sample, ngroups)).astype(np.int64))
+    rows = np.asarray(order)[(picks[:, None] * G +
+                              np.arange(G)[None, :]).ravel()]
+    S = A[rows]
+    grp = np.repeat(np.repeat(np.arange(picks.size), G), np.diff(S.indptr))
+    keys = grp.astype(np.int64) * A.shape[1] + S.indices
+    union = np.bincount(np.unique(keys) // A.shape[1], minlength=picks.size)
+    nnz = np.bincount(grp, minlength=picks.size)
+    ok = union > 0
+    return float(np.mean(nnz[ok] / (G * union[ok])))
+
+
+def _np_spread(A, perm=None, sample=20000):
+    """numpy restatement of the sampled order spread (slq_order_spread)."""
+    n = A.shape[0]
+    rows = np.unique(np.linspace(0, n - 1, min(n, sample)).astype(np.int64))
+    S = A[rows]
+    ri = np.repeat(rows, np.diff(S.indptr))
+    cols = S.indices.astype(np.int64)
+    if perm is None:
+        return float(np.mean(np.abs(cols - ri)))
+    inv = np.empty(n, np.int64)
+    inv[perm] = np.arange(n)
+    return float(np.mean(np.abs(inv[cols] - inv[ri])))
+
+
+def test_order_statistics_match_numpy(lib):
+    from imate_b200.linear_operator import (_group_fill, order_spread,
+                                            rcm_order)
+    R = sp.random(5000, 5000, density=0.002, random_state=3, format="csr")
+    cases = [ib.correlation_matrix(20000, scale=0.01, shift=0.1, seed=2),
+             sp.csr_matrix(R + R.T + sp.eye(5000))]
+    for A in cases:
+        A = sp.csr_matrix(A)
+        perm = rcm_order(A)
+        for G in (4, 8, 16):
+            for order in (perm, np.arange(A.shape[0], dtype=np.int32)):
+                assert abs(_group_fill(A, order, G) -
+                           _np_group_fill(A, order, G)) < 1e-12
+        assert abs(order_spread(A) - _np_spread(A)) < 1e-9 * _np_spread(A)
+        assert abs(order_spread(A, perm) - _np_spread(A, perm)) < \
+            1e-9 * _np_spread(A, perm)
+
+
+def test_group_order_is_independent_of_threads_and_chunked(lib):
+    # 16 chunks of the base order (n >= 16 x 16384), each group inside one
+    from imate_b200.linear_operator import group_order, rcm_order
+    A = ib.correlation_matrix(262144, scale=0.005, threshold=0.05, shift=0.1,
+                              seed=1, dtype="float32")
+    base = rcm_order(A)
+    order = group_order(A, base, 16)
+    assert np.array_equal(np.sort(order), np.arange(A.shape[0]))
+    assert np.array_equal(order, group_order(A, base, 16))
+    pos = np.empty(A.shape[0], np.int64)
+    pos[base] = np.arange(A.shape[0])
+    chunk = 16384
+    owner = pos[order.reshape(-1, 16)] // chunk
+    assert np.all(owner == owner[:, :1])
+    assert _np_group_fill(sp.csr_matrix(A), order, 16) > 0.6
