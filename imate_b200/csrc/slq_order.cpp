@@ -22,10 +22,8 @@
 // not-yet-placed rows of the base order, so that every group except the
 // last has exactly G rows and lines up with the device format's groups.
 // Groups keep the base order's sequence, so the SpMM's gather window stays
-// as local as the base order made it.  The base order is cut into a fixed
-// number of chunks (a multiple of G rows each; the count depends on n only)
-// that are aggregated independently and in parallel, a group taking rows of
-// its own chunk only.
+// as local as the base order made it.  Large orders run two such sweeps
+// in parallel from the middle of the base order outwards (see aggregate).
 
 #include <algorithm>
 #include <atomic>
@@ -172,6 +170,16 @@ bool valid_pattern(Pool& P, int64_t n, const int32_t* indptr, const int32_t* ind
     return true;
 }
 
+// row r's entries lie inside the index array (0 <= indptr[r] <= indptr[r+1]
+// <= indptr[n]) and index [0, n): the checks a sampled row needs
+bool valid_row(int64_t n, const int32_t* indptr, const int32_t* indices, int64_t r)
+{
+    if (indptr[r] < 0 || indptr[r + 1] < indptr[r] || indptr[r + 1] > indptr[n]) return false;
+    for (int32_t e = indptr[r]; e < indptr[r + 1]; ++e)
+        if (indices[e] < 0 || indices[e] >= n) return false;
+    return true;
+}
+
 // inverse of a permutation, or false if perm is not one
 bool inverse_perm(int64_t n, const int32_t* perm, std::vector<int32_t>& inv)
 {
@@ -291,34 +299,32 @@ bool stronger(const Cand& a, const Cand& b)
     return a.w > b.w || (a.w == b.w && a.row < b.row);
 }
 
-// chunks of the base order aggregated independently: a multiple of G rows
-// each, at least 16384 rows, at most 16 (the count depends on n only)
-void chunking(int64_t n, int G, int64_t& nchunks, int64_t& chunk)
-{
-    nchunks = std::max<int64_t>(1, std::min<int64_t>(16, n / 16384));
-    const int64_t groups = (n + G - 1) / G;
-    chunk = static_cast<int64_t>(G) * ((groups + nchunks - 1) / nchunks);
-    nchunks = std::max<int64_t>(1, (n + chunk - 1) / chunk);
-}
+// Groups found by one sweep: their rows (G each, the last possibly fewer)
+// and the base position of each group's seed.
+struct Groups {
+    std::vector<int32_t> rows;
+    std::vector<int64_t> seed_pos;
+};
 
-// Aggregate the rows at base positions [k0, k1) into order[k0 .. k1).
-// Only rows of this chunk join its groups (owner test by base position).
+// One sweep over the seeds at base positions k0, k0 + step, ... (step +1 or
+// -1, stopping before `stop`); rows at base positions in [lo, hi) may join.
+// A group whose neighbourhood runs out is filled with the next unplaced rows
+// of the sweep.
 template <typename VT>
-void aggregate_chunk(const int32_t* indptr, const int32_t* indices, const VT* data, int G,
-                     const int32_t* base, const int32_t* base_pos, int64_t k0, int64_t k1,
-                     uint8_t* placed, int32_t* order)
+void aggregate_sweep(const int32_t* indptr, const int32_t* indices, const VT* data, int G,
+                     const int32_t* base, const int32_t* base_pos, int64_t k0, int64_t stop,
+                     int step, int64_t lo, int64_t hi, uint8_t* placed, Groups& out)
 {
     auto row_at = [&](int64_t k) { return base ? base[k] : static_cast<int32_t>(k); };
     auto owned = [&](int32_t r) {
         const int64_t p = base_pos ? base_pos[r] : r;
-        return p >= k0 && p < k1;
+        return p >= lo && p < hi;
     };
     std::vector<int32_t> group, frontier, next;
     std::vector<Cand> best;
     group.reserve(G);
-    int64_t out = k0;
-    int64_t fill_cursor = k0;  // next base position for the fallback
-    for (int64_t k = k0; k < k1; ++k)
+    int64_t fill_cursor = k0;  // next sweep position for the fallback
+    for (int64_t k = k0; k != stop; k += step)
     {
         const int32_t seed = row_at(k);
         if (placed[seed]) continue;
@@ -368,34 +374,72 @@ void aggregate_chunk(const int32_t* indptr, const int32_t* indices, const VT* da
         }
         while (static_cast<int>(group.size()) < G)
         {
-            while (fill_cursor < k1 && placed[row_at(fill_cursor)]) ++fill_cursor;
-            if (fill_cursor >= k1) break;
+            while (fill_cursor != stop && placed[row_at(fill_cursor)]) fill_cursor += step;
+            if (fill_cursor == stop) break;
             const int32_t r = row_at(fill_cursor);
             placed[r] = 1;
             group.push_back(r);
         }
-        for (int32_t r : group) order[out++] = r;
+        out.rows.insert(out.rows.end(), group.begin(), group.end());
+        out.seed_pos.push_back(k);
     }
 }
 
+// Orders of at least 2 x 16384 rows run two sweeps on two threads, both
+// starting at the middle of the base order and moving apart (the first half
+// backwards, the second forwards), so that neither front runs into rows the
+// other has placed; smaller ones one forward sweep.  Groups are then listed
+// by their seeds' base positions, the short groups at the two ends merged
+// and put last.
 template <typename VT>
 void aggregate(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices, const VT* data,
                int G, const int32_t* base, const int32_t* base_pos, int32_t* order)
 {
     std::vector<uint8_t> placed(static_cast<size_t>(n), 0);
-    int64_t nchunks, chunk;
-    chunking(n, G, nchunks, chunk);
-    std::atomic<int64_t> next_chunk(0);
-    P.run([&](int, int) {
-        for (;;)
+    Groups sweep[2];
+    if (n >= 2 * 16384 && P.size() >= 2)
+    {
+        const int64_t mid = n / 2;
+        P.run([&](int t, int) {
+            if (t == 0)
+                aggregate_sweep<VT>(indptr, indices, data, G, base, base_pos, mid - 1, -1, -1, 0,
+                                    mid, placed.data(), sweep[0]);
+            else if (t == 1)
+                aggregate_sweep<VT>(indptr, indices, data, G, base, base_pos, mid, n, 1, mid, n,
+                                    placed.data(), sweep[1]);
+        });
+    }
+    else
+    {
+        aggregate_sweep<VT>(indptr, indices, data, G, base, base_pos, 0, n, 1, 0, n,
+                            placed.data(), sweep[1]);
+    }
+    struct Ref {
+        int64_t seed_pos;
+        int s;
+        int64_t index;
+    };
+    std::vector<Ref> refs;
+    std::vector<int32_t> tail;  // rows of the short groups
+    for (int s = 0; s < 2; ++s)
+    {
+        const int64_t ng = static_cast<int64_t>(sweep[s].seed_pos.size());
+        for (int64_t i = 0; i < ng; ++i)
         {
-            const int64_t c = next_chunk.fetch_add(1);
-            if (c >= nchunks) return;
-            const int64_t k0 = c * chunk, k1 = std::min(n, k0 + chunk);
-            aggregate_chunk<VT>(indptr, indices, data, G, base, base_pos, k0, k1, placed.data(),
-                                order);
+            const int64_t b = i * G;
+            const int64_t e = std::min<int64_t>(b + G, static_cast<int64_t>(sweep[s].rows.size()));
+            if (e - b < G)
+                tail.insert(tail.end(), sweep[s].rows.begin() + b, sweep[s].rows.begin() + e);
+            else
+                refs.push_back(Ref{sweep[s].seed_pos[i], s, i});
         }
-    });
+    }
+    std::sort(refs.begin(), refs.end(),
+              [](const Ref& a, const Ref& b) { return a.seed_pos < b.seed_pos; });
+    int64_t out = 0;
+    for (const Ref& rf : refs)
+        for (int64_t i = rf.index * G; i < rf.index * G + G; ++i) order[out++] = sweep[rf.s].rows[i];
+    for (int32_t r : tail) order[out++] = r;
 }
 
 }  // namespace
@@ -452,8 +496,6 @@ extern "C" slq_status slq_order_spread(int64_t n, const int32_t* indptr, const i
         slq::set_error("order_spread: bad arguments");
         return SLQ_ERR_BAD_ARG;
     }
-    Pool P(host_threads());
-    if (!valid_pattern(P, n, indptr, indices, "order_spread")) return SLQ_ERR_BAD_CSR;
     std::vector<int32_t> inv;
     if (perm && !inverse_perm(n, perm, inv))
     {
@@ -463,16 +505,39 @@ extern "C" slq_status slq_order_spread(int64_t n, const int32_t* indptr, const i
     *spread = 0.0;
     if (n == 0) return SLQ_OK;
     const std::vector<int64_t> rows = sample_positions(n - 1, std::min(n, sample_rows));
+    for (int64_t r : rows)
+        if (!valid_row(n, indptr, indices, r))
+        {
+            slq::set_error("order_spread: bad CSR pattern");
+            return SLQ_ERR_BAD_CSR;
+        }
+    // per-row sums in parallel, added in row order (thread-count independent)
+    const int64_t m = static_cast<int64_t>(rows.size());
+    std::vector<double> row_sum(static_cast<size_t>(m), 0.0);
+    Pool P(host_threads());
+    P.run([&](int t, int nt) {
+        int64_t b, e;
+        part_range(m, t, nt, b, e);
+        for (int64_t i = b; i < e; ++i)
+        {
+            const int64_t r = rows[i];
+            double sum = 0.0;
+            for (int32_t x = indptr[r]; x < indptr[r + 1]; ++x)
+            {
+                const int64_t c = indices[x];
+                const int64_t d = perm ? static_cast<int64_t>(inv[c]) - inv[r] : c - r;
+                sum += static_cast<double>(d < 0 ? -d : d);
+            }
+            row_sum[i] = sum;
+        }
+    });
     double sum = 0.0;
     int64_t count = 0;
-    for (int64_t r : rows)
-        for (int32_t e = indptr[r]; e < indptr[r + 1]; ++e)
-        {
-            const int64_t c = indices[e];
-            const int64_t d = perm ? static_cast<int64_t>(inv[c]) - inv[r] : c - r;
-            sum += static_cast<double>(d < 0 ? -d : d);
-            ++count;
-        }
+    for (int64_t i = 0; i < m; ++i)
+    {
+        sum += row_sum[i];
+        count += indptr[rows[i] + 1] - indptr[rows[i]];
+    }
     *spread = count ? sum / static_cast<double>(count) : 0.0;
     return SLQ_OK;
 }
@@ -486,42 +551,55 @@ extern "C" slq_status slq_group_fill(int64_t n, const int32_t* indptr, const int
         slq::set_error("group_fill: bad arguments");
         return SLQ_ERR_BAD_ARG;
     }
-    Pool P(host_threads());
-    if (!valid_pattern(P, n, indptr, indices, "group_fill")) return SLQ_ERR_BAD_CSR;
-    if (order)
-    {
-        std::vector<int32_t> inv;
-        if (!inverse_perm(n, order, inv))
-        {
-            slq::set_error("group_fill: order is not a permutation");
-            return SLQ_ERR_BAD_ARG;
-        }
-    }
     const int G = group_rows;
     const int64_t ngroups = n / G;
     *fill = 0.0;
     if (ngroups == 0) return SLQ_OK;
     const std::vector<int64_t> picks =
         sample_positions(ngroups - 1, std::min(sample_groups, ngroups));
-    double sum = 0.0;
-    int64_t ok = 0;
-    std::vector<int32_t> cols;
     for (int64_t p : picks)
-    {
-        cols.clear();
         for (int g = 0; g < G; ++g)
         {
             const int64_t k = p * G + g;
             const int32_t r = order ? order[k] : static_cast<int32_t>(k);
-            cols.insert(cols.end(), indices + indptr[r], indices + indptr[r + 1]);
+            if (r < 0 || r >= n || !valid_row(n, indptr, indices, r))
+            {
+                slq::set_error("group_fill: bad CSR pattern or order");
+                return SLQ_ERR_BAD_CSR;
+            }
         }
-        if (cols.empty()) continue;
-        const int64_t nnz = static_cast<int64_t>(cols.size());
-        std::sort(cols.begin(), cols.end());
-        const int64_t uni = std::unique(cols.begin(), cols.end()) - cols.begin();
-        sum += static_cast<double>(nnz) / (static_cast<double>(G) * static_cast<double>(uni));
-        ++ok;
-    }
+    // per-group fills in parallel, averaged in group order
+    const int64_t m = static_cast<int64_t>(picks.size());
+    std::vector<double> ratio(static_cast<size_t>(m), -1.0);  // < 0: no entries
+    Pool P(host_threads());
+    P.run([&](int t, int nt) {
+        int64_t b, e;
+        part_range(m, t, nt, b, e);
+        std::vector<int32_t> cols;
+        for (int64_t i = b; i < e; ++i)
+        {
+            cols.clear();
+            for (int g = 0; g < G; ++g)
+            {
+                const int64_t k = picks[i] * G + g;
+                const int32_t r = order ? order[k] : static_cast<int32_t>(k);
+                cols.insert(cols.end(), indices + indptr[r], indices + indptr[r + 1]);
+            }
+            if (cols.empty()) continue;
+            const int64_t nnz = static_cast<int64_t>(cols.size());
+            std::sort(cols.begin(), cols.end());
+            const int64_t uni = std::unique(cols.begin(), cols.end()) - cols.begin();
+            ratio[i] = static_cast<double>(nnz) / (static_cast<double>(G) * static_cast<double>(uni));
+        }
+    });
+    double sum = 0.0;
+    int64_t ok = 0;
+    for (int64_t i = 0; i < m; ++i)
+        if (ratio[i] >= 0.0)
+        {
+            sum += ratio[i];
+            ++ok;
+        }
     *fill = ok ? sum / static_cast<double>(ok) : 0.0;
     return SLQ_OK;
 }

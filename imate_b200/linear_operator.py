@@ -144,10 +144,8 @@ def group_order(A, base_perm, G):
     """Row order whose consecutive groups of G rows share many columns
     (``slq_group_order``: each group is a seed row and its strongest
     neighbours, groups following ``base_perm``).  Square matrices only."""
+    # the order does not depend on the order of a row's entries
     A = sp.csr_matrix(A)
-    if not A.has_sorted_indices:
-        A = A.copy()
-        A.sort_indices()
     n = A.shape[0]
     ip = np.ascontiguousarray(A.indptr, dtype=np.int32)
     ind = np.ascontiguousarray(A.indices, dtype=np.int32)

@@ -330,18 +330,27 @@ def test_order_statistics_match_numpy(lib):
             1e-9 * _np_spread(A, perm)
 
 
-def test_group_order_is_independent_of_threads_and_chunked(lib):
-    # 16 chunks of the base order (n >= 16 x 16384), each group inside one
+def test_group_order_two_sweeps_keep_groups_compact(lib):
+    # large orders: two sweeps from the middle of the base order outwards,
+    # each group drawn from one half; the result does not depend on timing
     from imate_b200.linear_operator import group_order, rcm_order
-    A = ib.correlation_matrix(262144, scale=0.005, threshold=0.05, shift=0.1,
-                              seed=1, dtype="float32")
+    A = sp.csr_matrix(ib.correlation_matrix(262144, scale=0.005, threshold=0.05,
+                                            shift=0.1, seed=1, dtype="float32"))
+    n, G = A.shape[0], 16
     base = rcm_order(A)
-    order = group_order(A, base, 16)
-    assert np.array_equal(np.sort(order), np.arange(A.shape[0]))
-    assert np.array_equal(order, group_order(A, base, 16))
-    pos = np.empty(A.shape[0], np.int64)
-    pos[base] = np.arange(A.shape[0])
-    chunk = 16384
-    owner = pos[order.reshape(-1, 16)] // chunk
-    assert np.all(owner == owner[:, :1])
-    assert _np_group_fill(sp.csr_matrix(A), order, 16) > 0.6
+    order = group_order(A, base, G)
+    assert np.array_equal(np.sort(order), np.arange(n))
+    for _ in range(2):
+        assert np.array_equal(order, group_order(A, base, G))
+    pos = np.empty(n, np.int64)
+    pos[base] = np.arange(n)
+    half = pos[order].reshape(-1, G) >= n // 2
+    # every group but the merged short ones at the end lies in one half
+    assert np.all(half[:-2] == half[:-2, :1])
+    # whole-matrix fill of the 16-row groups, and no group far beyond it
+    B = A[order]
+    rows = np.repeat(np.arange(n), np.diff(B.indptr))
+    union = np.bincount(np.unique((rows // G).astype(np.int64) * n + B.indices)
+                        // n, minlength=n // G)
+    assert A.nnz / (G * union.sum()) > 0.63
+    assert np.percentile(union, 99.9) < 1.5 * np.median(union)
