@@ -747,9 +747,7 @@ slq_status spmm_rgt_inst(Launcher& L, const CUtensorMap* xmap, const int32_t* gp
     const double bytes = nnz * 8.0 + (nrows + 1) * 4.0 + double(xrows) * b * 4.0 +
                          double(nrows) * b * 4.0 * (Z ? 2.0 : 1.0);
     ProfScope prof(SLQ_K_SPMM, bytes, L.st);
-    constexpr int STAGE = RGT_ROWS * 128 * 4 + RGT_ROWS * G * 4;
-    constexpr size_t ring = static_cast<size_t>(RGT_WARPS) * RGT_STAGES * STAGE;
-    constexpr size_t smem = 1024 + (ring > RGT_WARPS * 256 * 8 ? ring : RGT_WARPS * 256 * 8);
+    constexpr size_t smem = RgtShape<G>::SMEM;
     static bool attr = false;
     if (!attr)
     {
@@ -758,10 +756,10 @@ slq_status spmm_rgt_inst(Launcher& L, const CUtensorMap* xmap, const int32_t* gp
         attr = true;
     }
     const int64_t ng = (nrows + G - 1) / G;
-    constexpr int GPC = RGT_WARPS / NS;
+    constexpr int GPC = RgtShape<G>::WARPS / NS;
     const int grid = static_cast<int>(
         std::max<int64_t>(1, std::min<int64_t>((ng + GPC - 1) / GPC, L.sms)));
-    k_spmm_rgt<G, NS><<<grid, RGT_WARPS * 32, smem, L.st>>>(
+    k_spmm_rgt<G, NS><<<grid, RgtShape<G>::WARPS * 32, smem, L.st>>>(
         *xmap, gptr, gcol, gval, nrows, ng, b, X, sx, shift, Y, Z, zc, zs, epi, partials, error);
     SLQ_LAUNCH_CK();
     ++L.launches;

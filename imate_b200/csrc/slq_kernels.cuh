@@ -1580,17 +1580,35 @@ k_spmm_rg(const int32_t* __restrict__ gptr, const int32_t* __restrict__ gcol,
 // Same row-group format as k_spmm_rg, but the union columns' X rows are
 // brought into shared memory by the copy engine (cp.async.bulk.tensor
 // tile::gather4: four rows of the [len][b] block per instruction) together
-// with the group's dense values (cp.async.bulk), three stages ahead per
+// with the group's dense values (cp.async.bulk), STAGES - 1 stages ahead per
 // warp.  Each warp owns its ring (no cross-warp waits); the FMAs read X from
 // shared memory, so the gather latency no longer stalls the warp.
 //
-// Lane l owns probes {c*128 + 4l .. c*128 + 4l + 3 : c < LV/4}, so every
-// shared-memory read of a stage row is a contiguous 512-byte span.
+// A warp's row groups (slice = warp % NS, groups gw, gw + gstride, ...: the
+// whole grid works through the groups in order, so the gather window stays
+// inside L2) form one stage stream: the stages of the next group are issued
+// while the current one is finished, and each group's offsets and first 32
+// column ids are loaded a group ahead, so no global-load latency sits between
+// stages.  FMAs are packed (fma.rn.f32x2: two rows of one probe), which
+// rounds exactly as the scalar FMA, so results are bit-identical to k_spmm.
+//
+// Lane l owns probes slice*128 + 4l .. 4l + 3, so every shared-memory read
+// of a stage row is a contiguous 512-byte span.
 // ===========================================================================
 
-constexpr int RGT_WARPS = 16;
-constexpr int RGT_STAGES = 3;
 constexpr int RGT_ROWS = 8;  // union columns per stage (two gather4)
+
+// warps and ring stages per CTA: 16-row groups hold 64 accumulators per
+// thread (12 warps, up to 168 registers), 8-row groups 32 (16 warps)
+template <int G>
+struct RgtShape {
+    static constexpr int WARPS = (G == 16) ? 12 : 16;
+    static constexpr int STAGES = (G == 16) ? 4 : 3;
+    static constexpr int STAGE = RGT_ROWS * 128 * 4 + RGT_ROWS * G * 4;
+    static constexpr size_t RING = static_cast<size_t>(WARPS) * STAGES * STAGE;
+    static constexpr size_t SMEM =
+        1024 + (RING > static_cast<size_t>(WARPS) * 256 * 8 ? RING : static_cast<size_t>(WARPS) * 256 * 8);
+};
 
 __device__ __forceinline__ void tma_gather4(void* dst, const CUtensorMap* map, int col,
                                             int r0, int r1, int r2, int r3, uint64_t* bar)
@@ -1604,10 +1622,9 @@ __device__ __forceinline__ void tma_gather4(void* dst, const CUtensorMap* map, i
 }
 
 // b = 128 * NS probes; NS warps share a row group, each owning a 128-probe
-// slice (lane l: probes slice*128 + 4l .. 4l+3); 16 warps per CTA.  The
-// tensor map's box is one row of 128 values.
+// slice.  The tensor map's box is one row of 128 values.
 template <int G, int NS>
-__global__ void __launch_bounds__(RGT_WARPS * 32, 1)
+__global__ void __launch_bounds__(RgtShape<G>::WARPS * 32, 1)
 k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__ gptr,
            const int32_t* __restrict__ gcol, const float* __restrict__ gval, int64_t nrows,
            int64_t ngroups, int b, const float* __restrict__ X, const double* __restrict__ sx,
@@ -1615,23 +1632,25 @@ k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__
            const double* __restrict__ zc, const double* __restrict__ zs, int epi,
            double* __restrict__ partials, int32_t* __restrict__ error)
 {
+    constexpr int WARPS = RgtShape<G>::WARPS;
+    constexpr int STAGES = RgtShape<G>::STAGES;
+    constexpr int STAGE = RgtShape<G>::STAGE;
     constexpr int LV = 4;
     constexpr int ROWB = 128 * 4;                    // bytes of one row slice
     constexpr int STAGE_X = RGT_ROWS * ROWB;
-    constexpr int STAGE_A = RGT_ROWS * G * 4;
-    constexpr int STAGE = STAGE_X + STAGE_A;
-    constexpr int GPC = RGT_WARPS / NS;              // groups in flight per CTA
+    constexpr int GPC = WARPS / NS;                  // groups in flight per CTA
+    static_assert(WARPS * STAGES * 8 <= 1024, "barrier area");
     extern __shared__ __align__(128) unsigned char smem_rgt[];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem_rgt);              // [warps][stages]
     unsigned char* ring0 = smem_rgt + 1024;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int slice = warp % NS;
-    unsigned char* ring = ring0 + static_cast<size_t>(warp) * RGT_STAGES * STAGE;
-    uint64_t* wbar = bars + warp * RGT_STAGES;
+    unsigned char* ring = ring0 + static_cast<size_t>(warp) * STAGES * STAGE;
+    uint64_t* wbar = bars + warp * STAGES;
 
     if (lane == 0)
-        for (int st = 0; st < RGT_STAGES; ++st) mbar_init(&wbar[st], 1);
+        for (int st = 0; st < STAGES; ++st) mbar_init(&wbar[st], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     __syncwarp();
 
@@ -1640,136 +1659,217 @@ k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__
 #pragma unroll
     for (int v = 0; v < LV; ++v) part[v] = 0.0;
 
-    uint32_t phases = 0;  // bit st = parity of stage st's next completion
-    bool ok = true;
-    const int dummy_flag = 0;
-    const int64_t gw = static_cast<int64_t>(blockIdx.x) * GPC + warp / NS;
+    // group sequence of this warp; groups i1 (offsets + first id chunk
+    // loaded), i2 (offsets loaded) and i3 come after the one being issued
     const int64_t gstride = static_cast<int64_t>(gridDim.x) * GPC;
-    for (int64_t g = gw; g < ngroups && ok; g += gstride)
+    int64_t snext = static_cast<int64_t>(blockIdx.x) * GPC + warp / NS;
+    auto fetch = [&]() {
+        const int64_t g = snext;
+        snext += gstride;
+        return g;
+    };
+    int64_t i1 = fetch(), i2 = fetch(), i3 = fetch();
+    int u1 = 0, e1 = 0, c1 = 0, u2 = 0, e2 = 0;
+    if (i1 < ngroups)
     {
-        const int u0 = gptr[g];
-        const int nu = gptr[g + 1] - u0;
-        const int nst = (nu + RGT_ROWS - 1) / RGT_ROWS;
-        // union column ids, 32 at a time, one per lane
-        int idx_cur = (lane < nu) ? gcol[u0 + lane] : 0;
-        const int last_col = (nu > 0) ? gcol[u0 + nu - 1] : 0;
-        auto issue = [&](int k) {
-            const int st = k % RGT_STAGES;
-            unsigned char* dst = ring + static_cast<size_t>(st) * STAGE;
-            const int e0 = k * RGT_ROWS;
-            const int cnt = min(RGT_ROWS, nu - e0);
-            int id[RGT_ROWS];
+        u1 = __ldg(gptr + i1);
+        e1 = __ldg(gptr + i1 + 1);
+        c1 = (u1 + lane < e1) ? __ldg(gcol + u1 + lane) : 0;
+    }
+    if (i2 < ngroups)
+    {
+        u2 = __ldg(gptr + i2);
+        e2 = __ldg(gptr + i2 + 1);
+    }
+
+    // producer cursor: group pg (-1: none left), next entry pe of [.., pend),
+    // ids of entries cb .. cb + 63 in cur / nxt (one per lane)
+    int64_t pg = -1;
+    int pe = 0, pend = 0, cb = 0, cur = 0, nxt = 0;
+    bool pfirst = true;
+    auto advance = [&]() {
+        pg = (i1 < ngroups) ? i1 : -1;
+        pe = u1;
+        pend = e1;
+        cb = u1;
+        cur = c1;
+        nxt = (pg >= 0 && u1 + 32 + lane < e1) ? __ldg(gcol + u1 + 32 + lane) : 0;
+        pfirst = true;
+        i1 = i2;
+        u1 = u2;
+        e1 = e2;
+        c1 = (i2 < ngroups && u2 + lane < e2) ? __ldg(gcol + u2 + lane) : 0;
+        i2 = i3;
+        if (i3 < ngroups)
+        {
+            u2 = __ldg(gptr + i3);
+            e2 = __ldg(gptr + i3 + 1);
+            i3 = fetch();
+        }
+    };
+    advance();
+
+    // stage metadata, oldest first: group (-1: none), cnt | first << 8 | last << 9
+    int64_t qg[STAGES];
+    int qf[STAGES];
+    auto issue = [&](int st, int64_t& og, int& of) {
+        if (pg < 0)
+        {
+            og = -1;
+            of = 0;
+            return;
+        }
+        const int cnt = min(RGT_ROWS, pend - pe);
+        unsigned char* dst = ring + static_cast<size_t>(st) * STAGE;
+        int id[RGT_ROWS];
 #pragma unroll
-            for (int i = 0; i < RGT_ROWS; ++i)
+        for (int i = 0; i < RGT_ROWS; ++i)
+        {
+            // entries past the group's end repeat its last one (copied, unused)
+            const int off = pe + min(i, max(cnt - 1, 0)) - cb;
+            id[i] = __shfl_sync(FULL_MASK, off < 32 ? cur : nxt, off & 31);
+        }
+        if (lane == 0)
+        {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (cnt > 0)
             {
-                const int e = e0 + i;
-                const int v = __shfl_sync(FULL_MASK, idx_cur, e & 31);
-                id[i] = (e < nu) ? v : last_col;
-            }
-            if (lane == 0)
-            {
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 mbar_expect_tx(&wbar[st], static_cast<uint32_t>(STAGE_X + cnt * G * 4));
                 tma_gather4(dst, &xmap, slice * 128, id[0], id[1], id[2], id[3], &wbar[st]);
                 tma_gather4(dst + 4 * ROWB, &xmap, slice * 128, id[4], id[5], id[6], id[7],
                             &wbar[st]);
-                bulk_copy_g2s(dst + STAGE_X, gval + static_cast<int64_t>(u0 + e0) * G,
+                bulk_copy_g2s(dst + STAGE_X, gval + static_cast<int64_t>(pe) * G,
                               static_cast<uint32_t>(cnt * G * 4), &wbar[st]);
             }
-        };
-        float acc[G][LV];
-#pragma unroll
-        for (int r = 0; r < G; ++r)
-#pragma unroll
-            for (int v = 0; v < LV; ++v) acc[r][v] = 0.0f;
-
-        const int pre = min(RGT_STAGES - 1, nst);
-        for (int k = 0; k < pre; ++k) issue(k);
-        for (int k = 0; k < nst; ++k)
-        {
-            const int kn = k + RGT_STAGES - 1;       // stage to issue now
-            if (kn < nst)
+            else
             {
-                if ((kn * RGT_ROWS) % 32 == 0 && kn > 0)
-                {
-                    // the entries of stage kn start a new 32-chunk
-                    const int nb = kn * RGT_ROWS + lane;
-                    idx_cur = (nb < nu) ? gcol[u0 + nb] : 0;
-                }
-                issue(kn);
+                mbar_expect_tx(&wbar[st], 0u);  // a group without entries
             }
-            const int st = k % RGT_STAGES;
-            if (!mbar_wait(&wbar[st], (phases >> st) & 1u, &dummy_flag))
-            {
-                ok = false;
-                if (lane == 0) atomicExch(error, 1);
-                break;
-            }
-            phases ^= (1u << st);
-            const unsigned char* src = ring + static_cast<size_t>(st) * STAGE;
-            const float* avals = reinterpret_cast<const float*>(src + STAGE_X);
-            const int cnt = min(RGT_ROWS, nu - k * RGT_ROWS);
-            for (int c = 0; c < cnt; ++c)
-            {
-                const float4 xv = *reinterpret_cast<const float4*>(src + c * ROWB + lane * 16);
-                const float x[4] = {xv.x, xv.y, xv.z, xv.w};
-                float a[G];
-#pragma unroll
-                for (int q = 0; q < G; q += 4)
-                {
-                    const float4 t = *reinterpret_cast<const float4*>(avals + c * G + q);
-                    a[q + 0] = t.x;
-                    a[q + 1] = t.y;
-                    a[q + 2] = t.z;
-                    a[q + 3] = t.w;
-                }
-#pragma unroll
-                for (int r = 0; r < G; ++r)
-#pragma unroll
-                    for (int v = 0; v < LV; ++v) acc[r][v] += a[r] * x[v];
-            }
-            __syncwarp();
         }
-        if (!ok)
+        const bool last = (pe + cnt == pend);
+        og = pg;
+        of = cnt | (pfirst ? 256 : 0) | (last ? 512 : 0);
+        pfirst = false;
+        pe += cnt;
+        if (pe - cb >= 32)
         {
-            // let this warp's copies in flight land before leaving
-            for (int st = 0; st < RGT_STAGES; ++st)
-                mbar_wait(&wbar[st], (phases >> st) & 1u, &dummy_flag);
+            cb += 32;
+            cur = nxt;
+            nxt = (cb + 32 + lane < pend) ? __ldg(gcol + cb + 32 + lane) : 0;
+        }
+        if (last) advance();
+    };
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) issue(s, qg[s], qf[s]);
+
+    float2 acc[G / 2][LV];  // (row 2q, row 2q + 1) of probe v
+    uint32_t phases = 0;    // bit st = parity of stage st's next completion
+    bool ok = true;
+    const int dummy_flag = 0;
+    int st = 0;             // slot of the stage consumed now
+    for (;;)
+    {
+        {
+            int nst = st + STAGES - 1;
+            if (nst >= STAGES) nst -= STAGES;
+            issue(nst, qg[STAGES - 1], qf[STAGES - 1]);
+        }
+        if (qg[0] < 0) break;
+        if (!mbar_wait(&wbar[st], (phases >> st) & 1u, &dummy_flag))
+        {
+            ok = false;
+            if (lane == 0) atomicExch(error, 1);
             break;
         }
-        double sxr[LV], zcr[LV];
-#pragma unroll
-        for (int v = 0; v < LV; ++v)
+        phases ^= (1u << st);
+        const int cnt = qf[0] & 255;
+        if (qf[0] & 256)
         {
-            sxr[v] = sx ? sx[pbase + v] : 1.0;
-            zcr[v] = Z ? zc[pbase + v] * zs[pbase + v] : 0.0;
+#pragma unroll
+            for (int q = 0; q < G / 2; ++q)
+#pragma unroll
+                for (int v = 0; v < LV; ++v) acc[q][v] = make_float2(0.0f, 0.0f);
         }
-#pragma unroll
-        for (int r = 0; r < G; ++r)
+        const unsigned char* src = ring + static_cast<size_t>(st) * STAGE;
+        const float* avals = reinterpret_cast<const float*>(src + STAGE_X);
+        for (int c = 0; c < cnt; ++c)
         {
-            const int64_t row = g * G + r;
-            if (row >= nrows) continue;
-            const int64_t o = row * b + pbase;
-            float4 xr = make_float4(0.f, 0.f, 0.f, 0.f), zr = xr;
-            if (shift != 0.0 || epi == 1) xr = __ldg(reinterpret_cast<const float4*>(X + o));
-            if (Z) zr = __ldg(reinterpret_cast<const float4*>(Z + o));
-            const float xs[4] = {xr.x, xr.y, xr.z, xr.w};
-            const float zsv[4] = {zr.x, zr.y, zr.z, zr.w};
-            float yr[4];
+            const float4 xv = *reinterpret_cast<const float4*>(src + c * ROWB + lane * 16);
+            const float x[4] = {xv.x, xv.y, xv.z, xv.w};
+            float2 a2[G / 2];
+#pragma unroll
+            for (int q = 0; q < G; q += 4)
+            {
+                const float4 t = *reinterpret_cast<const float4*>(avals + c * G + q);
+                a2[q / 2] = make_float2(t.x, t.y);
+                a2[q / 2 + 1] = make_float2(t.z, t.w);
+            }
 #pragma unroll
             for (int v = 0; v < LV; ++v)
             {
-                double y = static_cast<double>(acc[r][v]) * sxr[v];
-                if (shift != 0.0) y += shift * (sxr[v] * static_cast<double>(xs[v]));
-                if (Z) y -= zcr[v] * static_cast<double>(zsv[v]);
-                yr[v] = static_cast<float>(y);
-                const double ys = static_cast<double>(yr[v]);
-                if (epi == 1) part[v] += (sxr[v] * static_cast<double>(xs[v])) * ys;
-                else if (epi == 2) part[v] += ys * ys;
-                else if (epi == 3)
-                    part[v] += (zs[pbase + v] * static_cast<double>(zsv[v])) * ys;
+                const float2 xx = make_float2(x[v], x[v]);
+#pragma unroll
+                for (int q = 0; q < G / 2; ++q) acc[q][v] = __ffma2_rn(a2[q], xx, acc[q][v]);
             }
-            *reinterpret_cast<float4*>(Y + o) = make_float4(yr[0], yr[1], yr[2], yr[3]);
+        }
+        __syncwarp();
+        if (qf[0] & 512)
+        {
+            const int64_t g = qg[0];
+            double sxr[LV], zcr[LV];
+#pragma unroll
+            for (int v = 0; v < LV; ++v)
+            {
+                sxr[v] = sx ? sx[pbase + v] : 1.0;
+                zcr[v] = Z ? zc[pbase + v] * zs[pbase + v] : 0.0;
+            }
+#pragma unroll
+            for (int r = 0; r < G; ++r)
+            {
+                const int64_t row = g * G + r;
+                if (row >= nrows) continue;
+                const int64_t o = row * b + pbase;
+                float4 xr = make_float4(0.f, 0.f, 0.f, 0.f), zr = xr;
+                if (shift != 0.0 || epi == 1) xr = __ldg(reinterpret_cast<const float4*>(X + o));
+                if (Z) zr = __ldg(reinterpret_cast<const float4*>(Z + o));
+                const float xs[4] = {xr.x, xr.y, xr.z, xr.w};
+                const float zsv[4] = {zr.x, zr.y, zr.z, zr.w};
+                float yr[4];
+#pragma unroll
+                for (int v = 0; v < LV; ++v)
+                {
+                    const float av = (r & 1) ? acc[r / 2][v].y : acc[r / 2][v].x;
+                    double y = static_cast<double>(av) * sxr[v];
+                    if (shift != 0.0) y += shift * (sxr[v] * static_cast<double>(xs[v]));
+                    if (Z) y -= zcr[v] * static_cast<double>(zsv[v]);
+                    yr[v] = static_cast<float>(y);
+                    const double ys = static_cast<double>(yr[v]);
+                    if (epi == 1) part[v] += (sxr[v] * static_cast<double>(xs[v])) * ys;
+                    else if (epi == 2) part[v] += ys * ys;
+                    else if (epi == 3)
+                        part[v] += (zs[pbase + v] * static_cast<double>(zsv[v])) * ys;
+                }
+                *reinterpret_cast<float4*>(Y + o) = make_float4(yr[0], yr[1], yr[2], yr[3]);
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < STAGES - 1; ++s)
+        {
+            qg[s] = qg[s + 1];
+            qf[s] = qf[s + 1];
+        }
+        if (++st == STAGES) st = 0;
+    }
+    if (!ok)
+    {
+        // let this warp's copies in flight land before leaving
+        int s2 = st;
+#pragma unroll
+        for (int s = 0; s < STAGES; ++s)
+        {
+            if (qg[s] >= 0) mbar_wait(&wbar[s2], (phases >> s2) & 1u, &dummy_flag);
+            if (++s2 == STAGES) s2 = 0;
         }
     }
 
@@ -1778,7 +1878,7 @@ k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__
     // memory can hold the CTA reduction: red[warp][256]
     __syncthreads();
     double* red = reinterpret_cast<double*>(ring0);
-    for (int i = threadIdx.x; i < RGT_WARPS * 256; i += blockDim.x) red[i] = 0.0;
+    for (int i = threadIdx.x; i < WARPS * 256; i += blockDim.x) red[i] = 0.0;
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < LV; ++v) red[warp * 256 + pbase + v] = part[v];
@@ -1786,7 +1886,7 @@ k_spmm_rgt(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__
     for (int p = threadIdx.x; p < b; p += blockDim.x)
     {
         double sum = 0.0;
-        for (int w = 0; w < RGT_WARPS; ++w) sum += red[w * 256 + p];
+        for (int w = 0; w < WARPS; ++w) sum += red[w * 256 + p];
         partials[static_cast<int64_t>(blockIdx.x) * b + p] = sum;
     }
 }
