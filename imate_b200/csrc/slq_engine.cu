@@ -655,11 +655,41 @@ slq_status spmm_inst(Launcher& L, int grid, const int32_t* ptr, const int32_t* i
     return SLQ_OK;
 }
 
-template <typename VT>
-int spmm_grid(const Launcher& L, int64_t nrows)
+// blocks of k_spmm<VT, LV, KS> resident per SM (occupancy query, at most 4)
+template <typename VT, int LV, int KS>
+int spmm_blocks_per_sm(int b)
 {
+    static int cached = 0;
+    if (cached == 0)
+    {
+        int v = 0;
+        const size_t smem = 8 * static_cast<size_t>(b) * sizeof(double);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_spmm<VT, LV, KS>, 256, smem) !=
+                cudaSuccess ||
+            v < 1)
+            v = 1;
+        cached = std::min(v, 4);
+    }
+    return cached;
+}
+
+// persistent grid of the CSR kernel: as many blocks as are resident on the
+// SMs at once (a partial second wave would leave SMs idle at the end)
+template <typename VT>
+int spmm_grid(const Launcher& L, int64_t nrows, int b)
+{
+    int per_sm = 4;
+    switch (b)
+    {
+        case 64: per_sm = spmm_blocks_per_sm<VT, 2, 1>(b); break;
+        case 128: per_sm = spmm_blocks_per_sm<VT, 4, 1>(b); break;
+        case 256: per_sm = spmm_blocks_per_sm<VT, 8, 1>(b); break;
+        case 512: per_sm = spmm_blocks_per_sm<VT, 16, 1>(b); break;
+        case 1024: per_sm = spmm_blocks_per_sm<VT, 32, 1>(b); break;
+        default: break;
+    }
     const int64_t g = (nrows + 7) / 8;
-    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(g, int64_t(L.sms) * 4)));
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(g, int64_t(L.sms) * per_sm)));
 }
 
 template <typename VT>
@@ -946,7 +976,7 @@ slq_status spmm_cand(Launcher& L, const slq_op* op, int transpose, const SpmmCan
     const int32_t* ptr = transpose ? op->t_ptr : op->a_ptr;
     const int32_t* ind = transpose ? op->t_ind : op->a_ind;
     const VT* val = static_cast<const VT*>(transpose ? op->t_data : op->a_data);
-    const int grid = spmm_grid<VT>(L, rows);
+    const int grid = spmm_grid<VT>(L, rows, b);
     *grid_out = grid;
     return spmm<VT>(L, grid, ptr, ind, val, rows, b, X, sx, shift, Y, Z, zc, zs, epi, partials,
                     op->nnz, xrows);

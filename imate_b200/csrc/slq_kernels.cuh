@@ -158,8 +158,15 @@ __device__ __forceinline__ int ring_slot(int vec, int bs)
 // the Krylov vector is Z and X is the intermediate A v)
 // ---------------------------------------------------------------------------
 
+// resident 256-thread blocks per SM the FP32 CSR kernel is compiled for:
+// more warps keep more row gathers in flight (short rows issue few per warp)
+template <typename VT, int LV>
+struct SpmmOcc {
+    static constexpr int MINB = (sizeof(VT) != 4) ? 1 : (LV <= 4) ? 4 : (LV == 8 ? 3 : 1);
+};
+
 template <typename VT, int LV, int KS>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, SpmmOcc<VT, LV>::MINB)
 k_spmm(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
        const VT* __restrict__ vals, int64_t nrows, int b,
        const VT* __restrict__ X, const double* __restrict__ sx, double shift,
@@ -176,14 +183,9 @@ k_spmm(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const int ks = lane / P;
     const int p0 = pl * LV;
 
-    double sxr[LV], zcr[LV], part[LV];
+    double part[LV];
 #pragma unroll
-    for (int v = 0; v < LV; ++v)
-    {
-        sxr[v] = sx ? sx[p0 + v] : 1.0;
-        zcr[v] = Z ? zc[p0 + v] * zs[p0 + v] : 0.0;
-        part[v] = 0.0;
-    }
+    for (int v = 0; v < LV; ++v) part[v] = 0.0;
 
     const int64_t gw = static_cast<int64_t>(blockIdx.x) * nwarps + warp;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * nwarps;
@@ -258,14 +260,16 @@ k_spmm(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
 #pragma unroll
             for (int v = 0; v < LV; ++v)
             {
-                double y = static_cast<double>(acc[v]) * sxr[v];
+                // per-probe scales from L1 (not held in registers)
+                const double sxv = sx ? __ldg(sx + p0 + v) : 1.0;
+                double y = static_cast<double>(acc[v]) * sxv;
                 if (shift != 0.0)
-                    y += shift * (sxr[v] * static_cast<double>(xr[v]));
-                if (Z) y -= zcr[v] * static_cast<double>(zr[v]);
+                    y += shift * (sxv * static_cast<double>(xr[v]));
+                if (Z) y -= (__ldg(zc + p0 + v) * __ldg(zs + p0 + v)) * static_cast<double>(zr[v]);
                 yr[v] = static_cast<VT>(y);
                 const double ys = static_cast<double>(yr[v]);
                 if (epi == 1)
-                    part[v] += (sxr[v] * static_cast<double>(xr[v])) * ys;
+                    part[v] += (sxv * static_cast<double>(xr[v])) * ys;
                 else if (epi == 2)
                     part[v] += ys * ys;
                 else if (epi == 3)
