@@ -232,17 +232,38 @@ class _DeviceOperator:
                  max(A.shape) <= np.iinfo(np.int32).max and
                  A.nnz <= np.iinfo(np.int32).max)
         pattern = None
+        upload = None
         if early:
-            # canonical CSR goes to the device as it is: upload first, so
-            # that the locality order is computed there
+            # canonical CSR goes to the device as it is: upload the pattern
+            # first, so that the locality order is computed there, and the
+            # values on a helper thread while the host aggregates (both
+            # release the GIL)
             self.indices = torch.from_numpy(
                 np.ascontiguousarray(A.indices, dtype=np.int32)).to(dev)
             self.indptr = torch.from_numpy(
                 np.ascontiguousarray(A.indptr, dtype=np.int32)).to(dev)
             pattern = (self.indptr, self.indices)
-        base = locality_order(A, reorder, device_pattern=pattern)
-        self.group_rows, perm = group_rows_for(A, base, group_rows,
-                                               aggregate=aggregate)
+            if A.dtype in (np.float32, np.float64):
+                import threading
+                box = {}
+
+                def _values():
+                    try:
+                        box["data"] = torch.from_numpy(
+                            np.ascontiguousarray(A.data)).to(dev)
+                    except BaseException as exc:  # re-raised on join
+                        box["error"] = exc
+                upload = (threading.Thread(target=_values, daemon=True), box)
+                upload[0].start()
+        try:
+            base = locality_order(A, reorder, device_pattern=pattern)
+            self.group_rows, perm = group_rows_for(A, base, group_rows,
+                                                   aggregate=aggregate)
+        finally:
+            if upload is not None:
+                upload[0].join()
+        if upload is not None and "error" in upload[1]:
+            raise upload[1]["error"]
         if perm is not None and A.format != "csr":
             A = A.tocsr()
         fmt = _lib.SLQ_CSC if A.format == "csc" else _lib.SLQ_CSR
@@ -260,7 +281,10 @@ class _DeviceOperator:
         if max(A.shape) > np.iinfo(np.int32).max or \
                 self.nnz > np.iinfo(np.int32).max:
             raise ValueError("matrix too large for 32-bit indices")
-        self.data = torch.from_numpy(np.ascontiguousarray(A.data)).to(dev)
+        if upload is not None and "data" in upload[1] and A.format == "csr":
+            self.data = upload[1]["data"]
+        else:
+            self.data = torch.from_numpy(np.ascontiguousarray(A.data)).to(dev)
         if not early:
             self.indices = torch.from_numpy(
                 np.ascontiguousarray(A.indices, dtype=np.int32)).to(dev)
