@@ -178,7 +178,46 @@ def run_reference_arm(args):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    gpu_ref = reference_gpu_sample(A, args)
+    if gpu_ref is not None:
+        line["reference_gpu"] = gpu_ref
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_sample(A, args, probes=8):
+    """The reference's own GPU SLQ (cuSPARSE SpMV, cuBLAS vector operations,
+    one probe at a time; oracle/_ref/libimate_ref_gpu.so compiled from its
+    sources for sm_100a) on a sample of the same workload, FP32 and FP64:
+    probe*steps/s over its own computation time, and over the whole call
+    (matrix upload included).  None without a GPU or the library."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+        from oracle import ref
+        if not ref.gpu_available():
+            return None
+    except ImportError:
+        return None
+    out = {}
+    for name, dt in (("f32", np.float32), ("f64", np.float64)):
+        Ad = A.astype(dt)
+        kw = dict(min_num_samples=probes, max_num_samples=probes,
+                  error_rtol=0.0, lanczos_degree=args.degree,
+                  orthogonalize=args.orthogonalize, seed=0)
+        ref.gpu_trace_estimator(Ad, "log", **dict(kw, min_num_samples=1,
+                                                  max_num_samples=1))
+        t0 = time.perf_counter()
+        r = ref.gpu_trace_estimator(Ad, "log", **kw)
+        wall = time.perf_counter() - t0
+        ps = probes * args.degree
+        out[name] = {"value": ps / max(r["alg_wall_time"], 1e-9),
+                     "unit": UNIT, "e2e": ps / wall, "probes": probes,
+                     "alg_wall_s": r["alg_wall_time"], "wall_s": wall,
+                     "estimate": float(r["trace"][0])}
+    out["path"] = ("imate cu_trace_estimator (cuSPARSE SpMV, cuBLAS), built "
+                   "from the reference sources for sm_100a, 1 GPU")
+    return out
 
 
 # ---------------------------------------------------------------------------

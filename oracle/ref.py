@@ -7,6 +7,13 @@ thin entry layer ``oracle/ref_harness.cpp``.  It is the checker for the CUDA
 path and the CPU baseline that ``bench.py --impl reference`` times; the
 product never imports this module.
 
+``libimate_ref_gpu.so`` is the reference's GPU SLQ
+(``imate/_cu_trace_estimator/cu_trace_estimator.cu:197-315`` over
+``cuCSRMatrix``: cuSPARSE SpMV and cuBLAS vector operations), compiled from
+its sources for sm_100a by the same Makefile (target ``ref_gpu``): a second
+checker for the tests and the reference GPU comparator of bench.py's
+reference arm.
+
 LAPACK is bound the way the reference binds it
 (``imate/_c_trace_estimator/lapack_api.pxi:14``): through
 ``scipy.linalg.cython_lapack``'s exported function pointers.
@@ -19,8 +26,10 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(_HERE, "_ref", "libimate_ref.so")
+REF_GPU_SO = os.path.join(_HERE, "_ref", "libimate_ref_gpu.so")
 
 _lib = None
+_gpu_lib = None
 
 
 def _capsule_pointer(capsule):
@@ -37,6 +46,17 @@ def available():
     return os.path.exists(REF_SO)
 
 
+def _bind_lapack(lib):
+    from scipy.linalg import cython_lapack
+    capi = cython_lapack.__pyx_capi__
+    ptrs = [_capsule_pointer(capi[k])
+            for k in ("dstev", "sstev", "dbdsdc", "sbdsdc")]
+    lib.ref_set_lapack.restype = ctypes.c_int
+    lib.ref_set_lapack.argtypes = [ctypes.c_void_p] * 4
+    if lib.ref_set_lapack(*ptrs) != 0:
+        raise RuntimeError("could not bind LAPACK for the reference library")
+
+
 def load():
     """Load the reference library (raises if it was not built)."""
     global _lib
@@ -47,16 +67,80 @@ def load():
             "reference CPU library not built: run `make -C oracle ref` "
             "where the reference sources are present")
     lib = ctypes.CDLL(REF_SO)
-    from scipy.linalg import cython_lapack
-    capi = cython_lapack.__pyx_capi__
-    ptrs = [_capsule_pointer(capi[k])
-            for k in ("dstev", "sstev", "dbdsdc", "sbdsdc")]
-    lib.ref_set_lapack.restype = ctypes.c_int
-    lib.ref_set_lapack.argtypes = [ctypes.c_void_p] * 4
-    if lib.ref_set_lapack(*ptrs) != 0:
-        raise RuntimeError("could not bind LAPACK for the reference library")
+    _bind_lapack(lib)
     _lib = lib
     return lib
+
+
+def gpu_available():
+    return os.path.exists(REF_GPU_SO)
+
+
+def load_gpu():
+    """Load the reference GPU library (``libimate_ref_gpu.so``: the
+    reference's cuSPARSE/cuBLAS SLQ, ``cu_trace_estimator.cu:197-315``);
+    raises if it was not built."""
+    global _gpu_lib
+    if _gpu_lib is not None:
+        return _gpu_lib
+    if not gpu_available():
+        raise FileNotFoundError(
+            "reference GPU library not built: run `make -C oracle ref_gpu` "
+            "where the reference sources are present")
+    lib = ctypes.CDLL(REF_GPU_SO)
+    _bind_lapack(lib)
+    _gpu_lib = lib
+    return lib
+
+
+def gpu_trace_estimator(A, func, gram=False, exponent=1.0, min_num_samples=10,
+                        max_num_samples=50, error_atol=0.0, error_rtol=1e-2,
+                        confidence_level=0.95,
+                        outlier_significance_level=0.001, lanczos_degree=20,
+                        lanczos_tol=None, orthogonalize=0, seed=0,
+                        num_gpu_devices=1):
+    """Run the reference GPU estimator on a CSR matrix (one inquiry; ``func``
+    in {'log', 'inv', 'id'}).  Returns the same dict as
+    ``trace_estimator``."""
+    import scipy.sparse as sp
+    lib = load_gpu()
+    A = sp.csr_matrix(A)
+    A.sort_indices()
+    indices = np.ascontiguousarray(A.indices, dtype=np.int32)
+    indptr = np.ascontiguousarray(A.indptr, dtype=np.int32)
+    dt = np.float64 if A.dtype == np.float64 else np.float32
+    data = np.ascontiguousarray(A.data, dtype=dt)
+    if lanczos_tol is None:
+        lanczos_tol = float(np.finfo(dt).eps)
+    trace = np.empty(1, dt)
+    error = np.empty(1, dt)
+    samples = np.empty(max_num_samples, dt)
+    order = np.zeros(max_num_samples, np.int32)
+    used = np.zeros(1, np.int32)
+    outl = np.zeros(1, np.int32)
+    conv = np.zeros(1, np.int32)
+    wall = ctypes.c_float(0.0)
+    fid = {"log": 0, "inv": 1, "id": 2}[func]
+    if dt == np.float64:
+        fn, real = lib.ref_gpu_trace_estimator_f64, ctypes.c_double
+    else:
+        fn, real = lib.ref_gpu_trace_estimator_f32, ctypes.c_float
+    fn.restype = ctypes.c_int
+    vp, i32, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64
+    fn.argtypes = [vp, vp, vp, i64, i64, i32, i32, real, i32, i64, i32, real,
+                   i32, i32, real, real, real, real, i32, vp, vp, vp, vp, vp,
+                   vp, vp, ctypes.POINTER(ctypes.c_float)]
+    allc = fn(_p(data), _p(indices), _p(indptr), A.shape[0], A.shape[1], fid,
+              int(gram), exponent, orthogonalize, seed, lanczos_degree,
+              lanczos_tol, min_num_samples, max_num_samples, error_atol,
+              error_rtol, confidence_level, outlier_significance_level,
+              num_gpu_devices, _p(trace), _p(error), _p(samples), _p(order),
+              _p(used), _p(outl), _p(conv), ctypes.byref(wall))
+    return dict(all_converged=bool(allc), trace=trace, error=error,
+                samples=samples.reshape(-1, 1),
+                processed_samples_indices=order, num_samples_used=used,
+                num_outliers=outl, converged=conv,
+                alg_wall_time=float(wall.value))
 
 
 def _p(a):
