@@ -306,8 +306,10 @@ def prepare(A, parameters, func, gram, exponent, min_num_samples,
         t_values = np.zeros(1)
 
     # gram with several shifts: the shift relation does not hold for
-    # (A + tI)^T (A + tI), so each t gets its own Krylov runs
-    if gram and affine and num_inquiries > 1:
+    # (A + tI)^T (A + tI), so each t gets its own Krylov runs; nor for
+    # A + t B with B other than I, where each t also gets its own operator
+    general_b = bool(getattr(Aop, "general_B", False))
+    if general_b or (gram and affine and num_inquiries > 1):
         groups = [[j] for j in range(num_inquiries)]
     else:
         groups = [list(range(num_inquiries))]
@@ -317,7 +319,11 @@ def prepare(A, parameters, func, gram, exponent, min_num_samples,
     if func_coeff is not None:
         coeff[:len(func_coeff)] = [float(c) for c in func_coeff]
     J.Aop = Aop
-    J.dev_op = Aop.get_device_operator(need_transpose=bool(gram) or normal)
+    J.per_group_t = t_values if general_b else None
+    J.need_transpose = bool(gram) or normal
+    J.dev_op = (Aop.device_operator_for(t_values[0], J.need_transpose)
+                if general_b else
+                Aop.get_device_operator(need_transpose=J.need_transpose))
     gram_mode = 2 if normal else int(bool(gram))
     J.groups = groups
     J.params = []
@@ -335,7 +341,9 @@ def prepare(A, parameters, func, gram, exponent, min_num_samples,
             block_size=options.block_size, rng=_lib.RNG_IDS[options.rng],
             first_probe=options.first_probe,
             func_coeff=(ctypes.c_double * 4)(*coeff)))
-        J.t_groups.append(np.ascontiguousarray(t_values[group],
+        # a per-t operator holds A + t B itself: no shift on top
+        J.t_groups.append(np.zeros(len(group)) if general_b else
+                          np.ascontiguousarray(t_values[group],
                                                dtype=np.float64))
     J.options = options
     J.dtype_str = dtype_str
@@ -443,6 +451,11 @@ def run_job(J):
     stream = torch.cuda.current_stream(dev_op.device)
     for gi, prm in enumerate(J.params):
         gq = len(J.groups[gi])
+        if J.per_group_t is not None and gi > 0:
+            J.dev_op = None
+            J.dev_op = J.Aop.device_operator_for(
+                J.per_group_t[J.groups[gi][0]], J.need_transpose)
+            dev_op = J.dev_op
         ws_bytes = ctypes.c_size_t(0)
         _lib.check(lib.slq_run_workspace_bytes(dev_op.handle,
                                                ctypes.byref(prm), gq,

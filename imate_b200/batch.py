@@ -142,6 +142,11 @@ class BatchPlan:
                         kw["orthogonalize"], kw["seed"], kw["num_threads"],
                         kw["num_gpu_devices"], kw["verbose"], kw["plot"],
                         kw["gpu"], engine, coeff)
+            if J.per_group_t is not None:
+                raise NotImplementedError(
+                    "batch plans record one device operator per estimate; "
+                    "A + t B with B other than the identity needs one per t "
+                    "(call logdet / traceinv / trace for it)")
             if autotune:
                 key = (id(J.dev_op), J.params[0].gram, J.max_num_samples)
                 if key not in tuned:

@@ -302,9 +302,11 @@ class _DeviceOperator:
     @classmethod
     def from_device(cls, indptr, indices, data, shape, affine=False,
                     need_transpose=False, group_rows=8, fmt=_lib.SLQ_CSR,
-                    check_indices=True):
+                    check_indices=True, perm=None):
         """Operator over CSR (or CSC) arrays already on the device (torch
-        int32 indptr / indices, float32 or float64 data), without copies."""
+        int32 indptr / indices, float32 or float64 data), without copies.
+        ``perm`` (a host int32 row order of a square CSR matrix, as
+        ``locality_order`` / ``group_rows_for`` give) stores it reordered."""
         import torch
         self = cls(None, affine, need_transpose)
         self.data = data.contiguous()
@@ -322,6 +324,12 @@ class _DeviceOperator:
         self.group_rows = int(group_rows)
         self.perm = None
         self.inv = None
+        if perm is not None:
+            pm = torch.from_numpy(np.ascontiguousarray(perm, dtype=np.int32))
+            self.perm = pm.to(self.device)
+            self.inv = torch.empty_like(self.perm)
+            self.inv[self.perm.long()] = torch.arange(
+                pm.numel(), dtype=torch.int32, device=self.device)
         self._create(fmt, affine, need_transpose, check_indices)
         return self
 
@@ -487,12 +495,17 @@ def _is_identity(B, n):
 
 
 class AffineMatrixFunction(LinearOperator):
-    """A + t B with B = I (``imate/linear_operator/affine_matrix_function.py``).
+    """A + t B (``imate/linear_operator/affine_matrix_function.py:278-360``).
 
     With B the identity the eigenvalues of A + t I are those of A shifted by
     t, so one Krylov run per probe serves every t
-    (``imate/_c_linear_operator/c_affine_matrix_function.cpp:98-113``).  A
-    general B is not served by this engine.
+    (``imate/_c_linear_operator/c_affine_matrix_function.cpp:98-113``).  With
+    another B no such relation holds and the reference runs a Krylov sequence
+    per inquiry on each probe (``imate/_c_trace_estimator/c_trace_estimator.cpp:
+    496-556``, ``cu_csr_affine_matrix_function.cu:124-211``); here each t
+    gets its own device operator over the union pattern of A and B with the
+    values of A + t B (written on the device), in the row order and
+    row-group width chosen once for that pattern.
     """
 
     def __init__(self, A, B=None, reorder="auto", group_rows="auto"):
@@ -503,13 +516,83 @@ class AffineMatrixFunction(LinearOperator):
         self.B = B
         self.num_parameters = 1
         self.set_data_type_name(A)
-        if not _is_identity(B, A.shape[0]):
-            raise NotImplementedError(
-                "AffineMatrixFunction with B other than the identity is not "
-                "served by the B200 SLQ engine")
+        self.general_B = not _is_identity(B, A.shape[0])
+        if self.general_B:
+            if np.isscalar(B) or not (sp.issparse(B) or
+                                      isinstance(B, np.ndarray)):
+                raise TypeError("B should be a numpy array or a scipy sparse "
+                                "matrix.")
+            if B.shape != A.shape:
+                raise ValueError("A and B should have the same shape.")
+            self._union = None
+            self._op_t = None
 
     def _affine(self):
-        return True
+        return not self.general_B
+
+    def _union_pattern(self):
+        """Host CSR pattern of A ∪ B and A's and B's values on it, with the
+        row order and row-group width of that pattern (computed once)."""
+        if self._union is not None:
+            return self._union
+        dt = np.dtype(self.get_data_type_name().decode())
+        Ac = sp.coo_matrix(self.A)
+        Bc = sp.coo_matrix(self.B)
+        n, m = self.A.shape
+        key = np.concatenate([Ac.row.astype(np.int64) * m + Ac.col,
+                              Bc.row.astype(np.int64) * m + Bc.col])
+        uk, where = np.unique(key, return_inverse=True)
+        a = np.zeros(uk.size, dtype=np.float64)
+        b = np.zeros(uk.size, dtype=np.float64)
+        np.add.at(a, where[:Ac.nnz], Ac.data)
+        np.add.at(b, where[Ac.nnz:], Bc.data)
+        rows = uk // m
+        indptr = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum(np.bincount(rows, minlength=n), out=indptr[1:])
+        if max(n, m) > np.iinfo(np.int32).max or \
+                uk.size > np.iinfo(np.int32).max:
+            raise ValueError("matrix too large for 32-bit indices")
+        P = sp.csr_matrix((np.abs(a) + np.abs(b), (uk % m).astype(np.int32),
+                           indptr.astype(np.int32)), shape=(n, m))
+        base = locality_order(P, self.reorder)
+        G, perm = group_rows_for(P, base, self.group_rows)
+        self._union = dict(indptr=P.indptr, indices=P.indices,
+                           a=a.astype(dt), b=b.astype(dt), G=int(G),
+                           perm=perm, shape=(n, m), device=None)
+        return self._union
+
+    def device_operator_for(self, t, need_transpose=False):
+        """The device operator of A + t B (general B; the previous one is
+        released first)."""
+        import torch
+        U = self._union_pattern()
+        dev = torch.device("cuda", torch.cuda.current_device())
+        if U["device"] is None or U["device"][0] != dev:
+            U["device"] = (dev,
+                           torch.from_numpy(U["indptr"]).to(dev),
+                           torch.from_numpy(U["indices"]).to(dev),
+                           torch.from_numpy(U["a"]).to(dev),
+                           torch.from_numpy(U["b"]).to(dev))
+        _, ip, ind, a, b = U["device"]
+        self._op_t = None
+        vals = torch.add(a, b, alpha=float(t))
+        self._op_t = _DeviceOperator.from_device(
+            ip, ind, vals, U["shape"], affine=False,
+            need_transpose=need_transpose, group_rows=U["G"],
+            perm=U["perm"])
+        return self._op_t
+
+    def get_device_operator(self, need_transpose=False):
+        if not self.general_B:
+            return super().get_device_operator(need_transpose)
+        return self.device_operator_for(0.0, need_transpose)
+
+    def release(self):
+        super().release()
+        if self.general_B:
+            self._op_t = None
+            if self._union is not None:
+                self._union["device"] = None
 
 
 class DeviceMatrix(LinearOperator):

@@ -217,6 +217,61 @@ def trace_estimator(A, func, gram=False, exponent=1.0, parameters=None,
                 alg_wall_time=float(wall.value))
 
 
+def trace_estimator_b(A, B, func, parameters, gram=False, exponent=1.0,
+                      min_num_samples=10, max_num_samples=50, error_atol=0.0,
+                      error_rtol=1e-2, confidence_level=0.95,
+                      outlier_significance_level=0.001, lanczos_degree=20,
+                      lanczos_tol=None, orthogonalize=0, seed=0,
+                      num_threads=1, coeff=None):
+    """The reference estimator on A + t B for a general (CSR) B, FP64:
+    ``imate.AffineMatrixFunction(A, B)``.  Returns the dict of
+    ``trace_estimator``."""
+    import scipy.sparse as sp
+    lib = load()
+    A = sp.csr_matrix(A, dtype=np.float64)
+    A.sort_indices()
+    B = sp.csr_matrix(B, dtype=np.float64)
+    B.sort_indices()
+    params = np.ascontiguousarray(np.atleast_1d(parameters), dtype=np.float64)
+    q = params.size
+    if lanczos_tol is None:
+        lanczos_tol = float(np.finfo(np.float64).eps)
+    arrays = [np.ascontiguousarray(x) for x in (
+        A.data, A.indices.astype(np.int32), A.indptr.astype(np.int32),
+        B.data, B.indices.astype(np.int32), B.indptr.astype(np.int32))]
+    trace = np.empty(q)
+    error = np.empty(q)
+    samples = np.empty((max_num_samples, q))
+    order = np.zeros(max_num_samples, np.int32)
+    used = np.zeros(q, np.int32)
+    outl = np.zeros(q, np.int32)
+    conv = np.zeros(q, np.int32)
+    wall = ctypes.c_float(0.0)
+    fid = {"log": 0, "inv": 1, "id": 2, "exp": 3, "linfrac": 4,
+           "indicator": 5, "gaussian": 6, "smoothstep": 7}[func]
+    fc = np.zeros(4)
+    if coeff is not None:
+        fc[:len(coeff)] = coeff
+    fn = lib.ref_trace_estimator_b_f64
+    fn.restype = ctypes.c_int
+    vp, i32, i64, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, \
+        ctypes.c_double
+    fn.argtypes = [vp] * 6 + [i64, i64, vp, i32, i32, vp, i32, d, i32, i64,
+                              i32, d, i32, i32, d, d, d, d, i32, vp, vp, vp,
+                              vp, vp, vp, vp, ctypes.POINTER(ctypes.c_float)]
+    allc = fn(*[_p(x) for x in arrays], A.shape[0], A.shape[1], _p(params),
+              q, fid, _p(fc), int(gram), exponent, orthogonalize, seed,
+              lanczos_degree, lanczos_tol, min_num_samples, max_num_samples,
+              error_atol, error_rtol, confidence_level,
+              outlier_significance_level, num_threads, _p(trace), _p(error),
+              _p(samples), _p(order), _p(used), _p(outl), _p(conv),
+              ctypes.byref(wall))
+    return dict(all_converged=bool(allc), trace=trace, error=error,
+                samples=samples, processed_samples_indices=order,
+                num_samples_used=used, num_outliers=outl, converged=conv,
+                alg_wall_time=float(wall.value))
+
+
 def random_probes(seed, n, num_probes):
     """Probe vectors the single-thread reference estimator draws, in order."""
     lib = load()

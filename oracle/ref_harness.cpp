@@ -178,7 +178,77 @@ static int run_trace_estimator(
     return all_converged;
 }
 
+// A + t B with a general CSR B (c_csr_affine_matrix_function.cpp:55-79):
+// the reference runs a Krylov sequence per inquiry on each probe.
+template <typename T>
+static int run_trace_estimator_b(
+        const T* data, const int* indices, const int* indptr,
+        const T* b_data, const int* b_indices, const int* b_indptr,
+        int64_t num_rows, int64_t num_cols, T* parameters, int num_inquiries,
+        int func_id, const double* coeff, int gram, T exponent,
+        int orthogonalize, int64_t seed, int lanczos_degree, T lanczos_tol,
+        int min_num_samples, int max_num_samples, T error_atol, T error_rtol,
+        T confidence_level, T outlier_significance_level, int num_threads,
+        T* trace, T* error, T* samples, int* processed_samples_indices,
+        int* num_samples_used, int* num_outliers, int* converged,
+        float* alg_wall_time)
+{
+    cLinearOperator<T>* A = new cCSRAffineMatrixFunction<T>(
+            data, reinterpret_cast<const LongIndexType*>(indices),
+            reinterpret_cast<const LongIndexType*>(indptr), num_rows, num_cols,
+            b_data, reinterpret_cast<const LongIndexType*>(b_indices),
+            reinterpret_cast<const LongIndexType*>(b_indptr));
+    Function* f = make_function(func_id, coeff);
+    T** rows = new T*[max_num_samples];
+    for (int i = 0; i < max_num_samples * num_inquiries; ++i)
+        samples[i] = NAN;
+    for (int i = 0; i < max_num_samples; ++i)
+        rows[i] = &samples[static_cast<int64_t>(i) * num_inquiries];
+    for (int j = 0; j < num_inquiries; ++j)
+    {
+        converged[j] = 0;
+        num_samples_used[j] = 0;
+        num_outliers[j] = 0;
+    }
+    float wall = 0.0f;
+    int all_converged = cTraceEstimator<T>::c_trace_estimator(
+            A, parameters, num_inquiries, f, gram, exponent, orthogonalize,
+            seed, lanczos_degree, lanczos_tol, min_num_samples,
+            max_num_samples, error_atol, error_rtol, confidence_level,
+            outlier_significance_level, num_threads, trace, error, rows,
+            processed_samples_indices, num_samples_used, num_outliers,
+            converged, wall);
+    *alg_wall_time = wall;
+    delete[] rows;
+    delete f;
+    delete A;
+    return all_converged;
+}
+
 extern "C" {
+
+int ref_trace_estimator_b_f64(
+        const double* data, const int* indices, const int* indptr,
+        const double* b_data, const int* b_indices, const int* b_indptr,
+        int64_t num_rows, int64_t num_cols, double* parameters,
+        int num_inquiries, int func_id, const double* coeff, int gram,
+        double exponent, int orthogonalize, int64_t seed, int lanczos_degree,
+        double lanczos_tol, int min_num_samples, int max_num_samples,
+        double error_atol, double error_rtol, double confidence_level,
+        double outlier_significance_level, int num_threads, double* trace,
+        double* error, double* samples, int* processed_samples_indices,
+        int* num_samples_used, int* num_outliers, int* converged,
+        float* alg_wall_time)
+{
+    return run_trace_estimator_b<double>(
+            data, indices, indptr, b_data, b_indices, b_indptr, num_rows,
+            num_cols, parameters, num_inquiries, func_id, coeff, gram,
+            exponent, orthogonalize, seed, lanczos_degree, lanczos_tol,
+            min_num_samples, max_num_samples, error_atol, error_rtol,
+            confidence_level, outlier_significance_level, num_threads, trace,
+            error, samples, processed_samples_indices, num_samples_used,
+            num_outliers, converged, alg_wall_time);
+}
 
 // Full reference estimator (c_trace_estimator.cpp:192-307) on a CSR/CSC
 // matrix, or on A + t I when affine != 0.

@@ -624,3 +624,49 @@ def test_device_rcm_order_rejects_bad_pattern(cuda):
     ind = torch.tensor([0, 5], dtype=torch.int32, device="cuda")
     with pytest.raises(_lib.SlqError):
         rcm_order_device(ip, ind, 2, 2)
+
+
+def _general_b(n, seed):
+    rng = np.random.default_rng(seed)
+    R = sp.random(n, n, density=2.0 / n, random_state=rng, format="csr")
+    return sp.csr_matrix(sp.diags(np.linspace(0.5, 2.0, n)) +
+                         0.05 * (R + R.T))
+
+
+@pytest.mark.parametrize("n,gram", [(500, False), (500, True),
+                                    (20000, False)])
+def test_affine_general_b_matches_reference(cuda, n, gram):
+    # A + t B with B other than I: a Krylov sequence per t on every probe
+    # (c_trace_estimator.cpp:496-556), here one device operator per t
+    from oracle import ref
+    A = ib.correlation_matrix(n, scale=0.05 if n < 1000 else 0.01,
+                              shift=0.1, seed=1)
+    B = _general_b(n, 7)
+    t = [0.1, 1.0, 3.0]
+    kw = dict(min_num_samples=6, max_num_samples=6, error_rtol=1e-8,
+              lanczos_degree=20, orthogonalize=-1, seed=0)
+    want = ref.trace_estimator_b(A, B, "log", t, gram=gram, **kw)
+    F = ib.AffineMatrixFunction(A, B=B)
+    tr, info = ib.logdet(F, parameters=t, gram=gram, method="slq", gpu=True,
+                         return_info=True, **kw)
+    got = np.asarray(info["convergence"]["samples"], float)
+    assert got.shape == (6, 3)
+    assert rel(got, want["samples"]) < 1e-9
+    assert rel(tr, want["trace"]) < 1e-9
+    assert list(info["convergence"]["num_samples_used"]) == \
+        list(want["num_samples_used"])
+
+
+def test_affine_general_b_float32_close_to_float64(cuda):
+    A = ib.correlation_matrix(3000, scale=0.02, shift=0.1, seed=2)
+    B = _general_b(3000, 3)
+    kw = dict(min_num_samples=32, max_num_samples=32, error_rtol=1e-8,
+              lanczos_degree=30, orthogonalize=-1, seed=1)
+    t64, _ = ib.traceinv(ib.AffineMatrixFunction(A, B=B),
+                         parameters=[0.2, 2.0], method="slq", gpu=True,
+                         return_info=True, **kw)
+    A32, B32 = A.astype(np.float32), B.astype(np.float32)
+    t32, _ = ib.traceinv(ib.AffineMatrixFunction(A32, B=B32),
+                         parameters=[0.2, 2.0], method="slq", gpu=True,
+                         return_info=True, **kw)
+    assert rel(t32, t64) < 1e-4

@@ -159,9 +159,33 @@ def test_operator_and_parameter_checks():
     assert k == 2 and p.dtype == np.float64
     with pytest.raises(ValueError):
         get_operator_parameters(np.ones((2, 2)), "float64")
-    with pytest.raises(NotImplementedError):
-        ib.AffineMatrixFunction(sp.eye(4, format="csr"),
+    F = ib.AffineMatrixFunction(sp.eye(4, format="csr"),
                                 B=2 * sp.eye(4, format="csr"))
+    assert F.general_B and not F._affine()
+    assert find_num_inquiries(F, 2) == 2
+    with pytest.raises(ValueError):
+        ib.AffineMatrixFunction(sp.eye(4, format="csr"),
+                                B=sp.eye(5, format="csr"))
+    with pytest.raises(TypeError):
+        ib.AffineMatrixFunction(sp.eye(4, format="csr"), B=2.0)
+
+
+def test_affine_general_b_union_pattern(lib):
+    # A + t B with B other than I: one CSR pattern holding both, A's and B's
+    # values on it (zeros where a matrix lacks an entry)
+    rng = np.random.default_rng(5)
+    for n, m in ((50, 50), (300, 300)):
+        A = sp.random(n, m, density=0.05, random_state=rng, format="csr")
+        B = sp.random(n, m, density=0.03, random_state=rng, format="csc")
+        F = ib.AffineMatrixFunction(A, B=B)
+        U = F._union_pattern()
+        P = sp.csr_matrix((np.ones(U["indices"].size), U["indices"],
+                           U["indptr"]), shape=(n, m))
+        Au = sp.csr_matrix((U["a"], U["indices"], U["indptr"]), shape=(n, m))
+        Bu = sp.csr_matrix((U["b"], U["indices"], U["indptr"]), shape=(n, m))
+        assert abs(Au - A).max() == 0 and abs(Bu - B).max() == 0
+        assert P.nnz == (abs(A) + abs(B)).nnz
+        assert U["G"] in (0, 4, 8, 16)
 
 
 def test_non_slq_methods_and_cpu_path_are_refused():
