@@ -39,6 +39,7 @@ EXPORTS = (
     "slq_batch_info", "slq_batch_destroy", "slq_group_order",
     "slq_rcm_order", "slq_tc_selftest", "slq_order_spread", "slq_group_fill",
     "slq_rcm_order_device_workspace_bytes", "slq_rcm_order_device",
+    "slq_dense_operator_workspace_bytes", "slq_dense_operator_create",
 )
 TUNE_MAX_CANDIDATES = 16
 SPMM_KINDS = ("csr", "row-group", "row-group-tma", "row-group-tc")
@@ -180,6 +181,9 @@ def _declare(lib):
         "slq_order_spread": (i32, [i64, vp, vp, vp, i64, vp]),
         "slq_group_fill": (i32, [i64, vp, vp, vp, i32, i64, vp]),
         "slq_rcm_order_device_workspace_bytes": (i32, [i64, vp]),
+        "slq_dense_operator_workspace_bytes": (i32, [i64, i64, i32, i32, psz]),
+        "slq_dense_operator_create": (i32, [vp, i64, i64, i32, i32, i32, vp, sz,
+                                            vp, ctypes.POINTER(vp)]),
         "slq_rcm_order_device": (i32, [i64, i64, vp, vp, i32, vp, vp, vp, sz,
                                         vp]),
         "slq_tc_selftest": (i32, [vp, vp, vp, i32, vp, vp]),

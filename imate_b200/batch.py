@@ -142,6 +142,11 @@ class BatchPlan:
                         kw["orthogonalize"], kw["seed"], kw["num_threads"],
                         kw["num_gpu_devices"], kw["verbose"], kw["plot"],
                         kw["gpu"], engine, coeff)
+            if getattr(J.dev_op, "dense", False):
+                raise NotImplementedError(
+                    "batch plans serve sparse operators; a dense operator "
+                    "holds the scratch of one product at a time (call "
+                    "logdet / traceinv / trace for it)")
             if J.per_group_t is not None:
                 raise NotImplementedError(
                     "batch plans record one device operator per estimate; "

@@ -221,6 +221,19 @@ struct slq_op {
     const int32_t* t_gptr = nullptr;
     const int32_t* t_gcol = nullptr;
     const void* t_gval = nullptr;
+    // dense FP32 operator (tensor-core product): TF32 parts of A, [nrows][ldk],
+    // and of A^T, [ncols][ldk_t], K-major with zero-padded pitches; the
+    // probe-block parts scratch [256][ldx]; TMA maps of the A parts
+    int dense = 0;
+    float* d_hi = nullptr;
+    float* d_lo = nullptr;
+    float* dt_hi = nullptr;
+    float* dt_lo = nullptr;
+    int64_t ldk = 0, ldk_t = 0, ldx = 0;
+    float* xt_hi = nullptr;
+    float* xt_lo = nullptr;
+    int32_t* d_error = nullptr;
+    CUtensorMap map_hi, map_lo, map_t_hi, map_t_lo;
     // autotuned SpMM candidate per direction and log2(block width); -1 = built-in
     int8_t tuned[2][11];
     slq_op()
@@ -766,6 +779,145 @@ slq_status row_map(CUtensorMap* m, const float* base, int64_t rows, int b)
     return SLQ_OK;
 }
 
+// ---------------------------------------------------------------------------
+// dense FP32 operators (tensor-core product, k_dense_tc)
+// ---------------------------------------------------------------------------
+
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+struct DenseBufs {
+    float *hi, *lo, *t_hi, *t_lo, *x_hi, *x_lo;
+    int32_t* error;
+    int64_t ldk, ldk_t, ldx;
+};
+
+void dense_layout(Carver& c, int64_t rows, int64_t cols, int need_transpose, DenseBufs* d)
+{
+    d->ldk = round_up(std::max<int64_t>(cols, 1), DT_BK);
+    d->ldk_t = need_transpose ? round_up(std::max<int64_t>(rows, 1), DT_BK) : 0;
+    d->ldx = std::max(d->ldk, d->ldk_t);
+    d->hi = c.take<float>(static_cast<size_t>(rows) * d->ldk);
+    d->lo = c.take<float>(static_cast<size_t>(rows) * d->ldk);
+    d->t_hi = need_transpose ? c.take<float>(static_cast<size_t>(cols) * d->ldk_t) : nullptr;
+    d->t_lo = need_transpose ? c.take<float>(static_cast<size_t>(cols) * d->ldk_t) : nullptr;
+    d->x_hi = c.take<float>(static_cast<size_t>(256) * d->ldx);
+    d->x_lo = c.take<float>(static_cast<size_t>(256) * d->ldx);
+    d->error = c.take<int32_t>(1);
+}
+
+// K-major TF32-part tensor map: [outer][ld] FP32, box 32 x box_rows,
+// SWIZZLE_128B (128-byte rows)
+slq_status part_map(CUtensorMap* m, const float* base, int64_t ld, int64_t outer,
+                    int box_rows)
+{
+    if (!g_encode_tiled)
+    {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        SLQ_CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess)
+            return fail(SLQ_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+        g_encode_tiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    cuuint64_t dims[2] = {static_cast<cuuint64_t>(ld), static_cast<cuuint64_t>(outer)};
+    cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * sizeof(float)};
+    cuuint32_t box[2] = {static_cast<cuuint32_t>(DT_BK), static_cast<cuuint32_t>(box_rows)};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = g_encode_tiled(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base),
+                                dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(SLQ_ERR_CUDA, "cuTensorMapEncodeTiled (dense) failed (" +
+                                      std::to_string(int(r)) + ")");
+    return SLQ_OK;
+}
+
+size_t dense_smem(int NB)
+{
+    const size_t stage = 2 * 128 * DT_BK * 4 + 2 * static_cast<size_t>(NB) * DT_BK * 4;
+    return 1023 + DT_STAGES * stage + 128 + 4 * 256 * sizeof(double);
+}
+
+// Y = A X (transpose: A^T X) on a dense operator, the SpMM epilogue fused;
+// at most 256 probes per GEMM launch.  *grid_out = the partial rows.
+slq_status dense_spmm(Launcher& L, const slq_op* op, int transpose, int b, const float* X,
+                      const double* sx, double shift, float* Y, const float* Z,
+                      const double* zc, const double* zs, int epi, double* partials,
+                      int* grid_out, int32_t* error)
+{
+    if (transpose && !op->dt_hi)
+        return fail(SLQ_ERR_BAD_ARG, "dense operator has no transpose");
+    const int64_t M = transpose ? op->ncols : op->nrows;
+    const int64_t K = transpose ? op->nrows : op->ncols;
+    const CUtensorMap& ahi = transpose ? op->map_t_hi : op->map_hi;
+    const CUtensorMap& alo = transpose ? op->map_t_lo : op->map_lo;
+    const int64_t ntm = (M + 127) / 128;
+    static bool attr = false;
+    if (!attr)
+    {
+        SLQ_CK(cudaFuncSetAttribute(k_dense_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(dense_smem(256))));
+        attr = true;
+    }
+    const double bytes = double(M) * K * 8.0 + double(K) * b * 4.0 + double(M) * b * 4.0;
+    ProfScope prof(SLQ_K_SPMM, bytes, L.st);
+    // one grid for every chunk (the finalize reads the same partial rows for
+    // all columns): the first chunk's, which has the most tiles; a CTA
+    // without a tile writes zero partials
+    int grid_all = 0;
+    for (int p_off = 0; p_off < b; p_off += 256)
+    {
+        const int nb = std::min(256, b - p_off);
+        // one probe tile per chunk: narrower tiles (more CTAs for small M)
+        // re-read the A tile from shared memory for less MMA work each and
+        // measured slower (n = 8192: 414 vs 369 us)
+        const int NB = static_cast<int>(round_up(nb, 16));
+        const int ntn = 1;
+        if (grid_all == 0)
+            grid_all = static_cast<int>(
+                std::max<int64_t>(1, std::min<int64_t>(ntm * ntn, L.sms)));
+        const int grid = grid_all;
+        dim3 tg(static_cast<unsigned>((K + 31) / 32), static_cast<unsigned>((nb + 31) / 32));
+        k_split_transpose<<<tg, dim3(32, 8), 0, L.st>>>(X, K, b, p_off, nb, op->ldx, op->xt_hi,
+                                                        op->xt_lo);
+        SLQ_LAUNCH_CK();
+        ++L.launches;
+        CUtensorMap xhi, xlo;
+        SLQ_TRY(part_map(&xhi, op->xt_hi, op->ldx, nb, NB));
+        SLQ_TRY(part_map(&xlo, op->xt_lo, op->ldx, nb, NB));
+        DenseArgs d;
+        d.M = M;
+        d.K = K;
+        d.nb = nb;
+        d.NB = NB;
+        d.ntn = ntn;
+        d.b = b;
+        d.p_off = p_off;
+        // running total and chunk accumulator: two power-of-two halves
+        uint32_t cols = 32;
+        while (cols < static_cast<uint32_t>(NB)) cols <<= 1;
+        d.tmem_cols = 2 * cols;
+        d.X = X;
+        d.sx = sx;
+        d.shift = shift;
+        d.Y = Y;
+        d.Z = Z;
+        d.zc = zc;
+        d.zs = zs;
+        d.epi = epi;
+        d.partials = partials;
+        d.error = error ? error : op->d_error;
+        k_dense_tc<<<grid, DT_THREADS, dense_smem(NB), L.st>>>(ahi, alo, xhi, xlo, d);
+        SLQ_LAUNCH_CK();
+        ++L.launches;
+    }
+    *grid_out = grid_all;
+    return SLQ_OK;
+}
+
+
 template <int G, int NS>
 slq_status spmm_rgt_inst(Launcher& L, const CUtensorMap* xmap, const int32_t* gptr,
                          const int32_t* gcol, const float* gval, int64_t nrows, int b,
@@ -1000,6 +1152,13 @@ slq_status op_spmm(Launcher& L, const slq_op* op, int transpose, int b, const VT
                    const double* zs, int epi, double* partials, int* grid_out,
                    const CUtensorMap* xmap = nullptr, int32_t* error = nullptr)
 {
+    if (op->dense)
+    {
+        if constexpr (sizeof(VT) == 4)
+            return dense_spmm(L, op, transpose, b, X, sx, shift, Y, Z, zc, zs, epi, partials,
+                              grid_out, error);
+        return fail(SLQ_ERR_BAD_ARG, "dense operators hold float32 data");
+    }
     SpmmCand cands[SLQ_TUNE_MAX_CANDIDATES];
     const int nc = spmm_candidates<VT>(op, transpose, b, cands);
     const int lg = log2_width(b);
@@ -1166,7 +1325,7 @@ slq_status make_plan(const slq_op* op, const slq_params* p, int q, RunPlan* r)
                     "eigenvalue shift across inquiries is not valid for Golub-Kahn runs");
     if (p->gram != 2 && op->nrows != op->ncols && (p->gram == 0 || op->affine))
         return fail(SLQ_ERR_BAD_ARG, "this run needs a square matrix");
-    if (p->gram && !op->t_ptr)
+    if (p->gram && !(op->dense ? op->dt_hi != nullptr : op->t_ptr != nullptr))
         return fail(SLQ_ERR_BAD_ARG, "gram runs need an operator created with need_transpose");
     if (p->orthogonalize > p->lanczos_degree)
         return fail(SLQ_ERR_BAD_ARG, "orthogonalize must be at most lanczos_degree");
@@ -1776,6 +1935,8 @@ slq_status check_width(const slq_op* op, int width)
 extern "C" slq_status slq_operator_tune_workspace_bytes(const slq_op* op, int width,
                                                         size_t* bytes)
 {
+    if (op && op->dense)
+        return fail(SLQ_ERR_BAD_ARG, "dense operators have one product kernel (no tuning)");
     SLQ_TRY(check_width(op, width));
     if (!bytes) return fail(SLQ_ERR_BAD_ARG, "bytes is NULL");
     int sms = 0;
@@ -1791,6 +1952,8 @@ extern "C" slq_status slq_operator_tune(slq_op* op, int width, int transpose, in
                                         void* workspace, size_t workspace_bytes, void* stream,
                                         slq_tune_result* result)
 {
+    if (op && op->dense)
+        return fail(SLQ_ERR_BAD_ARG, "dense operators have one product kernel (no tuning)");
     SLQ_TRY(check_width(op, width));
     if (!result) return fail(SLQ_ERR_BAD_ARG, "tune: result is NULL");
     if (transpose && !op->t_ptr) return fail(SLQ_ERR_BAD_ARG, "tune: operator has no transpose");
@@ -1809,6 +1972,8 @@ extern "C" slq_status slq_operator_tune(slq_op* op, int width, int transpose, in
 extern "C" slq_status slq_operator_set_variant(slq_op* op, int width, int transpose,
                                                int candidate)
 {
+    if (op && op->dense)
+        return fail(SLQ_ERR_BAD_ARG, "dense operators have one product kernel (no tuning)");
     SLQ_TRY(check_width(op, width));
     if (candidate < -1 || candidate >= SLQ_TUNE_MAX_CANDIDATES)
         return fail(SLQ_ERR_BAD_ARG, "set_variant: candidate out of range");
@@ -1960,6 +2125,9 @@ slq_status batch_plan(int count, slq_op* const* ops, const slq_params* params,
     {
         BatchRun& R = (*runs)[i];
         if (!ops[i]) return fail(SLQ_ERR_BAD_ARG, "batch: operator " + std::to_string(i) + " is NULL");
+        if (ops[i]->dense)
+            return fail(SLQ_ERR_BAD_ARG, "batch: operator " + std::to_string(i) +
+                                             " is dense (one product at a time)");
         R.op = ops[i];
         R.p = params[i];
         const int q = num_inquiries[i];
@@ -2270,7 +2438,7 @@ extern "C" slq_status slq_operator_dot(slq_op* op, int transpose, double t, cons
     if (x == y) return fail(SLQ_ERR_BAD_ARG, "operator_dot: x and y must not alias");
     if (!is_pow2(width) || width > ((op->dtype == SLQ_F64) ? 512 : 1024))
         return fail(SLQ_ERR_BAD_ARG, "operator_dot: width must be a power of two");
-    if (transpose && !op->t_ptr)
+    if (transpose && !(op->dense ? op->dt_hi != nullptr : op->t_ptr != nullptr))
         return fail(SLQ_ERR_BAD_ARG, "operator_dot: operator has no transpose");
     Launcher L;
     L.st = static_cast<cudaStream_t>(stream);
@@ -2465,6 +2633,87 @@ extern "C" slq_status slq_rcm_order_device(int64_t n, int64_t nnz, const int32_t
     *done = 1;
     return SLQ_OK;
 }
+
+
+extern "C" slq_status slq_dense_operator_workspace_bytes(int64_t num_rows, int64_t num_cols,
+                                                         int dtype, int need_transpose,
+                                                         size_t* bytes)
+{
+    if (!bytes || num_rows < 1 || num_cols < 1 || num_rows > INT32_MAX || num_cols > INT32_MAX)
+        return fail(SLQ_ERR_BAD_ARG, "dense_operator: bad size");
+    if (dtype != SLQ_F32)
+        return fail(SLQ_ERR_BAD_ARG, "dense_operator: float32 data only");
+    Carver c(nullptr, 0);
+    DenseBufs d;
+    dense_layout(c, num_rows, num_cols, need_transpose, &d);
+    *bytes = c.off + 256;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_dense_operator_create(const void* data, int64_t num_rows,
+                                                int64_t num_cols, int dtype, int affine,
+                                                int need_transpose, void* workspace,
+                                                size_t workspace_bytes, void* stream,
+                                                slq_op** out)
+{
+    if (!out || !data) return fail(SLQ_ERR_BAD_ARG, "dense_operator: NULL argument");
+    size_t need = 0;
+    SLQ_TRY(slq_dense_operator_workspace_bytes(num_rows, num_cols, dtype, need_transpose,
+                                               &need));
+    if (!workspace || workspace_bytes < need)
+        return fail(SLQ_ERR_WORKSPACE, "dense_operator: workspace too small (need " +
+                                           std::to_string(need) + " bytes)");
+    if (affine && num_rows != num_cols)
+        return fail(SLQ_ERR_BAD_ARG, "dense_operator: A + t I needs a square A");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Carver c(workspace, workspace_bytes);
+    DenseBufs d;
+    dense_layout(c, num_rows, num_cols, need_transpose, &d);
+    // zero padding, then the parts
+    SLQ_CK(cudaMemsetAsync(workspace, 0, c.off, st));
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
+    const float* A = static_cast<const float*>(data);
+    k_split_rows<<<sms * 8, 256, 0, st>>>(A, num_rows, num_cols, num_cols, d.ldk, d.hi, d.lo);
+    SLQ_LAUNCH_CK();
+    if (need_transpose)
+    {
+        dim3 tg(static_cast<unsigned>((num_rows + 31) / 32),
+                static_cast<unsigned>((num_cols + 31) / 32));
+        k_split_transpose<<<tg, dim3(32, 8), 0, st>>>(A, num_rows, num_cols, 0, num_cols,
+                                                      d.ldk_t, d.t_hi, d.t_lo);
+        SLQ_LAUNCH_CK();
+    }
+    slq_op* op = new slq_op();
+    op->dtype = dtype;
+    op->affine = affine;
+    op->nrows = num_rows;
+    op->ncols = num_cols;
+    op->nnz = num_rows * num_cols;
+    op->dense = 1;
+    op->d_hi = d.hi;
+    op->d_lo = d.lo;
+    op->dt_hi = d.t_hi;
+    op->dt_lo = d.t_lo;
+    op->ldk = d.ldk;
+    op->ldk_t = d.ldk_t;
+    op->ldx = d.ldx;
+    op->xt_hi = d.x_hi;
+    op->xt_lo = d.x_lo;
+    op->d_error = d.error;
+    slq_status s = part_map(&op->map_hi, d.hi, d.ldk, num_rows, 128);
+    if (s == SLQ_OK) s = part_map(&op->map_lo, d.lo, d.ldk, num_rows, 128);
+    if (s == SLQ_OK && need_transpose) s = part_map(&op->map_t_hi, d.t_hi, d.ldk_t, num_cols, 128);
+    if (s == SLQ_OK && need_transpose) s = part_map(&op->map_t_lo, d.t_lo, d.ldk_t, num_cols, 128);
+    if (s != SLQ_OK)
+    {
+        delete op;
+        return s;
+    }
+    *out = op;
+    return SLQ_OK;
+}
+
 
 extern "C" slq_status slq_generate_probes_workspace_bytes(int64_t len, int width,
                                                           size_t* bytes)

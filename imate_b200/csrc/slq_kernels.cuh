@@ -2253,6 +2253,365 @@ k_spmm_tc(const __grid_constant__ CUtensorMap xmap, const int32_t* __restrict__ 
 }
 
 // ===========================================================================
+// Dense operator product on the tensor cores (FP32 data, three TF32 terms).
+//
+// Y[M][b] = A[M][K] X[K][b] for a dense row-major A.  A is split once into
+// TF32 parts, hi = rn_tf32(a), lo = rn_tf32(a - hi), stored K-major with a
+// row pitch ldk (a multiple of 32, zero-padded); each product splits and
+// transposes the probe block likewise (XT[p][k], k contiguous), at most 256
+// probes at a time.  A CTA computes 128-row tiles of Y (persistent over the
+// tiles): TMA loads 32-value K slices of A_hi, A_lo, XT_hi, XT_lo
+// (128-byte rows, SWIZZLE_128B) into a two-stage ring, one thread issues
+// per K step of 8 the three kind::tf32 MMAs A_hi XT_hi + A_hi XT_lo +
+// A_lo XT_hi into an FP32 accumulator in tensor memory (D[128][N], lane =
+// row, column = probe).  The tensor core's FP32 accumulation does not round
+// to nearest, so each 512-value K chunk goes to a fresh accumulator that
+// four warps add into a running total (also in tensor memory) with
+// round-to-nearest FP32 adds, and then apply the SpMM epilogue to it (thread
+// t = row t of the tile).  The dropped lo*lo term and the rounding of the lo
+// parts leave ~2^-21 relative error per product.  Probe partial sums are
+// reduced across the tile's rows in a fixed order.
+// ===========================================================================
+
+constexpr int DT_BK = 32;       // K values per stage (one 128-byte row)
+constexpr int DT_STAGES = 2;
+constexpr int DT_CHUNK = 16;    // stages per accumulation chunk (512 K values)
+constexpr int DT_THREADS = 192; // warps 0-3 accumulate, 4 loads, 5 issues MMAs
+
+__device__ __forceinline__ void split_tf32_f(float x, float& hi, float& lo)
+{
+    uint32_t h, l;
+    tc::split_tf32(x, h, l);
+    hi = __uint_as_float(h);
+    lo = __uint_as_float(l);
+}
+
+// out[r * ldo + c] = parts of src[r * lds + c] for r < rows, c < cols
+__global__ void k_split_rows(const float* __restrict__ src, int64_t rows, int64_t cols,
+                             int64_t lds, int64_t ldo, float* __restrict__ hi,
+                             float* __restrict__ lo)
+{
+    const int64_t total = rows * cols;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        const int64_t r = i / cols, c = i % cols;
+        float h, l;
+        split_tf32_f(src[r * lds + c], h, l);
+        hi[r * ldo + c] = h;
+        lo[r * ldo + c] = l;
+    }
+}
+
+// out[j * ldo + r] = parts of src[r * lds + col0 + j] for r < rows, j < ncols
+// (32 x 32 tiles through shared memory; block 32 x 8)
+__global__ void k_split_transpose(const float* __restrict__ src, int64_t rows, int64_t lds,
+                                  int64_t col0, int64_t ncols, int64_t ldo,
+                                  float* __restrict__ hi, float* __restrict__ lo)
+{
+    __shared__ float t[32][33];
+    const int64_t r0 = static_cast<int64_t>(blockIdx.x) * 32;
+    const int64_t c0 = static_cast<int64_t>(blockIdx.y) * 32;
+    for (int j = threadIdx.y; j < 32; j += 8)
+    {
+        const int64_t r = r0 + j, c = c0 + threadIdx.x;
+        t[j][threadIdx.x] = (r < rows && c < ncols) ? src[r * lds + col0 + c] : 0.0f;
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += 8)
+    {
+        const int64_t c = c0 + j, r = r0 + threadIdx.x;
+        if (c < ncols && r < rows)
+        {
+            float h, l;
+            split_tf32_f(t[threadIdx.x][j], h, l);
+            hi[c * ldo + r] = h;
+            lo[c * ldo + r] = l;
+        }
+    }
+}
+
+struct DenseArgs {
+    int64_t M, K;        // rows of Y, inner dimension
+    int nb, NB, ntn;     // probes in this chunk; probes per tile (a multiple
+                         // of 16); probe tiles per row tile
+    int b, p_off;        // block width (row pitch of X, Y, Z) and chunk offset
+    uint32_t tmem_cols;  // power of two >= max(32, NB)
+    const float* X;
+    const double* sx;
+    double shift;
+    float* Y;
+    const float* Z;
+    const double* zc;
+    const double* zs;
+    int epi;
+    double* partials;    // [grid][b]
+    int32_t* error;
+};
+
+__global__ void __launch_bounds__(DT_THREADS, 1)
+k_dense_tc(const __grid_constant__ CUtensorMap a_hi, const __grid_constant__ CUtensorMap a_lo,
+           const __grid_constant__ CUtensorMap x_hi, const __grid_constant__ CUtensorMap x_lo,
+           const DenseArgs d)
+{
+    extern __shared__ __align__(1024) unsigned char smem_dense[];
+    // [stages][A_hi 16 KB | A_lo 16 KB | B_hi NB*128 | B_lo NB*128] at a
+    // 1024-aligned base, then barriers, tensor-memory address, reduction
+    const uint32_t a_bytes = 128 * DT_BK * 4;
+    const uint32_t b_bytes = static_cast<uint32_t>(d.NB) * DT_BK * 4;
+    const uint32_t stage_bytes = 2 * a_bytes + 2 * b_bytes;
+    unsigned char* base = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_dense) + 1023) & ~uintptr_t(1023));
+    unsigned char* tail = base + DT_STAGES * stage_bytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(tail);
+    uint64_t* empty = full + DT_STAGES;
+    uint64_t* chunk_full = empty + DT_STAGES;
+    uint64_t* chunk_empty = chunk_full + 1;
+    uint64_t* drain = chunk_empty + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 2);  // [2]
+    double* red = reinterpret_cast<double*>(tail + 128);     // [4][256]
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
+    if (tid == 0)
+    {
+        for (int s = 0; s < DT_STAGES; ++s)
+        {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(chunk_full, 1);
+        mbar_init(chunk_empty, 4);  // one arrival per accumulating warp
+        mbar_init(drain, 1);
+        abort_flag[0] = 0;
+        abort_flag[1] = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = tid; i < 4 * 256; i += DT_THREADS) red[i] = 0.0;
+    if (warp == 0)
+    {
+        tc::tmem_alloc(tmem_slot, d.tmem_cols);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tmem_slot;
+    // running total in columns [0, NB), the chunk accumulator after it
+    const uint32_t d_chunk = tmem + d.tmem_cols / 2;
+
+    // tiles: 128 rows x NB probes, the probe tiles of a row tile adjacent
+    // (they share the A stream through L2)
+    const int64_t ntiles = (d.M + 127) / 128 * d.ntn;
+    const int64_t nk = (d.K + DT_BK - 1) / DT_BK;
+    const int64_t nch = (nk + DT_CHUNK - 1) / DT_CHUNK;  // chunks per tile
+    const uint32_t idesc = tc::idesc_tf32_m128(static_cast<uint32_t>(d.NB));
+    auto give_up = [&]() {
+        abort_flag[0] = 1;
+        atomicExch(d.error, 1);
+    };
+
+    if (warp == 4)
+    {
+        // producer: the A and probe-block parts of every stage of every tile
+        int64_t it = 0;
+        if (lane == 0)
+        {
+            bool ok = true;
+            for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
+            {
+                const int row0 = static_cast<int>(tile / d.ntn * 128);
+                const int col0 = static_cast<int>(tile % d.ntn) * d.NB;
+                for (int64_t k = 0; k < nk; ++k, ++it)
+                {
+                    const int s = static_cast<int>(it % DT_STAGES);
+                    const uint32_t ph = static_cast<uint32_t>((it / DT_STAGES) & 1);
+                    if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag))
+                    {
+                        give_up();
+                        ok = false;
+                        break;
+                    }
+                    unsigned char* st = base + static_cast<size_t>(s) * stage_bytes;
+                    mbar_expect_tx(&full[s], stage_bytes);
+                    const int kx = static_cast<int>(k * DT_BK);
+                    tc::tma_load_2d(st, &a_hi, kx, row0, &full[s]);
+                    tc::tma_load_2d(st + a_bytes, &a_lo, kx, row0, &full[s]);
+                    tc::tma_load_2d(st + 2 * a_bytes, &x_hi, kx, col0, &full[s]);
+                    tc::tma_load_2d(st + 2 * a_bytes + b_bytes, &x_lo, kx, col0, &full[s]);
+                }
+            }
+            // the copies in flight land before the CTA leaves
+            for (int64_t k = it - DT_STAGES; k < it; ++k)
+            {
+                if (k < 0) continue;
+                mbar_wait(&full[k % DT_STAGES], static_cast<uint32_t>((k / DT_STAGES) & 1),
+                          abort_flag + 1);
+            }
+        }
+        __syncwarp();
+    }
+    else if (warp == 5)
+    {
+        // MMA issuer: one chunk accumulator per 512 K values
+        if (lane == 0)
+        {
+            int64_t it = 0, cc = 0;
+            bool ok = true;
+            for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
+            {
+                for (int64_t k = 0; k < nk && ok; ++k, ++it)
+                {
+                    const int64_t kc = k % DT_CHUNK;
+                    if (kc == 0 && cc > 0 &&
+                        !mbar_wait(chunk_empty, static_cast<uint32_t>((cc - 1) & 1), abort_flag))
+                    {
+                        give_up();
+                        ok = false;
+                        break;
+                    }
+                    const int s = static_cast<int>(it % DT_STAGES);
+                    const uint32_t ph = static_cast<uint32_t>((it / DT_STAGES) & 1);
+                    if (!mbar_wait(&full[s], ph, abort_flag))
+                    {
+                        give_up();
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    unsigned char* st = base + static_cast<size_t>(s) * stage_bytes;
+                    const uint64_t ah = tc::smem_desc_sw128(st);
+                    const uint64_t al = tc::smem_desc_sw128(st + a_bytes);
+                    const uint64_t bh = tc::smem_desc_sw128(st + 2 * a_bytes);
+                    const uint64_t bl = tc::smem_desc_sw128(st + 2 * a_bytes + b_bytes);
+#pragma unroll
+                    for (int kk = 0; kk < DT_BK / 8; ++kk)
+                    {
+                        // K step kk: 8 TF32 values = 32 bytes further into each row
+                        const uint64_t o = static_cast<uint64_t>(kk * 32) >> 4;
+                        const uint32_t acc = (kc > 0 || kk > 0) ? 1u : 0u;
+                        tc::mma_tf32_ss(d_chunk, al + o, bh + o, idesc, acc);
+                        tc::mma_tf32_ss(d_chunk, ah + o, bl + o, idesc, 1u);
+                        tc::mma_tf32_ss(d_chunk, ah + o, bh + o, idesc, 1u);
+                    }
+                    tc::commit(&empty[s]);
+                    if (kc == DT_CHUNK - 1 || k == nk - 1)
+                    {
+                        tc::commit(chunk_full);
+                        ++cc;
+                    }
+                }
+            }
+            // every issued MMA completes before the tensor memory is freed
+            tc::commit(drain);
+            mbar_wait(drain, 0, abort_flag + 1);
+        }
+        __syncwarp();
+    }
+    else
+    {
+        // warps 0-3: add each chunk into the running total (round to
+        // nearest), then the epilogue; thread tid owns tile row tid
+        int64_t cc = 0;
+        bool ok = true;
+        const uint32_t lanes = static_cast<uint32_t>(32 * warp) << 16;
+        for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
+        {
+            for (int64_t ch = 0; ch < nch; ++ch, ++cc)
+            {
+                if (!__all_sync(FULL_MASK,
+                                mbar_wait(chunk_full, static_cast<uint32_t>(cc & 1), abort_flag)))
+                {
+                    if (lane == 0) give_up();
+                    ok = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                for (int c0 = 0; c0 < d.NB; c0 += 16)
+                {
+                    uint32_t v[16], t[16];
+                    tc::ld_x16(d_chunk + lanes + c0, v);
+                    if (ch > 0) tc::ld_x16(tmem + lanes + c0, t);
+                    tc::wait_ld();
+                    if (ch > 0)
+                    {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                            v[j] = __float_as_uint(__uint_as_float(t[j]) + __uint_as_float(v[j]));
+                    }
+                    tc::st_x16(tmem + lanes + c0, v);
+                }
+                tc::wait_st();
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(chunk_empty);
+            }
+            if (!ok) break;
+            tc::fence_after_sync();
+            const int64_t row = tile / d.ntn * 128 + tid;
+            const int col0 = static_cast<int>(tile % d.ntn) * d.NB;
+            const bool live = row < d.M;
+            for (int c0 = 0; c0 < d.NB; c0 += 16)
+            {
+                uint32_t v[16];
+                tc::ld_x16(tmem + lanes + c0, v);
+                tc::wait_ld();
+                double add[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                {
+                    add[j] = 0.0;
+                    const int q = col0 + c0 + j;
+                    if (!live || q >= d.nb) continue;
+                    const int p = d.p_off + q;
+                    const int64_t o = row * d.b + p;
+                    const double sxv = d.sx ? d.sx[p] : 1.0;
+                    const float xv = (d.shift != 0.0 || d.epi == 1) ? d.X[o] : 0.0f;
+                    const float zv = d.Z ? d.Z[o] : 0.0f;
+                    double y = static_cast<double>(__uint_as_float(v[j])) * sxv;
+                    if (d.shift != 0.0) y += d.shift * (sxv * static_cast<double>(xv));
+                    if (d.Z) y -= (d.zc[p] * d.zs[p]) * static_cast<double>(zv);
+                    const float yr = static_cast<float>(y);
+                    d.Y[o] = yr;
+                    const double ys = static_cast<double>(yr);
+                    if (d.epi == 1) add[j] = (sxv * static_cast<double>(xv)) * ys;
+                    else if (d.epi == 2) add[j] = ys * ys;
+                    else if (d.epi == 3) add[j] = (d.zs[p] * static_cast<double>(zv)) * ys;
+                }
+                if (d.epi != 0)
+                {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                    {
+                        double a = add[j];
+#pragma unroll
+                        for (int off = 16; off > 0; off >>= 1)
+                            a += __shfl_xor_sync(FULL_MASK, a, off);
+                        if (lane == 0 && col0 + c0 + j < d.nb)
+                            red[warp * 256 + col0 + c0 + j] += a;
+                    }
+                }
+            }
+            tc::fence_before_sync();
+        }
+    }
+
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0)
+    {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, d.tmem_cols);
+    }
+    if (d.epi != 0)
+        for (int q = tid; q < d.nb; q += DT_THREADS)
+            d.partials[static_cast<int64_t>(blockIdx.x) * d.b + d.p_off + q] =
+                ((red[q] + red[256 + q]) + red[512 + q]) + red[768 + q];
+}
+
+// ===========================================================================
 // Tensor-core self-test: D[128][16] = A[128][8] B[8][16] for one tile
 // through tcgen05 (one CTA of 128 threads; thread m owns row m).  mode:
 //   0  A in tensor memory (written by its owning warps), B in shared

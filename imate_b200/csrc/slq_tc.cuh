@@ -30,6 +30,7 @@
 #define SLQ_TC_CUH_
 
 #include <cstdint>
+#include <cuda.h>
 
 namespace slq {
 namespace tc {
@@ -82,6 +83,17 @@ __device__ __forceinline__ void st_x8(uint32_t taddr, const uint32_t (&v)[8])
     asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};"
                  ::"r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]),
                    "r"(v[6]), "r"(v[7])
+                 : "memory");
+}
+
+// 16 consecutive columns of this thread's lane.
+__device__ __forceinline__ void st_x16(uint32_t taddr, const uint32_t (&v)[16])
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, "
+                 "%9, %10, %11, %12, %13, %14, %15, %16};"
+                 ::"r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]),
+                   "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]),
+                   "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
                  : "memory");
 }
 
@@ -172,6 +184,38 @@ __device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo)
 __device__ __forceinline__ uint32_t kmajor_offset(int r, int k)
 {
     return static_cast<uint32_t>((r & 7) * 16 + (r >> 3) * 256 + (k >> 2) * 128 + (k & 3) * 4);
+}
+
+// Instruction descriptor, kind::tf32, D FP32, M = 128, A and B K-major, for
+// N a multiple of 16 in [16, 256] (N >> 3 in bits 17-22, M >> 4 in 24-28).
+__host__ __device__ constexpr uint32_t idesc_tf32_m128(uint32_t n)
+{
+    return 0x00000910u | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+// Shared-memory descriptor of a K-major tile written by a SWIZZLE_128B TMA
+// load (rows of 128 bytes = 32 TF32 values, 8-row atoms of 1024 bytes):
+// stride byte offset 1024, leading byte offset unused (1), version 1, layout
+// type SWIZZLE_128B (2 in bits 61-63).  The tile must start on a 1024-byte
+// boundary; a K step of 8 values inside the atom advances the start by 32
+// bytes.
+__device__ __forceinline__ uint64_t smem_desc_sw128(const void* p)
+{
+    const uint64_t start = (smem_addr(p) >> 4) & 0x3FFFu;
+    return start | (uint64_t(1) << 16) | (uint64_t(1024 >> 4) << 32) | (uint64_t(1) << 46) |
+           (uint64_t(2) << 61);
+}
+
+// 2-D tiled TMA load of box (x, y) .. into shared memory, completing on bar.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y),
+          "r"(smem_addr(bar))
+        : "memory");
 }
 
 }  // namespace tc

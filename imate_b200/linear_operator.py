@@ -224,8 +224,9 @@ class _DeviceOperator:
             raise RuntimeError("no CUDA device is available for the SLQ "
                                "engine (it has no CPU path)")
         self.device = torch.device("cuda", torch.cuda.current_device())
+        self.dense = False
         if A is None:
-            return  # from_device fills the fields
+            return  # from_device / from_dense fill the fields
         dev = self.device
         early = (A.format == "csr" and A.shape[0] == A.shape[1] and
                  A.has_sorted_indices and A.has_canonical_format and
@@ -331,6 +332,43 @@ class _DeviceOperator:
             self.inv[self.perm.long()] = torch.arange(
                 pm.numel(), dtype=torch.int32, device=self.device)
         self._create(fmt, affine, need_transpose, check_indices)
+        return self
+
+    @classmethod
+    def from_dense(cls, A, affine=False, need_transpose=False):
+        """Dense float32 operator over a host array A (row-major copy on the
+        device; ``slq_dense_operator_create``: TF32 parts of A, and of A^T
+        with ``need_transpose``, for the tensor-core product)."""
+        import torch
+        self = cls(None, affine, need_transpose)
+        A = np.ascontiguousarray(A, dtype=np.float32)
+        self.data = torch.from_numpy(A).to(self.device)
+        self.indices = None
+        self.indptr = None
+        self.dtype_code, self.np_dtype = _lib.SLQ_F32, np.dtype(np.float32)
+        self.shape = tuple(int(x) for x in A.shape)
+        self.nnz = int(A.size)
+        self.group_rows = 0
+        self.perm = None
+        self.inv = None
+        self.dense = True
+        lib = _lib.load()
+        nbytes = ctypes.c_size_t(0)
+        _lib.check(lib.slq_dense_operator_workspace_bytes(
+            self.shape[0], self.shape[1], _lib.SLQ_F32, int(need_transpose),
+            ctypes.byref(nbytes)))
+        self.workspace = torch.empty(max(int(nbytes.value), 256),
+                                     dtype=torch.uint8, device=self.device)
+        self.handle = ctypes.c_void_p(None)
+        stream = torch.cuda.current_stream(self.device)
+        _lib.check(lib.slq_dense_operator_create(
+            self.data.data_ptr(), self.shape[0], self.shape[1], _lib.SLQ_F32,
+            int(affine), int(need_transpose), self.workspace.data_ptr(),
+            self.workspace.numel(), stream.cuda_stream,
+            ctypes.byref(self.handle)))
+        self.affine = affine
+        self.has_transpose = bool(need_transpose)
+        self._lib = lib
         return self
 
     def _create(self, fmt, affine, need_transpose, check_indices):
@@ -440,6 +478,12 @@ class LinearOperator:
         op = self._device_ops.get(key)
         if op is None and not need_transpose:
             op = self._device_ops.get((dev, True))
+        if op is None and isinstance(self.A, np.ndarray) and \
+                self.A.dtype == np.float32 and self.A.ndim == 2:
+            # dense float32: tensor-core product (cuDenseMatrix's role)
+            op = _DeviceOperator.from_dense(self.A, self._affine(),
+                                            need_transpose)
+            self._device_ops[key] = op
         if op is None:
             A = self.A if sp.issparse(self.A) else sp.csr_matrix(self.A)
             op = _DeviceOperator(A, self._affine(), need_transpose,

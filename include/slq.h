@@ -175,6 +175,25 @@ slq_status slq_group_fill(int64_t n, const int32_t* indptr,
                           int group_rows, int64_t sample_groups,
                           double* fill);
 
+/* Dense FP32 operator (no counterpart in the reference's sparse path; it
+ * takes the role of cuDenseMatrix, imate/_cu_linear_operator/
+ * cu_dense_matrix.cu): A is num_rows x num_cols, row-major, in device
+ * memory.  Creation splits A (and, with need_transpose, A^T) into TF32
+ * hi/lo parts in the workspace; products run on the tensor cores
+ * (tcgen05 kind::tf32, three terms: ~FP32 accuracy) with the SpMM
+ * epilogue.  The workspace also holds the probe-block parts of one product,
+ * so an operator serves one product at a time (not two runs at once, and
+ * not batch plans); the tuner does not apply to it.  Float32 only. */
+slq_status slq_dense_operator_workspace_bytes(int64_t num_rows,
+                                              int64_t num_cols, int dtype,
+                                              int need_transpose,
+                                              size_t* bytes);
+slq_status slq_dense_operator_create(const void* data, int64_t num_rows,
+                                     int64_t num_cols, int dtype, int affine,
+                                     int need_transpose, void* workspace,
+                                     size_t workspace_bytes, void* stream,
+                                     slq_op** out);
+
 /* Release the host-side operator record (device arrays stay with their
  * owners).  Replaces the cuLinearOperator destructors
  * (imate/_cu_linear_operator/cu_csr_matrix.cu:95-154). */
