@@ -65,11 +65,14 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="c2prime",
-                    choices=["c2prime", "batched", "sweep", "gram-large"],
+                    choices=["c2prime", "batched", "sweep", "gram-large",
+                             "dense"],
                     help="c2prime: the headline line (default); batched: 64 "
                          "correlation matrices in one graph; sweep: 512-point "
                          "t-sweep by the surrogate; gram-large: logdet(X^T X "
-                         "+ lambda I) of an 8388608 x 2097152 sparse X")
+                         "+ lambda I) of an 8388608 x 2097152 sparse X; "
+                         "dense: logdet of a 16384 x 16384 dense correlation "
+                         "matrix by the tensor-core operator")
     ap.add_argument("--batch-count", type=int, default=64)
     ap.add_argument("--spmm", default="auto",
                     choices=["auto", "csr", "row-group", "row-group-tma",
@@ -184,12 +187,13 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def reference_gpu_sample(A, args, probes=8):
-    """The reference's own GPU SLQ (cuSPARSE SpMV, cuBLAS vector operations,
-    one probe at a time; oracle/_ref/libimate_ref_gpu.so compiled from its
-    sources for sm_100a) on a sample of the same workload, FP32 and FP64:
-    probe*steps/s over its own computation time, and over the whole call
-    (matrix upload included).  None without a GPU or the library."""
+def reference_gpu_sample(A, args, probes=8, path=None):
+    """The reference's own GPU SLQ (cuSPARSE SpMV -- cuBLAS gemv for a dense
+    ndarray -- and cuBLAS vector operations, one probe at a time;
+    oracle/_ref/libimate_ref_gpu.so compiled from its sources for sm_100a)
+    on a sample of the same workload, FP32 and FP64: probe*steps/s over its
+    own computation time, and over the whole call (matrix upload included).
+    None without a GPU or the library."""
     try:
         import torch
         if not torch.cuda.is_available():
@@ -214,9 +218,12 @@ def reference_gpu_sample(A, args, probes=8):
         out[name] = {"value": ps / max(r["alg_wall_time"], 1e-9),
                      "unit": UNIT, "e2e": ps / wall, "probes": probes,
                      "alg_wall_s": r["alg_wall_time"], "wall_s": wall,
-                     "estimate": float(r["trace"][0])}
-    out["path"] = ("imate cu_trace_estimator (cuSPARSE SpMV, cuBLAS), built "
-                   "from the reference sources for sm_100a, 1 GPU")
+                     "estimate": float(r["trace"][0]),
+                     "samples": [float(x) for x in r["samples"][:probes, 0]]}
+        del Ad
+    out["path"] = path or ("imate cu_trace_estimator (cuSPARSE SpMV, "
+                           "cuBLAS), built from the reference sources for "
+                           "sm_100a, 1 GPU")
     return out
 
 
@@ -793,6 +800,158 @@ def run_gram_large(args):
     print(json.dumps(line), flush=True)
 
 
+def run_dense(args):
+    """logdet of a dense SPD exponential-kernel correlation matrix: n = 16384
+    points uniform in the unit square (PCG64 seed 1), scale 0.02, every pair
+    kept, diagonal shift --shift; FP32 row-major on the host.  256 probes,
+    lanczos_degree 50, full reorthogonalisation.  The operator is the
+    tensor-core dense product (3-term TF32 split, FP32 accumulation)."""
+    import torch
+    import imate_b200 as ib
+    from imate_b200 import _lib
+    from imate_b200.sample_matrices import dense_correlation_matrix
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    n = 16384 if args.n == 262144 else args.n
+    t0 = time.perf_counter()
+    A32 = dense_correlation_matrix(n, scale=0.02, shift=args.shift, seed=1,
+                                   dtype="float32", device="cuda")
+    build_s = time.perf_counter() - t0
+    # FP64 oracle: dense Cholesky of the stored (float32) matrix in float64
+    L = torch.linalg.cholesky(torch.from_numpy(A32).to("cuda",
+                                                        torch.float64))
+    exact = float(2.0 * torch.log(torch.diagonal(L)).sum())
+    del L
+    torch.cuda.empty_cache()
+
+    Aop = ib.Matrix(A32)
+    Aop.get_device_operator()  # upload + TF32 split, outside the timing
+    eng = ib.EngineOptions(block_size=args.probes, rng="parity")
+    kw = dict(method="slq", gpu=True, return_info=True,
+              min_num_samples=args.probes, max_num_samples=args.probes,
+              error_rtol=0.0, lanczos_degree=args.degree,
+              orthogonalize=args.orthogonalize, seed=0)
+
+    def step(i):
+        eng.first_probe = i * args.probes
+        return ib.logdet(Aop, engine=eng, **kw)
+
+    for i in range(args.warmup):
+        step(i)
+    clocks = ClockSampler(local)
+    clocks.start()
+    _lib.profile_begin()
+    outs, elapsed = _timed(lambda i: step(args.warmup + i), args.steps)
+    kstats = _lib.profile_end()
+    clk = clocks.stop()
+    ps = sum(int(np.sum(info["engine"]["lanczos_size"][:args.probes]))
+             for _, info in outs)
+    launches = sum(int(info["engine"]["gpu_launches"]) for _, info in outs)
+    value = ps / elapsed
+    est = float(np.mean([float(tr) for tr, _ in outs]))
+
+    # tensor roofline of the dense product: useful 2 n^2 b flops per call,
+    # issued as three TF32 products; TF32 runs at half the bf16 rate
+    nl, ms, _ = kstats["spmm"]
+    per_call = ms / nl * 1e-3 if nl else float("nan")
+    useful = 2.0 * n * n * args.probes / per_call / 1e12
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            bf16 = float(json.load(f)["bf16_tflops"])
+        src = "measured bf16 burst / 2"
+    except (OSError, KeyError, ValueError):
+        bf16, src = 1590.0, "fallback bf16 burst / 2"
+    tf32_peak = bf16 / 2.0
+    # DRAM bytes per product from the committed ncu capture at n = 8192
+    # (traffic there equals the algorithmic bytes: A parts once, probe parts
+    # and Y once), scaled by the algorithmic bytes of this size
+    t8 = ncu_traffic("dense") if args.probes == 256 else None
+    alg = lambda m: 8.0 * m * m + 12.0 * m * args.probes  # noqa: E731
+    traffic = t8 * alg(n) / alg(8192) if t8 else None
+    line = {
+        "workload_kind": "dense", "metric": "dense SLQ logdet probe*steps/s "
+        "(tensor-core operator)", "value": value, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "dense SPD exponential-kernel correlation "
+                               "matrix (scale 0.02, diag shift %g), SLQ "
+                               "logdet" % args.shift, "n": n,
+                   "probes_per_step": args.probes,
+                   "lanczos_degree": args.degree,
+                   "orthogonalize": args.orthogonalize, "rng": "parity",
+                   "host_build_s": build_s,
+                   "l2": "inputs larger than L2 (split matrix %.1f GB)"
+                         % (8.0 * n * n / 1e9)},
+        "roofline": {"bound": "tensor", "kernel": "k_dense_tc (+ probe "
+                     "split)", "achieved": 3.0 * useful, "peak": tf32_peak,
+                     "unit": "TFLOP/s", "frac": 3.0 * useful / tf32_peak,
+                     "traffic": traffic, "peak_source": src,
+                     "traffic_note": "DRAM bytes per product: ncu at n = "
+                                     "8192 scaled by algorithmic bytes",
+                     "algorithmic_bytes_per_call": alg(n),
+                     "useful_tflops": useful, "ms_per_call": per_call * 1e3,
+                     "calls": nl,
+                     "share_of_kernel_time": ms / max(1e-12, sum(
+                         v[1] for v in kstats.values()))},
+        "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in
+                    kstats.items() if v[0]},
+        "gpu_launches": launches, "clocks": clk,
+        "accuracy": {"estimate_mean": est, "fp64_cholesky": exact,
+                     "rel_err_vs_oracle": abs(est - exact) / abs(exact),
+                     "probes_in_mean": args.probes * args.steps},
+    }
+    if not args.no_e2e:
+        h2d = A32.nbytes
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e_ps = 0
+        nsteps = max(1, min(args.steps, 3))
+        for i in range(nsteps):
+            fresh = ib.Matrix(A32)
+            eng.first_probe = i * args.probes
+            tr, info = ib.logdet(fresh, engine=eng, **kw)
+            e_ps += int(np.sum(info["engine"]["lanczos_size"][:args.probes]))
+            del fresh
+        torch.cuda.synchronize()
+        te = time.perf_counter() - t0
+        line["e2e"] = {"value": e_ps / te, "unit": UNIT,
+                       "h2d_bytes_per_step": int(h2d),
+                       "d2h_bytes_per_step": int(args.probes * 8 * 2),
+                       "steps": nsteps,
+                       "path": "imate_b200.logdet(numpy float32 array)"}
+    del Aop
+    torch.cuda.empty_cache()
+    if args.fp64_probes > 0:
+        nprb = args.fp64_probes
+        gpu_ref = reference_gpu_sample(
+            A32, args, probes=nprb,
+            path="imate cu_trace_estimator on cuDenseMatrix (cuBLAS gemv), "
+                 "built from the reference sources for sm_100a, 1 GPU")
+        if gpu_ref is not None:
+            # the same probes through this engine (parity stream, seed 0)
+            e8 = ib.EngineOptions(block_size=nprb, rng="parity")
+            _, info8 = ib.logdet(ib.Matrix(A32), engine=e8, **dict(
+                kw, min_num_samples=nprb, max_num_samples=nprb))
+            mine = np.asarray(info8["convergence"]["samples"][:nprb], float)
+            s64 = np.asarray(gpu_ref["f64"]["samples"], float)
+            gpu_ref["rel_diff_same_probes_vs_f64"] = float(
+                np.max(np.abs(mine - s64) / np.abs(s64)))
+            gpu_ref["speedup_vs_f64"] = value / gpu_ref["f64"]["value"]
+            gpu_ref["speedup_vs_f32"] = value / gpu_ref["f32"]["value"]
+            line["reference_gpu"] = gpu_ref
+    if not args.no_cpu_baseline:
+        threads = cpu_threads()
+        probes = min(threads, 64)
+        v, secs, kind = reference_sample(A32, args, probes, threads)
+        line["cpu_baseline"] = {
+            "value": v, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": "%d probes x %d steps, FP32 dense, full reorth, %.1f s"
+                      % (probes, args.degree, secs)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.workload != "c2prime":
@@ -802,7 +961,7 @@ def main():
                               "headline workload only"}), flush=True)
             return
         {"batched": run_batched, "sweep": run_sweep,
-         "gram-large": run_gram_large}[args.workload](args)
+         "gram-large": run_gram_large, "dense": run_dense}[args.workload](args)
         return
     if args.impl == "reference":
         run_reference_arm(args)

@@ -20,7 +20,7 @@ import scipy.sparse as sp
 __all__ = ["toeplitz", "toeplitz_logdet", "toeplitz_traceinv",
            "toeplitz_trace", "correlation_matrix", "correlation_points",
            "correlation_matrix_device", "batched_correlation_sizes",
-           "sparse_gram_design"]
+           "sparse_gram_design", "dense_correlation_matrix"]
 
 
 def toeplitz(a, b, size=20, gram=False, format="csr", dtype="float64"):
@@ -63,6 +63,42 @@ def toeplitz_traceinv(a, b, size, gram=False):
         return (1.0 / (a**2 - b**2)) * \
             (size - q**2 * ((q**(2.0 * size) - 1.0) / (q**2 - 1.0)))
     return (1.0 / (a**2 - b**2)) * (size - q**2 / (1.0 - q**2))
+
+
+def dense_correlation_matrix(size=None, dimension=2, scale=0.1, shift=1e-3,
+                             seed=1, points=None, dtype="float64",
+                             device=None):
+    """Dense exponential-kernel correlation matrix plus ``shift * I``, as
+    imate builds it for ``sparse=False``
+    (``imate/sample_matrices/_dense_correlation_matrix.pyx:41-150``):
+    K_ij = exp(-|x_i - x_j| / scale) for every pair, unit diagonal.
+
+    Returns a C-contiguous numpy array.  Distances and kernel values are
+    computed in float64 (on ``device`` with torch when given, in row blocks)
+    and cast to ``dtype`` at the end.
+    """
+    if points is None:
+        points = correlation_points(size, dimension, seed)
+    n = points.shape[0]
+    out = np.empty((n, n), dtype=dtype)
+    rows = max(1, (1 << 25) // max(n, 1))
+    if device is not None:
+        import torch
+        P = torch.as_tensor(points, dtype=torch.float64, device=device)
+        for r0 in range(0, n, rows):
+            D = torch.cdist(P[r0:r0 + rows], P,
+                            compute_mode="donot_use_mm_for_euclid_dist")
+            K = torch.exp(-D / scale)
+            out[r0:r0 + rows] = K.to(getattr(torch, np.dtype(dtype).name)) \
+                .cpu().numpy()
+    else:
+        for r0 in range(0, n, rows):
+            d = points[r0:r0 + rows, None, :] - points[None, :, :]
+            out[r0:r0 + rows] = np.exp(-np.sqrt(np.sum(d * d, axis=-1)) /
+                                       scale)
+    idx = np.arange(n)
+    out[idx, idx] = 1.0 + shift
+    return out
 
 
 def correlation_points(size, dimension=2, seed=1):

@@ -175,9 +175,9 @@ slq_status slq_group_fill(int64_t n, const int32_t* indptr,
                           int group_rows, int64_t sample_groups,
                           double* fill);
 
-/* Dense FP32 operator (no counterpart in the reference's sparse path; it
- * takes the role of cuDenseMatrix, imate/_cu_linear_operator/
- * cu_dense_matrix.cu): A is num_rows x num_cols, row-major, in device
+/* Dense FP32 operator (the role of cuDenseMatrix: construction and upload
+ * imate/_cu_linear_operator/cu_dense_matrix.cu:39-61 and :94-122, cuBLAS
+ * gemv products :130-238): A is num_rows x num_cols, row-major, in device
  * memory.  Creation splits A (and, with need_transpose, A^T) into TF32
  * hi/lo parts in the workspace; products run on the tensor cores
  * (tcgen05 kind::tf32, three terms: ~FP32 accuracy) with the SpMM

@@ -99,17 +99,22 @@ def gpu_trace_estimator(A, func, gram=False, exponent=1.0, min_num_samples=10,
                         outlier_significance_level=0.001, lanczos_degree=20,
                         lanczos_tol=None, orthogonalize=0, seed=0,
                         num_gpu_devices=1):
-    """Run the reference GPU estimator on a CSR matrix (one inquiry; ``func``
-    in {'log', 'inv', 'id'}).  Returns the same dict as
-    ``trace_estimator``."""
+    """Run the reference GPU estimator on a CSR matrix, or on a dense
+    ndarray (row-major, cuBLAS gemv products), for one inquiry (``func`` in
+    {'log', 'inv', 'id'}).  Returns the same dict as ``trace_estimator``."""
     import scipy.sparse as sp
     lib = load_gpu()
-    A = sp.csr_matrix(A)
-    A.sort_indices()
-    indices = np.ascontiguousarray(A.indices, dtype=np.int32)
-    indptr = np.ascontiguousarray(A.indptr, dtype=np.int32)
     dt = np.float64 if A.dtype == np.float64 else np.float32
-    data = np.ascontiguousarray(A.data, dtype=dt)
+    if isinstance(A, np.ndarray):
+        # dense row-major operator (cu_dense_matrix.cu)
+        data = np.ascontiguousarray(A, dtype=dt)
+        indices = indptr = None
+    else:
+        A = sp.csr_matrix(A)
+        A.sort_indices()
+        indices = np.ascontiguousarray(A.indices, dtype=np.int32)
+        indptr = np.ascontiguousarray(A.indptr, dtype=np.int32)
+        data = np.ascontiguousarray(A.data, dtype=dt)
     if lanczos_tol is None:
         lanczos_tol = float(np.finfo(dt).eps)
     trace = np.empty(1, dt)
@@ -130,7 +135,9 @@ def gpu_trace_estimator(A, func, gram=False, exponent=1.0, min_num_samples=10,
     fn.argtypes = [vp, vp, vp, i64, i64, i32, i32, real, i32, i64, i32, real,
                    i32, i32, real, real, real, real, i32, vp, vp, vp, vp, vp,
                    vp, vp, ctypes.POINTER(ctypes.c_float)]
-    allc = fn(_p(data), _p(indices), _p(indptr), A.shape[0], A.shape[1], fid,
+    allc = fn(_p(data), _p(indices) if indices is not None else None,
+              _p(indptr) if indptr is not None else None, A.shape[0],
+              A.shape[1], fid,
               int(gram), exponent, orthogonalize, seed, lanczos_degree,
               lanczos_tol, min_num_samples, max_num_samples, error_atol,
               error_rtol, confidence_level, outlier_significance_level,
@@ -148,7 +155,12 @@ def _p(a):
 
 
 def _csr_parts(A):
+    """(A, fmt, indices, indptr): fmt 0 = CSR, 1 = CSC, 2 = dense row-major
+    ndarray (no index arrays)."""
     import scipy.sparse as sp
+    if isinstance(A, np.ndarray):
+        empty = np.zeros(1, np.int32)
+        return np.ascontiguousarray(A), 2, empty, empty
     fmt = 1 if sp.isspmatrix_csc(A) or getattr(A, "format", "") == "csc" else 0
     if fmt == 0:
         A = sp.csr_matrix(A)
@@ -174,7 +186,7 @@ def trace_estimator(A, func, gram=False, exponent=1.0, parameters=None,
     lib = load()
     A, fmt, indices, indptr = _csr_parts(A)
     dt = np.float64 if A.dtype == np.float64 else np.float32
-    data = np.ascontiguousarray(A.data, dtype=dt)
+    data = np.ascontiguousarray(A if fmt == 2 else A.data, dtype=dt)
     affine = parameters is not None
     params = np.atleast_1d(np.asarray(
         parameters if affine else [0.0], dtype=dt)).copy()
@@ -287,7 +299,7 @@ def krylov(A, v, m, gram=False, orthogonalize=0, tol=None, t=None):
     """Per-probe alpha/beta of the reference Lanczos / Golub-Kahn (FP64)."""
     lib = load()
     A, fmt, indices, indptr = _csr_parts(A)
-    data = np.ascontiguousarray(A.data, dtype=np.float64)
+    data = np.ascontiguousarray(A if fmt == 2 else A.data, dtype=np.float64)
     v = np.ascontiguousarray(v, dtype=np.float64)
     alpha = np.zeros(m, np.float64)
     beta = np.zeros(m, np.float64)

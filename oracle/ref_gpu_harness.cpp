@@ -17,6 +17,7 @@
 
 #include "_definitions/types.h"
 #include "_cu_linear_operator/cu_csr_matrix.h"
+#include "_cu_linear_operator/cu_dense_matrix.h"
 #include "_cu_trace_estimator/cu_trace_estimator.h"
 #include "functions/functions.h"
 #include "functions/logarithm.h"
@@ -35,6 +36,8 @@ Function* gpu_function(int func_id)
     }
 }
 
+// indices == NULL selects the dense row-major operator (cu_dense_matrix.cu:
+// 40-61, cuBLAS gemv per product) over `data`; otherwise the CSR operator.
 template <typename T>
 int run_gpu_trace_estimator(
         const T* data, const int* indices, const int* indptr, int64_t num_rows,
@@ -46,10 +49,15 @@ int run_gpu_trace_estimator(
         int* num_samples_used, int* num_outliers, int* converged,
         float* alg_wall_time)
 {
-    const LongIndexType* ind = reinterpret_cast<const LongIndexType*>(indices);
-    const LongIndexType* ptr = reinterpret_cast<const LongIndexType*>(indptr);
-    cuCSRMatrix<T>* A = new cuCSRMatrix<T>(data, ind, ptr, num_rows, num_cols,
-                                           num_gpu_devices);
+    cuLinearOperator<T>* A;
+    if (indices)
+        A = new cuCSRMatrix<T>(
+                data, reinterpret_cast<const LongIndexType*>(indices),
+                reinterpret_cast<const LongIndexType*>(indptr), num_rows,
+                num_cols, num_gpu_devices);
+    else
+        A = new cuDenseMatrix<T>(data, num_rows, num_cols, 1,
+                                 num_gpu_devices);
     Function* f = gpu_function(func_id);
     T** rows = new T*[max_num_samples];
     for (int i = 0; i < max_num_samples; ++i)
@@ -87,8 +95,9 @@ int ref_gpu_device_count(void)
     return n;
 }
 
-// The reference GPU estimator on a CSR matrix (one inquiry, func_id 0 = log,
-// 1 = inv, 2 = identity).
+// The reference GPU estimator on a CSR matrix, or on a dense row-major one
+// when indices and indptr are NULL (one inquiry, func_id 0 = log, 1 = inv,
+// 2 = identity).
 int ref_gpu_trace_estimator_f64(
         const double* data, const int* indices, const int* indptr,
         int64_t num_rows, int64_t num_cols, int func_id, int gram,

@@ -21,6 +21,8 @@
 #include "_c_linear_operator/c_csc_matrix.h"
 #include "_c_linear_operator/c_csr_affine_matrix_function.h"
 #include "_c_linear_operator/c_csc_affine_matrix_function.h"
+#include "_c_linear_operator/c_dense_matrix.h"
+#include "_c_linear_operator/c_dense_affine_matrix_function.h"
 #include "_c_trace_estimator/c_trace_estimator.h"
 #include "_c_trace_estimator/c_lanczos_tridiagonalization.h"
 #include "_c_trace_estimator/c_golub_kahn_bidiagonalization.h"
@@ -99,12 +101,20 @@ int ref_set_lapack(void* dstev, void* sstev, void* dbdsdc, void* sbdsdc)
 // helpers
 // ---------------------------------------------------------------------------
 
-// fmt: 0 = CSR, 1 = CSC.  shift_given: build A + t I operator (B = I).
+// fmt: 0 = CSR, 1 = CSC, 2 = dense row-major (data only; c_dense_matrix.cpp
+// and c_dense_affine_matrix_function.cpp).  affine: the A + t I operator.
 template <typename T>
 static cLinearOperator<T>* make_operator(
         const T* data, const int* indices, const int* indptr,
         int64_t num_rows, int64_t num_cols, int fmt, int affine)
 {
+    if (fmt == 2)
+    {
+        if (affine)
+            return new cDenseAffineMatrixFunction<T>(data, 1, num_rows,
+                                                     num_cols);
+        return new cDenseMatrix<T>(data, num_rows, num_cols, 1);
+    }
     const LongIndexType* ind = reinterpret_cast<const LongIndexType*>(indices);
     const LongIndexType* ptr = reinterpret_cast<const LongIndexType*>(indptr);
     if (fmt == 0)
@@ -250,8 +260,8 @@ int ref_trace_estimator_b_f64(
             num_outliers, converged, alg_wall_time);
 }
 
-// Full reference estimator (c_trace_estimator.cpp:192-307) on a CSR/CSC
-// matrix, or on A + t I when affine != 0.
+// Full reference estimator (c_trace_estimator.cpp:192-307) on a CSR, CSC or
+// dense row-major matrix, or on A + t I when affine != 0.
 int ref_trace_estimator_f64(
         const double* data, const int* indices, const int* indptr,
         int64_t num_rows, int64_t num_cols, int fmt, int affine,

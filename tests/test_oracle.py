@@ -183,6 +183,44 @@ def test_oracle_matches_reference_library(corr_small):
         assert np.array_equal(a["num_samples_used"], b["num_samples_used"])
 
 
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+def test_reference_dense_operator_matches_csr():
+    """The reference's dense row-major operator (cDenseMatrix,
+    cDenseAffineMatrixFunction) gives the CSR operator's samples on the same
+    matrix; the oracle matches it on the dense matrix too."""
+    import scipy.sparse as sp
+    from imate_b200.sample_matrices import dense_correlation_matrix
+    A = dense_correlation_matrix(200, scale=0.05, shift=0.1, seed=5)
+    kw = dict(min_num_samples=10, max_num_samples=10, error_rtol=0.0,
+              lanczos_degree=20, orthogonalize=-1, seed=7)
+    d = ref.trace_estimator(A, "log", **kw)
+    c = ref.trace_estimator(sp.csr_matrix(A), "log", **kw)
+    assert rel(d["samples"], c["samples"]) < 1e-12
+    d = ref.trace_estimator(A, "inv", parameters=[0.3, 2.0], **kw)
+    c = ref.trace_estimator(sp.csr_matrix(A), "inv", parameters=[0.3, 2.0],
+                            **kw)
+    assert rel(d["samples"], c["samples"]) < 1e-12
+    o = oracle.trace_estimator(sp.csr_matrix(A), func="log", **kw)
+    assert rel(o["samples"], ref.trace_estimator(A, "log", **kw)["samples"]) \
+        < 1e-10
+
+
+def test_dense_correlation_matrix_builders_agree():
+    """The torch (row-block) and numpy paths of the dense correlation
+    builder give the same matrix; it is symmetric with the shifted unit
+    diagonal."""
+    from imate_b200.sample_matrices import dense_correlation_matrix
+    a = dense_correlation_matrix(300, scale=0.03, shift=0.2, seed=2)
+    b = dense_correlation_matrix(300, scale=0.03, shift=0.2, seed=2,
+                                 device="cpu")
+    assert np.max(np.abs(a - b)) < 1e-14
+    assert np.array_equal(a, a.T)
+    assert np.all(np.diag(a) == 1.2)
+    pts = np.random.default_rng(2).random((300, 2))
+    r = np.linalg.norm(pts[3] - pts[17])
+    assert abs(a[3, 17] - np.exp(-r / 0.03)) < 1e-15
+
+
 def test_erfinv():
     from math import erf, sqrt
     for x in (0.0, 0.1, 0.5, 0.9, 0.95, 0.99, 0.999, -0.7):
