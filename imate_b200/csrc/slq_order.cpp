@@ -29,6 +29,7 @@
 #include <atomic>
 #include <cmath>
 #include <condition_variable>
+#include <cstring>
 #include <cstdint>
 #include <functional>
 #include <mutex>
@@ -126,6 +127,20 @@ class Pool
     std::atomic<int> pending_{0};
     std::atomic<bool> stop_{false};
 };
+
+// The pool every entry point uses, created on first use and kept for the
+// life of the process (its workers block when idle); one job at a time.
+Pool& shared_pool()
+{
+    static Pool* pool = new Pool(host_threads());
+    return *pool;
+}
+
+std::mutex& pool_mutex()
+{
+    static std::mutex m;
+    return m;
+}
 
 // [begin, end) of part t of n of a range of `total` items
 inline void part_range(int64_t total, int t, int n, int64_t& begin, int64_t& end)
@@ -288,15 +303,15 @@ void cm_order(int64_t n, const int32_t* indptr, const int32_t* indices, std::vec
 // row-group aggregation
 // ---------------------------------------------------------------------------
 
-struct Cand {
-    double w;
-    int32_t row;
-};
-
-// a is stronger than b: larger |a_ij|, then the smaller row index
-bool stronger(const Cand& a, const Cand& b)
+// Candidate strength as one integer: |a_ij| rounded to float (the bits of a
+// non-negative float order like its value) above, the complement of the row
+// below, so that a larger key is a larger |a_ij|, then a smaller row.
+inline uint64_t strength_key(float a, int32_t row)
 {
-    return a.w > b.w || (a.w == b.w && a.row < b.row);
+    uint32_t bits;
+    const float m = std::fabs(a);
+    std::memcpy(&bits, &m, sizeof(bits));
+    return (static_cast<uint64_t>(bits) << 32) | static_cast<uint32_t>(~static_cast<uint32_t>(row));
 }
 
 // Groups found by one sweep: their rows (G each, the last possibly fewer)
@@ -307,30 +322,31 @@ struct Groups {
 };
 
 // One sweep over the seeds at base positions k0, k0 + step, ... (step +1 or
-// -1, stopping before `stop`); rows at base positions in [lo, hi) may join.
-// A group whose neighbourhood runs out is filled with the next unplaced rows
-// of the sweep.
+// -1, stopping before `stop`); a row may join while state[row] == me (the
+// rows this sweep owns and has not placed yet; placing stores 0).  A
+// group's seed takes its `want` strongest joinable neighbours (selected by
+// strength_key), then theirs, and a group whose neighbourhood runs out is
+// filled with the next unplaced rows of the sweep.  The other sweep's rows
+// are read, never written, so `state` is relaxed atomics.
 template <typename VT>
 void aggregate_sweep(const int32_t* indptr, const int32_t* indices, const VT* data, int G,
-                     const int32_t* base, const int32_t* base_pos, int64_t k0, int64_t stop,
-                     int step, int64_t lo, int64_t hi, uint8_t* placed, Groups& out)
+                     const int32_t* base, int64_t k0, int64_t stop, int step, uint8_t me,
+                     std::atomic<uint8_t>* state, Groups& out)
 {
     auto row_at = [&](int64_t k) { return base ? base[k] : static_cast<int32_t>(k); };
-    auto owned = [&](int32_t r) {
-        const int64_t p = base_pos ? base_pos[r] : r;
-        return p >= lo && p < hi;
-    };
+    auto mine = [&](int32_t r) { return state[r].load(std::memory_order_relaxed) == me; };
+    auto take = [&](int32_t r) { state[r].store(0, std::memory_order_relaxed); };
     std::vector<int32_t> group, frontier, next;
-    std::vector<Cand> best;
+    std::vector<uint64_t> keys;
     group.reserve(G);
     int64_t fill_cursor = k0;  // next sweep position for the fallback
     for (int64_t k = k0; k != stop; k += step)
     {
         const int32_t seed = row_at(k);
-        if (placed[seed]) continue;
+        if (!mine(seed)) continue;
         group.clear();
         group.push_back(seed);
-        placed[seed] = 1;
+        take(seed);
         frontier.assign(1, seed);
         while (static_cast<int>(group.size()) < G && !frontier.empty())
         {
@@ -339,45 +355,42 @@ void aggregate_sweep(const int32_t* indptr, const int32_t* indices, const VT* da
             {
                 const int want = G - static_cast<int>(group.size());
                 if (want <= 0) break;
-                // the `want` strongest unplaced neighbours of f: a heap whose
-                // front is the weakest kept candidate
-                best.clear();
-                for (int32_t e = indptr[f]; e < indptr[f + 1]; ++e)
+                // every unplaced row of this sweep among f's neighbours, then
+                // the `want` strongest of them
+                const int32_t e0 = indptr[f], e1 = indptr[f + 1];
+                keys.resize(static_cast<size_t>(e1 - e0));
+                int m = 0;
+                for (int32_t e = e0; e < e1; ++e)
                 {
                     const int32_t c = indices[e];
-                    if (placed[c] || !owned(c)) continue;
-                    const double w = data ? std::fabs(static_cast<double>(data[e])) : 1.0;
-                    const Cand cand{w, c};
-                    if (static_cast<int>(best.size()) < want)
-                    {
-                        best.push_back(cand);
-                        std::push_heap(best.begin(), best.end(), stronger);
-                    }
-                    else if (stronger(cand, best.front()))
-                    {
-                        std::pop_heap(best.begin(), best.end(), stronger);
-                        best.back() = cand;
-                        std::push_heap(best.begin(), best.end(), stronger);
-                    }
+                    keys[m] = strength_key(data ? static_cast<float>(data[e]) : 1.0f, c);
+                    m += mine(c) ? 1 : 0;
                 }
-                std::sort(best.begin(), best.end(), stronger);
-                for (const Cand& bc : best)
+                keys.resize(static_cast<size_t>(m));
+                if (m > want)
                 {
-                    // a row that f lists twice joins once
-                    if (placed[bc.row]) continue;
-                    placed[bc.row] = 1;
-                    group.push_back(bc.row);
-                    next.push_back(bc.row);
+                    std::nth_element(keys.begin(), keys.begin() + want, keys.end(),
+                                     std::greater<uint64_t>());
+                    keys.resize(static_cast<size_t>(want));
+                }
+                std::sort(keys.begin(), keys.end(), std::greater<uint64_t>());
+                for (uint64_t key : keys)
+                {
+                    const int32_t r = static_cast<int32_t>(~static_cast<uint32_t>(key));
+                    if (!mine(r)) continue;  // a row that f lists twice joins once
+                    take(r);
+                    group.push_back(r);
+                    next.push_back(r);
                 }
             }
             frontier.swap(next);
         }
         while (static_cast<int>(group.size()) < G)
         {
-            while (fill_cursor != stop && placed[row_at(fill_cursor)]) fill_cursor += step;
+            while (fill_cursor != stop && !mine(row_at(fill_cursor))) fill_cursor += step;
             if (fill_cursor == stop) break;
             const int32_t r = row_at(fill_cursor);
-            placed[r] = 1;
+            take(r);
             group.push_back(r);
         }
         out.rows.insert(out.rows.end(), group.begin(), group.end());
@@ -395,24 +408,34 @@ template <typename VT>
 void aggregate(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices, const VT* data,
                int G, const int32_t* base, const int32_t* base_pos, int32_t* order)
 {
-    std::vector<uint8_t> placed(static_cast<size_t>(n), 0);
+    // state[r]: the sweep that owns unplaced row r (1 or 2), 0 once placed
+    std::vector<std::atomic<uint8_t>> state(static_cast<size_t>(n));
     Groups sweep[2];
     if (n >= 2 * 16384 && P.size() >= 2)
     {
         const int64_t mid = n / 2;
+        P.run([&](int t, int nt) {
+            int64_t b, e;
+            part_range(n, t, nt, b, e);
+            for (int64_t r = b; r < e; ++r)
+            {
+                const int64_t p = base_pos ? base_pos[r] : r;
+                state[r].store(p < mid ? 1 : 2, std::memory_order_relaxed);
+            }
+        });
         P.run([&](int t, int) {
             if (t == 0)
-                aggregate_sweep<VT>(indptr, indices, data, G, base, base_pos, mid - 1, -1, -1, 0,
-                                    mid, placed.data(), sweep[0]);
+                aggregate_sweep<VT>(indptr, indices, data, G, base, mid - 1, -1, -1, 1,
+                                    state.data(), sweep[0]);
             else if (t == 1)
-                aggregate_sweep<VT>(indptr, indices, data, G, base, base_pos, mid, n, 1, mid, n,
-                                    placed.data(), sweep[1]);
+                aggregate_sweep<VT>(indptr, indices, data, G, base, mid, n, 1, 2, state.data(),
+                                    sweep[1]);
         });
     }
     else
     {
-        aggregate_sweep<VT>(indptr, indices, data, G, base, base_pos, 0, n, 1, 0, n,
-                            placed.data(), sweep[1]);
+        for (int64_t r = 0; r < n; ++r) state[r].store(2, std::memory_order_relaxed);
+        aggregate_sweep<VT>(indptr, indices, data, G, base, 0, n, 1, 2, state.data(), sweep[1]);
     }
     struct Ref {
         int64_t seed_pos;
@@ -452,7 +475,8 @@ extern "C" slq_status slq_rcm_order(int64_t n, const int32_t* indptr, const int3
         slq::set_error("rcm_order: bad arguments");
         return SLQ_ERR_BAD_ARG;
     }
-    Pool P(host_threads());
+    std::lock_guard<std::mutex> lock(pool_mutex());
+    Pool& P = shared_pool();
     if (!valid_pattern(P, n, indptr, indices, "rcm_order")) return SLQ_ERR_BAD_CSR;
     std::vector<int32_t> out;
     cm_order(n, indptr, indices, out);
@@ -470,7 +494,8 @@ extern "C" slq_status slq_group_order(int64_t n, const int32_t* indptr, const in
         slq::set_error("group_order: bad arguments");
         return SLQ_ERR_BAD_ARG;
     }
-    Pool P(host_threads());
+    std::lock_guard<std::mutex> lock(pool_mutex());
+    Pool& P = shared_pool();
     if (!valid_pattern(P, n, indptr, indices, "group_order")) return SLQ_ERR_BAD_CSR;
     std::vector<int32_t> base_pos;
     if (base_order && !inverse_perm(n, base_order, base_pos))
@@ -505,22 +530,24 @@ extern "C" slq_status slq_order_spread(int64_t n, const int32_t* indptr, const i
     *spread = 0.0;
     if (n == 0) return SLQ_OK;
     const std::vector<int64_t> rows = sample_positions(n - 1, std::min(n, sample_rows));
-    for (int64_t r : rows)
-        if (!valid_row(n, indptr, indices, r))
-        {
-            slq::set_error("order_spread: bad CSR pattern");
-            return SLQ_ERR_BAD_CSR;
-        }
-    // per-row sums in parallel, added in row order (thread-count independent)
+    // per-row sums in parallel (each sampled row checked first), added in
+    // row order (thread-count independent)
     const int64_t m = static_cast<int64_t>(rows.size());
     std::vector<double> row_sum(static_cast<size_t>(m), 0.0);
-    Pool P(host_threads());
+    std::atomic<bool> bad(false);
+    std::lock_guard<std::mutex> lock(pool_mutex());
+    Pool& P = shared_pool();
     P.run([&](int t, int nt) {
         int64_t b, e;
         part_range(m, t, nt, b, e);
         for (int64_t i = b; i < e; ++i)
         {
             const int64_t r = rows[i];
+            if (!valid_row(n, indptr, indices, r))
+            {
+                bad.store(true, std::memory_order_relaxed);
+                return;
+            }
             double sum = 0.0;
             for (int32_t x = indptr[r]; x < indptr[r + 1]; ++x)
             {
@@ -531,6 +558,11 @@ extern "C" slq_status slq_order_spread(int64_t n, const int32_t* indptr, const i
             row_sum[i] = sum;
         }
     });
+    if (bad.load())
+    {
+        slq::set_error("order_spread: bad CSR pattern");
+        return SLQ_ERR_BAD_CSR;
+    }
     double sum = 0.0;
     int64_t count = 0;
     for (int64_t i = 0; i < m; ++i)
@@ -557,21 +589,13 @@ extern "C" slq_status slq_group_fill(int64_t n, const int32_t* indptr, const int
     if (ngroups == 0) return SLQ_OK;
     const std::vector<int64_t> picks =
         sample_positions(ngroups - 1, std::min(sample_groups, ngroups));
-    for (int64_t p : picks)
-        for (int g = 0; g < G; ++g)
-        {
-            const int64_t k = p * G + g;
-            const int32_t r = order ? order[k] : static_cast<int32_t>(k);
-            if (r < 0 || r >= n || !valid_row(n, indptr, indices, r))
-            {
-                slq::set_error("group_fill: bad CSR pattern or order");
-                return SLQ_ERR_BAD_CSR;
-            }
-        }
-    // per-group fills in parallel, averaged in group order
+    // per-group fills in parallel (each sampled row checked first), averaged
+    // in group order
     const int64_t m = static_cast<int64_t>(picks.size());
     std::vector<double> ratio(static_cast<size_t>(m), -1.0);  // < 0: no entries
-    Pool P(host_threads());
+    std::atomic<bool> bad(false);
+    std::lock_guard<std::mutex> lock(pool_mutex());
+    Pool& P = shared_pool();
     P.run([&](int t, int nt) {
         int64_t b, e;
         part_range(m, t, nt, b, e);
@@ -583,6 +607,11 @@ extern "C" slq_status slq_group_fill(int64_t n, const int32_t* indptr, const int
             {
                 const int64_t k = picks[i] * G + g;
                 const int32_t r = order ? order[k] : static_cast<int32_t>(k);
+                if (r < 0 || r >= n || !valid_row(n, indptr, indices, r))
+                {
+                    bad.store(true, std::memory_order_relaxed);
+                    return;
+                }
                 cols.insert(cols.end(), indices + indptr[r], indices + indptr[r + 1]);
             }
             if (cols.empty()) continue;
@@ -592,6 +621,11 @@ extern "C" slq_status slq_group_fill(int64_t n, const int32_t* indptr, const int
             ratio[i] = static_cast<double>(nnz) / (static_cast<double>(G) * static_cast<double>(uni));
         }
     });
+    if (bad.load())
+    {
+        slq::set_error("group_fill: bad CSR pattern or order");
+        return SLQ_ERR_BAD_CSR;
+    }
     double sum = 0.0;
     int64_t ok = 0;
     for (int64_t i = 0; i < m; ++i)
