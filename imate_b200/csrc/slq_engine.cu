@@ -223,8 +223,11 @@ struct slq_op {
     const void* t_gval = nullptr;
     // dense FP32 operator (tensor-core product): TF32 parts of A, [nrows][ldk],
     // and of A^T, [ncols][ldk_t], K-major with zero-padded pitches; the
-    // probe-block parts scratch [256][ldx]; TMA maps of the A parts
+    // probe-block parts scratch [256][ldx]; running totals of split products
+    // (dense_ksplit of the SM count at creation); TMA maps of the A parts
     int dense = 0;
+    float* d_acc = nullptr;
+    int dense_sms = 0;
     float* d_hi = nullptr;
     float* d_lo = nullptr;
     float* dt_hi = nullptr;
@@ -787,12 +790,25 @@ slq_status row_map(CUtensorMap* m, const float* base, int64_t rows, int b)
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
 struct DenseBufs {
-    float *hi, *lo, *t_hi, *t_lo, *x_hi, *x_lo;
+    float *hi, *lo, *t_hi, *t_lo, *x_hi, *x_lo, *acc;
     int32_t* error;
     int64_t ldk, ldk_t, ldx;
 };
 
-void dense_layout(Carver& c, int64_t rows, int64_t cols, int need_transpose, DenseBufs* d)
+// K parts per 128-row tile of an M x K dense product: when the row tiles
+// fill at most half of the SMs, each tile's K range is split (on
+// accumulation-chunk boundaries, at most 8 parts) so that more SMs work;
+// the parts' FP32 totals are added by k_dense_epi.
+int dense_ksplit(int64_t M, int64_t K, int sms)
+{
+    const int64_t ntm = (M + 127) / 128;
+    const int64_t nch = ((K + DT_BK - 1) / DT_BK + DT_CHUNK - 1) / DT_CHUNK;
+    if (ntm * 2 > sms) return 1;
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({8, sms / ntm, nch})));
+}
+
+void dense_layout(Carver& c, int64_t rows, int64_t cols, int need_transpose, int sms,
+                  DenseBufs* d)
 {
     d->ldk = round_up(std::max<int64_t>(cols, 1), DT_BK);
     d->ldk_t = need_transpose ? round_up(std::max<int64_t>(rows, 1), DT_BK) : 0;
@@ -803,6 +819,11 @@ void dense_layout(Carver& c, int64_t rows, int64_t cols, int need_transpose, Den
     d->t_lo = need_transpose ? c.take<float>(static_cast<size_t>(cols) * d->ldk_t) : nullptr;
     d->x_hi = c.take<float>(static_cast<size_t>(256) * d->ldx);
     d->x_lo = c.take<float>(static_cast<size_t>(256) * d->ldx);
+    // running totals of split products, for either direction
+    int64_t acc_rows = dense_ksplit(rows, cols, sms) > 1 ? dense_ksplit(rows, cols, sms) * rows : 0;
+    if (need_transpose && dense_ksplit(cols, rows, sms) > 1)
+        acc_rows = std::max<int64_t>(acc_rows, dense_ksplit(cols, rows, sms) * cols);
+    d->acc = acc_rows ? c.take<float>(static_cast<size_t>(acc_rows) * 256) : nullptr;
     d->error = c.take<int32_t>(1);
 }
 
@@ -854,6 +875,9 @@ slq_status dense_spmm(Launcher& L, const slq_op* op, int transpose, int b, const
     const CUtensorMap& ahi = transpose ? op->map_t_hi : op->map_hi;
     const CUtensorMap& alo = transpose ? op->map_t_lo : op->map_lo;
     const int64_t ntm = (M + 127) / 128;
+    // split K when the row tiles leave most SMs idle (the same choice as the
+    // scratch was sized for)
+    const int ksplit = op->d_acc ? dense_ksplit(M, K, op->dense_sms) : 1;
     static bool attr = false;
     if (!attr)
     {
@@ -867,6 +891,9 @@ slq_status dense_spmm(Launcher& L, const slq_op* op, int transpose, int b, const
     // all columns): the first chunk's, which has the most tiles; a CTA
     // without a tile writes zero partials
     int grid_all = 0;
+    // the split products' epilogue: one block per 32 rows, at most 2 per SM
+    const int epi_grid = static_cast<int>(
+        std::max<int64_t>(1, std::min<int64_t>((M + 31) / 32, 2 * static_cast<int64_t>(L.sms))));
     for (int p_off = 0; p_off < b; p_off += 256)
     {
         const int nb = std::min(256, b - p_off);
@@ -877,7 +904,7 @@ slq_status dense_spmm(Launcher& L, const slq_op* op, int transpose, int b, const
         const int ntn = 1;
         if (grid_all == 0)
             grid_all = static_cast<int>(
-                std::max<int64_t>(1, std::min<int64_t>(ntm * ntn, L.sms)));
+                std::max<int64_t>(1, std::min<int64_t>(ntm * ntn * ksplit, L.sms)));
         const int grid = grid_all;
         dim3 tg(static_cast<unsigned>((K + 31) / 32), static_cast<unsigned>((nb + 31) / 32));
         k_split_transpose<<<tg, dim3(32, 8), 0, L.st>>>(X, K, b, p_off, nb, op->ldx, op->xt_hi,
@@ -909,11 +936,19 @@ slq_status dense_spmm(Launcher& L, const slq_op* op, int transpose, int b, const
         d.epi = epi;
         d.partials = partials;
         d.error = error ? error : op->d_error;
+        d.ksplit = ksplit;
+        d.acc = op->d_acc;
         k_dense_tc<<<grid, DT_THREADS, dense_smem(NB), L.st>>>(ahi, alo, xhi, xlo, d);
         SLQ_LAUNCH_CK();
         ++L.launches;
+        if (ksplit > 1)
+        {
+            k_dense_epi<<<epi_grid, 256, 0, L.st>>>(d);
+            SLQ_LAUNCH_CK();
+            ++L.launches;
+        }
     }
-    *grid_out = grid_all;
+    *grid_out = ksplit > 1 ? epi_grid : grid_all;
     return SLQ_OK;
 }
 
@@ -2643,9 +2678,11 @@ extern "C" slq_status slq_dense_operator_workspace_bytes(int64_t num_rows, int64
         return fail(SLQ_ERR_BAD_ARG, "dense_operator: bad size");
     if (dtype != SLQ_F32)
         return fail(SLQ_ERR_BAD_ARG, "dense_operator: float32 data only");
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
     Carver c(nullptr, 0);
     DenseBufs d;
-    dense_layout(c, num_rows, num_cols, need_transpose, &d);
+    dense_layout(c, num_rows, num_cols, need_transpose, sms, &d);
     *bytes = c.off + 256;
     return SLQ_OK;
 }
@@ -2666,13 +2703,13 @@ extern "C" slq_status slq_dense_operator_create(const void* data, int64_t num_ro
     if (affine && num_rows != num_cols)
         return fail(SLQ_ERR_BAD_ARG, "dense_operator: A + t I needs a square A");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    Carver c(workspace, workspace_bytes);
-    DenseBufs d;
-    dense_layout(c, num_rows, num_cols, need_transpose, &d);
-    // zero padding, then the parts
-    SLQ_CK(cudaMemsetAsync(workspace, 0, c.off, st));
     int sms = 0;
     SLQ_TRY(device_sms(&sms));
+    Carver c(workspace, workspace_bytes);
+    DenseBufs d;
+    dense_layout(c, num_rows, num_cols, need_transpose, sms, &d);
+    // zero padding, then the parts
+    SLQ_CK(cudaMemsetAsync(workspace, 0, c.off, st));
     const float* A = static_cast<const float*>(data);
     k_split_rows<<<sms * 8, 256, 0, st>>>(A, num_rows, num_cols, num_cols, d.ldk, d.hi, d.lo);
     SLQ_LAUNCH_CK();
@@ -2700,6 +2737,8 @@ extern "C" slq_status slq_dense_operator_create(const void* data, int64_t num_ro
     op->ldx = d.ldx;
     op->xt_hi = d.x_hi;
     op->xt_lo = d.x_lo;
+    op->d_acc = d.acc;
+    op->dense_sms = sms;
     op->d_error = d.error;
     slq_status s = part_map(&op->map_hi, d.hi, d.ldk, num_rows, 128);
     if (s == SLQ_OK) s = part_map(&op->map_lo, d.lo, d.ldk, num_rows, 128);

@@ -218,6 +218,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
+// L2 prefetch of one box of a 2-D tiled tensor map (no completion to wait
+// on; coordinates as tma_load_2d)
+__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];"
+                 ::"l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y)
+                 : "memory");
+}
+
 }  // namespace tc
 }  // namespace slq
 

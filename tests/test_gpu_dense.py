@@ -16,8 +16,12 @@ def _err(y, ref):
     return float(np.max(np.abs(y - ref)) / np.max(np.abs(ref)))
 
 
+# products of fewer than 75 row tiles split K over the idle SMs (up to 8
+# parts, added by k_dense_epi): (10000, 600) runs unsplit one way and split
+# the other; (129, 20000) splits 8 ways
 @pytest.mark.parametrize("rows,cols", [(1000, 1000), (300, 700), (129, 33),
-                                       (4096, 4096)])
+                                       (4096, 4096), (10000, 600),
+                                       (129, 20000)])
 @pytest.mark.parametrize("width", [1, 16, 100, 256, 300])
 def test_dense_product_matches_fp64(cuda, rows, cols, width):
     import torch
@@ -99,3 +103,18 @@ def test_dense_wide_block_partials(cuda):
     s32 = np.asarray(i32["convergence"]["samples"], float)
     s64 = np.asarray(i64["convergence"]["samples"], float)
     assert np.max(np.abs(s32 - s64) / np.abs(s64)) < 1e-5
+
+
+def test_dense_split_products_are_deterministic(cuda):
+    """A split product adds its K parts in a fixed order: repeated products
+    are bitwise equal."""
+    import torch
+    rng = np.random.default_rng(5)
+    A = rng.standard_normal((1500, 5000)).astype(np.float32)
+    op = ib.Matrix(A).get_device_operator(need_transpose=True)
+    X = torch.from_numpy(rng.standard_normal((5000, 64)).astype(np.float32))
+    Y1 = op.dot(X.cuda()).cpu().numpy()
+    Y2 = op.dot(X.cuda()).cpu().numpy()
+    assert np.array_equal(Y1, Y2)
+    ref = A.astype(np.float64) @ X.numpy().astype(np.float64)
+    assert _err(Y1.astype(np.float64), ref) < 5e-5
