@@ -37,7 +37,8 @@ EXPORTS = (
     "slq_operator_tune", "slq_operator_set_variant",
     "slq_batch_workspace_bytes", "slq_batch_create", "slq_batch_run",
     "slq_batch_info", "slq_batch_destroy", "slq_group_order",
-    "slq_rcm_order", "slq_tc_selftest", "slq_order_spread", "slq_group_fill",
+    "slq_rcm_order", "slq_tc_selftest", "slq_tc_selftest_mn",
+    "slq_order_spread", "slq_group_fill",
     "slq_rcm_order_device_workspace_bytes", "slq_rcm_order_device",
     "slq_dense_operator_workspace_bytes", "slq_dense_operator_create",
 )
@@ -187,6 +188,7 @@ def _declare(lib):
         "slq_rcm_order_device": (i32, [i64, i64, vp, vp, i32, vp, vp, vp, sz,
                                         vp]),
         "slq_tc_selftest": (i32, [vp, vp, vp, i32, vp, vp]),
+        "slq_tc_selftest_mn": (i32, [vp, vp, vp, i32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -2997,4 +2997,47 @@ extern "C" slq_status slq_tc_selftest(const float* a, const float* b, float* d, 
     return SLQ_OK;
 }
 
+extern "C" slq_status slq_tc_selftest_mn(const float* a, const float* b, float* d, int gather,
+                                         int32_t* error, void* stream)
+{
+    if (!a || !b || !d || !error) return fail(SLQ_ERR_BAD_ARG, "tc_selftest_mn: NULL argument");
+    if (gather != 0 && gather != 1)
+        return fail(SLQ_ERR_BAD_ARG, "tc_selftest_mn: gather must be 0 or 1");
+    if (reinterpret_cast<uintptr_t>(b) % 16 != 0)
+        return fail(SLQ_ERR_BAD_ARG, "tc_selftest_mn: b must be 16-byte aligned");
+    if (!g_encode_tiled)
+    {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        SLQ_CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess)
+            return fail(SLQ_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+        g_encode_tiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    // B as [8][32] FP32 rows of 128 bytes, one row per box (gather4 form)
+    CUtensorMap bmap;
+    cuuint64_t dims[2] = {32, 8};
+    cuuint64_t strides[1] = {32 * sizeof(float)};
+    cuuint32_t box[2] = {32, 1};
+    cuuint32_t es[2] = {1, 1};
+    const CUresult r = g_encode_tiled(&bmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                                      const_cast<float*>(b), dims, strides, box, es,
+                                      CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                      CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
+                                      CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(SLQ_ERR_CUDA, "cuTensorMapEncodeTiled (selftest) failed (" +
+                                      std::to_string(int(r)) + ")");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    SLQ_CK(cudaMemsetAsync(error, 0, sizeof(int32_t), st));
+    k_tc_selftest_mn<<<1, 128, 0, st>>>(bmap, a, b, d, gather, error);
+    SLQ_LAUNCH_CK();
+    int32_t herr = 0;
+    SLQ_CK(cudaMemcpyAsync(&herr, error, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    SLQ_CK(cudaStreamSynchronize(st));
+    if (herr) return fail(SLQ_ERR_TIMEOUT, "tc_selftest_mn: a wait did not complete");
+    return SLQ_OK;
+}
+
 extern "C" int slq_abi_version(void) { return SLQ_ABI_VERSION; }

@@ -2802,6 +2802,119 @@ k_tc_selftest(const float* __restrict__ a, const float* __restrict__ b, float* _
     if (warp == 0) tc::tmem_dealloc(base, 64);
 }
 
+// ===========================================================================
+// MN-major operand self-test: D[128][32] = A[128][8] B'[8][32] through one
+// kind::tf32 MMA with B' MN-major in shared memory.  A TF32 MN-major operand
+// takes the 128-byte swizzle with 32-byte atoms (descriptor layout type 1,
+// SWIZZLE_128B_BASE32B): atoms of 4 K rows x 128 bytes (32 N values), the
+// 32-byte chunk c of row k stored at chunk c ^ (k % 4); the leading byte
+// offset is the stride between 32-value N atoms, the stride byte offset the
+// stride between 4-row K atoms (here 512: K rows 0-3, then 4-7).  The plain
+// 128-byte swizzle (layout type 2) reads an MN-major TF32 operand as zeros.
+// gather == 0: the threads write B' = B; gather == 1: two TMA tile::gather4
+// loads bring B' rows k = B rows perm[k] (perm = 3 0 7 1 6 2 5 4) through
+// bmap (B as [8][32] FP32, box 32 x 1, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
+// which writes exactly this layout), the load form of a block SpMM's probe
+// rows.  A is K-major without swizzling (as k_tc_selftest mode 3).  One CTA
+// of 128 threads; thread m owns row m.
+// ===========================================================================
+
+__global__ void __launch_bounds__(128, 1)
+k_tc_selftest_mn(const __grid_constant__ CUtensorMap bmap, const float* __restrict__ a,
+                 const float* __restrict__ b, float* __restrict__ d, int gather,
+                 int32_t* __restrict__ error)
+{
+    __shared__ __align__(1024) unsigned char atile[4096];
+    __shared__ __align__(1024) unsigned char btile[1024];
+    __shared__ __align__(8) uint64_t bars[2];  // [0] B loaded, [1] MMA done
+    __shared__ uint32_t tbase;
+    __shared__ int abort_none;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    if (warp == 0)
+    {
+        tc::tmem_alloc(&tbase, 32);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0)
+    {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        abort_none = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t base = tbase;
+    const uint32_t lanes = static_cast<uint32_t>(32 * warp) << 16;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+    {
+        uint32_t h, l;
+        tc::split_tf32(a[tid * 8 + k], h, l);
+        *reinterpret_cast<uint32_t*>(atile + tc::kmajor_offset(tid, k)) = h;
+    }
+    if (!gather)
+    {
+        // 256 values, two per thread: (k, n) at (k / 4) * 512 + (k % 4) * 128 +
+        // ((n / 8) ^ (k % 4)) * 32 + (n % 8) * 4
+        for (int e = tid; e < 256; e += 128)
+        {
+            const int k = e >> 5, n = e & 31;
+            uint32_t h, l;
+            tc::split_tf32(b[k * 32 + n], h, l);
+            *reinterpret_cast<uint32_t*>(btile + (k >> 2) * 512 + (k & 3) * 128 +
+                                         (((n >> 3) ^ (k & 3)) << 5) + (n & 7) * 4) = h;
+        }
+    }
+    tc::fence_proxy_async_smem();
+    __syncthreads();
+    bool ok = true;
+    if (gather)
+    {
+        if (tid == 0)
+        {
+            mbar_expect_tx(&bars[0], 1024u);
+            tma_gather4(btile, &bmap, 0, 3, 0, 7, 1, &bars[0]);
+            tma_gather4(btile + 512, &bmap, 0, 6, 2, 5, 4, &bars[0]);
+        }
+        ok = __all_sync(FULL_MASK, mbar_wait(&bars[0], 0, &abort_none));
+        ok = __syncthreads_and(ok);
+    }
+    tc::fence_after_sync();
+    if (tid == 0 && ok)
+    {
+        const uint64_t ad = tc::smem_desc(atile, 128, 256);
+        // MN-major, 128-byte swizzle with 32-byte atoms (layout type 1): one
+        // N atom, K atoms 512 bytes apart
+        const uint64_t bd = tc::smem_desc(btile, 1024, 512) | (uint64_t(1) << 61);
+        tc::mma_tf32_ss(base, ad, bd, tc::idesc_tf32_m128(32) | (1u << 16), 0);
+    }
+    if (tid == 0) tc::commit(&bars[1]);  // with no MMA issued it arrives at once
+    ok = __all_sync(FULL_MASK, mbar_wait(&bars[1], 0, &abort_none)) && ok;
+    tc::fence_after_sync();
+    if (ok)
+    {
+        uint32_t v[16];
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+        {
+            tc::ld_x16(base + lanes + 16 * h, v);
+            tc::wait_ld();
+#pragma unroll
+            for (int n = 0; n < 16; ++n) d[tid * 32 + 16 * h + n] = __uint_as_float(v[n]);
+        }
+    }
+    else if ((tid & 31) == 0)
+    {
+        atomicExch(error, 1);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(base, 32);
+}
+
 }  // namespace slq
 
 #endif  // SLQ_KERNELS_CUH_

@@ -20,8 +20,11 @@
 //     (r / 8) * SBO + (k / 4) * LBO + (k % 4) * 4, here LBO = 128 bytes
 //     (the two 4-wide K halves of a core row group side by side) and SBO =
 //     256 bytes (next 8 rows).  B (N = 16 rows of the group) is stored this
-//     way; the MN-major form of B (transpose bit 16 set) read back as zero
-//     on this hardware for tf32 without swizzling, so it is not used.
+//     way.  An MN-major TF32 operand (transpose bit 15 for A, 16 for B) reads
+//     back as zero without swizzling and with the plain 128-byte swizzle; it
+//     needs the 128-byte swizzle with 32-byte atoms (layout type 1, see
+//     k_tc_selftest_mn), which TMA writes with
+//     CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B.
 //   A in tensor memory (TS form): lane m = row m, columns = the K values.
 //   Tensor-memory addresses: lane << 16 | column; warp w of a warpgroup
 //     reaches lanes 32 (w % 4) .. 32 (w % 4) + 31.

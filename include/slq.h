@@ -373,6 +373,19 @@ slq_status slq_batch_destroy(slq_batch* batch);
 slq_status slq_tc_selftest(const float* a, const float* b, float* d, int mode,
                            int32_t* error, void* stream);
 
+/* No counterpart in the reference: one kind::tf32 MMA with an MN-major
+ * operand, D[128][32] = A[128][8] B'[8][32] (device arrays, row-major).  B'
+ * sits in shared memory in the MN-major layout a TF32 operand needs: the
+ * 128-byte swizzle with 32-byte atoms (descriptor layout type 1; 4-row K
+ * atoms of 128-byte rows, 32-byte chunks swizzled by the row; the plain
+ * 128-byte swizzle reads such an operand as zeros).  gather 0: B' = B, written by
+ * the threads; gather 1: B' rows k = B rows perm[k], perm = 3 0 7 1 6 2 5 4,
+ * loaded by two TMA tile::gather4 copies (the load form of a block SpMM's
+ * probe rows).  Only TF32 hi parts are used.  b must be 16-byte aligned;
+ * error as slq_tc_selftest. */
+slq_status slq_tc_selftest_mn(const float* a, const float* b, float* d,
+                              int gather, int32_t* error, void* stream);
+
 /* Probe generator alone: writes probes [first, first+count) of the stream for
  * (seed, rng) as a row-major block [len][width] of +-1 in the given dtype
  * (columns >= count are zero).  Replaces

@@ -115,3 +115,27 @@ def test_tensor_core_candidate_is_tuned(cuda):
         assert len(tcs) == 1 and tcs[0]["ms"] > 0
     cands, _ = tune_operator(op, 64, reps=1)
     assert not [c for c in cands if c["kind"] == "row-group-tc"]
+
+
+def _tile_mn(lib, a, b, gather):
+    import torch
+    A = torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    B = torch.from_numpy(np.ascontiguousarray(b, np.float32)).cuda()
+    D = torch.full((128, 32), np.nan, dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.check(lib.slq_tc_selftest_mn(A.data_ptr(), B.data_ptr(), D.data_ptr(),
+                                      int(gather), err.data_ptr(),
+                                      torch.cuda.current_stream().cuda_stream))
+    return D.cpu().numpy()
+
+
+@pytest.mark.parametrize("gather", [0, 1])
+def test_tc_mn_major_operand_exact_on_small_integers(cuda, gather):
+    # B in the 128-byte-swizzled MN-major layout (gather 1: rows brought by
+    # TMA tile::gather4 in the order perm), one kind::tf32 MMA
+    rng = np.random.default_rng(11 + gather)
+    a = rng.integers(-8, 9, (128, 8)).astype(np.float32)
+    b = rng.integers(-8, 9, (8, 32)).astype(np.float32)
+    perm = [3, 0, 7, 1, 6, 2, 5, 4] if gather else list(range(8))
+    want = a.astype(np.float64) @ b[perm].astype(np.float64)
+    assert np.array_equal(_tile_mn(cuda, a, b, gather), want)
