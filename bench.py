@@ -143,6 +143,20 @@ def reference_sample(A, args, probes, threads, seed=0):
     return float(np.sum(r["lanczos_sizes"][:probes])) / secs, secs, "port"
 
 
+def reference_baseline(A, args, threads, min_secs=10.0, max_rounds=8):
+    """The reference CPU SLQ timed over rounds of one probe per host thread
+    (seeds 0, 1, ...) until at least ``min_secs`` of its own computation
+    time: (probe*steps/s, probes, seconds, kind)."""
+    probes = min(threads, 64)
+    total_ps, total_s, rounds, kind = 0.0, 0.0, 0, "reference"
+    while rounds < max_rounds and (rounds == 0 or total_s < min_secs):
+        v, secs, kind = reference_sample(A, args, probes, threads, seed=rounds)
+        total_ps += v * secs
+        total_s += secs
+        rounds += 1
+    return total_ps / total_s, probes * rounds, total_s, kind
+
+
 def cpu_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -496,8 +510,7 @@ def run_engine_arm(args):
 
         if not args.no_cpu_baseline:
             threads = cpu_threads()
-            probes = min(threads, 64)
-            v, secs, kind = reference_sample(A32, args, probes, threads)
+            v, probes, secs, kind = reference_baseline(A32, args, threads)
             line["cpu_baseline"] = {
                 "value": v, "unit": UNIT, "cores": threads, "kind": kind,
                 "sample": "%d probes x %d steps, FP32, full reorth, %.1f s"
@@ -943,8 +956,7 @@ def run_dense(args):
             line["reference_gpu"] = gpu_ref
     if not args.no_cpu_baseline:
         threads = cpu_threads()
-        probes = min(threads, 64)
-        v, secs, kind = reference_sample(A32, args, probes, threads)
+        v, probes, secs, kind = reference_baseline(A32, args, threads)
         line["cpu_baseline"] = {
             "value": v, "unit": UNIT, "cores": threads, "kind": kind,
             "sample": "%d probes x %d steps, FP32 dense, full reorth, %.1f s"
