@@ -670,3 +670,66 @@ def test_affine_general_b_float32_close_to_float64(cuda):
                          parameters=[0.2, 2.0], method="slq", gpu=True,
                          return_info=True, **kw)
     assert rel(t32, t64) < 1e-4
+
+
+def test_edge_shapes_match_reference_library(cuda):
+    """Shapes at the edges of the estimator against the reference CPU SLQ
+    built from its sources, on identical probes: a 1 x 1 matrix, a Krylov
+    degree above the order, empty rows and explicit zeros under A + t I (CSR
+    and CSC), and a last probe block holding a single probe."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("oracle/_ref not built")
+    kw = dict(error_rtol=0.0, seed=5)
+
+    def both(fn, func, A, engine=None, **k):
+        extra = {} if engine is None else {"engine": engine}
+        tr, info = fn(A if not isinstance(A, tuple) else A[0], method="slq",
+                      gpu=True, return_info=True, **dict(kw, **k), **extra)
+        B = A if not isinstance(A, tuple) else A[1]
+        want = ref.trace_estimator(B, func, **dict(kw, **k))
+        return tr, info, want
+
+    one = sp.csr_matrix(np.array([[2.5]]))
+    tr, info, want = both(ib.logdet, "log", one, min_num_samples=4,
+                          max_num_samples=4, lanczos_degree=10,
+                          orthogonalize=0)
+    assert rel(info["convergence"]["samples"][:4], want["samples"][:4, 0]) < 1e-12
+    assert abs(float(tr) - np.log(2.5)) < 1e-12
+
+    T = sp.diags([np.full(4, -1.0), np.full(5, 4.0), np.full(4, -1.0)],
+                 [-1, 0, 1]).tocsr()
+    tr, info, want = both(ib.logdet, "log", T, min_num_samples=7,
+                          max_num_samples=7, lanczos_degree=20,
+                          orthogonalize=-1)
+    assert np.all(info["engine"]["lanczos_size"][:7] <= 5)
+    assert rel(info["convergence"]["samples"][:7], want["samples"][:7, 0]) < 1e-9
+
+    rng = np.random.default_rng(3)
+    M = sp.random(60, 60, density=0.08, random_state=rng, format="csr")
+    M = sp.csr_matrix(M @ M.T)
+    keep = np.ones(60, bool)
+    keep[rng.choice(60, 10, replace=False)] = False
+    D = sp.diags(keep.astype(float))
+    P = (D @ M @ D).tocoo()                 # 10 empty rows and columns
+    # explicit stored zeros at symmetric pairs of empty positions
+    dense = P.toarray()
+    cand = [(i, j) for i in range(60) for j in range(i + 1, 60)
+            if keep[i] and keep[j] and dense[i, j] == 0.0]
+    pick = [cand[k] for k in rng.choice(len(cand), 20, replace=False)]
+    zi = [i for i, j in pick] + [j for i, j in pick]
+    zj = [j for i, j in pick] + [i for i, j in pick]
+    P = sp.csr_matrix((np.r_[P.data, np.zeros(40)],
+                       (np.r_[P.row, zi], np.r_[P.col, zj])), shape=(60, 60))
+    assert P.nnz == np.count_nonzero(P.data) + 40
+    assert np.allclose(P.toarray(), P.toarray().T)
+    for fmt in ("csr", "csc"):
+        Q = P.asformat(fmt)
+        tr, info, want = both(ib.traceinv, "inv",
+                              (ib.AffineMatrixFunction(Q), Q),
+                              engine=ib.EngineOptions(block_size=32),
+                              parameters=[0.5, 2.0], min_num_samples=33,
+                              max_num_samples=33, lanczos_degree=15,
+                              orthogonalize=-1)
+        s = np.asarray(info["convergence"]["samples"]).reshape(33, -1)
+        assert rel(s, want["samples"][:33]) < 1e-9
