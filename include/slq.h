@@ -124,12 +124,14 @@ slq_status slq_rcm_order(int64_t n, const int32_t* indptr,
  * rows in base_order (NULL = identity) and makes each row not yet placed the
  * seed of a group of group_rows rows: the seed, its not-yet-placed
  * neighbours by decreasing |a_ij|, their neighbours, and, when the
- * neighbourhood runs out, the next unplaced rows of the base order.  The
- * base order is cut into chunks of at least 16384 rows (at most 16, a
- * multiple of group_rows each; the cut depends on n only) aggregated in
- * parallel, each group from one chunk's rows.
- * order[k] receives the row at position k; every group but the last has
- * exactly group_rows rows, so passing order as slq_operator_create's perm
+ * neighbourhood runs out, the next unplaced rows of the base order.  Orders
+ * of at least 32768 rows run two sweeps on two host threads, both from the
+ * middle of the base order outwards (the first half backwards, the second
+ * forwards), each group from one half's rows; groups are then listed by
+ * their seeds' base positions, the short groups at the two ends last.  The
+ * order depends on n and the inputs only, not on the thread count.
+ * order[k] receives the row at position k; every group but the short ones
+ * has exactly group_rows rows, so passing order as slq_operator_create's perm
  * lines the groups up with the row-group format's, whose cost falls with
  * the overlap of the rows' column sets. */
 slq_status slq_group_order(int64_t n, const int32_t* indptr,
