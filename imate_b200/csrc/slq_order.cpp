@@ -513,6 +513,144 @@ extern "C" slq_status slq_group_order(int64_t n, const int32_t* indptr, const in
     return SLQ_OK;
 }
 
+extern "C" slq_status slq_block_order(int64_t n, const int32_t* indptr, const int32_t* indices,
+                                      const int32_t* group_order, int group_rows,
+                                      int groups_per_block, int32_t* order)
+{
+    if (n < 0 || !indptr || !indices || !group_order || !order || group_rows < 1 ||
+        group_rows > 1024 || groups_per_block < 1 || groups_per_block > 1024)
+    {
+        slq::set_error("block_order: bad arguments");
+        return SLQ_ERR_BAD_ARG;
+    }
+    std::lock_guard<std::mutex> lock(pool_mutex());
+    Pool& P = shared_pool();
+    if (!valid_pattern(P, n, indptr, indices, "block_order")) return SLQ_ERR_BAD_CSR;
+    std::vector<int32_t> pos;
+    if (!inverse_perm(n, group_order, pos))
+    {
+        slq::set_error("block_order: group_order is not a permutation");
+        return SLQ_ERR_BAD_ARG;
+    }
+    const int G = group_rows;
+    const int64_t ng = n / G;  // whole groups; the remaining rows stay last
+    // each group's column set, sorted and unique (in parallel)
+    std::vector<int64_t> gsize(static_cast<size_t>(ng) + 1, 0);
+    std::vector<std::vector<int32_t>> gcols(static_cast<size_t>(ng));
+    P.run([&](int t, int nt) {
+        int64_t b, e;
+        part_range(ng, t, nt, b, e);
+        // union by a per-thread stamp per column, then a sort of the union
+        std::vector<int64_t> stamp(b < e ? static_cast<size_t>(n) : 0, -1);
+        for (int64_t g = b; g < e; ++g)
+        {
+            std::vector<int32_t>& c = gcols[g];
+            for (int r = 0; r < G; ++r)
+            {
+                const int32_t row = group_order[g * G + r];
+                for (int32_t x = indptr[row]; x < indptr[row + 1]; ++x)
+                {
+                    const int32_t col = indices[x];
+                    if (stamp[col] == g) continue;
+                    stamp[col] = g;
+                    c.push_back(col);
+                }
+            }
+            std::sort(c.begin(), c.end());
+        }
+    });
+    // groups of each column (counting sort by column)
+    std::vector<int64_t> cptr(static_cast<size_t>(n) + 1, 0);
+    for (int64_t g = 0; g < ng; ++g)
+        for (int32_t c : gcols[g]) ++cptr[static_cast<size_t>(c) + 1];
+    for (int64_t c = 0; c < n; ++c) cptr[c + 1] += cptr[c];
+    std::vector<int32_t> cgroups(static_cast<size_t>(cptr[n]));
+    {
+        std::vector<int64_t> fill(cptr.begin(), cptr.end() - 1);
+        for (int64_t g = 0; g < ng; ++g)
+            for (int32_t c : gcols[g]) cgroups[fill[c]++] = static_cast<int32_t>(g);
+    }
+    // group graph: for each group, its neighbours and the number of shared
+    // columns (in parallel; each thread counts into its own stamp arrays)
+    std::vector<std::vector<std::pair<int32_t, int32_t>>> adj(static_cast<size_t>(ng));
+    P.run([&](int t, int nt) {
+        int64_t b, e;
+        part_range(ng, t, nt, b, e);
+        std::vector<int32_t> cnt(b < e ? static_cast<size_t>(ng) : 0, 0);
+        std::vector<int32_t> touched;
+        for (int64_t g = b; g < e; ++g)
+        {
+            touched.clear();
+            for (int32_t c : gcols[g])
+                for (int64_t k = cptr[c]; k < cptr[c + 1]; ++k)
+                {
+                    const int32_t h = cgroups[k];
+                    if (h == g) continue;
+                    if (cnt[h]++ == 0) touched.push_back(h);
+                }
+            std::sort(touched.begin(), touched.end());
+            adj[g].reserve(touched.size());
+            for (int32_t h : touched)
+            {
+                adj[g].emplace_back(h, cnt[h]);
+                cnt[h] = 0;
+            }
+        }
+    });
+    // greedy blocks on the graph: a seed group, then the unplaced neighbour
+    // with the largest summed overlap with the block's groups per column
+    std::vector<uint8_t> placed(static_cast<size_t>(ng), 0);
+    std::vector<int64_t> grp_stamp(static_cast<size_t>(ng), -1);
+    std::vector<int64_t> score(static_cast<size_t>(ng), 0);
+    std::vector<int32_t> cand, block;
+    int64_t out = 0, cursor = 0, bid = 0;
+    auto join = [&](int64_t g) {
+        placed[g] = 1;
+        block.push_back(static_cast<int32_t>(g));
+        for (const auto& hw : adj[g])
+        {
+            const int32_t h = hw.first;
+            if (placed[h]) continue;
+            if (grp_stamp[h] != bid)
+            {
+                grp_stamp[h] = bid;
+                score[h] = 0;
+                cand.push_back(h);
+            }
+            score[h] += hw.second;
+        }
+    };
+    for (int64_t s = 0; s < ng; ++s, ++bid)
+    {
+        if (placed[s]) continue;
+        block.clear();
+        cand.clear();
+        join(s);
+        while (static_cast<int>(block.size()) < groups_per_block)
+        {
+            int64_t best = -1;
+            for (int32_t h : cand)
+            {
+                if (placed[h]) continue;
+                const int64_t lhs = score[h] * static_cast<int64_t>(best < 0 ? 1 : gcols[best].size());
+                const int64_t rhs = (best < 0 ? -1 : score[best]) * static_cast<int64_t>(gcols[h].size());
+                if (best < 0 || lhs > rhs || (lhs == rhs && h < best)) best = h;
+            }
+            if (best < 0)
+            {
+                while (cursor < ng && placed[cursor]) ++cursor;
+                if (cursor == ng) break;
+                best = cursor;
+            }
+            join(best);
+        }
+        for (int32_t g : block)
+            for (int r = 0; r < G; ++r) order[out++] = group_order[static_cast<int64_t>(g) * G + r];
+    }
+    for (int64_t k = ng * G; k < n; ++k) order[out++] = group_order[k];
+    return SLQ_OK;
+}
+
 extern "C" slq_status slq_order_spread(int64_t n, const int32_t* indptr, const int32_t* indices,
                                        const int32_t* perm, int64_t sample_rows, double* spread)
 {

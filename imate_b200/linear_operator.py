@@ -163,6 +163,21 @@ def group_order(A, base_perm, G):
     return order
 
 
+def block_order(A, group_order, group_rows=16, groups_per_block=8):
+    """Row order whose consecutive blocks of ``groups_per_block`` groups of
+    ``group_rows`` rows (the groups of ``group_order``, kept whole) have
+    overlapping column sets (``slq_block_order``).  Square matrices only."""
+    A = sp.csr_matrix(A)
+    n = A.shape[0]
+    ip, ind = _pattern(A)
+    go = np.ascontiguousarray(group_order, dtype=np.int32)
+    order = np.empty(n, dtype=np.int32)
+    _lib.check(_lib.load().slq_block_order(
+        n, ip.ctypes.data, ind.ctypes.data, go.ctypes.data, int(group_rows),
+        int(groups_per_block), order.ctypes.data))
+    return order
+
+
 def group_rows_for(A, perm, group_rows="auto", sample=256, aggregate=True):
     """Row-group width for the device format (0 = CSR only) and the row
     order to store the matrix in: (G, perm).

@@ -378,3 +378,54 @@ def test_group_order_two_sweeps_keep_groups_compact(lib):
                         // n, minlength=n // G)
     assert A.nnz / (G * union.sum()) > 0.63
     assert np.percentile(union, 99.9) < 1.5 * np.median(union)
+
+
+def _block_unions(A, order, rows):
+    B = A[order]
+    n = A.shape[0]
+    r = np.repeat(np.arange(n), np.diff(B.indptr))
+    return np.bincount(np.unique((r // rows).astype(np.int64) * n + B.indices)
+                       // n, minlength=n // rows)
+
+
+def test_block_order_keeps_groups_and_shrinks_block_unions(lib):
+    # blocks of 8 whole 16-row groups with overlapping column sets: a
+    # permutation, every group of group_order kept whole, deterministic, and
+    # 128-row blocks with far smaller column unions than 128 consecutive rows
+    from imate_b200.linear_operator import (block_order, group_order,
+                                            rcm_order)
+    A = sp.csr_matrix(ib.correlation_matrix(40000, scale=0.01, threshold=0.05,
+                                            shift=0.1, seed=4,
+                                            dtype="float32"))
+    n, G, B = A.shape[0], 16, 8
+    go = group_order(A, rcm_order(A), G)
+    bo = block_order(A, go, G, B)
+    assert np.array_equal(np.sort(bo), np.arange(n))
+    assert np.array_equal(bo, block_order(A, go, G, B))
+    groups = {tuple(sorted(go[i * G:(i + 1) * G])) for i in range(n // G)}
+    assert {tuple(sorted(bo[i * G:(i + 1) * G])) for i in range(n // G)} \
+        == groups
+    before = _block_unions(A, go, G * B)[:n // (G * B)]
+    after = _block_unions(A, bo, G * B)[:n // (G * B)]
+    assert after.mean() < 0.6 * before.mean()
+
+
+def test_block_order_rejects_bad_input(lib):
+    n = 8
+    ip = np.arange(n + 1, dtype=np.int32)
+    ind = np.arange(n, dtype=np.int32)
+    out = np.empty(n, np.int32)
+    bad = np.array([0, 0, 1, 2, 3, 4, 5, 6], np.int32)
+    assert lib.slq_block_order(n, ip.ctypes.data, ind.ctypes.data,
+                               bad.ctypes.data, 2, 2, out.ctypes.data) == 1
+    good = np.arange(n, dtype=np.int32)[::-1].copy()
+    assert lib.slq_block_order(n, ip.ctypes.data, ind.ctypes.data,
+                               good.ctypes.data, 0, 2, out.ctypes.data) == 1
+    ind2 = ind.copy()
+    ind2[3] = 99
+    assert lib.slq_block_order(n, ip.ctypes.data, ind2.ctypes.data,
+                               good.ctypes.data, 2, 2, out.ctypes.data) == 2
+    # diagonal pattern: no group shares a column, blocks follow the order
+    assert lib.slq_block_order(n, ip.ctypes.data, ind.ctypes.data,
+                               good.ctypes.data, 2, 2, out.ctypes.data) == 0
+    assert np.array_equal(out, good)
