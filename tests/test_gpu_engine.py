@@ -1,7 +1,7 @@
 """Parity of the CUDA engine with the oracle and with the reference's own
 golden outputs.  Tolerances: bit-exact for probe bits and sample counts;
 1e-10 relative for FP64 Lanczos/Golub-Kahn coefficients, nodes, weights and
-per-probe samples (the accuracy BASELINE's north star states for FP64);
+per-probe samples (the FP64 parity bar against the reference CPU path);
 FP32 operator products within 1e-5 relative of scipy."""
 
 import ctypes
