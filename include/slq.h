@@ -35,7 +35,7 @@ typedef enum {
     SLQ_ERR_CUDA = 4,             /* a CUDA runtime call failed             */
     SLQ_ERR_NAN = 5,              /* NaN/Inf in a Lanczos coefficient       */
     SLQ_ERR_EIGEN = 6,            /* tridiagonal eigen-solve did not converge */
-    SLQ_ERR_UNSUPPORTED = 7,      /* valid request this build does not serve */
+    SLQ_ERR_UNSUPPORTED = 7,      /* valid request this library does not serve */
     SLQ_ERR_TIMEOUT = 8           /* a bounded device-side wait ran out     */
 } slq_status;
 

@@ -1,6 +1,6 @@
 """Test infrastructure: numpy (FP64) restatement of the surrogate network.
 
-The checker for the device kernels in imate_b200/csrc/slq_mlp.cu
+The oracle for the device kernels in imate_b200/csrc/slq_mlp.cu
 (slq_mlp_forward, slq_mlp_grad, slq_mlp_train): the same 1 -> 64 -> 64 -> 1
 tanh network with the same packed parameter layout
 W1[64] b1[64] W2[64][64] b2[64] W3[64] b3[1], the mean-squared-error loss and

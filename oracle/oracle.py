@@ -1,6 +1,6 @@
 """Loader for the C restatement ``oracle/slq_oracle.c`` -- test infrastructure.
 
-The oracle is the checker for the CUDA engine: only ``tests/``,
+The oracle checks the CUDA engine: only ``tests/``,
 ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use it.  Its
 functions follow the reference CPU SLQ (ameli/imate v0.25.2,
 ``imate/_c_trace_estimator/c_trace_estimator.cpp:192-654`` and callees); see

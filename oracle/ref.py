@@ -3,7 +3,7 @@
 The library is the reference's own CPU SLQ (ameli/imate v0.25.2,
 ``imate/_c_trace_estimator/c_trace_estimator.cpp:192-307`` and the sources it
 calls), compiled from its own source files by ``oracle/Makefile`` with the
-thin entry layer ``oracle/ref_harness.cpp``.  It is the checker for the CUDA
+thin entry layer ``oracle/ref_harness.cpp``.  It checks the CUDA
 path and the CPU baseline that ``bench.py --impl reference`` times; the
 product never imports this module.
 
@@ -11,7 +11,7 @@ product never imports this module.
 (``imate/_cu_trace_estimator/cu_trace_estimator.cu:197-315`` over
 ``cuCSRMatrix``: cuSPARSE SpMV and cuBLAS vector operations), compiled from
 its sources for sm_100a by the same Makefile (target ``ref_gpu``): a second
-checker for the tests and the reference GPU comparator of bench.py's
+reference for the tests and the reference GPU comparator of bench.py's
 reference arm.
 
 LAPACK is bound the way the reference binds it

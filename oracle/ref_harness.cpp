@@ -2,7 +2,7 @@
 // CPU SLQ sources (ameli/imate v0.25.2), compiled from where they lie by
 // oracle/Makefile into oracle/_ref/libimate_ref.so.  Nothing in the product
 // links or loads this file; tests/, __graft_entry__.smoke() and bench.py's
-// reference arm use it as the checker and as the timed CPU baseline.
+// reference arm use it to check the engine and as the timed CPU baseline.
 //
 // The reference binds LAPACK through Cython (`lapack_api.pxi`, which exports
 // lapack_dstev / lapack_dbdsdc from scipy.linalg.cython_lapack).  Here the

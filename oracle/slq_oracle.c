@@ -3,7 +3,7 @@
  *
  * A plain-C, single-threaded restatement of the reference CPU stochastic
  * Lanczos quadrature (ameli/imate v0.25.2, imate/_c_trace_estimator/) used as
- * the checker for the CUDA engine.  Only tests/, __graft_entry__.smoke() and
+ * the oracle of the CUDA engine.  Only tests/, __graft_entry__.smoke() and
  * bench.py's cpu_baseline leg load it.  Each function names the reference
  * file:line it follows.  Arithmetic follows the reference: FP64 data, long
  * double accumulators in inner products, norms and CSR row sums
