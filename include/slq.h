@@ -143,15 +143,15 @@ slq_status slq_group_order(int64_t n, const int32_t* indptr,
  * the groups of group_rows consecutive rows of group_order (a row order such
  * as slq_group_order gives) into blocks of groups_per_block groups whose
  * column sets overlap.  Blocks start at the unplaced groups in order; each
- * then takes the unplaced group whose summed column overlap with the
- * block's groups, per column of its own, is largest (ties: the earlier
- * group), or the next unplaced groups when no group shares a column (the
- * group overlaps are counted once, in parallel).  order[k] receives
+ * then takes the unplaced group with the most row pairs (a row of the
+ * group, a neighbour row in the block) per row pair of its own (ties: the
+ * earlier group), or the next unplaced groups when no row links them (the
+ * group graph is counted once, in parallel).  order[k] receives
  * the row at position k: blocks in order, their groups in joining order,
  * each group's rows as in group_order; the n % group_rows rows after the
  * last whole group stay last.  On the benchmark correlation matrix, blocks
  * of eight 16-row groups have a mean column union of about 650 against
- * about 1,500 for 128 consecutive rows of group_order (about 0.23 s on 8
+ * about 1,500 for 128 consecutive rows of group_order (about 70 ms on 8
  * host threads). */
 slq_status slq_block_order(int64_t n, const int32_t* indptr,
                            const int32_t* indices, const int32_t* group_order,
