@@ -76,7 +76,7 @@ def parse():
     ap.add_argument("--batch-count", type=int, default=64)
     ap.add_argument("--spmm", default="auto",
                     choices=["auto", "csr", "row-group", "row-group-tma",
-                             "row-group-tc"],
+                             "row-group-tc", "block-tc"],
                     help="SpMM kernel of the headline run: the built-in "
                          "choice (auto) or a forced autotuner candidate")
     ap.add_argument("--block", type=int, default=256)
@@ -349,7 +349,7 @@ def run_engine_arm(args):
     A32 = build_matrix(args, "float32")
     # the tensor-core SpMM serves 16-row groups only
     Aop = ib.Matrix(A32, group_rows=16 if args.spmm == "row-group-tc"
-                    else "auto")
+                    else "auto", blocks=args.spmm == "block-tc")
     dev_op = Aop.get_device_operator()  # one-time upload, outside the timed region
     if args.spmm != "auto":
         from imate_b200.batch import tune_operator, set_variant

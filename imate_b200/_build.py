@@ -16,7 +16,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["slq_engine.cu", "slq_mlp.cu", "slq_rng.cpp", "slq_stats.cpp",
            "slq_order.cpp"]
-HEADERS = ["slq_kernels.cuh", "slq_rng.h", "slq_tc.cuh"]
+HEADERS = ["slq_kernels.cuh", "slq_blk.cuh", "slq_rng.h", "slq_tc.cuh"]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

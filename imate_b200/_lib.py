@@ -41,9 +41,11 @@ EXPORTS = (
     "slq_order_spread", "slq_group_fill", "slq_block_order",
     "slq_rcm_order_device_workspace_bytes", "slq_rcm_order_device",
     "slq_dense_operator_workspace_bytes", "slq_dense_operator_create",
+    "slq_operator_blocks_scratch_bytes", "slq_operator_blocks_bytes",
+    "slq_operator_add_blocks",
 )
 TUNE_MAX_CANDIDATES = 16
-SPMM_KINDS = ("csr", "row-group", "row-group-tma", "row-group-tc")
+SPMM_KINDS = ("csr", "row-group", "row-group-tma", "row-group-tc", "block-tc")
 MLP_WIDTH = 64
 MLP_PARAMS = 64 + 64 + 64 * 64 + 64 + 64 + 1
 MLP_MAX_BATCH = 64
@@ -189,6 +191,9 @@ def _declare(lib):
         "slq_rcm_order_device": (i32, [i64, i64, vp, vp, i32, vp, vp, vp, sz,
                                         vp]),
         "slq_tc_selftest": (i32, [vp, vp, vp, i32, vp, vp]),
+        "slq_operator_blocks_scratch_bytes": (i32, [vp, i32, psz]),
+        "slq_operator_blocks_bytes": (i32, [vp, i32, vp, sz, vp, psz]),
+        "slq_operator_add_blocks": (i32, [vp, i32, vp, sz, vp, sz, vp]),
         "slq_tc_selftest_mn": (i32, [vp, vp, vp, i32, vp, vp]),
     }
     for name, (res, args) in sig.items():

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/slq.h"
+#include "slq_blk.cuh"
 #include "slq_kernels.cuh"
 #include "slq_rng.h"
 
@@ -237,6 +238,16 @@ struct slq_op {
     float* xt_lo = nullptr;
     int32_t* d_error = nullptr;
     CUtensorMap map_hi, map_lo, map_t_hi, map_t_lo;
+    // tensor-core block format (k_spmm_blk, FP32) of A and of A^T: 128-row
+    // blocks, first stage per block, union columns, stage value images
+    int64_t a_nblk = 0, t_nblk = 0;
+    const int32_t* a_bstage = nullptr;
+    const int32_t* a_ucol = nullptr;
+    const float* a_img = nullptr;
+    const int32_t* t_bstage = nullptr;
+    const int32_t* t_ucol = nullptr;
+    const float* t_img = nullptr;
+    int32_t* blk_error = nullptr;  // error word of the block kernel in slq_operator_dot
     // autotuned SpMM candidate per direction and log2(block width); -1 = built-in
     int8_t tuned[2][11];
     slq_op()
@@ -633,6 +644,256 @@ extern "C" slq_status slq_operator_destroy(slq_op* op)
 }
 
 // ---------------------------------------------------------------------------
+// tensor-core block format (k_spmm_blk)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct BlkScratch {
+    uint64_t* keys_in;
+    uint64_t* keys_out;
+    int32_t* pos_in;
+    int32_t* pos_out;
+    uint8_t* rr;
+    int32_t* flags;
+    int32_t* uidx;
+    int32_t* cnt;     // [nblk + 1]
+    int32_t* stg;     // [nblk + 1]
+    int32_t* bstage;  // [nblk + 1]
+    int32_t* ufirst;  // [nblk + 1]
+    void* temp;
+    size_t temp_bytes;
+};
+
+int bits_for(int64_t v)  // bits to hold 0 .. v
+{
+    int b = 1;
+    while (b < 63 && (int64_t(1) << b) <= v) ++b;
+    return b;
+}
+
+slq_status blk_scratch_layout(Carver& c, int64_t rows, int64_t nnz, BlkScratch* s)
+{
+    const int64_t nblk = (rows + BLK_ROWS - 1) / BLK_ROWS;
+    const int nz = static_cast<int>(std::max<int64_t>(nnz, 1));
+    size_t t1 = 0, t2 = 0, t3 = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(
+        nullptr, t1, static_cast<const uint64_t*>(nullptr), static_cast<uint64_t*>(nullptr),
+        static_cast<const int32_t*>(nullptr), static_cast<int32_t*>(nullptr), nz);
+    if (e == cudaSuccess)
+        e = cub::DeviceScan::InclusiveSum(nullptr, t2, static_cast<const int32_t*>(nullptr),
+                                          static_cast<int32_t*>(nullptr), nz);
+    if (e == cudaSuccess)
+        e = cub::DeviceScan::ExclusiveSum(nullptr, t3, static_cast<const int32_t*>(nullptr),
+                                          static_cast<int32_t*>(nullptr),
+                                          static_cast<int>(nblk + 1));
+    if (e != cudaSuccess)
+        return fail(SLQ_ERR_CUDA, std::string("cub sizing (blocks): ") + cudaGetErrorString(e));
+    s->keys_in = c.take<uint64_t>(nz);
+    s->keys_out = c.take<uint64_t>(nz);
+    s->pos_in = c.take<int32_t>(nz);
+    s->pos_out = c.take<int32_t>(nz);
+    s->rr = c.take<uint8_t>(nz);
+    s->flags = c.take<int32_t>(nz);
+    s->uidx = c.take<int32_t>(nz);
+    s->cnt = c.take<int32_t>(nblk + 1);
+    s->stg = c.take<int32_t>(nblk + 1);
+    s->bstage = c.take<int32_t>(nblk + 1);
+    s->ufirst = c.take<int32_t>(nblk + 1);
+    s->temp_bytes = std::max({t1, t2, t3});
+    s->temp = c.take<char>(s->temp_bytes);
+    return SLQ_OK;
+}
+
+// Sorted (block, column) keys, union sizes and first stages of an R x C CSR
+// matrix in the scratch; *stages receives the total (host synchronisation).
+slq_status blk_prepare(const int32_t* ptr, const int32_t* ind, int64_t R, int64_t C, int64_t nnz,
+                       BlkScratch* s, cudaStream_t st, int64_t* stages)
+{
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
+    const int grid = sms * 4;
+    const int64_t nblk = (R + BLK_ROWS - 1) / BLK_ROWS;
+    const int cbits = bits_for(std::max<int64_t>(C - 1, 1));
+    const int bbits = bits_for(std::max<int64_t>(nblk - 1, 1));
+    SLQ_CK(cudaMemsetAsync(s->cnt, 0, sizeof(int32_t) * (nblk + 1), st));
+    if (nnz > 0)
+    {
+        k_blk_keys<<<grid, 256, 0, st>>>(ptr, ind, R, cbits, s->keys_in, s->pos_in, s->rr);
+        SLQ_LAUNCH_CK();
+        size_t tb = s->temp_bytes;
+        cudaError_t e = cub::DeviceRadixSort::SortPairs(s->temp, tb, s->keys_in, s->keys_out,
+                                                        s->pos_in, s->pos_out,
+                                                        static_cast<int>(nnz), 0, cbits + bbits,
+                                                        st);
+        if (e != cudaSuccess)
+            return fail(SLQ_ERR_CUDA, std::string("cub sort (blocks): ") + cudaGetErrorString(e));
+        k_blk_flags<<<grid, 256, 0, st>>>(s->keys_out, nnz, s->flags);
+        SLQ_LAUNCH_CK();
+        tb = s->temp_bytes;
+        e = cub::DeviceScan::InclusiveSum(s->temp, tb, s->flags, s->uidx, static_cast<int>(nnz),
+                                          st);
+        if (e != cudaSuccess)
+            return fail(SLQ_ERR_CUDA, std::string("cub scan (blocks): ") + cudaGetErrorString(e));
+        k_blk_count<<<grid, 256, 0, st>>>(s->keys_out, s->flags, nnz, cbits, s->cnt);
+        SLQ_LAUNCH_CK();
+    }
+    k_blk_stages<<<std::max<int64_t>(1, std::min<int64_t>(grid, (nblk + 256) / 256)), 256, 0,
+                   st>>>(s->cnt, nblk, s->stg);
+    SLQ_LAUNCH_CK();
+    size_t tb = s->temp_bytes;
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(s->temp, tb, s->stg, s->bstage,
+                                                  static_cast<int>(nblk + 1), st);
+    if (e == cudaSuccess)
+    {
+        tb = s->temp_bytes;
+        e = cub::DeviceScan::ExclusiveSum(s->temp, tb, s->cnt, s->ufirst,
+                                          static_cast<int>(nblk + 1), st);
+    }
+    if (e != cudaSuccess)
+        return fail(SLQ_ERR_CUDA, std::string("cub scan (blocks): ") + cudaGetErrorString(e));
+    int32_t total = 0;
+    SLQ_CK(cudaMemcpyAsync(&total, s->bstage + nblk, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    SLQ_CK(cudaStreamSynchronize(st));
+    *stages = total;
+    return SLQ_OK;
+}
+
+void blk_format_layout(Carver& c, int64_t nblk, int64_t stages, int32_t** bstage, int32_t** ucol,
+                       float** img, int32_t** error)
+{
+    *error = c.take<int32_t>(1);
+    *bstage = c.take<int32_t>(nblk + 1);
+    *ucol = c.take<int32_t>(stages * BLK_BK);
+    *img = c.take<float>(stages * BLK_IMG_STAGE);
+}
+
+slq_status blk_source(const slq_op* op, int transpose, const int32_t** ptr, const int32_t** ind,
+                      const float** val, int64_t* R, int64_t* C)
+{
+    if (!op) return fail(SLQ_ERR_BAD_ARG, "blocks: NULL operator");
+    if (op->dense || op->dtype != SLQ_F32)
+        return fail(SLQ_ERR_UNSUPPORTED, "blocks: the block format serves float32 sparse operators");
+    if (transpose != 0 && transpose != 1)
+        return fail(SLQ_ERR_BAD_ARG, "blocks: transpose must be 0 or 1");
+    if (transpose && !op->t_ptr) return fail(SLQ_ERR_BAD_ARG, "blocks: operator has no transpose");
+    *ptr = transpose ? op->t_ptr : op->a_ptr;
+    *ind = transpose ? op->t_ind : op->a_ind;
+    *val = static_cast<const float*>(transpose ? op->t_data : op->a_data);
+    *R = transpose ? op->ncols : op->nrows;
+    *C = transpose ? op->nrows : op->ncols;
+    return SLQ_OK;
+}
+
+}  // namespace
+
+extern "C" slq_status slq_operator_blocks_scratch_bytes(const slq_op* op, int transpose,
+                                                        size_t* bytes)
+{
+    if (!bytes) return fail(SLQ_ERR_BAD_ARG, "blocks: bytes is NULL");
+    const int32_t *ptr, *ind;
+    const float* val;
+    int64_t R, C;
+    SLQ_TRY(blk_source(op, transpose, &ptr, &ind, &val, &R, &C));
+    Carver c(nullptr, 0);
+    BlkScratch s;
+    SLQ_TRY(blk_scratch_layout(c, R, op->nnz, &s));
+    *bytes = c.off + 256;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_operator_blocks_bytes(const slq_op* op, int transpose, void* scratch,
+                                                size_t scratch_bytes, void* stream,
+                                                size_t* format_bytes)
+{
+    if (!format_bytes) return fail(SLQ_ERR_BAD_ARG, "blocks: format_bytes is NULL");
+    const int32_t *ptr, *ind;
+    const float* val;
+    int64_t R, C;
+    SLQ_TRY(blk_source(op, transpose, &ptr, &ind, &val, &R, &C));
+    Carver c(scratch, scratch_bytes);
+    BlkScratch s;
+    SLQ_TRY(blk_scratch_layout(c, R, op->nnz, &s));
+    if (!scratch || !c.fits()) return fail(SLQ_ERR_WORKSPACE, "blocks: scratch too small");
+    int64_t stages = 0;
+    SLQ_TRY(blk_prepare(ptr, ind, R, C, op->nnz, &s, static_cast<cudaStream_t>(stream), &stages));
+    Carver f(nullptr, 0);
+    int32_t *bs, *uc, *er;
+    float* im;
+    blk_format_layout(f, (R + BLK_ROWS - 1) / BLK_ROWS, stages, &bs, &uc, &im, &er);
+    *format_bytes = f.off + 256;
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* scratch,
+                                              size_t scratch_bytes, void* format,
+                                              size_t format_bytes, void* stream)
+{
+    const int32_t *ptr, *ind;
+    const float* val;
+    int64_t R, C;
+    SLQ_TRY(blk_source(op, transpose, &ptr, &ind, &val, &R, &C));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Carver c(scratch, scratch_bytes);
+    BlkScratch s;
+    SLQ_TRY(blk_scratch_layout(c, R, op->nnz, &s));
+    if (!scratch || !c.fits()) return fail(SLQ_ERR_WORKSPACE, "blocks: scratch too small");
+    int64_t stages = 0;
+    SLQ_TRY(blk_prepare(ptr, ind, R, C, op->nnz, &s, st, &stages));
+    const int64_t nblk = (R + BLK_ROWS - 1) / BLK_ROWS;
+    Carver f(format, format_bytes);
+    int32_t *bstage, *ucol, *err;
+    float* img;
+    blk_format_layout(f, nblk, stages, &bstage, &ucol, &img, &err);
+    if (!format || !f.fits())
+        return fail(SLQ_ERR_WORKSPACE, "blocks: format buffer too small (need " +
+                                           std::to_string(f.off) + " bytes)");
+    int sms = 0;
+    SLQ_TRY(device_sms(&sms));
+    const int grid = sms * 4;
+    const int cbits = bits_for(std::max<int64_t>(C - 1, 1));
+    SLQ_CK(cudaMemcpyAsync(bstage, s.bstage, sizeof(int32_t) * (nblk + 1),
+                           cudaMemcpyDeviceToDevice, st));
+    SLQ_CK(cudaMemsetAsync(img, 0, sizeof(float) * stages * BLK_IMG_STAGE, st));
+    if (op->nnz > 0)
+    {
+        k_blk_ucol<<<grid, 256, 0, st>>>(s.keys_out, s.flags, s.uidx, op->nnz, cbits, s.ufirst,
+                                         bstage, ucol);
+        SLQ_LAUNCH_CK();
+    }
+    k_blk_pad<<<std::max<int64_t>(1, std::min<int64_t>(grid, (nblk + 255) / 256)), 256, 0, st>>>(
+        s.cnt, bstage, nblk, ucol);
+    SLQ_LAUNCH_CK();
+    if (op->nnz > 0)
+    {
+        k_blk_scatter<<<grid, 256, 0, st>>>(s.keys_out, s.pos_out, s.uidx, op->nnz, cbits,
+                                            s.ufirst, bstage, val, s.rr, img);
+        SLQ_LAUNCH_CK();
+    }
+    k_blk_split<<<grid, 256, 0, st>>>(img, stages);
+    SLQ_LAUNCH_CK();
+    SLQ_CK(cudaMemsetAsync(err, 0, sizeof(int32_t), st));
+    // the scratch may be released once the build has run
+    SLQ_CK(cudaStreamSynchronize(st));
+    if (!op->blk_error) op->blk_error = err;
+    if (transpose)
+    {
+        op->t_nblk = nblk;
+        op->t_bstage = bstage;
+        op->t_ucol = ucol;
+        op->t_img = img;
+    }
+    else
+    {
+        op->a_nblk = nblk;
+        op->a_bstage = bstage;
+        op->a_ucol = ucol;
+        op->a_img = img;
+    }
+    return SLQ_OK;
+}
+
+// ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------
 
@@ -779,6 +1040,20 @@ slq_status row_map(CUtensorMap* m, const float* base, int64_t rows, int b)
                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
         return fail(SLQ_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+    return SLQ_OK;
+}
+
+// The tensor map of one probe-block buffer for the row gathers of the TMA
+// and tensor-core row-group kernels (has_row = false: none).
+struct XMaps {
+    CUtensorMap row;
+    bool has_row = false;
+};
+
+slq_status make_xmaps(XMaps* m, const float* base, int64_t rows, int b, bool row)
+{
+    if (row) SLQ_TRY(row_map(&m->row, base, rows, b));
+    m->has_row = row;
     return SLQ_OK;
 }
 
@@ -1040,6 +1315,52 @@ slq_status spmm_tc_inst(Launcher& L, const CUtensorMap* xmap, const int32_t* gpt
     return SLQ_OK;
 }
 
+// Tensor-core block SpMM (k_spmm_blk): b = 128 or 256 probes, one CTA per
+// SM over the operator's 128-row blocks.
+slq_status spmm_blk_inst(Launcher& L, const slq_op* op, int transpose, int b, const float* X, const double* sx, double shift, float* Y,
+                         const float* Z, const double* zc, const double* zs, int epi,
+                         double* partials, int32_t* error, int64_t xrows, int* grid_out)
+{
+    const int64_t rows = transpose ? op->ncols : op->nrows;
+    const int64_t nblk = transpose ? op->t_nblk : op->a_nblk;
+    // compulsory traffic as for the CSR kernels (the algorithm's bytes, not
+    // the block format's)
+    const double bytes = op->nnz * 8.0 + (rows + 1) * 4.0 + double(xrows) * b * 4.0 +
+                         double(rows) * b * 4.0 * (Z ? 2.0 : 1.0);
+    ProfScope prof(SLQ_K_SPMM, bytes, L.st);
+    const size_t smem = blk_smem_bytes(b);
+    static bool attr = false;
+    if (!attr)
+    {
+        SLQ_CK(cudaFuncSetAttribute(k_spmm_blk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(blk_smem_bytes(256))));
+        attr = true;
+    }
+    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(nblk, L.sms)));
+    BlkArgs d;
+    d.M = rows;
+    d.nblk = nblk;
+    d.NB = b;
+    d.bstage = transpose ? op->t_bstage : op->a_bstage;
+    d.ucol = transpose ? op->t_ucol : op->a_ucol;
+    d.img = transpose ? op->t_img : op->a_img;
+    d.X = X;
+    d.sx = sx;
+    d.shift = shift;
+    d.Y = Y;
+    d.Z = Z;
+    d.zc = zc;
+    d.zs = zs;
+    d.epi = epi;
+    d.partials = partials;
+    d.error = error;
+    k_spmm_blk<<<grid, BLK_THREADS, smem, L.st>>>(d);
+    SLQ_LAUNCH_CK();
+    ++L.launches;
+    *grid_out = grid;
+    return SLQ_OK;
+}
+
 // ---------------------------------------------------------------------------
 // SpMM candidates: storage format x tile.  A row-group candidate is the tile
 // of LV probes per lane and NS warps sharing one row group (b = 32 LV NS);
@@ -1048,7 +1369,7 @@ slq_status spmm_tc_inst(Launcher& L, const CUtensorMap* xmap, const int32_t* gpt
 // (FP32, G = 8, b = 128 or 256), row-group with the widest LV <= 4, CSR.
 // ---------------------------------------------------------------------------
 
-enum { CAND_CSR = 0, CAND_RG = 1, CAND_TMA = 2, CAND_TC = 3 };
+enum { CAND_CSR = 0, CAND_RG = 1, CAND_TMA = 2, CAND_TC = 3, CAND_BLK = 4 };
 
 struct SpmmCand {
     int kind, g, lv, ns;
@@ -1059,6 +1380,8 @@ int spmm_candidates(const slq_op* op, int transpose, int b, SpmmCand* out)
 {
     int n = 0;
     out[n++] = {CAND_CSR, 0, 0, 0};
+    if (sizeof(VT) == 4 && (transpose ? op->t_bstage : op->a_bstage) && (b == 128 || b == 256))
+        out[n++] = {CAND_BLK, BLK_ROWS, 0, b / 128};
     const int32_t* gptr = transpose ? op->t_gptr : op->a_gptr;
     const int G = op->group_rows;
     if (!G || !gptr) return n;
@@ -1083,11 +1406,22 @@ template <typename VT>
 slq_status spmm_cand(Launcher& L, const slq_op* op, int transpose, const SpmmCand& c, int b,
                      const VT* X, const double* sx, double shift, VT* Y, const VT* Z,
                      const double* zc, const double* zs, int epi, double* partials,
-                     int* grid_out, const CUtensorMap* xmap, int32_t* error)
+                     int* grid_out, const XMaps* maps, int32_t* error)
 {
     const int64_t rows = transpose ? op->ncols : op->nrows;
     const int64_t xrows = transpose ? op->nrows : op->ncols;
     const int32_t* gptr = transpose ? op->t_gptr : op->a_gptr;
+    const CUtensorMap* xmap = (maps && maps->has_row) ? &maps->row : nullptr;
+    if (c.kind == CAND_BLK)
+    {
+        if constexpr (sizeof(VT) == 4)
+        {
+            if (!error) return fail(SLQ_ERR_BAD_ARG, "block SpMM needs an error word");
+            return spmm_blk_inst(L, op, transpose, b, X, sx, shift, Y, Z, zc, zs, epi, partials,
+                                 error, xrows, grid_out);
+        }
+        return fail(SLQ_ERR_BAD_ARG, "block SpMM is FP32 only");
+    }
     const int32_t* gcol = transpose ? op->t_gcol : op->a_gcol;
     if (c.kind == CAND_TMA)
     {
@@ -1185,7 +1519,7 @@ template <typename VT>
 slq_status op_spmm(Launcher& L, const slq_op* op, int transpose, int b, const VT* X,
                    const double* sx, double shift, VT* Y, const VT* Z, const double* zc,
                    const double* zs, int epi, double* partials, int* grid_out,
-                   const CUtensorMap* xmap = nullptr, int32_t* error = nullptr)
+                   const XMaps* maps = nullptr, int32_t* error = nullptr)
 {
     if (op->dense)
     {
@@ -1198,17 +1532,31 @@ slq_status op_spmm(Launcher& L, const slq_op* op, int transpose, int b, const VT
     const int nc = spmm_candidates<VT>(op, transpose, b, cands);
     const int lg = log2_width(b);
     const int ti = (lg <= 10) ? op->tuned[transpose ? 1 : 0][lg] : -1;
-    const bool needs_map = cands[ti >= 0 && ti < nc ? ti : 0].kind == CAND_TMA ||
-                           cands[ti >= 0 && ti < nc ? ti : 0].kind == CAND_TC;
-    if (ti >= 0 && ti < nc && (!needs_map || (xmap && error)))
+    const bool have_row = maps && maps->has_row && error;
+    const bool have_blk = error != nullptr;
+    auto usable = [&](const SpmmCand& c) {
+        if (c.kind == CAND_TMA || c.kind == CAND_TC) return have_row;
+        if (c.kind == CAND_BLK) return have_blk;
+        return true;
+    };
+    if (ti >= 0 && ti < nc && usable(cands[ti]))
         return spmm_cand<VT>(L, op, transpose, cands[ti], b, X, sx, shift, Y, Z, zc, zs, epi,
-                             partials, grid_out, xmap, error);
-    // built-in choice: TMA, then the row-group tile with the widest LV, then CSR
+                             partials, grid_out, maps, error);
+    // built-in choice: the tensor-core block kernel, TMA, then the row-group
+    // tile with the widest LV, then CSR
     int pick = 0;
     for (int i = 0; i < nc; ++i)
     {
-        if (cands[i].kind == CAND_TC) continue;  // chosen by the tuner only
-        if (cands[i].kind == CAND_TMA && !(xmap && error)) continue;
+        if (cands[i].kind == CAND_BLK && have_blk)
+        {
+            pick = i;
+            break;
+        }
+    }
+    for (int i = 0; i < nc && cands[pick].kind != CAND_BLK; ++i)
+    {
+        if (cands[i].kind == CAND_TC || cands[i].kind == CAND_BLK) continue;  // tuner / above
+        if (cands[i].kind == CAND_TMA && !have_row) continue;
         if (cands[i].kind == CAND_TMA)
         {
             pick = i;
@@ -1218,7 +1566,7 @@ slq_status op_spmm(Launcher& L, const slq_op* op, int transpose, int b, const VT
             pick = i;
     }
     return spmm_cand<VT>(L, op, transpose, cands[pick], b, X, sx, shift, Y, Z, zc, zs, epi,
-                         partials, grid_out, xmap, error);
+                         partials, grid_out, maps, error);
 }
 
 // TMA-streamed pass (k_stream): MODE 0 = update + inner products,
@@ -1472,30 +1820,35 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
     auto Vs = [&](int vec) { return V + static_cast<int64_t>(((vec % bs) + bs) % bs) * vslot; };
     auto Us = [&](int vec) { return U + static_cast<int64_t>(((vec % bs) + bs) % bs) * uslot; };
 
-    // TMA row-gather SpMM: one tensor map per basis slot
-    std::vector<CUtensorMap> vmaps, umaps;
+    // TMA-fed SpMM kernels: tensor maps per basis slot (V slots feed A
+    // products, U slots and the normal-equations buffer T feed A^T products)
+    std::vector<XMaps> vmaps, umaps;
     bool use_tma = false;
     if constexpr (sizeof(VT) == 4)
     {
-        if ((op->group_rows == 8 || op->group_rows == 16) && (b == 128 || b == 256))
+        const bool wide = (b == 128 || b == 256);
+        const bool row_a = wide && (op->group_rows == 8 || op->group_rows == 16);
+        if (row_a)
         {
             use_tma = true;
             vmaps.resize(bs);
             for (int sl = 0; sl < bs; ++sl)
-                SLQ_TRY(row_map(&vmaps[sl], V + static_cast<int64_t>(sl) * vslot, r.nv, b));
-            if (r.gram)
+                SLQ_TRY(make_xmaps(&vmaps[sl], V + static_cast<int64_t>(sl) * vslot, r.nv, b,
+                                   true));
+            if (r.gram == 1)
             {
                 umaps.resize(bs);
                 for (int sl = 0; sl < bs; ++sl)
-                    SLQ_TRY(row_map(&umaps[sl], U + static_cast<int64_t>(sl) * uslot, r.nu, b));
+                    SLQ_TRY(make_xmaps(&umaps[sl], U + static_cast<int64_t>(sl) * uslot, r.nu,
+                                       b, true));
             }
         }
     }
-    auto vmap_of = [&](int vec) -> const CUtensorMap* {
+    auto vmap_of = [&](int vec) -> const XMaps* {
         return use_tma ? &vmaps[((vec % bs) + bs) % bs] : nullptr;
     };
-    auto umap_of = [&](int vec) -> const CUtensorMap* {
-        return (use_tma && r.gram) ? &umaps[((vec % bs) + bs) % bs] : nullptr;
+    auto umap_of = [&](int vec) -> const XMaps* {
+        return (use_tma && r.gram == 1) ? &umaps[((vec % bs) + bs) % bs] : nullptr;
     };
 
     // dots + finalize(COEF) + reorth over chunks of MAX_J basis vectors;
@@ -1553,7 +1906,7 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
                 SLQ_TRY(op_spmm<VT>(L, op, 0, b, vj, sv_of(j), 0.0, T, nullptr, nullptr,
                                     nullptr, 0, B.partials, &sg1, vmap_of(j), B.error));
                 SLQ_TRY(op_spmm<VT>(L, op, 1, b, T, nullptr, 0.0, W, vj, B.negshift, sv_of(j),
-                                    3, B.partials, &sg));
+                                    3, B.partials, &sg, nullptr, B.error));
             }
             double* aj = B.alpha + static_cast<int64_t>(j) * b;
             SLQ_TRY(finalize<VT>(L, B.partials, sg, b, FIN_STORE, aj, nullptr, nullptr, b, bs, 0,
@@ -1906,13 +2259,13 @@ slq_status tune_typed(slq_op* op, int width, int transpose, int reps, const Tune
     SLQ_CK(cudaMemsetAsync(t.error, 0, sizeof(int32_t), st));
     k_fill_f64<<<(width + 255) / 256, 256, 0, st>>>(t.sx, width, 1.0);
     SLQ_LAUNCH_CK();
-    CUtensorMap map;
+    XMaps map;
     bool have_map = false;
     if constexpr (sizeof(VT) == 4)
     {
         if (width == 128 || width == 256)
         {
-            SLQ_TRY(row_map(&map, static_cast<const float*>(t.X), xrows, width));
+            SLQ_TRY(make_xmaps(&map, static_cast<const float*>(t.X), xrows, width, true));
             have_map = true;
         }
     }
@@ -2484,8 +2837,24 @@ extern "C" slq_status slq_operator_dot(slq_op* op, int transpose, double t, cons
         return op_spmm<double>(L, op, transpose, width, static_cast<const double*>(x), nullptr,
                                shift, static_cast<double*>(y), nullptr, nullptr, nullptr, 0,
                                nullptr, &grid);
-    return op_spmm<float>(L, op, transpose, width, static_cast<const float*>(x), nullptr, shift,
-                          static_cast<float*>(y), nullptr, nullptr, nullptr, 0, nullptr, &grid);
+    // an operator with the block format runs its block-wide products on the
+    // block kernel, whose error word lives in the format buffer (checked
+    // after the product)
+    const bool blk = (transpose ? op->t_bstage : op->a_bstage) != nullptr && op->blk_error &&
+                     (width == 128 || width == 256);
+    if (blk) SLQ_CK(cudaMemsetAsync(op->blk_error, 0, sizeof(int32_t), L.st));
+    SLQ_TRY(op_spmm<float>(L, op, transpose, width, static_cast<const float*>(x), nullptr, shift,
+                           static_cast<float*>(y), nullptr, nullptr, nullptr, 0, nullptr, &grid,
+                           nullptr, blk ? op->blk_error : nullptr));
+    if (blk)
+    {
+        int32_t herr = 0;
+        SLQ_CK(cudaMemcpyAsync(&herr, op->blk_error, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                               L.st));
+        SLQ_CK(cudaStreamSynchronize(L.st));
+        if (herr) return fail(SLQ_ERR_TIMEOUT, "operator_dot: the block kernel gave up waiting");
+    }
+    return SLQ_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -2535,13 +2904,6 @@ slq_status rcm_layout(Carver& c, int64_t n, RcmBufs* B)
     B->temp_bytes = std::max(t1, t2);
     B->temp = c.take<char>(B->temp_bytes);
     return SLQ_OK;
-}
-
-int bits_for(int64_t v)  // bits to hold 0 .. v
-{
-    int b = 1;
-    while (b < 63 && (int64_t(1) << b) <= v) ++b;
-    return b;
 }
 
 }  // namespace
@@ -2850,7 +3212,11 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 
 std::mutex g_noalloc_mutex;
 // device address of the scratch array, per device (host code must not use
-// the array's name as a device pointer)
+// the array's name as a device pointer).  Resolved by the first call on a
+// device and kept for the process: a cudaDeviceReset (or any reset of the
+// device's primary context) reloads the module and may move the array, after
+// which this cached address is stale, so this entry point must not be called
+// again on a device after its context was reset.
 uint64_t* g_noalloc_dev[NOALLOC_MAX_DEVICES] = {};
 // host staging of the scratch contents (static storage, no heap)
 uint64_t g_noalloc_host[NOALLOC_WORDS];
@@ -2877,6 +3243,19 @@ extern "C" slq_status slq_generate_probes_noalloc(int64_t seed, int rng, int64_t
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
         return fail(SLQ_ERR_BAD_ARG, "generate_probes_noalloc: device index out of range");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (rng == SLQ_RNG_PARITY)
+    {
+        // parity mode stages its scratch through host memory and waits for
+        // the copies; both would break a capture the caller has open on this
+        // stream, so refuse before touching the stream
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        SLQ_CK(cudaStreamIsCapturing(st, &cap));
+        if (cap != cudaStreamCaptureStatusNone)
+            return fail(SLQ_ERR_BAD_ARG,
+                        "generate_probes_noalloc: the parity probe stream (rng = "
+                        "SLQ_RNG_PARITY) copies host staging and synchronizes the "
+                        "stream, which a stream capture does not allow");
+    }
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!g_noalloc_dev[dev])
     {

@@ -233,13 +233,15 @@ class _DeviceOperator:
     """An ``slq_op`` plus the tensors it points into (kept alive here)."""
 
     def __init__(self, A, affine, need_transpose, check_indices=True,
-                 reorder="auto", group_rows="auto", aggregate=True):
+                 reorder="auto", group_rows="auto", aggregate=True,
+                 blocks=False):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("no CUDA device is available for the SLQ "
                                "engine (it has no CPU path)")
         self.device = torch.device("cuda", torch.cuda.current_device())
         self.dense = False
+        self.block_formats = []
         if A is None:
             return  # from_device / from_dense fill the fields
         dev = self.device
@@ -275,6 +277,13 @@ class _DeviceOperator:
             base = locality_order(A, reorder, device_pattern=pattern)
             self.group_rows, perm = group_rows_for(A, base, group_rows,
                                                    aggregate=aggregate)
+            blocks = blocks and A.dtype == np.float32
+            if blocks and self.group_rows == 16 and perm is not None and \
+                    A.shape[0] == A.shape[1]:
+                # 128-row blocks of eight aggregated 16-row groups whose
+                # column sets overlap (the groups stay whole, so the
+                # row-group format keeps its fill)
+                perm = block_order(A, perm, 16, 8)
         finally:
             if upload is not None:
                 upload[0].join()
@@ -314,11 +323,13 @@ class _DeviceOperator:
             self.inv[self.perm.long()] = torch.arange(
                 perm.size, dtype=torch.int32, device=dev)
         self._create(fmt, affine, need_transpose, check_indices)
+        if blocks:
+            self.add_blocks(need_transpose or fmt == _lib.SLQ_CSC)
 
     @classmethod
     def from_device(cls, indptr, indices, data, shape, affine=False,
                     need_transpose=False, group_rows=8, fmt=_lib.SLQ_CSR,
-                    check_indices=True, perm=None):
+                    check_indices=True, perm=None, blocks=False):
         """Operator over CSR (or CSC) arrays already on the device (torch
         int32 indptr / indices, float32 or float64 data), without copies.
         ``perm`` (a host int32 row order of a square CSR matrix, as
@@ -347,7 +358,35 @@ class _DeviceOperator:
             self.inv[self.perm.long()] = torch.arange(
                 pm.numel(), dtype=torch.int32, device=self.device)
         self._create(fmt, affine, need_transpose, check_indices)
+        if blocks and self.dtype_code == _lib.SLQ_F32:
+            self.add_blocks(need_transpose or fmt == _lib.SLQ_CSC)
         return self
+
+    def add_blocks(self, with_transpose=False):
+        """Attach the tensor-core block format (``slq_operator_add_blocks``:
+        128-row blocks of the stored rows, float32) for A and, with
+        ``with_transpose``, for A^T; block-wide SpMMs (128 or 256 probes)
+        then run on the tensor cores."""
+        import torch
+        lib = self._lib
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        for tr in ((0, 1) if with_transpose else (0,)):
+            nb = ctypes.c_size_t(0)
+            _lib.check(lib.slq_operator_blocks_scratch_bytes(
+                self.handle, tr, ctypes.byref(nb)))
+            scratch = torch.empty(max(int(nb.value), 256), dtype=torch.uint8,
+                                  device=self.device)
+            fb = ctypes.c_size_t(0)
+            _lib.check(lib.slq_operator_blocks_bytes(
+                self.handle, tr, scratch.data_ptr(), scratch.numel(), stream,
+                ctypes.byref(fb)))
+            fmt = torch.empty(max(int(fb.value), 256), dtype=torch.uint8,
+                              device=self.device)
+            _lib.check(lib.slq_operator_add_blocks(
+                self.handle, tr, scratch.data_ptr(), scratch.numel(),
+                fmt.data_ptr(), fmt.numel(), stream))
+            del scratch
+            self.block_formats.append(fmt)
 
     @classmethod
     def from_dense(cls, A, affine=False, need_transpose=False):
@@ -505,7 +544,8 @@ class LinearOperator:
                                  reorder=getattr(self, "reorder", "auto"),
                                  group_rows=getattr(self, "group_rows",
                                                     "auto"),
-                                 aggregate=getattr(self, "aggregate", True))
+                                 aggregate=getattr(self, "aggregate", True),
+                                 blocks=getattr(self, "blocks", False))
             self._device_ops[key] = op
         return op
 
@@ -523,14 +563,19 @@ class Matrix(LinearOperator):
     or 16) adds the row-group format and ``aggregate`` lets its groups be
     formed by neighbour aggregation (see ``group_rows_for``); the format
     itself changes no result bit, the aggregated order only the order of
-    floating-point sums.
+    floating-point sums.  ``blocks`` (float32) stores the rows in 128-row
+    blocks of overlapping column sets (``block_order``) and adds the
+    tensor-core block format, which block-wide SpMMs then use; results
+    change only by rounding (TF32 parts, three terms).
     """
 
-    def __init__(self, A, reorder="auto", group_rows="auto", aggregate=True):
+    def __init__(self, A, reorder="auto", group_rows="auto", aggregate=True,
+                 blocks=False):
         super().__init__()
         self.reorder = reorder
         self.group_rows = group_rows
         self.aggregate = aggregate
+        self.blocks = blocks
         if not (sp.issparse(A) or isinstance(A, np.ndarray)):
             raise TypeError("A should be a numpy array or a scipy sparse "
                             "matrix.")
@@ -567,10 +612,12 @@ class AffineMatrixFunction(LinearOperator):
     row-group width chosen once for that pattern.
     """
 
-    def __init__(self, A, B=None, reorder="auto", group_rows="auto"):
+    def __init__(self, A, B=None, reorder="auto", group_rows="auto",
+                 blocks=False):
         super().__init__()
         self.reorder = reorder
         self.group_rows = group_rows
+        self.blocks = blocks
         self.A = A
         self.B = B
         self.num_parameters = 1
@@ -717,7 +764,7 @@ class GramAffineMatrixFunction(LinearOperator):
     shift with t, so one Krylov run per probe serves a sweep of t.
     """
 
-    def __init__(self, A):
+    def __init__(self, A, blocks=False):
         super().__init__()
         if not sp.issparse(A):
             A = sp.csr_matrix(A)
@@ -726,6 +773,7 @@ class GramAffineMatrixFunction(LinearOperator):
         self.normal_equations = True
         self.reorder = False
         self.group_rows = 0
+        self.blocks = blocks
         self.set_data_type_name(A)
 
     def _affine(self):

@@ -109,6 +109,33 @@ slq_status slq_operator_create(const void* data, const int32_t* indices,
                                size_t workspace_bytes, void* stream,
                                slq_op** out);
 
+/* Tensor-core block format of a float32 sparse operator (no counterpart in
+ * the reference, whose products are one cusparseSpMV per probe,
+ * imate/_cu_basic_algebra/cusparse_interface.cu:243, through
+ * cuCSRMatrix::dot, imate/_cu_linear_operator/cu_csr_matrix.cu:278-318).
+ * The stored rows of A (transpose = 0) or of A^T (transpose = 1) are cut
+ * into blocks of 128 consecutive rows; each block keeps the sorted union of
+ * its column indices and its values as a dense 128 x union matrix (TF32
+ * parts are taken in the product), so that one SpMM over b = 128 or 256
+ * probes runs on the tensor cores (tcgen05 kind::tf32, three terms: about
+ * FP32 accuracy).  Its cost follows the union sizes: store the operator with
+ * a row order whose consecutive 128-row blocks share columns
+ * (slq_block_order).  Built on the device in two calls that use the same
+ * scratch: slq_operator_blocks_bytes sizes the format (it synchronizes the
+ * stream), slq_operator_add_blocks builds it into `format` (caller memory
+ * that must outlive the operator) and attaches it; the scratch can be
+ * released after it returns.  Duplicate (row, column) entries are summed.
+ * Products at b = 128 / 256 then use it (slq_run, batch plans, the tuner)
+ * unless the tuner picked another candidate. */
+slq_status slq_operator_blocks_scratch_bytes(const slq_op* op, int transpose,
+                                             size_t* bytes);
+slq_status slq_operator_blocks_bytes(const slq_op* op, int transpose,
+                                     void* scratch, size_t scratch_bytes,
+                                     void* stream, size_t* format_bytes);
+slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* scratch,
+                                   size_t scratch_bytes, void* format,
+                                   size_t format_bytes, void* stream);
+
 /* Reverse Cuthill-McKee order of a square CSR pattern (host arrays; the
  * pattern is taken as symmetric).  Each connected component starts at its
  * lowest-degree row and is visited breadth-first with the children of a row
@@ -428,9 +455,13 @@ slq_status slq_generate_probes_workspace_bytes(int64_t len, int width,
  * fixed 288 KB array inside the library, held by every GPU that loads it.
  * Limit: width <= 1024 probes per call (SLQ_ERR_BAD_ARG beyond).  The first
  * call on a device resolves the array's device address, so make that first
- * call before any stream capture.  All calls share the array: calls that
- * overlap on the GPU (other streams, other host threads) race; each call
- * synchronizes its stream after staging the parity-mode scratch. */
+ * call before any stream capture; the address is kept for the process, so
+ * after a reset of the device's context (cudaDeviceReset) do not call this
+ * function on that device again.  All calls share the array: calls that
+ * overlap on the GPU (other streams, other host threads) race.  In parity
+ * mode (SLQ_RNG_PARITY) each call stages the scratch through host memory and
+ * synchronizes its stream, and it returns SLQ_ERR_BAD_ARG, before touching
+ * the stream, when that stream is capturing. */
 slq_status slq_generate_probes_noalloc(int64_t seed, int rng, int64_t len,
                                        int64_t first, int count, int width,
                                        int dtype, void* out, void* stream);

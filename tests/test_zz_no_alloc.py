@@ -24,6 +24,10 @@ CASES = [
     (1, 0, 65, 2, 1, 1, _lib.SLQ_F32),
     (11, 1, 4097, 3, 200, 256, _lib.SLQ_F32),
     (0, 0, 262144, 0, 256, 256, _lib.SLQ_F32),
+    # 531,251 words per probe: more than the fixed scratch's 8192 chunks of
+    # 64 words, so this call takes 128-word chunks where the workspace path
+    # keeps 64 (136 MB of output)
+    (5, 0, 34_000_000, 1, 1, 1, _lib.SLQ_F32),
 ]
 
 
@@ -70,3 +74,48 @@ def test_noalloc_rejects_width_beyond_its_scratch(cuda):
         torch.cuda.current_stream().cuda_stream)
     assert st == 1  # SLQ_ERR_BAD_ARG
     assert b"1024" in cuda.slq_last_error()
+
+
+def test_noalloc_calls_leave_device_free_memory_unchanged(cuda):
+    """The point of this entry point: after a first call on the device has
+    resolved the scratch array's address and loaded the kernels, further
+    calls take no device memory (free bytes before and after are equal)."""
+    import torch
+    seed, rng, n, first, count, width, dtype = 7, 0, 70001, 5, 50, 64, \
+        _lib.SLQ_F32
+    out = torch.empty((n, width), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for r in (0, 1):  # warm-up: both probe streams' kernels loaded
+        _lib.check(cuda.slq_generate_probes_noalloc(
+            seed, r, n, first, count, width, dtype, out.data_ptr(), stream))
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for r in (0, 1, 0, 1):
+        _lib.check(cuda.slq_generate_probes_noalloc(
+            seed, r, n, first, count, width, dtype, out.data_ptr(), stream))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+
+
+def test_noalloc_parity_mode_refuses_a_capturing_stream(cuda):
+    """Parity mode copies its scratch from host staging and waits for the
+    copies; on a stream that is being captured it must return
+    SLQ_ERR_BAD_ARG without touching the stream, so the caller's capture
+    stays valid, and the next ordinary call still gives the right probes."""
+    import torch
+    case = (3, 0, 1000, 0, 8, 8, _lib.SLQ_F32)
+    want = _with_workspace(cuda, *case)
+    out = torch.zeros((1000, 8), dtype=torch.float32, device="cuda")
+    side = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=side):
+        st = cuda.slq_generate_probes_noalloc(
+            3, 0, 1000, 0, 8, 8, _lib.SLQ_F32, out.data_ptr(),
+            side.cuda_stream)
+        msg = cuda.slq_last_error()
+        out.add_(1.0)  # the capture itself stays usable
+    del graph
+    torch.cuda.synchronize()
+    assert st == 1  # SLQ_ERR_BAD_ARG
+    assert b"capture" in msg
+    assert np.array_equal(_without_workspace(cuda, *case), want)
