@@ -1,97 +1,103 @@
-// Block SpMM on the tensor cores (tcgen05 kind::tf32), sm_100a.
+// Block SpMM on the tensor cores (tcgen05 kind::f16, FP32 accumulation),
+// sm_100a.
 //
 // Y[M][b] = A[M][K] X[K][b] for a sparse FP32 A whose rows are cut into
 // blocks of 128 consecutive rows.  Each block keeps the sorted union of its
 // rows' column indices (padded to a multiple of 16 with copies of its last
 // column, zero-valued) and its values as a dense 128 x union matrix, zero
 // where a row lacks a column.  A block is one M = 128 tile: its union
-// columns are the K dimension, the b <= 256 probes the N dimension, so every
-// gathered row of X (1 KB at b = 256) feeds 128 rows of products and the
-// tensor core does the multiply-adds.  Fill (nonzeros over 128 x union)
-// decides the cost: blocks made of rows with overlapping neighbourhoods
-// (slq_block_order) matter.
+// columns are the K dimension, the b = 128 or 256 probes the N dimension, so
+// every gathered row of X feeds 128 rows of products on the tensor core.
+// Fill (nonzeros over 128 x union) decides the cost: blocks made of rows
+// with overlapping neighbourhoods (slq_block_order) matter.
+//
+// FP32 accuracy from FP16 operands: each operand is split into two FP16
+// parts, hi = rn_f16(v) and lo = rn_f16(v - hi) (22 significant bits
+// together), after a power-of-two scaling that keeps the parts in FP16's
+// range: row r of A by 2^f_r (its largest |a| to [2^13, 2^14)), probe p of X
+// by 2^e_p (its norm 1 / s_p, or its largest |x| when no norm is known, to
+// at most 2^14, so every element fits).  Three products per K step, A_lo
+// X_hi + A_hi X_lo + A_hi X_hi, accumulate in FP32 in tensor memory; the
+// dropped lo x lo term and the rounding of the lo parts leave about 2^-22
+// relative error per product.  The epilogue multiplies by 2^-f_r 2^-e_p s_p
+// (exact powers of two times s_p).  The tensor core's FP32 accumulation
+// truncates; over the ~40 K steps of a block that shrinks |y| by about 1e-6
+// relative.
 //
 // Format (built on the device by k_blk_* below):
 //   bstage[nblk + 1]   first 16-column stage of each block (exclusive sum)
 //   ucol[16 * stages]  union column indices, stage by stage
-//   img[stages][2][2048]  TF32 parts of each stage's values, hi = rn_tf32(a)
-//                      then lo = rn_tf32(a - hi), each 128 rows x 16 columns
-//                      in the K-major no-swizzle layout the MMA reads:
-//                      element (r, k) at float offset (r % 8) * 4 + (r / 8) *
-//                      128 + (k / 4) * 32 + (k % 4) (core matrices of 8 rows
-//                      x 4 values; leading byte offset 128 between K-adjacent
-//                      core matrices, stride byte offset 512 between 8-row
-//                      groups)
-// so one stage of A is one contiguous 16 KB bulk copy.
+//   rsc[nblk * 128]    2^-f_r per stored row (1 for the padding rows)
+//   img[stages][2][2048]  FP16 parts (hi then lo) of each stage's scaled
+//                      values, 128 rows x 16 columns in the K-major
+//                      no-swizzle layout the MMA reads: element (r, k) at
+//                      half offset (r % 8) * 8 + (r / 8) * 128 + (k / 8) * 64
+//                      + (k % 8) (core matrices of 8 rows x 8 values; leading
+//                      byte offset 128 between the two K core matrices,
+//                      stride byte offset 256 between 8-row groups)
+// so one stage of A is one contiguous 8 KB bulk copy.
 //
 // Kernel k_spmm_blk (persistent, one CTA per SM, blocks dealt round-robin):
 //   warp 8        producer: per stage, one cp.async.bulk of the A parts;
 //   warps 10-17   converters: load the stage's 16 X rows from global memory
-//                 (two stages ahead, into registers), split them into TF32
-//                 parts, hi = rn_tf32(x) and lo = rn_tf32(x - hi) (integer
-//                 rounding of the bit patterns), and store both in the
-//                 MN-major 128-byte-swizzle-with-32-byte-atoms layout (4 K
-//                 rows x 32 probes per atom).  TMA gathers of the X rows would
-//                 need one gather4 per 512 bytes (the swizzle limits a box row
-//                 to 128 bytes), which measured slower than these loads;
-//   warp 9        MMA issuer: per K step of 8 the three products A_lo X_hi
-//                 + A_hi X_lo + A_hi X_hi into an FP32 accumulator in tensor
-//                 memory (lane = block row, column = probe), two
-//                 accumulators so the epilogue of one block overlaps the
-//                 products of the next;
+//                 (two stages ahead, into registers), scale and split them
+//                 into FP16 parts and store both in the MN-major 128-byte
+//                 swizzled layout (atoms of 8 K rows x 64 probes).  TMA
+//                 gathers of X rows (one 128-byte box row per gathered row
+//                 segment under the swizzle) measured slower than these loads;
+//   warp 9        MMA issuer: per stage (K = 16) the three products into an
+//                 FP32 accumulator in tensor memory (lane = block row,
+//                 column = probe), two accumulators so the epilogue of one
+//                 block overlaps the products of the next;
 //   warps 0-7     epilogue: the SpMM epilogue of the other kernels (probe
 //                 scales, affine shift, three-term subtraction, partial sums
 //                 of alpha or |y|^2) on the finished accumulator; its
-//                 element arithmetic is FP32 (y = s A x rounded once more
-//                 than the FP64 form, the terms x y, y y, z y one rounding
-//                 each) and the row sums FP64, the per-probe factor applied
-//                 to the sums.
-// The dropped A_lo X_lo term and the rounding of the lo parts leave about
-// 2^-22 relative error per product; the accumulation runs in the tensor
-// core's FP32.  Every mbarrier wait is bounded; a wait that runs out sets
-// the error word and the CTA drains its copies and MMAs before it leaves.
-// No multicast: every TMA load reads this GPU's own buffers.
+//                 element arithmetic is FP32 (y rounded once more than the
+//                 FP64 form, the terms x y, y y, z y one rounding each), the
+//                 sums over a warp's 32 rows FP32 and all further sums FP64,
+//                 the per-probe factor applied to the sums.
+// Every mbarrier wait is bounded; a wait that runs out sets the error word
+// and the CTA drains its copies and MMAs before it leaves.  No multicast: the
+// only TMA copies read this GPU's own format buffer.
 
 #ifndef SLQ_BLK_CUH_
 #define SLQ_BLK_CUH_
+
+#include <cuda_fp16.h>
 
 #include "slq_kernels.cuh"
 
 namespace slq {
 
 constexpr int BLK_ROWS = 128;
-constexpr int BLK_BK = 16;            // union columns per stage
-constexpr int BLK_STAGES = 4;
-constexpr int BLK_A_BYTES = BLK_ROWS * BLK_BK * 4;  // 8 KB per A part
-constexpr int BLK_IMG_STAGE = 2 * BLK_ROWS * BLK_BK;   // floats per stage image (hi, lo)
+constexpr int BLK_BK = 16;            // union columns per stage (one K step)
+constexpr int BLK_STAGES = 8;
+constexpr int BLK_A_PART = BLK_ROWS * BLK_BK * 2;     // 4 KB per FP16 part
+constexpr int BLK_IMG_STAGE = 2 * BLK_ROWS * BLK_BK;  // halves per stage image
 constexpr int BLK_EPI_WARPS = 8;
 constexpr int BLK_PRODUCER = 8;       // warp indices
 constexpr int BLK_MMA = 9;
 constexpr int BLK_CONV0 = 10;
 constexpr int BLK_CONV_WARPS = 8;
 constexpr int BLK_THREADS = (BLK_CONV0 + BLK_CONV_WARPS) * 32;  // 576
-constexpr int BLK_AHEAD = 2;          // stages of X rows loaded ahead
+constexpr int BLK_TAIL = 512;         // barriers, tensor-memory address, flags
+
+__host__ __device__ constexpr uint32_t blk_x_part(int nb)
+{
+    return static_cast<uint32_t>(nb) * BLK_BK * 2u;   // one FP16 part of X
+}
 
 __host__ __device__ constexpr uint32_t blk_stage_bytes(int nb)
 {
-    return 2u * BLK_A_BYTES + 2u * static_cast<uint32_t>(nb) * BLK_BK * 4u;
+    return 2u * BLK_A_PART + 2u * blk_x_part(nb);
 }
 
-// stages, barriers (256 bytes), partial sums [4][256] (doubles) and the
-// per-probe epilogue constants [3][256] (floats)
+// stages, barriers, partial sums [4][256] (doubles), the per-probe
+// constants [4][256] (floats)
 __host__ __device__ constexpr size_t blk_smem_bytes(int nb)
 {
-    return 1023 + static_cast<size_t>(BLK_STAGES) * blk_stage_bytes(nb) + 256 +
-           4 * 256 * sizeof(double) + 3 * 256 * sizeof(float);
-}
-
-// TF32 parts by integer rounding of the bit patterns (round half away
-// from zero on the 13 dropped mantissa bits): hi = rn_tf32(x), lo =
-// rn_tf32(x - hi), the x - hi difference exact in FP32.  Integer adds and
-// masks keep the conversion off the conversion pipe.
-__device__ __forceinline__ float round_tf32_bits(float x)
-{
-    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+    return 1023 + static_cast<size_t>(BLK_STAGES) * blk_stage_bytes(nb) + BLK_TAIL +
+           4 * 256 * sizeof(double) + 4 * 256 * sizeof(float);
 }
 
 // ---------------------------------------------------------------------------
@@ -180,13 +186,48 @@ __global__ void k_blk_pad(const int32_t* __restrict__ cnt, const int32_t* __rest
     }
 }
 
-// values into the stage images (zeroed first); atomic adds only sum
-// duplicate (row, column) entries, each slot otherwise receives one value
+// Row scales: fsc[r] = 2^f_r with the row's largest |a| scaled into
+// [2^13, 2^14) (f_r = 0 for an empty or all-zero row), rsc[r] = 2^-f_r;
+// rows past `rows` (the last block's padding) get 1.  One warp per row.
+__global__ void k_blk_rowscale(const int32_t* __restrict__ ptr, const float* __restrict__ val,
+                               int64_t rows, int64_t padded, float* __restrict__ fsc,
+                               float* __restrict__ rsc)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t row = w0; row < padded; row += nw)
+    {
+        float mx = 0.0f;
+        if (row < rows)
+            for (int64_t e = ptr[row] + lane; e < ptr[row + 1]; e += 32)
+                mx = fmaxf(mx, fabsf(val[e]));
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(FULL_MASK, mx, off));
+        if (lane == 0)
+        {
+            int f = 0;
+            if (mx > 0.0f && isfinite(mx))
+            {
+                int ex = 0;
+                frexpf(mx, &ex);  // mx = m 2^ex, m in [0.5, 1)
+                f = min(max(14 - ex, -120), 120);
+            }
+            fsc[row] = ldexpf(1.0f, f);
+            rsc[row] = ldexpf(1.0f, -f);
+        }
+    }
+}
+
+// values into FP32 staging images, tmp[stage][128][16] (zeroed first; the
+// same 8 KB per stage that the FP16 parts take afterwards); atomic adds only
+// sum duplicate (row, column) entries, each slot otherwise receives one
+// value
 __global__ void k_blk_scatter(const uint64_t* __restrict__ keys, const int32_t* __restrict__ pos,
                               const int32_t* __restrict__ uidx, int64_t nnz, int cbits,
                               const int32_t* __restrict__ ufirst,
                               const int32_t* __restrict__ bstage, const float* __restrict__ vals,
-                              const uint8_t* __restrict__ rr, float* __restrict__ img)
+                              const uint8_t* __restrict__ rr, float* __restrict__ tmp)
 {
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nnz;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
@@ -194,30 +235,67 @@ __global__ void k_blk_scatter(const uint64_t* __restrict__ keys, const int32_t* 
         const int64_t blk = static_cast<int64_t>(keys[i] >> cbits);
         const int64_t j = uidx[i] - 1 - ufirst[blk];
         const int32_t e = pos[i];
-        const int r = rr[e];
-        const int kk = static_cast<int>(j % BLK_BK);
         const int64_t stage = bstage[blk] + j / BLK_BK;
-        const int64_t off = stage * BLK_IMG_STAGE + (r & 7) * 4 + (r >> 3) * 128 +
-                            (kk >> 2) * 32 + (kk & 3);
-        atomicAdd(&img[off], vals[e]);
+        atomicAdd(&tmp[(stage * BLK_ROWS + rr[e]) * BLK_BK + j % BLK_BK], vals[e]);
     }
 }
 
-// TF32 parts of the stage images in place: the values (scattered into the
-// hi half) become hi = rn_tf32(a), the lo half rn_tf32(a - hi)
-
-__global__ void k_blk_split(float* __restrict__ img, int64_t stages)
+// In place, per stage (one CTA of 256 threads per stage at a time): the
+// 2048 staged FP32 values of a stage become its FP16 parts, hi =
+// rn_f16(a 2^f_r) and lo = rn_f16(a 2^f_r - hi), in the MMA's K-major
+// layout; the stage's block comes from a binary search of bstage.
+__global__ void __launch_bounds__(256)
+k_blk_split(void* __restrict__ img, const int32_t* __restrict__ bstage, int64_t nblk,
+            const float* __restrict__ fsc, int64_t stages)
 {
-    const int64_t total = stages * (BLK_ROWS * BLK_BK);
-    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    constexpr int PER = BLK_ROWS * BLK_BK / 256;  // values per thread
+    for (int64_t st = blockIdx.x; st < stages; st += gridDim.x)
     {
-        float* h = img + (i / (BLK_ROWS * BLK_BK)) * BLK_IMG_STAGE + i % (BLK_ROWS * BLK_BK);
-        const float a = *h;
-        const float hi = round_tf32_bits(a);
-        h[BLK_ROWS * BLK_BK] = round_tf32_bits(a - hi);
-        *h = hi;
+        int64_t lo_b = 0, hi_b = nblk - 1;  // last block with bstage <= st
+        while (lo_b < hi_b)
+        {
+            const int64_t mid = (lo_b + hi_b + 1) / 2;
+            if (bstage[mid] <= st) lo_b = mid;
+            else hi_b = mid - 1;
+        }
+        float* src = reinterpret_cast<float*>(img) + st * (BLK_ROWS * BLK_BK);
+        float a[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u) a[u] = src[threadIdx.x + u * 256];
+        __syncthreads();
+        __half* dst = reinterpret_cast<__half*>(img) + st * BLK_IMG_STAGE;
+#pragma unroll
+        for (int u = 0; u < PER; ++u)
+        {
+            const int i = threadIdx.x + u * 256;
+            const int r = i / BLK_BK, k = i % BLK_BK;
+            const float v = a[u] * fsc[lo_b * BLK_ROWS + r];
+            const __half h = __float2half_rn(v);
+            const __half l = __float2half_rn(v - __half2float(h));
+            __half* o = dst + (r & 7) * 8 + (r >> 3) * 128 + (k >> 3) * 64 + (k & 7);
+            o[0] = h;
+            o[BLK_ROWS * BLK_BK] = l;
+        }
+        __syncthreads();
     }
+}
+
+// Per-probe largest |x| of an X whose norms are not known (the products
+// that get no probe scale): mx[p] (zeroed first) receives the maximum as the
+// bit pattern of a non-negative float, by atomicMax; non-finite values count
+// as zero.  Block = 256 threads = 8 rows x 32 probes; grid.y = b / 32.
+__global__ void k_blk_colmax(const float* __restrict__ X, int64_t rows, int b,
+                             unsigned int* __restrict__ mx)
+{
+    const int q = blockIdx.y * 32 + (threadIdx.x & 31);
+    float m = 0.0f;
+    for (int64_t r = static_cast<int64_t>(blockIdx.x) * 8 + (threadIdx.x >> 5); r < rows;
+         r += static_cast<int64_t>(gridDim.x) * 8)
+    {
+        const float v = fabsf(X[r * b + q]);
+        if (isfinite(v)) m = fmaxf(m, v);
+    }
+    atomicMax(&mx[q], __float_as_uint(m));
 }
 
 // ---------------------------------------------------------------------------
@@ -230,9 +308,11 @@ struct BlkArgs {
     int NB;                    // probes = b (128 or 256)
     const int32_t* bstage;
     const int32_t* ucol;
-    const float* img;
+    const float* rsc;
+    const __half* img;
     const float* X;
-    const double* sx;
+    const double* sx;          // per-probe scale s_p of X (norm 1 / s_p), or NULL
+    const unsigned int* xmax;  // sx == NULL: per-probe max |x| (float bits)
     double shift;
     float* Y;
     const float* Z;
@@ -243,31 +323,32 @@ struct BlkArgs {
     int32_t* error;
 };
 
-__device__ __forceinline__ void split1(float& x, float& lo)
+// FP16 parts of four scaled values, packed: hi = rn_f16(v), lo =
+// rn_f16(v - hi)
+__device__ __forceinline__ void split_h4(float4 v, uint2& hi, uint2& lo)
 {
-    const float h = round_tf32_bits(x);
-    lo = round_tf32_bits(x - h);
-    x = h;
-}
-
-__device__ __forceinline__ void split4(float4& v, float4& lo)
-{
-    split1(v.x, lo.x);
-    split1(v.y, lo.y);
-    split1(v.z, lo.z);
-    split1(v.w, lo.w);
+    const __half2 h01 = __floats2half2_rn(v.x, v.y);
+    const __half2 h23 = __floats2half2_rn(v.z, v.w);
+    const float2 f01 = __half22float2(h01);
+    const float2 f23 = __half22float2(h23);
+    const __half2 l01 = __floats2half2_rn(v.x - f01.x, v.y - f01.y);
+    const __half2 l23 = __floats2half2_rn(v.z - f23.x, v.w - f23.y);
+    hi = make_uint2(*reinterpret_cast<const uint32_t*>(&h01),
+                    *reinterpret_cast<const uint32_t*>(&h23));
+    lo = make_uint2(*reinterpret_cast<const uint32_t*>(&l01),
+                    *reinterpret_cast<const uint32_t*>(&l23));
 }
 
 // Reduce-scatter of 16 per-lane values over the warp's 32 lanes: on return
 // lanes 0-15 hold the sum over all lanes of value blk_col(lane), lanes
-// 16-31 the same sums again.  16 shuffles of doubles instead of 16 x 5 for
-// 16 separate tree reductions; the order of the additions is fixed.
+// 16-31 the same sums again.  16 shuffles instead of 16 x 5 for 16 separate
+// tree reductions; the order of the additions is fixed.
 __device__ __forceinline__ int blk_col(int lane)
 {
     return 8 * (lane & 1) + 4 * ((lane >> 1) & 1) + 2 * ((lane >> 2) & 1) + ((lane >> 3) & 1);
 }
 
-__device__ __forceinline__ double reduce_scatter16(double (&a)[16], int lane)
+__device__ __forceinline__ float reduce_scatter16(float (&a)[16], int lane)
 {
 #pragma unroll
     for (int st = 0; st < 4; ++st)
@@ -277,20 +358,66 @@ __device__ __forceinline__ double reduce_scatter16(double (&a)[16], int lane)
 #pragma unroll
         for (int i = 0; i < h; ++i)
         {
-            const double send = upper ? a[i] : a[i + h];
-            const double keep = upper ? a[i + h] : a[i];
+            const float send = upper ? a[i] : a[i + h];
+            const float keep = upper ? a[i + h] : a[i];
             a[i] = keep + __shfl_xor_sync(FULL_MASK, send, 1 << st);
         }
     }
     return a[0] + __shfl_xor_sync(FULL_MASK, a[0], 16);
 }
 
+// Position in a CTA's stage sequence: its blocks blockIdx.x, + gridDim.x, ...
+// and each block's stages in order.
+struct BlkCursor {
+    int64_t blk;
+    int st, s1;
+
+    __device__ void start(const int32_t* bstage, int64_t nblk)
+    {
+        blk = blockIdx.x;
+        st = s1 = 0;
+        if (blk < nblk)
+        {
+            st = bstage[blk];
+            s1 = bstage[blk + 1];
+        }
+    }
+
+    __device__ void advance(const int32_t* bstage, int64_t nblk)
+    {
+        if (blk >= nblk) return;
+        if (++st >= s1)
+        {
+            blk += gridDim.x;
+            if (blk < nblk)
+            {
+                st = bstage[blk];
+                s1 = bstage[blk + 1];
+            }
+        }
+    }
+
+    // union row k of the current stage (-1 past the end)
+    __device__ int row(const int32_t* ucol, int64_t nblk, int k) const
+    {
+        return blk < nblk ? ucol[int64_t(st) * BLK_BK + k] : -1;
+    }
+};
+
+// Instruction descriptor, kind::f16 with FP16 A and B, FP32 D, M = 128, A
+// K-major, B MN-major (transpose bit 16), N = nb
+__host__ __device__ constexpr uint32_t blk_idesc(uint32_t nb)
+{
+    return (1u << 4) | (1u << 16) | ((nb >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+template <int NB>
 __global__ void __launch_bounds__(BLK_THREADS, 1)
 k_spmm_blk(const BlkArgs d)
 {
     extern __shared__ __align__(1024) unsigned char smem_blk[];
-    const uint32_t stage_bytes = blk_stage_bytes(d.NB);
-    const uint32_t x_bytes = static_cast<uint32_t>(d.NB) * BLK_BK * 4;  // one X part
+    const uint32_t stage_bytes = blk_stage_bytes(NB);
+    const uint32_t x_bytes = blk_x_part(NB);
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_blk) + 1023) & ~uintptr_t(1023));
     unsigned char* tail = base + BLK_STAGES * stage_bytes;
@@ -302,17 +429,18 @@ k_spmm_blk(const BlkArgs d)
     uint64_t* drain = acc_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 2);  // [2]
-    double* red = reinterpret_cast<double*>(tail + 256);      // [4][256]
-    // per-probe epilogue constants in FP32: s_p, t s_p (affine shift) and
-    // zc_p zs_p (three-term subtraction)
-    float* c_sx = reinterpret_cast<float*>(red + 4 * 256);
+    double* red = reinterpret_cast<double*>(tail + BLK_TAIL);  // [4][256]
+    // per-probe constants in FP32: 2^e_p (X scaling), s_p 2^-e_p, t s_p
+    // (affine shift), zc_p zs_p (three-term subtraction)
+    float* c_xs = reinterpret_cast<float*>(red + 4 * 256);
+    float* c_sx = c_xs + 256;
     float* c_ts = c_sx + 256;
     float* c_zcs = c_ts + 256;
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const int lane = tid & 31;
-    const uint32_t tmem_cols = 2u * static_cast<uint32_t>(d.NB);
+    const uint32_t tmem_cols = 2u * static_cast<uint32_t>(NB);
     if (tid == 0)
     {
         for (int s = 0; s < BLK_STAGES; ++s)
@@ -332,10 +460,28 @@ k_spmm_blk(const BlkArgs d)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = tid; i < 4 * 256; i += BLK_THREADS) red[i] = 0.0;
-    for (int p = tid; p < d.NB; p += BLK_THREADS)
+    for (int p = tid; p < NB; p += BLK_THREADS)
     {
+        // 2^e_p keeps every scaled |x| <= 2^14: |x| <= |x|_2 = 1 / s_p, or
+        // the measured maximum when no scale is given
         const double sxv = d.sx ? d.sx[p] : 1.0;
-        c_sx[p] = static_cast<float>(sxv);
+        int e = 0;
+        if (d.sx)
+        {
+            if (sxv > 0.0 && isfinite(sxv)) e = min(max(ilogb(sxv) + 13, -120), 120);
+        }
+        else
+        {
+            const float m = __uint_as_float(d.xmax[p]);
+            if (m > 0.0f)
+            {
+                int ex = 0;
+                frexpf(m, &ex);
+                e = min(max(14 - ex, -120), 120);
+            }
+        }
+        c_xs[p] = ldexpf(1.0f, e);
+        c_sx[p] = static_cast<float>(ldexp(sxv, -e));
         c_ts[p] = static_cast<float>(d.shift * sxv);
         c_zcs[p] = d.Z ? static_cast<float>(d.zc[p] * d.zs[p]) : 0.0f;
     }
@@ -355,7 +501,7 @@ k_spmm_blk(const BlkArgs d)
 
     if (warp == BLK_PRODUCER)
     {
-        // producer: the A parts of every stage, one 16 KB bulk copy each
+        // producer: the A parts of every stage, one 8 KB bulk copy each
         if (lane == 0)
         {
             int64_t it = 0;
@@ -374,8 +520,8 @@ k_spmm_blk(const BlkArgs d)
                         break;
                     }
                     unsigned char* stp = base + static_cast<size_t>(s) * stage_bytes;
-                    mbar_expect_tx(&full[s], static_cast<uint32_t>(2 * BLK_A_BYTES));
-                    bulk_copy_g2s(stp, d.img + int64_t(st) * BLK_IMG_STAGE, 2 * BLK_A_BYTES,
+                    mbar_expect_tx(&full[s], static_cast<uint32_t>(2 * BLK_A_PART));
+                    bulk_copy_g2s(stp, d.img + int64_t(st) * BLK_IMG_STAGE, 2 * BLK_A_PART,
                                   &full[s]);
                 }
             }
@@ -391,73 +537,42 @@ k_spmm_blk(const BlkArgs d)
     }
     else if (warp >= BLK_CONV0)
     {
-        // converters.  X: thread ct takes union row k = ct / 16 of each stage
-        // and its float4 slices f = ct % 16 + 16 j (probes 4f .. 4f + 3),
-        // loaded from global memory BLK_AHEAD stages ahead (row index one
-        // stage before that), split into TF32 parts and stored in the
-        // MN-major layout: probe n of row k at atom n / 32 (2 KB apart), K
-        // atom k / 4 (512 bytes apart), row k % 4 (128 bytes), 32-byte chunk
-        // (n % 32) / 8 XOR k % 4.
+        // converters.  Thread ct takes union row k = ct / 16 of each stage
+        // and its float4 slices f = ct % 16 + 16 j (probes 4f .. 4f + 3, MN
+        // atom j), loaded from global memory two stages ahead (row index one
+        // stage before that), scaled by 2^e_p, split into FP16 parts and
+        // stored in the MN-major 128-byte swizzled layout: probe n of row k
+        // at atom n / 64 (2 KB apart), K atom k / 8 (1 KB apart), row k % 8
+        // (128 bytes), 16-byte chunk (n % 64) / 8 XOR k % 8.
         const int ct = tid - BLK_CONV0 * 32;
         const int k = ct >> 4;
-        const int nj = d.NB / 64;          // float4 slices per thread (2 or 4)
-        uint32_t xoff[4];                  // byte offsets of the slices in an X part
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-        {
-            const int f = (ct & 15) + 16 * j;
-            const int c = ((f & 7) >> 1) ^ (k & 3);
-            xoff[j] = static_cast<uint32_t>((f >> 3) * 2048 + (k >> 2) * 512 + (k & 3) * 128 +
-                                            c * 32 + (f & 1) * 16);
-        }
-        // stage cursors: the one being converted, the one whose X rows are
-        // loading, the one whose row index is loading
-        struct Cursor {
-            int64_t blk;
-            int st, s1;
-        };
-        auto start = [&](Cursor& c) {
-            c.blk = blockIdx.x;
-            c.st = c.s1 = 0;
-            if (c.blk < d.nblk)
-            {
-                c.st = d.bstage[c.blk];
-                c.s1 = d.bstage[c.blk + 1];
-            }
-        };
-        auto advance = [&](Cursor& c) {
-            if (c.blk >= d.nblk) return;
-            if (++c.st >= c.s1)
-            {
-                c.blk += gridDim.x;
-                if (c.blk < d.nblk)
-                {
-                    c.st = d.bstage[c.blk];
-                    c.s1 = d.bstage[c.blk + 1];
-                }
-            }
-        };
-        auto row_of = [&](const Cursor& c) -> int {
-            return c.blk < d.nblk ? d.ucol[int64_t(c.st) * BLK_BK + k] : -1;
-        };
+        constexpr int nj = NB / 64;        // float4 slices per thread (2 or 4)
+        const uint32_t xoff0 = static_cast<uint32_t>(
+            (k >> 3) * 1024 + (k & 7) * 128 + ((((ct & 15) >> 1) ^ (k & 7)) << 4) + (ct & 1) * 8);
         auto load_x = [&](int row, float4 (&buf)[4]) {
+            if (row < 0) return;
+            const float4* src = reinterpret_cast<const float4*>(d.X + int64_t(row) * NB) + (ct & 15);
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (j < nj && row >= 0)
-                    buf[j] = __ldg(reinterpret_cast<const float4*>(d.X + int64_t(row) * d.NB) +
-                                   (ct & 15) + 16 * j);
+            for (int j = 0; j < nj; ++j) buf[j] = __ldg(src + 16 * j);
         };
-        Cursor cur, ix;
-        start(cur);
-        start(ix);
+        // the scales of this thread's probes
+        float4 xs[nj];
+#pragma unroll
+        for (int j = 0; j < nj; ++j)
+            xs[j] = *reinterpret_cast<const float4*>(c_xs + 4 * ((ct & 15) + 16 * j));
+        // stage cursors: the one being converted and the one whose row index
+        // is loading
+        BlkCursor cur, ix;
+        cur.start(d.bstage, d.nblk);
+        ix.start(d.bstage, d.nblk);
         float4 b0[4], b1[4];
         // prologue: rows of stages 0 and 1 loading, the index of stage 2
-        load_x(row_of(ix), b0);
-        advance(ix);
-        load_x(row_of(ix), b1);
-        advance(ix);
-        int next_row = row_of(ix);
-        advance(ix);
+        load_x(ix.row(d.ucol, d.nblk, k), b0);
+        ix.advance(d.bstage, d.nblk);
+        load_x(ix.row(d.ucol, d.nblk, k), b1);
+        ix.advance(d.bstage, d.nblk);
+        int next_row = ix.row(d.ucol, d.nblk, k);
+        ix.advance(d.bstage, d.nblk);
         int64_t it = 0;
         bool ok = true;
         auto step = [&](float4 (&buf)[4]) -> bool {
@@ -472,26 +587,27 @@ k_spmm_blk(const BlkArgs d)
                 return false;
             }
             __syncwarp();
-            unsigned char* xh = base + static_cast<size_t>(s) * stage_bytes + 2 * BLK_A_BYTES;
+            unsigned char* xh = base + static_cast<size_t>(s) * stage_bytes + 2 * BLK_A_PART;
             unsigned char* xl = xh + x_bytes;
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < nj; ++j)
             {
-                if (j >= nj) continue;
-                float4 v = buf[j], lo;
-                split4(v, lo);
-                *reinterpret_cast<float4*>(xh + xoff[j]) = v;
-                *reinterpret_cast<float4*>(xl + xoff[j]) = lo;
+                const float4 v = make_float4(buf[j].x * xs[j].x, buf[j].y * xs[j].y,
+                                             buf[j].z * xs[j].z, buf[j].w * xs[j].w);
+                uint2 hi, lo;
+                split_h4(v, hi, lo);
+                *reinterpret_cast<uint2*>(xh + xoff0 + j * 2048) = hi;
+                *reinterpret_cast<uint2*>(xl + xoff0 + j * 2048) = lo;
             }
             tc::fence_proxy_async_smem();
             __syncwarp();
             if (lane == 0) mbar_arrive(&conv[s]);
             ++it;
-            advance(cur);
-            // refill: X rows of the stage BLK_AHEAD ahead, the next index
+            cur.advance(d.bstage, d.nblk);
+            // refill: X rows of the stage two ahead, the next index
             load_x(next_row, buf);
-            next_row = row_of(ix);
-            advance(ix);
+            next_row = ix.row(d.ucol, d.nblk, k);
+            ix.advance(d.bstage, d.nblk);
             return true;
         };
         while (ok && cur.blk < d.nblk)
@@ -505,7 +621,7 @@ k_spmm_blk(const BlkArgs d)
     {
         if (lane == 0)
         {
-            const uint32_t idesc = tc::idesc_tf32_m128(static_cast<uint32_t>(d.NB)) | (1u << 16);
+            const uint32_t idesc = blk_idesc(static_cast<uint32_t>(NB));
             int64_t it = 0, lb = 0;
             bool ok = true;
             for (int64_t blk = blockIdx.x; blk < d.nblk && ok; blk += gridDim.x, ++lb)
@@ -520,7 +636,7 @@ k_spmm_blk(const BlkArgs d)
                     break;
                 }
                 tc::fence_after_sync();
-                const uint32_t dacc = tmem + static_cast<uint32_t>(buf * d.NB);
+                const uint32_t dacc = tmem + static_cast<uint32_t>(buf * NB);
                 const int s0 = d.bstage[blk], s1 = d.bstage[blk + 1];
                 for (int st = s0; st < s1; ++st, ++it)
                 {
@@ -534,27 +650,20 @@ k_spmm_blk(const BlkArgs d)
                     }
                     tc::fence_after_sync();
                     unsigned char* stp = base + static_cast<size_t>(s) * stage_bytes;
-                    const uint64_t ah = tc::smem_desc(stp, 128, 512);
-                    const uint64_t al = tc::smem_desc(stp + BLK_A_BYTES, 128, 512);
-                    // MN-major, 128-byte swizzle with 32-byte atoms: N atoms 2 KB
-                    // apart, K atoms (4 rows) 512 bytes apart
+                    // A: K-major, no swizzle (K core matrices 128 bytes apart,
+                    // 8-row groups 256); X: MN-major, 128-byte swizzle (MN
+                    // atoms 2 KB apart, K atoms 1 KB)
+                    const uint64_t ah = tc::smem_desc(stp, 128, 256);
+                    const uint64_t al = tc::smem_desc(stp + BLK_A_PART, 128, 256);
                     const uint64_t xh =
-                        tc::smem_desc(stp + 2 * BLK_A_BYTES, 2048, 512) | (uint64_t(1) << 61);
+                        tc::smem_desc(stp + 2 * BLK_A_PART, 2048, 1024) | (uint64_t(2) << 61);
                     const uint64_t xl =
-                        tc::smem_desc(stp + 2 * BLK_A_BYTES + x_bytes, 2048, 512) |
-                        (uint64_t(1) << 61);
-#pragma unroll
-                    for (int kk = 0; kk < BLK_BK / 8; ++kk)
-                    {
-                        // K step kk: two K core matrices of A (256 bytes), two K
-                        // atoms of X (1 KB)
-                        const uint64_t ao = static_cast<uint64_t>(kk * 256) >> 4;
-                        const uint64_t xo = static_cast<uint64_t>(kk * 1024) >> 4;
-                        const uint32_t acc = (st > s0 || kk > 0) ? 1u : 0u;
-                        tc::mma_tf32_ss(dacc, al + ao, xh + xo, idesc, acc);
-                        tc::mma_tf32_ss(dacc, ah + ao, xl + xo, idesc, 1u);
-                        tc::mma_tf32_ss(dacc, ah + ao, xh + xo, idesc, 1u);
-                    }
+                        tc::smem_desc(stp + 2 * BLK_A_PART + x_bytes, 2048, 1024) |
+                        (uint64_t(2) << 61);
+                    const uint32_t acc = (st > s0) ? 1u : 0u;
+                    tc::mma_f16_ss(dacc, al, xh, idesc, acc);
+                    tc::mma_f16_ss(dacc, ah, xl, idesc, 1u);
+                    tc::mma_f16_ss(dacc, ah, xh, idesc, 1u);
                     tc::commit(&empty[s]);
                 }
                 if (!ok) break;
@@ -573,14 +682,21 @@ k_spmm_blk(const BlkArgs d)
         const int qd = warp & 3;
         const int half = warp >> 2;
         const uint32_t lanes = static_cast<uint32_t>(32 * qd) << 16;
-        const int cols = d.NB / 2;
+        constexpr int cols = NB / 2;
         const int c_begin = half * cols;
         const bool need_x = d.shift != 0.0 || d.epi == 1;
+        const bool need_z = d.Z != nullptr;
+        // the partial-sum term as a branch-free blend: x y, y y or z y
+        const float wx = d.epi == 1 ? 1.0f : 0.0f;
+        const float wy = d.epi == 2 ? 1.0f : 0.0f;
+        const float wz = d.epi == 3 ? 1.0f : 0.0f;
         const int my_col = blk_col(lane);
         int64_t lb = 0;
         for (int64_t blk = blockIdx.x; blk < d.nblk; blk += gridDim.x, ++lb)
         {
             const int buf = static_cast<int>(lb & 1);
+            const int64_t row = blk * BLK_ROWS + 32 * qd + lane;
+            const float rs = d.rsc[row];  // 2^-f_r (padding rows hold 1)
             bool got = true;
             if (lane == 0)
                 got = mbar_wait(&acc_full[buf], static_cast<uint32_t>((lb >> 1) & 1), abort_flag);
@@ -591,44 +707,41 @@ k_spmm_blk(const BlkArgs d)
             }
             __syncwarp();
             tc::fence_after_sync();
-            const int64_t row = blk * BLK_ROWS + 32 * qd + lane;
             const bool live = row < d.M;
-            const uint32_t dacc = tmem + static_cast<uint32_t>(buf * d.NB);
+            const uint32_t dacc = tmem + static_cast<uint32_t>(buf * NB);
             for (int c0 = c_begin; c0 < c_begin + cols; c0 += 16)
             {
                 uint32_t v[16];
                 tc::ld_x16(dacc + lanes + static_cast<uint32_t>(c0), v);
                 // this row's 16 X and Z values (64 bytes each, 16-byte aligned)
                 float xv[16], zv[16];
-                const int64_t o = row * d.NB + c0;
+                const int64_t o = row * NB + c0;
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
                 {
                     float4 x4 = make_float4(0.f, 0.f, 0.f, 0.f), z4 = x4;
                     if (live && need_x) x4 = __ldg(reinterpret_cast<const float4*>(d.X + o) + q);
-                    if (live && d.Z) z4 = __ldg(reinterpret_cast<const float4*>(d.Z + o) + q);
+                    if (live && need_z) z4 = __ldg(reinterpret_cast<const float4*>(d.Z + o) + q);
                     xv[4 * q] = x4.x; xv[4 * q + 1] = x4.y; xv[4 * q + 2] = x4.z; xv[4 * q + 3] = x4.w;
                     zv[4 * q] = z4.x; zv[4 * q + 1] = z4.y; zv[4 * q + 2] = z4.z; zv[4 * q + 3] = z4.w;
                 }
                 tc::wait_ld();
                 // y = s A x (+ t s x) (- zc zs z) in FP32; the partial-sum
-                // terms x y, y y or z y in FP32, summed over rows in FP64
-                // (the per-probe factor s_p or zs_p is applied to the sums)
-                double add[16];
+                // terms x y, y y or z y in FP32, summed over the warp's 32
+                // rows in FP32 and over warps and blocks in FP64 (the
+                // per-probe factor s_p or zs_p is applied to the sums)
+                float add[16];
                 float yv[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j)
                 {
                     const int p = c0 + j;
-                    float y = __uint_as_float(v[j]) * c_sx[p];
-                    if (d.shift != 0.0) y = fmaf(c_ts[p], xv[j], y);
-                    if (d.Z) y = fmaf(-c_zcs[p], zv[j], y);
+                    // the shift and three-term constants are zero where unused
+                    float y = __uint_as_float(v[j]) * (c_sx[p] * rs);
+                    y = fmaf(c_ts[p], xv[j], y);
+                    y = fmaf(-c_zcs[p], zv[j], y);
                     yv[j] = y;
-                    float a = 0.0f;
-                    if (d.epi == 1) a = xv[j] * y;
-                    else if (d.epi == 2) a = y * y;
-                    else if (d.epi == 3) a = zv[j] * y;
-                    add[j] = live ? static_cast<double>(a) : 0.0;
+                    add[j] = y * fmaf(wx, xv[j], fmaf(wy, y, wz * zv[j]));
                 }
                 if (live)
                 {
@@ -637,10 +750,15 @@ k_spmm_blk(const BlkArgs d)
                         reinterpret_cast<float4*>(d.Y + o)[q] =
                             make_float4(yv[4 * q], yv[4 * q + 1], yv[4 * q + 2], yv[4 * q + 3]);
                 }
+                if (!live)
+                {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) add[j] = 0.0f;
+                }
                 if (d.epi != 0)
                 {
-                    const double sum = reduce_scatter16(add, lane);
-                    if (lane < 16) red[qd * 256 + c0 + my_col] += sum;
+                    const float sum = reduce_scatter16(add, lane);
+                    if (lane < 16) red[qd * 256 + c0 + my_col] += static_cast<double>(sum);
                 }
             }
             tc::fence_before_sync();
@@ -657,11 +775,11 @@ k_spmm_blk(const BlkArgs d)
         tc::tmem_dealloc(tmem, tmem_cols);
     }
     if (d.epi != 0)
-        for (int q = tid; q < d.NB; q += BLK_THREADS)
+        for (int q = tid; q < NB; q += BLK_THREADS)
         {
             // the per-probe factor of the terms: s_p (alpha), 1 (|y|^2), zs_p
             const double f = d.epi == 1 ? (d.sx ? d.sx[q] : 1.0) : d.epi == 3 ? d.zs[q] : 1.0;
-            d.partials[static_cast<int64_t>(blockIdx.x) * d.NB + q] =
+            d.partials[static_cast<int64_t>(blockIdx.x) * NB + q] =
                 f * (((red[q] + red[256 + q]) + red[512 + q]) + red[768 + q]);
         }
 }

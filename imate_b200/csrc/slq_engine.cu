@@ -238,16 +238,22 @@ struct slq_op {
     float* xt_lo = nullptr;
     int32_t* d_error = nullptr;
     CUtensorMap map_hi, map_lo, map_t_hi, map_t_lo;
-    // tensor-core block format (k_spmm_blk, FP32) of A and of A^T: 128-row
-    // blocks, first stage per block, union columns, stage value images
+    // tensor-core block format (k_spmm_blk, FP32 operators) of A and of A^T:
+    // 128-row blocks, first stage per block, union columns, row scales,
+    // FP16 stage images
     int64_t a_nblk = 0, t_nblk = 0;
     const int32_t* a_bstage = nullptr;
     const int32_t* a_ucol = nullptr;
-    const float* a_img = nullptr;
+    const float* a_rsc = nullptr;
+    const __half* a_img = nullptr;
     const int32_t* t_bstage = nullptr;
     const int32_t* t_ucol = nullptr;
-    const float* t_img = nullptr;
-    int32_t* blk_error = nullptr;  // error word of the block kernel in slq_operator_dot
+    const float* t_rsc = nullptr;
+    const __half* t_img = nullptr;
+    // slq_operator_dot's error word and per-probe maxima of X for the block
+    // kernel (inside the first format buffer)
+    int32_t* blk_error = nullptr;
+    unsigned int* blk_xmax = nullptr;
     // autotuned SpMM candidate per direction and log2(block width); -1 = built-in
     int8_t tuned[2][11];
     slq_op()
@@ -661,6 +667,7 @@ struct BlkScratch {
     int32_t* stg;     // [nblk + 1]
     int32_t* bstage;  // [nblk + 1]
     int32_t* ufirst;  // [nblk + 1]
+    float* fsc;       // [nblk * 128] row scales 2^f_r
     void* temp;
     size_t temp_bytes;
 };
@@ -700,6 +707,7 @@ slq_status blk_scratch_layout(Carver& c, int64_t rows, int64_t nnz, BlkScratch* 
     s->stg = c.take<int32_t>(nblk + 1);
     s->bstage = c.take<int32_t>(nblk + 1);
     s->ufirst = c.take<int32_t>(nblk + 1);
+    s->fsc = c.take<float>(nblk * BLK_ROWS);
     s->temp_bytes = std::max({t1, t2, t3});
     s->temp = c.take<char>(s->temp_bytes);
     return SLQ_OK;
@@ -759,13 +767,23 @@ slq_status blk_prepare(const int32_t* ptr, const int32_t* ind, int64_t R, int64_
     return SLQ_OK;
 }
 
-void blk_format_layout(Carver& c, int64_t nblk, int64_t stages, int32_t** bstage, int32_t** ucol,
-                       float** img, int32_t** error)
+struct BlkFormat {
+    int32_t* error;
+    unsigned int* xmax;  // [256]
+    int32_t* bstage;
+    int32_t* ucol;
+    float* rsc;
+    __half* img;
+};
+
+void blk_format_layout(Carver& c, int64_t nblk, int64_t stages, BlkFormat* f)
 {
-    *error = c.take<int32_t>(1);
-    *bstage = c.take<int32_t>(nblk + 1);
-    *ucol = c.take<int32_t>(stages * BLK_BK);
-    *img = c.take<float>(stages * BLK_IMG_STAGE);
+    f->error = c.take<int32_t>(1);
+    f->xmax = c.take<unsigned int>(256);
+    f->bstage = c.take<int32_t>(nblk + 1);
+    f->ucol = c.take<int32_t>(stages * BLK_BK);
+    f->rsc = c.take<float>(nblk * BLK_ROWS);
+    f->img = c.take<__half>(stages * BLK_IMG_STAGE);
 }
 
 slq_status blk_source(const slq_op* op, int transpose, const int32_t** ptr, const int32_t** ind,
@@ -818,9 +836,8 @@ extern "C" slq_status slq_operator_blocks_bytes(const slq_op* op, int transpose,
     int64_t stages = 0;
     SLQ_TRY(blk_prepare(ptr, ind, R, C, op->nnz, &s, static_cast<cudaStream_t>(stream), &stages));
     Carver f(nullptr, 0);
-    int32_t *bs, *uc, *er;
-    float* im;
-    blk_format_layout(f, (R + BLK_ROWS - 1) / BLK_ROWS, stages, &bs, &uc, &im, &er);
+    BlkFormat bf;
+    blk_format_layout(f, (R + BLK_ROWS - 1) / BLK_ROWS, stages, &bf);
     *format_bytes = f.off + 256;
     return SLQ_OK;
 }
@@ -842,9 +859,8 @@ extern "C" slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* s
     SLQ_TRY(blk_prepare(ptr, ind, R, C, op->nnz, &s, st, &stages));
     const int64_t nblk = (R + BLK_ROWS - 1) / BLK_ROWS;
     Carver f(format, format_bytes);
-    int32_t *bstage, *ucol, *err;
-    float* img;
-    blk_format_layout(f, nblk, stages, &bstage, &ucol, &img, &err);
+    BlkFormat bf;
+    blk_format_layout(f, nblk, stages, &bf);
     if (!format || !f.fits())
         return fail(SLQ_ERR_WORKSPACE, "blocks: format buffer too small (need " +
                                            std::to_string(f.off) + " bytes)");
@@ -852,43 +868,54 @@ extern "C" slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* s
     SLQ_TRY(device_sms(&sms));
     const int grid = sms * 4;
     const int cbits = bits_for(std::max<int64_t>(C - 1, 1));
-    SLQ_CK(cudaMemcpyAsync(bstage, s.bstage, sizeof(int32_t) * (nblk + 1),
+    SLQ_CK(cudaMemcpyAsync(bf.bstage, s.bstage, sizeof(int32_t) * (nblk + 1),
                            cudaMemcpyDeviceToDevice, st));
-    SLQ_CK(cudaMemsetAsync(img, 0, sizeof(float) * stages * BLK_IMG_STAGE, st));
+    // the FP32 staging images take the same bytes as the FP16 parts
+    SLQ_CK(cudaMemsetAsync(bf.img, 0, sizeof(__half) * stages * BLK_IMG_STAGE, st));
+    k_blk_rowscale<<<grid, 256, 0, st>>>(ptr, val, R, nblk * BLK_ROWS, s.fsc, bf.rsc);
+    SLQ_LAUNCH_CK();
     if (op->nnz > 0)
     {
         k_blk_ucol<<<grid, 256, 0, st>>>(s.keys_out, s.flags, s.uidx, op->nnz, cbits, s.ufirst,
-                                         bstage, ucol);
+                                         bf.bstage, bf.ucol);
         SLQ_LAUNCH_CK();
     }
     k_blk_pad<<<std::max<int64_t>(1, std::min<int64_t>(grid, (nblk + 255) / 256)), 256, 0, st>>>(
-        s.cnt, bstage, nblk, ucol);
+        s.cnt, bf.bstage, nblk, bf.ucol);
     SLQ_LAUNCH_CK();
     if (op->nnz > 0)
     {
         k_blk_scatter<<<grid, 256, 0, st>>>(s.keys_out, s.pos_out, s.uidx, op->nnz, cbits,
-                                            s.ufirst, bstage, val, s.rr, img);
+                                            s.ufirst, bf.bstage, val, s.rr,
+                                            reinterpret_cast<float*>(bf.img));
         SLQ_LAUNCH_CK();
     }
-    k_blk_split<<<grid, 256, 0, st>>>(img, stages);
+    k_blk_split<<<std::max<int64_t>(1, std::min<int64_t>(stages, int64_t(sms) * 8)), 256, 0, st>>>(
+        bf.img, bf.bstage, nblk, s.fsc, stages);
     SLQ_LAUNCH_CK();
-    SLQ_CK(cudaMemsetAsync(err, 0, sizeof(int32_t), st));
+    SLQ_CK(cudaMemsetAsync(bf.error, 0, sizeof(int32_t), st));
     // the scratch may be released once the build has run
     SLQ_CK(cudaStreamSynchronize(st));
-    if (!op->blk_error) op->blk_error = err;
+    if (!op->blk_error)
+    {
+        op->blk_error = bf.error;
+        op->blk_xmax = bf.xmax;
+    }
     if (transpose)
     {
         op->t_nblk = nblk;
-        op->t_bstage = bstage;
-        op->t_ucol = ucol;
-        op->t_img = img;
+        op->t_bstage = bf.bstage;
+        op->t_ucol = bf.ucol;
+        op->t_rsc = bf.rsc;
+        op->t_img = bf.img;
     }
     else
     {
         op->a_nblk = nblk;
-        op->a_bstage = bstage;
-        op->a_ucol = ucol;
-        op->a_img = img;
+        op->a_bstage = bf.bstage;
+        op->a_ucol = bf.ucol;
+        op->a_rsc = bf.rsc;
+        op->a_img = bf.img;
     }
     return SLQ_OK;
 }
@@ -1332,20 +1359,40 @@ slq_status spmm_blk_inst(Launcher& L, const slq_op* op, int transpose, int b, co
     static bool attr = false;
     if (!attr)
     {
-        SLQ_CK(cudaFuncSetAttribute(k_spmm_blk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SLQ_CK(cudaFuncSetAttribute(k_spmm_blk<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(blk_smem_bytes(128))));
+        SLQ_CK(cudaFuncSetAttribute(k_spmm_blk<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(blk_smem_bytes(256))));
         attr = true;
     }
     const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(nblk, L.sms)));
+    // an X without probe scales: its per-probe maxima first (into the
+    // partial-sum buffer past this launch's rows, or, for a product without
+    // one, into the format's slot)
+    unsigned int* xmax = nullptr;
+    if (!sx)
+    {
+        xmax = partials ? reinterpret_cast<unsigned int*>(partials + int64_t(L.sms) * b)
+                        : op->blk_xmax;
+        if (!xmax) return fail(SLQ_ERR_BAD_ARG, "block SpMM: no room for the probe maxima");
+        SLQ_CK(cudaMemsetAsync(xmax, 0, sizeof(unsigned int) * b, L.st));
+        k_blk_colmax<<<dim3(static_cast<unsigned>(std::min<int64_t>((xrows + 7) / 8, L.sms * 4)),
+                            static_cast<unsigned>(b / 32)),
+                       256, 0, L.st>>>(X, xrows, b, xmax);
+        SLQ_LAUNCH_CK();
+        ++L.launches;
+    }
     BlkArgs d;
     d.M = rows;
     d.nblk = nblk;
     d.NB = b;
     d.bstage = transpose ? op->t_bstage : op->a_bstage;
     d.ucol = transpose ? op->t_ucol : op->a_ucol;
+    d.rsc = transpose ? op->t_rsc : op->a_rsc;
     d.img = transpose ? op->t_img : op->a_img;
     d.X = X;
     d.sx = sx;
+    d.xmax = xmax;
     d.shift = shift;
     d.Y = Y;
     d.Z = Z;
@@ -1354,7 +1401,10 @@ slq_status spmm_blk_inst(Launcher& L, const slq_op* op, int transpose, int b, co
     d.epi = epi;
     d.partials = partials;
     d.error = error;
-    k_spmm_blk<<<grid, BLK_THREADS, smem, L.st>>>(d);
+    if (b == 256)
+        k_spmm_blk<256><<<grid, BLK_THREADS, smem, L.st>>>(d);
+    else
+        k_spmm_blk<128><<<grid, BLK_THREADS, smem, L.st>>>(d);
     SLQ_LAUNCH_CK();
     ++L.launches;
     *grid_out = grid;

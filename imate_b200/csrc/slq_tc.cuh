@@ -150,6 +150,22 @@ __device__ __forceinline__ void mma_tf32_ss(uint32_t d, uint64_t adesc, uint64_t
         : "memory");
 }
 
+// kind::f16 (FP16 or BF16 operands as the instruction descriptor says, FP32
+// D): D (tensor memory) [+]= A (shared memory) * B (shared memory); one
+// thread.
+__device__ __forceinline__ void mma_f16_ss(uint32_t d, uint64_t adesc, uint64_t bdesc,
+                                           uint32_t idesc, uint32_t accumulate)
+{
+    const uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(m0), "r"(m1),
+          "r"(m2), "r"(m3)
+        : "memory");
+}
+
 // Arrive once on the mbarrier when every MMA this thread issued so far has
 // completed (their operand reads included).
 __device__ __forceinline__ void commit(uint64_t* bar)
