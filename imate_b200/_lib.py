@@ -18,6 +18,9 @@ STATUS_NAMES = {
     5: "NAN", 6: "EIGEN", 7: "UNSUPPORTED", 8: "TIMEOUT",
 }
 SLQ_F32, SLQ_F64 = 0, 1
+ABI_VERSION = 3
+# per-probe status bits (slq_result.probe_status)
+PROBE_NONFINITE, PROBE_EIGEN, PROBE_NODE, PROBE_SAMPLE = 1, 2, 4, 8
 SLQ_CSR, SLQ_CSC = 0, 1
 FUNC_IDS = {"log": 0, "inv": 1, "id": 2, "exp": 3, "linfrac": 4,
             "indicator": 5, "gaussian": 6, "smoothstep": 7}
@@ -42,7 +45,7 @@ EXPORTS = (
     "slq_rcm_order_device_workspace_bytes", "slq_rcm_order_device",
     "slq_dense_operator_workspace_bytes", "slq_dense_operator_create",
     "slq_operator_blocks_scratch_bytes", "slq_operator_blocks_bytes",
-    "slq_operator_add_blocks",
+    "slq_operator_add_blocks", "slq_debug_fail_stream_waits",
 )
 TUNE_MAX_CANDIDATES = 16
 SPMM_KINDS = ("csr", "row-group", "row-group-tma", "row-group-tc", "block-tc")
@@ -105,6 +108,7 @@ class SlqResult(ctypes.Structure):
         ("lanczos_size", ctypes.c_void_p),
         ("alpha", ctypes.c_void_p),
         ("beta", ctypes.c_void_p),
+        ("probe_status", ctypes.c_void_p),
         ("all_converged", ctypes.c_int32),
         ("num_blocks", ctypes.c_int32),
         ("num_probes_computed", ctypes.c_int64),
@@ -194,6 +198,7 @@ def _declare(lib):
         "slq_operator_blocks_scratch_bytes": (i32, [vp, i32, psz]),
         "slq_operator_blocks_bytes": (i32, [vp, i32, vp, sz, vp, psz]),
         "slq_operator_add_blocks": (i32, [vp, i32, vp, sz, vp, sz, vp]),
+        "slq_debug_fail_stream_waits": (i32, [i32]),
         "slq_tc_selftest_mn": (i32, [vp, vp, vp, i32, vp, vp]),
     }
     for name, (res, args) in sig.items():

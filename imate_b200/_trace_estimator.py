@@ -378,6 +378,7 @@ def reset_outputs(J):
     J.num_outliers = np.zeros(q, dtype=np.int32)
     J.converged = np.zeros(q, dtype=np.int32)
     J.lanczos_size = np.zeros((mx, ng), dtype=np.int32)
+    J.probe_status = np.full((mx, ng), -1, dtype=np.int32)
     J.alphas = J.betas = None
     if J.options.return_coefficients:
         J.alphas = np.full((ng, mx, m), np.nan)
@@ -399,6 +400,7 @@ def run_outputs(J, gi):
         order=np.zeros(mx, dtype=np.int32),
         used=np.zeros(gq, dtype=np.int32), out=np.zeros(gq, dtype=np.int32),
         conv=np.zeros(gq, dtype=np.int32), size=np.zeros(mx, dtype=np.int32),
+        status=np.full(mx, -1, dtype=np.int32),
         alpha=np.zeros((mx, m)) if J.alphas is not None else None,
         beta=np.zeros((mx, m)) if J.betas is not None else None)
 
@@ -409,7 +411,8 @@ def run_outputs(J, gi):
         samples=ptr(a["samples"]), processed_samples_indices=ptr(a["order"]),
         num_samples_used=ptr(a["used"]), num_outliers=ptr(a["out"]),
         converged=ptr(a["conv"]), lanczos_size=ptr(a["size"]),
-        alpha=ptr(a["alpha"]), beta=ptr(a["beta"]))
+        alpha=ptr(a["alpha"]), beta=ptr(a["beta"]),
+        probe_status=ptr(a["status"]))
     return res, a
 
 
@@ -433,6 +436,7 @@ def collect(J, gi, res, a, status):
     if gi == 0:
         J.processed = a["order"]
     J.lanczos_size[:, gi] = a["size"]
+    J.probe_status[:, gi] = a["status"]
     if J.alphas is not None:
         J.alphas[gi] = a["alpha"]
         J.betas[gi] = a["beta"]
@@ -470,6 +474,59 @@ def run_job(J):
                              ctypes.byref(res))
         del workspace
         collect(J, gi, res, a, status)
+
+
+PROBE_FLAG_NAMES = (
+    (_lib.PROBE_NONFINITE, "non-finite Lanczos coefficients"),
+    (_lib.PROBE_EIGEN, "tridiagonal eigen-solve did not converge"),
+    (_lib.PROBE_NODE, "non-positive quadrature node under log (or zero "
+                      "node under 1/x): is the matrix positive definite?"),
+    (_lib.PROBE_SAMPLE, "non-finite sample"),
+)
+
+
+def _warn_probe_status(J):
+    """One warning naming the flags the engine set on the samples the
+    estimate used (the reference warns only for a vanishing vector in its
+    Gram-Schmidt step, c_orthogonalization.cpp:186-192)."""
+    used = J.processed[:int(np.max(J.num_samples_used))] \
+        if J.num_samples_used.size else J.processed[:0]
+    st = J.probe_status[used]
+    st = st[st > 0]
+    if st.size == 0:
+        return
+    import warnings
+    names = [name for bit, name in PROBE_FLAG_NAMES
+             if np.any(st & bit)]
+    warnings.warn("SLQ: %d of %d samples flagged: %s (per-sample flags in "
+                  "info['engine']['probe_status'])"
+                  % (st.size, used.size, "; ".join(names)))
+
+
+def _precision_info(J):
+    """The arithmetic of the run: operator dtype, where each part of the
+    computation runs in which precision, and the SpMM format the operator
+    holds."""
+    op = J.dev_op
+    b = J.engine.get("block_size") or 0
+    fp64 = J.dtype_str == "float64"
+    if getattr(op, "dense", False):
+        spmm = "dense, tensor cores (TF32 three-term products, FP32 sums)"
+    elif getattr(op, "block_formats", None) and b in (128, 256):
+        spmm = ("128-row blocks, tensor cores (FP16 three-product split of "
+                "scaled FP32 values, FP32 accumulation)")
+    elif getattr(op, "group_rows", 0):
+        spmm = "row groups of %d rows, CUDA cores" % op.group_rows
+    else:
+        spmm = "CSR, CUDA cores"
+    return {
+        "operator_dtype": J.dtype_str,
+        "mode": "fp64" if fp64 else "mixed",
+        "spmm": spmm,
+        "vector_storage": J.dtype_str,
+        "reductions": "float64",
+        "eigensolve_quadrature": "float64",
+    }
 
 
 def block_width(max_num_samples, block_size, dtype_str):
@@ -551,8 +608,12 @@ def finish(J):
             "method": "slq",
         },
         "engine": dict(J.engine, lanczos_size=J.lanczos_size[:, 0]
-                       if ngroups == 1 else J.lanczos_size),
+                       if ngroups == 1 else J.lanczos_size,
+                       probe_status=J.probe_status[:, 0]
+                       if ngroups == 1 else J.probe_status),
+        "precision": _precision_info(J),
     }
+    _warn_probe_status(J)
     if J.alphas is not None:
         info["engine"]["alpha"] = J.alphas[0] if ngroups == 1 else J.alphas
         info["engine"]["beta"] = J.betas[0] if ngroups == 1 else J.betas

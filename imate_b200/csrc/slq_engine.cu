@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -88,6 +89,10 @@ struct Carver {
 };
 
 int g_num_sms = 0;
+
+// test hook (slq_debug_fail_stream_waits): streaming launches left whose
+// first wait is to run out at once
+std::atomic<int> g_fail_stream_waits{0};
 
 slq_status device_sms(int* sms)
 {
@@ -1672,6 +1677,9 @@ slq_status stream_pass(Launcher& L, int64_t n, int b, const VT* W, VT* Wout, int
     a.want_norm = want_norm;
     a.partials = partials;
     a.error = error;
+    a.fail_first_wait = 0;
+    if (g_fail_stream_waits.load() > 0 && g_fail_stream_waits.fetch_sub(1) > 0)
+        a.fail_first_wait = 1;
     const int gy = b / PT;
     const int gx = std::max(1, L.sms / gy);
     const double vb = double(n) * b * sizeof(VT);
@@ -2092,6 +2100,7 @@ slq_status run_typed(slq_op* op, const slq_params* p, const double* parameters, 
     {
         res->processed_samples_indices[i] = 0;
         if (res->lanczos_size) res->lanczos_size[i] = 0;
+        if (res->probe_status) res->probe_status[i] = -1;
     }
     for (int j = 0; j < q; ++j)
     {
@@ -2177,6 +2186,8 @@ slq_status run_typed(slq_op* op, const slq_params* p, const double* parameters, 
         SLQ_CK(cudaStreamSynchronize(st));
         if (herr)
             return fail(SLQ_ERR_TIMEOUT, "a streaming kernel gave up waiting for its copies");
+        if (res->probe_status)
+            for (int pi = 0; pi < count; ++pi) res->probe_status[g + pi] = hstat[pi];
         ++blocks;
         computed += count;
         for (int pi = 0; pi < count && !all; ++pi)
@@ -2185,7 +2196,7 @@ slq_status run_typed(slq_op* op, const slq_params* p, const double* parameters, 
             for (int j = 0; j < q; ++j)
                 res->samples[static_cast<int64_t>(s) * q + j] = hs[static_cast<size_t>(pi) * q + j];
             if (res->lanczos_size) res->lanczos_size[s] = hsize[pi];
-            if (hstat[pi] == 2) eig_failed = true;
+            if (hstat[pi] & 2) eig_failed = true;
             if (!ha.empty())
                 for (int i = 0; i < m; ++i)
                 {
@@ -2604,6 +2615,7 @@ slq_status batch_replay(const BatchRun& R, const char* host, const char* dev_bas
     {
         res->processed_samples_indices[i] = 0;
         if (res->lanczos_size) res->lanczos_size[i] = 0;
+        if (res->probe_status) res->probe_status[i] = -1;
     }
     for (int j = 0; j < q; ++j)
     {
@@ -2634,7 +2646,8 @@ slq_status batch_replay(const BatchRun& R, const char* host, const char* dev_bas
         for (int j = 0; j < q; ++j)
             res->samples[static_cast<int64_t>(s) * q + j] = hs[static_cast<size_t>(s) * q + j];
         if (res->lanczos_size) res->lanczos_size[s] = hsize[s];
-        if (hstat[s] == 2) eig_failed = true;
+        if (hstat[s] & 2) eig_failed = true;
+        if (res->probe_status) res->probe_status[s] = hstat[s];
         const size_t base = static_cast<size_t>(blk) * m * b;
         for (int i = 0; i < m; ++i)
         {
@@ -3470,3 +3483,10 @@ extern "C" slq_status slq_tc_selftest_mn(const float* a, const float* b, float* 
 }
 
 extern "C" int slq_abi_version(void) { return SLQ_ABI_VERSION; }
+
+extern "C" slq_status slq_debug_fail_stream_waits(int count)
+{
+    if (count < 0) return fail(SLQ_ERR_BAD_ARG, "debug_fail_stream_waits: count < 0");
+    g_fail_stream_waits.store(count);
+    return SLQ_OK;
+}

@@ -460,10 +460,12 @@ k_eig_quad(int count, int b, int m, const double* __restrict__ alpha,
     if (p >= count) return;
     double d[EIG_MAX], e[EIG_MAX], z[EIG_MAX];
     const int k = size[p];
+    bool bad = false;
     for (int i = 0; i < k; ++i)
     {
         const double a = alpha[static_cast<int64_t>(i) * b + p];
         const double bt = beta[static_cast<int64_t>(i) * b + p];
+        if (!isfinite(a) || (i < k - 1 && !isfinite(bt))) bad = true;
         if (gram)
         {
             const double bp = (i > 0) ? beta[static_cast<int64_t>(i - 1) * b + p] : 0.0;
@@ -477,7 +479,6 @@ k_eig_quad(int count, int b, int m, const double* __restrict__ alpha,
         }
     }
     int st = ql_first_row(d, e, z, k);
-    bool bad = false;
     for (int i = 0; i < k; ++i)
         if (!isfinite(d[i]) || !isfinite(z[i])) bad = true;
     if (theta_out)
@@ -487,17 +488,26 @@ k_eig_quad(int count, int b, int m, const double* __restrict__ alpha,
             tau_out[static_cast<int64_t>(i) * b + p] = z[i];
         }
     const double t0 = (q > 0) ? params[0] : 0.0;
+    bool node = false, nonfinite = false;
     for (int j = 0; j < q; ++j)
     {
         double acc = 0.0;
         for (int i = 0; i < k; ++i)
         {
             const double th = (j > 0) ? d[i] - t0 + params[j] : d[i];
-            acc += z[i] * z[i] * apply_func(func, pow(th, exponent), fc);
+            const double x = pow(th, exponent);
+            // log of a non-positive node, 1/x of a zero node (weighted)
+            if (z[i] != 0.0 && ((func == 0 && !(x > 0.0)) || (func == 1 && x == 0.0)))
+                node = true;
+            acc += z[i] * z[i] * apply_func(func, x, fc);
         }
         samples[static_cast<int64_t>(p) * q + j] = nscale * acc;
+        if (!isfinite(nscale * acc)) nonfinite = true;
     }
-    status[p] = st ? 2 : (bad ? 1 : 0);
+    // bit mask: 1 non-finite coefficients or eigen-solve results, 2 QL did
+    // not converge, 4 a non-positive node under log (zero node under 1/x),
+    // 8 a non-finite sample
+    status[p] = (bad ? 1 : 0) | (st ? 2 : 0) | (node ? 4 : 0) | (nonfinite ? 8 : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -1004,6 +1014,7 @@ struct StreamArgs {
     int want_norm;
     double* partials;     // dots: [grid.x][J][b]; reorth: [grid.x][b]
     int32_t* error;       // set to 1 when a wait runs out
+    int fail_first_wait;  // test hook: the consumers' first wait runs out at once
 };
 
 // MODE 0: dots, MODE 1: reorth.  R = rows per consumer thread per tile.
@@ -1195,7 +1206,10 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
                 const int ib = skip + (item - npre);
                 double prev = 0.0;
                 if (MODE == 0 && item >= npre) prev = extra[ib * STREAM_CONSUMERS + tid];
-                if (!mbar_wait(&full[s], phase, abort_flag))
+                // the test hook makes the first wait of the launch run out
+                // (the simulated timeout takes the abort path below)
+                const bool first = tile == blockIdx.x && item == 0;
+                if ((a.fail_first_wait && first) || !mbar_wait(&full[s], phase, abort_flag))
                 {
                     *abort_flag = 1;
                     atomicExch(a.error, 1);

@@ -454,8 +454,11 @@ class _DeviceOperator:
     def __del__(self):
         h = getattr(self, "handle", None)
         if h is not None and h.value:
-            self._lib.slq_operator_destroy(h)
-            self.handle = ctypes.c_void_p(None)
+            try:
+                self._lib.slq_operator_destroy(h)
+                self.handle = ctypes.c_void_p(None)
+            except (AttributeError, TypeError):
+                pass  # interpreter shutdown: ctypes is already torn down
 
     def dot(self, x, transpose=False, t=0.0):
         """y = A x (or A^T x) (+ t x for affine operators) for a torch

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define SLQ_ABI_VERSION 2
+#define SLQ_ABI_VERSION 3
 
 typedef enum {
     SLQ_OK = 0,
@@ -292,7 +292,15 @@ typedef struct {
  * py_cu_trace_estimator.pyx:199-247).  samples is [max_num_samples][q]
  * row-major and NaN where not computed.  lanczos_size is per sample.
  * alpha/beta (optional, may be NULL) receive the per-sample coefficients,
- * [max_num_samples][lanczos_degree]. */
+ * [max_num_samples][lanczos_degree].  probe_status (optional, may be NULL)
+ * receives per sample a bit mask, -1 where not computed: 1 non-finite
+ * Lanczos coefficients or eigen-solve results, 2 the eigen-solve did not
+ * converge, 4 a quadrature node under log was not positive (or a node under
+ * 1/x was zero), 8 a non-finite sample.  The reference prints a warning for
+ * a vanishing basis vector in its Gram-Schmidt step
+ * (imate/_c_trace_estimator/c_orthogonalization.cpp:186-192) and otherwise
+ * averages whatever the samples are; here the flags say which samples are
+ * suspect. */
 typedef struct {
     double* trace;                     /* [q]   */
     double* error;                     /* [q]   */
@@ -304,6 +312,7 @@ typedef struct {
     int32_t* lanczos_size;             /* [max] */
     double* alpha;                     /* [max][m] or NULL */
     double* beta;                      /* [max][m] or NULL */
+    int32_t* probe_status;             /* [max] or NULL */
     int32_t all_converged;
     int32_t num_blocks;                /* probe blocks launched              */
     int64_t num_probes_computed;       /* incl. the unused tail of a block   */
@@ -470,7 +479,8 @@ slq_status slq_generate_probes_noalloc(int64_t seed, int rng, int64_t len,
  * device, by implicit QL in FP64.  All arrays are device memory in
  * probe-minor layout: alpha, beta, theta, tau are [m][count] (entry i of
  * matrix p at i*count + p); sizes [count] gives each matrix's order; status
- * [count] receives 0, 1 (non-finite result) or 2 (QL did not converge).
+ * [count] receives a bit mask: 1 non-finite coefficients or results, 2 QL
+ * did not converge (0 when neither).
  * gram != 0 treats (alpha, beta) as an upper bidiagonal B and solves B^T B.
  * Replaces Diagonalization::eigh_tridiagonal / svd_bidiagonal
  * (imate/_c_trace_estimator/diagonalization.cpp:89-231). */
@@ -556,6 +566,15 @@ slq_status slq_device_info(int* num_devices, int* num_sms,
 
 const char* slq_last_error(void);
 int slq_abi_version(void);
+
+/* Test hook (no counterpart in the reference): the next `count` launches of
+ * the streaming update / reorthogonalisation kernel treat their first
+ * mbarrier wait as timed out.  That wait then takes the path of a real one
+ * that ran out -- the CTA sets the run's error word, stops, waits (with the
+ * full bound) for the copies it issued, and the call returns
+ * SLQ_ERR_TIMEOUT -- so the failure path can be exercised without a fault.
+ * 0 switches it off. */
+slq_status slq_debug_fail_stream_waits(int count);
 
 #ifdef __cplusplus
 }
