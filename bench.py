@@ -365,7 +365,7 @@ def run_engine_arm(args):
                              % args.spmm)
         set_variant(dev_op, args.probes, pick[-1])
     eng = ib.EngineOptions(block_size=args.probes, rng="parity")
-    kw = dict(method="slq", gpu=True, return_info=True,
+    kw = dict(method="slq", gpu=True, num_gpu_devices=1, return_info=True,
               min_num_samples=args.probes, max_num_samples=args.probes,
               error_rtol=0.0, lanczos_degree=args.degree,
               orthogonalize=args.orthogonalize, seed=0)
@@ -619,7 +619,7 @@ def run_batched(args):
             shift=args.shift, seed=1000 + i, dtype="float64")
         M64 = ib.DeviceMatrix(ip, ind, dat, (int(sizes[i]),) * 2,
                               group_rows=0)
-        kw64 = dict(method="slq", gpu=True, return_info=True,
+        kw64 = dict(method="slq", gpu=True, num_gpu_devices=1, return_info=True,
                     min_num_samples=4, max_num_samples=4, error_rtol=0.0,
                     lanczos_degree=degree, orthogonalize=0, seed=i,
                     engine=ib.EngineOptions(block_size=1))
@@ -676,6 +676,7 @@ def run_sweep(args):
     A32 = build_matrix(args, "float32")
     t_grid = np.logspace(-4, 2, 512)
     opts = dict(min_num_samples=args.probes, max_num_samples=args.probes,
+                num_gpu_devices=1,
                 error_rtol=0.0, lanczos_degree=args.degree,
                 orthogonalize=args.orthogonalize, seed=0)
     funcs = {"log": ib.logdet, "inv": ib.traceinv}
@@ -760,7 +761,7 @@ def run_gram_large(args):
     degree = 60 if args.degree == 50 else args.degree
     G = ib.GramAffineMatrixFunction(X)
     G.get_device_operator(need_transpose=True)
-    kw = dict(method="slq", gpu=True, return_info=True, parameters=1e-2,
+    kw = dict(method="slq", gpu=True, num_gpu_devices=1, return_info=True, parameters=1e-2,
               min_num_samples=probes, max_num_samples=probes,
               error_rtol=0.0, lanczos_degree=degree, orthogonalize=0, seed=0)
     eng = ib.EngineOptions(block_size=args.block)
@@ -850,7 +851,7 @@ def run_dense(args):
     Aop = ib.Matrix(A32)
     Aop.get_device_operator()  # upload + TF32 split, outside the timing
     eng = ib.EngineOptions(block_size=args.probes, rng="parity")
-    kw = dict(method="slq", gpu=True, return_info=True,
+    kw = dict(method="slq", gpu=True, num_gpu_devices=1, return_info=True,
               min_num_samples=args.probes, max_num_samples=args.probes,
               error_rtol=0.0, lanczos_degree=args.degree,
               orthogonalize=args.orthogonalize, seed=0)

@@ -360,6 +360,7 @@ def prepare(A, parameters, func, gram, exponent, min_num_samples,
     J.orthogonalize, J.seed, J.seed_used = orthogonalize, seed, seed_used
     J.num_threads = num_threads
     J.verbose, J.plot = verbose, plot
+    J.num_devices = resolve_num_devices(num_gpu_devices)
     reset_outputs(J)
     return J
 
@@ -447,9 +448,135 @@ def collect(J, gi, res, a, status):
     J.engine["gpu_launches"] += int(res.gpu_launches)
 
 
-def run_job(J):
-    """Run every group of J with slq_run on the current stream."""
+def resolve_num_devices(num_gpu_devices):
+    """Devices an estimate runs on: all visible devices for 0 (the
+    reference's convention, trace_estimator.pyx:215-216), else at most the
+    number asked for."""
     import torch
+    avail = max(1, torch.cuda.device_count())
+    n = int(num_gpu_devices)
+    return avail if n == 0 else max(1, min(n, avail))
+
+
+def _block_on_device(J, device, first, count):
+    """Samples of global probes ``first`` .. ``first+count-1`` of job J's
+    single run on CUDA device ``device`` (run by the calling host thread):
+    a replica of the operator on that device and one block of slq_run."""
+    import torch
+    lib = _lib.load()
+    torch.cuda.set_device(device)
+    op = J.Aop.get_device_operator(need_transpose=J.need_transpose)
+    base = J.params[0]
+    prm = _lib.SlqParams.from_buffer_copy(base)
+    prm.first_probe = base.first_probe + first
+    prm.min_num_samples = count
+    prm.max_num_samples = count
+    prm.error_rtol = 0.0
+    prm.error_atol = 0.0
+    gq = J.num_inquiries
+    m = int(J.lanczos_degree)
+    ws_bytes = ctypes.c_size_t(0)
+    _lib.check(lib.slq_run_workspace_bytes(op.handle, ctypes.byref(prm), gq,
+                                           ctypes.byref(ws_bytes)))
+    workspace = torch.empty(int(ws_bytes.value), dtype=torch.uint8,
+                            device=op.device)
+    a = dict(trace=np.zeros(gq), error=np.zeros(gq),
+             samples=np.zeros((count, gq)),
+             order=np.zeros(count, dtype=np.int32),
+             used=np.zeros(gq, dtype=np.int32), out=np.zeros(gq, dtype=np.int32),
+             conv=np.zeros(gq, dtype=np.int32),
+             size=np.zeros(count, dtype=np.int32),
+             status=np.full(count, -1, dtype=np.int32),
+             alpha=np.zeros((count, m)) if J.alphas is not None else None,
+             beta=np.zeros((count, m)) if J.betas is not None else None)
+
+    def ptr(x):
+        return x.ctypes.data if x is not None else None
+    res = _lib.SlqResult(
+        trace=ptr(a["trace"]), error=ptr(a["error"]),
+        samples=ptr(a["samples"]), processed_samples_indices=ptr(a["order"]),
+        num_samples_used=ptr(a["used"]), num_outliers=ptr(a["out"]),
+        converged=ptr(a["conv"]), lanczos_size=ptr(a["size"]),
+        alpha=ptr(a["alpha"]), beta=ptr(a["beta"]),
+        probe_status=ptr(a["status"]))
+    t_g = J.t_groups[0]
+    stream = torch.cuda.current_stream(op.device)
+    status = lib.slq_run(op.handle, ctypes.byref(prm), t_g.ctypes.data, gq,
+                         workspace.data_ptr(), workspace.numel(),
+                         stream.cuda_stream, ctypes.byref(res))
+    if status not in (_lib.SLQ_OK, 6):
+        _lib.check(status)
+    return dict(samples=a["samples"], lanczos_size=a["size"],
+                probe_status=a["status"], alpha=a["alpha"], beta=a["beta"],
+                launches=int(res.gpu_launches))
+
+
+def run_job_multi(J, num_devices, device_of=None):
+    """Job J (one run) with its probe blocks dealt over ``num_devices``
+    devices, one host thread each (multi_device_trace_estimator); the result
+    equals that of one device.  ``device_of`` maps the dealing index to a
+    CUDA device (default: the identity)."""
+    from .distributed import multi_device_trace_estimator
+    import torch
+    b = block_width(J.max_num_samples, J.params[0].block_size, J.dtype_str)
+    q = J.num_inquiries
+    affine_many = bool(J.Aop.get_num_parameters() > 0 and q > 1)
+    launches = []
+    if device_of is None:
+        def device_of(d):
+            return d
+    home = torch.cuda.current_device()
+    # the operator replicas first, one device after the other (their host
+    # orders run on the process's thread pool)
+    for d in range(num_devices):
+        torch.cuda.set_device(device_of(d))
+        J.Aop.get_device_operator(need_transpose=J.need_transpose)
+    torch.cuda.set_device(home)
+
+    def run_block(device, first, count):
+        out = _block_on_device(J, device_of(device), first, count)
+        launches.append(out.pop("launches"))
+        return out
+    t0 = time.perf_counter()
+    r = multi_device_trace_estimator(
+        run_block, num_devices, q, b, J.min_num_samples, J.max_num_samples,
+        confidence_level=J.confidence_level, error_atol=J.error_atol,
+        error_rtol=J.error_rtol,
+        outlier_significance_level=J.outlier_significance_level,
+        affine_many=affine_many)
+    torch.cuda.set_device(home)
+    J.trace[:] = r["trace"]
+    J.error[:] = r["error"]
+    J.samples[:] = r["samples"]
+    J.processed = r["processed_samples_indices"]
+    J.num_samples_used[:] = r["num_samples_used"]
+    J.num_outliers[:] = r["num_outliers"]
+    J.converged[:] = r["converged"]
+    n = len(r.get("lanczos_size", []))
+    J.lanczos_size[:n, 0] = r["lanczos_size"][:n]
+    st = r.get("probe_status")
+    if st is not None:
+        J.probe_status[:len(st), 0] = st
+    if J.alphas is not None and r.get("alpha") is not None:
+        k = min(J.max_num_samples, len(r["alpha"]))
+        J.alphas[0][:k] = r["alpha"][:k]
+        J.betas[0][:k] = r["beta"][:k]
+    J.all_converged = bool(r["all_converged"])
+    J.alg_wall_time += time.perf_counter() - t0
+    J.engine["num_blocks"] += (r["num_probes_computed"] + b - 1) // b
+    J.engine["num_probes_computed"] += int(r["num_probes_computed"])
+    J.engine["gpu_launches"] += int(sum(launches))
+
+
+def run_job(J):
+    """Run every group of J with slq_run on the current stream (on several
+    devices when the job asks for them and has one run)."""
+    import torch
+    D = getattr(J, "num_devices", 1)
+    if D > 1 and len(J.params) == 1:
+        run_job_multi(J, D)
+        return
+    J.num_devices = 1
     lib = _lib.load()
     dev_op = J.dev_op
     stream = torch.cuda.current_stream(dev_op.device)
@@ -593,7 +720,7 @@ def finish(J):
         },
         "device": {
             "num_cpu_threads": J.num_threads,
-            "num_gpu_devices": 1,
+            "num_gpu_devices": getattr(J, "num_devices", 1),
             "num_gpu_multiprocessors": props.multi_processor_count,
             "num_gpu_threads_per_multiprocessor":
                 props.max_threads_per_multi_processor,

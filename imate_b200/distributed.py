@@ -20,7 +20,8 @@ import ctypes
 
 import numpy as np
 
-__all__ = ["shard_block", "replay_convergence", "distributed_trace_estimator"]
+__all__ = ["shard_block", "replay_convergence", "distributed_trace_estimator",
+           "multi_device_trace_estimator"]
 
 
 def shard_block(round_index, world_size, rank, block):
@@ -128,6 +129,87 @@ def distributed_trace_estimator(run_block, q, block, min_num_samples,
                 processed_samples_indices=order, num_samples_used=used,
                 num_outliers=outl, converged=converged.copy(),
                 all_converged=bool(done), rounds=k, world_size=world)
+
+
+def multi_device_trace_estimator(run_block, num_devices, q, block,
+                                 min_num_samples, max_num_samples,
+                                 confidence_level=0.95, error_atol=0.0,
+                                 error_rtol=1e-2,
+                                 outlier_significance_level=0.001,
+                                 affine_many=False, first_probe=0):
+    """Probe blocks of one estimate dealt over the devices of one process,
+    as the reference deals its samples over one OpenMP thread per GPU
+    (imate/_cu_trace_estimator/cu_trace_estimator.cu:229-299), but by global
+    probe index: in round k device d runs the block of global probes
+    [first_probe + (k D + d) b, ... + b) (D devices, b = ``block``), one
+    host thread per device, and the host then feeds the round's samples, in
+    global order, through the reference's sequential stopping rule.  A round
+    is taken only while the rule has not stopped, so every device count gives
+    the estimate, samples used, error and outliers of one device (it may
+    compute up to D - 1 blocks past the stopping point).
+
+    ``run_block(device, first, count)`` returns a dict with 'samples'
+    ([count][q]) and optionally 'lanczos_size', 'probe_status' ([count]),
+    'alpha', 'beta' ([count][m]) for global probes first .. first+count-1
+    (``first`` counted from ``first_probe``).  Returns the merged outputs."""
+    from concurrent.futures import ThreadPoolExecutor
+    from . import _lib
+    lib = _lib.load()
+    D = max(1, int(num_devices))
+    rows = []
+    extra = {}
+    processed = []
+    converged = np.zeros(q, dtype=np.int32)
+    done = False
+    used = np.zeros(q, dtype=np.int32)
+    k = 0
+    with ThreadPoolExecutor(max_workers=D) as pool:
+        while not done and len(rows) < max_num_samples:
+            jobs = []
+            for d in range(D):
+                first = (k * D + d) * block
+                count = min(block, max_num_samples - first)
+                if count > 0:
+                    jobs.append((first, pool.submit(run_block, d, first, count)))
+            for first, fut in jobs:
+                out = fut.result()
+                s = np.asarray(out["samples"], dtype=np.float64)
+                rows.extend(list(s.reshape(s.shape[0], q)))
+                for key in ("lanczos_size", "probe_status", "alpha", "beta"):
+                    if out.get(key) is not None:
+                        extra.setdefault(key, []).extend(list(out[key]))
+            S = np.asarray(rows, dtype=np.float64).reshape(len(rows), q)
+            done, _, used = replay_convergence(
+                S, q, min_num_samples, confidence_level, error_atol,
+                error_rtol, processed, converged, affine_many)
+            k += 1
+    # as one device reports them: samples past the stopping point NaN,
+    # Krylov sizes only for the samples the rule took
+    nproc = len(processed)
+    S = np.full((max_num_samples, q), np.nan)
+    S[:nproc] = np.asarray(rows[:nproc]).reshape(nproc, q)
+    order = np.zeros(max_num_samples, dtype=np.int32)
+    order[:nproc] = processed
+    used = np.ascontiguousarray(used, dtype=np.int32)
+    outl = np.zeros(q, dtype=np.int32)
+    trace = np.zeros(q)
+    err = np.zeros(q)
+    lib.slq_average_estimates(float(confidence_level),
+                              float(outlier_significance_level), q,
+                              max_num_samples, used.ctypes.data,
+                              order.ctypes.data, S.ctypes.data,
+                              outl.ctypes.data, trace.ctypes.data,
+                              err.ctypes.data)
+    if "lanczos_size" in extra:
+        extra["lanczos_size"] = list(extra["lanczos_size"][:nproc])
+    res = dict(trace=trace, error=err, samples=S,
+               processed_samples_indices=order, num_samples_used=used,
+               num_outliers=outl, converged=converged.copy(),
+               all_converged=bool(done), rounds=k, num_devices=D,
+               num_probes_computed=len(rows))
+    for key, vals in extra.items():
+        res[key] = np.asarray(vals)
+    return res
 
 
 def engine_block_runner(Aop, func, gram=False, exponent=1.0, parameters=None,

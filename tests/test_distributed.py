@@ -98,3 +98,43 @@ def test_sharded_estimate_equals_single_process(tmp_path, world, block):
             1e-13 * abs(want["trace"][0])
         np.testing.assert_array_equal(r["num_outliers"], want["num_outliers"])
     assert int(res[0]["rounds"]) >= 1
+
+
+@pytest.mark.parametrize("devices,block", [(1, 4), (2, 4), (3, 5), (4, 16)])
+def test_multi_device_estimate_equals_single_device(devices, block):
+    # the probe blocks of one estimate dealt over the devices of one process
+    # (one host thread each, here a stand-in that serves the oracle's
+    # samples): every device count gives the single-device answer, and
+    # device d gets the blocks d, d + D, ... of the global probe order
+    from oracle import oracle
+    from imate_b200.distributed import multi_device_trace_estimator
+    A = _matrix()
+    want = oracle.trace_estimator(A, "log", min_num_samples=6,
+                                  max_num_samples=40, error_rtol=2e-3, **KW)
+    every = oracle.trace_estimator(A, "log", min_num_samples=40,
+                                   max_num_samples=40, error_rtol=0.0,
+                                   **KW)["samples"]
+    calls = []
+
+    def run_block(device, first, count):
+        calls.append((device, first, count))
+        return {"samples": every[first:first + count],
+                "lanczos_size": np.full(count, 12, dtype=np.int32),
+                "probe_status": np.zeros(count, dtype=np.int32)}
+    res = multi_device_trace_estimator(run_block, devices, 1, block, 6, 40,
+                                       error_rtol=2e-3)
+    used = int(want["num_samples_used"][0])
+    assert int(res["num_samples_used"][0]) == used
+    np.testing.assert_array_equal(res["samples"][:used, 0],
+                                  want["samples"][:used, 0])
+    assert np.all(np.isnan(res["samples"][used:, 0]))
+    np.testing.assert_array_equal(res["processed_samples_indices"][:used],
+                                  want["processed_samples_indices"][:used])
+    assert abs(res["trace"][0] - want["trace"][0]) <= \
+        1e-13 * abs(want["trace"][0])
+    np.testing.assert_array_equal(res["num_outliers"], want["num_outliers"])
+    assert len(res["lanczos_size"]) == used
+    for device, first, count in calls:
+        assert (first // block) % devices == device
+    # no round is started once the rule has stopped
+    assert res["num_probes_computed"] < used + devices * block
