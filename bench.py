@@ -43,6 +43,13 @@ sys.path.insert(0, ROOT)
 
 METRIC = ("SLQ logdet probe·steps/s on 1 B200, mixed+batched vs plain "
           "FP64, at 1e-3 rel err")
+# the function of the c2prime line: the reference's function code and the
+# public entry point's name (traceinv: imate/traceinv/_slq_method.pyx:24)
+FUNC_CODES = {"logdet": "log", "traceinv": "inv"}
+
+
+def metric_of(args):
+    return METRIC.replace("logdet", args.func)
 UNIT = "probe*steps/s"
 # FP64 oracle of the workload's logdet: sparse LU (scipy splu, MMD_AT_PLUS_A,
 # symmetric mode) of the float64 matrix; tests/golden/make_c2_oracle.py
@@ -83,6 +90,14 @@ def parse():
                          "(auto) or a forced autotuner candidate; the e2e leg "
                          "always takes the public API's default path")
     ap.add_argument("--block", type=int, default=256)
+    ap.add_argument("--func", default="logdet", choices=sorted(FUNC_CODES),
+                    help="function of the c2prime line (same kernels; "
+                         "traceinv takes f = 1/x at the Ritz values)")
+    ap.add_argument("--fp64-ref-probes", type=int, default=-1,
+                    help="probes of the high-sample FP64 SLQ the c2prime "
+                         "line states its error against (-1: 1024 for "
+                         "traceinv, which has no direct FP64 oracle at full "
+                         "size, 0 for logdet, whose oracle is sparse LU)")
     return ap.parse_args()
 
 
@@ -95,7 +110,7 @@ def build_matrix(args, dtype):
 def workload_config(args, nnz):
     return {
         "workload": "sparse SPD correlation matrix (exp(-r/0.005), cut 0.05, "
-                    "diag shift %g), SLQ logdet" % args.shift,
+                    "diag shift %g), SLQ %s" % (args.shift, args.func),
         "n": args.n, "nnz": int(nnz), "value_dtype": "float32",
         "index_dtype": "int32", "probes_per_step": args.probes,
         "lanczos_degree": args.degree,
@@ -107,6 +122,8 @@ def workload_config(args, nnz):
 
 
 def load_oracle(args):
+    if args.func != "logdet":
+        return None
     try:
         with open(ORACLE_FILE) as f:
             d = json.load(f)
@@ -126,7 +143,8 @@ def reference_sample(A, args, probes, threads, seed=0):
     (probe*steps/s, seconds, kind)."""
     from oracle import ref
     if ref.available():
-        r = ref.trace_estimator(A, "log", min_num_samples=probes,
+        r = ref.trace_estimator(A, FUNC_CODES[args.func],
+                                min_num_samples=probes,
                                 max_num_samples=probes, error_rtol=0.0,
                                 lanczos_degree=args.degree,
                                 orthogonalize=args.orthogonalize, seed=seed,
@@ -137,7 +155,7 @@ def reference_sample(A, args, probes, threads, seed=0):
         return probes * args.degree / secs, secs, "reference"
     from oracle import oracle
     t = time.perf_counter()
-    r = oracle.trace_estimator(A.astype(np.float64), "log",
+    r = oracle.trace_estimator(A.astype(np.float64), FUNC_CODES[args.func],
                                min_num_samples=probes,
                                max_num_samples=probes, error_rtol=0.0,
                                lanczos_degree=args.degree,
@@ -184,7 +202,8 @@ def run_reference_arm(args):
         secs += t
     value = probes * args.degree * args.steps / secs
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "impl": "reference", "metric": metric_of(args), "value": value,
+        "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -349,6 +368,7 @@ def run_engine_arm(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
 
+    fn = getattr(ib, args.func)
     A32 = build_matrix(args, "float32")
     # the tensor-core row-group SpMM serves 16-row groups only; the block
     # kernel needs the block format
@@ -373,7 +393,7 @@ def run_engine_arm(args):
     def step(i, op=Aop):
         # disjoint probe indices per rank and step (parity stream offsets)
         eng.first_probe = (rank * (args.warmup + args.steps) + i) * args.probes
-        return ib.logdet(op, engine=eng, **kw)
+        return fn(op, engine=eng, **kw)
 
     for i in range(args.warmup):
         step(i)
@@ -391,8 +411,10 @@ def run_engine_arm(args):
     probe_steps = 0
     launches = 0
     estimates = []
+    samples = []
     for i in range(args.steps):
         tr, info = step(args.warmup + i)
+        samples.append(info["convergence"]["samples"])
         probe_steps += int(np.sum(info["engine"]["lanczos_size"]
                                   [:args.probes]))
         launches += int(info["engine"]["gpu_launches"])
@@ -436,7 +458,8 @@ def run_engine_arm(args):
                             for k, v in kstats.items() if v[0]}}
 
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "metric": metric_of(args), "value": value, "unit": UNIT,
+        "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -456,6 +479,42 @@ def run_engine_arm(args):
         "note": "precision error (mixed vs FP64 on identical probes) is in "
                 "fp64_plain.rel_diff_same_probes",
     }
+    s_mixed = np.concatenate([np.ravel(np.asarray(x, float)[:args.probes])
+                              for x in samples])
+    line["accuracy"]["standard_error"] = float(
+        np.std(s_mixed, ddof=1) / np.sqrt(s_mixed.size)) \
+        if s_mixed.size > 1 else None
+    nref = args.fp64_ref_probes
+    if nref < 0:
+        nref = 1024 if args.func != "logdet" else 0
+    if rank == 0 and nref > 0:
+        # high-sample FP64 SLQ (FP64 operator and vectors, block width 256)
+        # on probes 0 .. nref-1 of the parity stream: the full-size FP64
+        # reference of a function without a direct FP64 oracle
+        A64 = A32.astype(np.float64)
+        Mref = ib.Matrix(A64)
+        eref = ib.EngineOptions(block_size=256, rng="parity")
+        t0 = time.perf_counter()
+        tr_ref, info_ref = fn(Mref, engine=eref, **dict(
+            kw, min_num_samples=nref, max_num_samples=nref))
+        torch.cuda.synchronize()
+        secs_ref = time.perf_counter() - t0
+        sref = np.asarray(info_ref["convergence"]["samples"][:nref], float)
+        se_ref = float(np.std(sref, ddof=1) / np.sqrt(nref))
+        se_mix = line["accuracy"]["standard_error"] or 0.0
+        diff = est - float(tr_ref)
+        line["accuracy"]["fp64_high_sample"] = {
+            "estimate": float(tr_ref), "probes": nref,
+            "standard_error": se_ref, "seconds": secs_ref,
+            "rel_standard_error": se_ref / abs(float(tr_ref)),
+            "rel_diff_of_mixed_mean": abs(diff) / abs(float(tr_ref)),
+            "z_of_mixed_mean": diff / max(np.hypot(se_ref, se_mix), 1e-300),
+            "note": "different probes (mixed: the timed steps' probes; "
+                    "FP64: probes 0..%d), so the difference is Monte-Carlo "
+                    "error, z in units of the combined standard error"
+                    % (nref - 1)}
+        del Mref
+        torch.cuda.empty_cache()
 
     if rank == 0 and args.fp64_probes > 0:
         # plain FP64 per-probe path (block width 1) on the same matrix
@@ -465,20 +524,20 @@ def run_engine_arm(args):
         e64 = ib.EngineOptions(block_size=1, rng="parity")
         nprb = args.fp64_probes
         kw64 = dict(kw, min_num_samples=nprb, max_num_samples=nprb)
-        ib.logdet(Aop64, engine=e64, **dict(kw64, min_num_samples=1,
+        fn(Aop64, engine=e64, **dict(kw64, min_num_samples=1,
                                               max_num_samples=1))
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        tr64, info64 = ib.logdet(Aop64, engine=e64, **kw64)
+        tr64, info64 = fn(Aop64, engine=e64, **kw64)
         e1.record()
         torch.cuda.synchronize()
         t64 = e0.elapsed_time(e1) * 1e-3
         ps64 = int(np.sum(info64["engine"]["lanczos_size"][:nprb]))
         # same probes in mixed precision
         e32 = ib.EngineOptions(block_size=min(args.probes, 256), rng="parity")
-        tr32, info32 = ib.logdet(Aop, engine=e32, **kw64)
+        tr32, info32 = fn(Aop, engine=e32, **kw64)
         s64 = np.asarray(info64["convergence"]["samples"][:nprb], float)
         s32 = np.asarray(info32["convergence"]["samples"][:nprb], float)
         v64 = ps64 / t64
@@ -504,7 +563,7 @@ def run_engine_arm(args):
                 # ~50 ms at this size, against ~25 ms saved per 256 probes)
                 fresh = ib.Matrix(A32)
                 eng.first_probe = i * args.probes
-                tr, info = ib.logdet(fresh, engine=eng, **kw)
+                tr, info = fn(fresh, engine=eng, **kw)
                 e_ps += int(np.sum(info["engine"]["lanczos_size"]
                                    [:args.probes]))
                 del fresh
@@ -514,7 +573,8 @@ def run_engine_arm(args):
                            "h2d_bytes_per_step": int(h2d),
                            "d2h_bytes_per_step": int(args.probes * 8 * 2),
                            "steps": nsteps,
-                           "path": "imate_b200.logdet(scipy CSR on host), "
+                           "path": "imate_b200.%s(scipy CSR on host), "
+                                   % args.func +
                                    "default Matrix options (row groups, no "
                                    "block format)"}
 
@@ -579,7 +639,7 @@ def run_batched(args):
                  lanczos_degree=degree, orthogonalize=0, seed=i)
             for i, M in enumerate(mats)]
     t0 = time.perf_counter()
-    plan = BatchPlan(ests, autotune=True)
+    plan = BatchPlan(ests, autotune=True, num_gpu_devices=1)
     plan_s = time.perf_counter() - t0
     for _ in range(args.warmup):
         plan.run()
@@ -685,7 +745,8 @@ def run_sweep(args):
     out = {}
     for func, f in funcs.items():
         S = SweepSurrogate(A32, func=func, t_min=1e-4, t_max=1e2,
-                           num_train=32, num_check=16, rtol=1e-3, **opts)
+                           num_train=32, checks_per_interval=4, rtol=1e-3,
+                           **opts)
         S.Aop = Aop  # share the resident operator
         torch.cuda.synchronize()
         t0 = time.perf_counter()

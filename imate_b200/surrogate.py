@@ -9,7 +9,9 @@ samples of the sweep on the device and answers the sweep from it:
 
 1. SLQ (this engine, one Krylov run per probe thanks to the shift relation)
    evaluates the sweep at ``num_train`` log-spaced training points and at
-   ``num_check`` held-out points between them;
+   ``checks_per_interval`` held-out points inside every interval between
+   them (evenly spread in log t; extra points of one Krylov run cost a few
+   quadrature evaluations);
 2. the network 1 -> 64 -> 64 -> 1 (tanh, FP32; input log t standardised)
    is trained on the device by ``slq_mlp_train`` on the standardised
    residual of a one-parameter base curve with the sweep's limits, tau
@@ -18,11 +20,13 @@ samples of the sweep on the device and answers the sweep from it:
    r = log(f/n) + log(t + tau) for traceinv (f/n ~ 1/(t + tau); in log space
    an absolute error of the network is a relative error of f), and
    r = f/n - (t + tau) for trace;
-3. each held-out point is compared with its SLQ value; an interval between
-   training points whose check point misses ``rtol`` (relative error,
-   judged against a floor of ``rtol_floor`` times the sweep's mean
-   magnitude where the values cross zero) is answered by SLQ instead (the
-   fallback), as is any t outside the trained range.
+3. every held-out point, and every training point, is compared with its
+   SLQ value; an interval between training points is trusted only when all
+   of its points and both of its ends are within ``margin * rtol`` (relative
+   error, judged against a floor of ``rtol_floor`` times the sweep's mean
+   magnitude where the values cross zero), the margin covering the error
+   between check points; an untrusted interval is answered by SLQ instead
+   (the fallback), as is any t outside the trained range.
 
 ``SweepSurrogate.timings`` records where the time goes so the sweep can be
 compared with per-t SLQ and with the shift relation alone.
@@ -69,19 +73,25 @@ class SweepSurrogate:
     """
 
     def __init__(self, A, func="log", t_min=1e-4, t_max=1e2, num_train=32,
-                 num_check=16, rtol=1e-3, rtol_floor=1e-3, steps=20000,
-                 lr=2e-3, seed=0, engine=None, **slq_options):
+                 checks_per_interval=4, rtol=1e-3, rtol_floor=1e-3,
+                 margin=0.5, steps=20000, lr=2e-3, seed=0, engine=None,
+                 **slq_options):
         if func not in _FUNCS:
             raise ValueError("func must be 'log', 'inv' or 'id'")
         if not 0 < t_min < t_max:
             raise ValueError("need 0 < t_min < t_max")
-        if num_train > _lib.MLP_MAX_BATCH:
-            raise ValueError("num_train is at most %d" % _lib.MLP_MAX_BATCH)
+        if not 2 <= num_train <= _lib.MLP_MAX_BATCH:
+            raise ValueError("num_train is between 2 and %d"
+                             % _lib.MLP_MAX_BATCH)
+        if checks_per_interval < 1 or not 0 < margin <= 1:
+            raise ValueError("need checks_per_interval >= 1 and "
+                             "0 < margin <= 1")
         self.A = A
         self.func = func
         self.t_min, self.t_max = float(t_min), float(t_max)
         self.num_train = int(num_train)
-        self.num_check = int(num_check)
+        self.checks_per_interval = int(checks_per_interval)
+        self.margin = float(margin)
         self.rtol = float(rtol)
         self.rtol_floor = float(rtol_floor)
         self.steps = int(steps)
@@ -117,12 +127,14 @@ class SweepSurrogate:
         lib = _lib.load()
         lt0, lt1 = np.log(self.t_min), np.log(self.t_max)
         self.t_train = np.exp(np.linspace(lt0, lt1, self.num_train))
-        # held-out points: midpoints (in log t) of evenly spread intervals
-        lmid = 0.5 * (np.log(self.t_train[:-1]) + np.log(self.t_train[1:]))
-        pick = np.unique(np.linspace(0, lmid.size - 1,
-                                     self.num_check).round().astype(int))
-        self.check_interval = pick
-        self.t_check = np.exp(lmid[pick])
+        # held-out points: c evenly spread points (in log t) strictly inside
+        # every interval between neighbouring training points
+        c = self.checks_per_interval
+        frac = (np.arange(c) + 0.5) / c
+        lt = np.log(self.t_train)
+        lcheck = lt[:-1, None] + (lt[1:] - lt[:-1])[:, None] * frac[None, :]
+        self.check_interval = np.repeat(np.arange(lt.size - 1), c)
+        self.t_check = np.exp(lcheck.ravel())
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         allt = np.concatenate([self.t_train, self.t_check])
@@ -165,11 +177,20 @@ class SweepSurrogate:
         self.loss_history = hist.cpu().numpy()[:self.steps]
         self.params = self._p.cpu().numpy()
 
-        pred = self.predict(self.t_check)
+        pred = self.predict(np.concatenate([self.t_check, self.t_train]))
         floor = self.rtol_floor * float(np.mean(np.abs(self.y_train)))
-        self.check_error = np.abs(pred - self.y_check) / np.maximum(
-            np.abs(self.y_check), floor)
-        self.check_passed = (self.check_error <= self.rtol) & self._usable
+        ref = np.concatenate([self.y_check, self.y_train])
+        err = np.abs(pred - ref) / np.maximum(np.abs(ref), floor)
+        self.check_error = err[:self.t_check.size]
+        self.train_error = err[self.t_check.size:]
+        bound = self.margin * self.rtol
+        nint = self.num_train - 1
+        worst = np.zeros(nint)
+        np.maximum.at(worst, self.check_interval, self.check_error)
+        worst = np.maximum(worst, np.maximum(self.train_error[:-1],
+                                             self.train_error[1:]))
+        self.interval_error = worst
+        self.interval_trusted = (worst <= bound) & self._usable
         self.fitted = True
         return self
 
@@ -217,18 +238,14 @@ class SweepSurrogate:
         return self._from_resid(t, z * self.y_scale + self.y_mean) * self.n
 
     def _trusted(self, t):
-        """True where t lies in the fitted range inside an interval whose
-        held-out check passed (intervals without a check point borrow the
-        nearest checked interval's verdict)."""
+        """True where t lies in the fitted range inside a trusted interval."""
         t = np.asarray(t, dtype=np.float64)
         inside = (t >= self.t_min * (1 - 1e-12)) & (t <= self.t_max * (1 + 1e-12))
         lt = np.log(np.clip(t, self.t_min, self.t_max))
         edges = np.log(self.t_train)
         interval = np.clip(np.searchsorted(edges, lt, side="right") - 1, 0,
                            edges.size - 2)
-        nearest = np.abs(interval[:, None] -
-                         self.check_interval[None, :]).argmin(axis=1)
-        return inside & self.check_passed[nearest]
+        return inside & self.interval_trusted[interval]
 
     def __call__(self, t):
         """Sweep values at t: the network where trusted, SLQ elsewhere."""

@@ -279,3 +279,27 @@ def test_device_built_correlation_matrix(cuda):
     assert np.array_equal(idv["convergence"]["samples"],
                           ih["convergence"]["samples"])
     assert td == th
+
+
+def test_batch_packed_over_two_logical_devices_equals_one_device(cuda):
+    """Estimates packed over two devices (both mapped onto this GPU, one
+    host thread per device graph) give the one-graph answers bit for bit."""
+    import torch
+    ests = _mixed_estimates()
+    one = BatchPlan(ests, autotune=False, num_gpu_devices=1)
+    assert len(one.plans) == 1
+    want = one.run()
+    two = BatchPlan(ests, autotune=False, num_gpu_devices=2,
+                    device_of=lambda d: torch.cuda.current_device())
+    assert sorted(set(two.assignment)) == [0, 1]
+    assert len(two.plans) == 2
+    got = two.run()
+    for g, w in zip(got, want):
+        _same(g, w)
+    devs = {g[1]["engine"]["batch"]["device"] for g in got}
+    assert devs == {torch.cuda.current_device()}
+    assert sum(p.graph_kernels for p in two.plans) == two.graph_kernels
+    # 0 = every visible device; on one GPU that is one graph
+    if torch.cuda.device_count() == 1:
+        assert len(BatchPlan(ests[:2], autotune=False,
+                             num_gpu_devices=0).plans) == 1
