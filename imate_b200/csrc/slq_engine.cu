@@ -259,6 +259,11 @@ struct slq_op {
     // kernel (inside the first format buffer)
     int32_t* blk_error = nullptr;
     unsigned int* blk_xmax = nullptr;
+    // the scratch slq_operator_blocks_bytes prepared per direction (sorted
+    // keys, unions, stages) and its stage count, so that
+    // slq_operator_add_blocks on the same scratch does not sort again
+    const void* blk_prep_scratch[2] = {nullptr, nullptr};
+    int64_t blk_prep_stages[2] = {0, 0};
     // autotuned SpMM candidate per direction and log2(block width); -1 = built-in
     int8_t tuned[2][11];
     slq_op()
@@ -840,6 +845,9 @@ extern "C" slq_status slq_operator_blocks_bytes(const slq_op* op, int transpose,
     if (!scratch || !c.fits()) return fail(SLQ_ERR_WORKSPACE, "blocks: scratch too small");
     int64_t stages = 0;
     SLQ_TRY(blk_prepare(ptr, ind, R, C, op->nnz, &s, static_cast<cudaStream_t>(stream), &stages));
+    slq_op* mop = const_cast<slq_op*>(op);  // the preparation cache only
+    mop->blk_prep_scratch[transpose] = scratch;
+    mop->blk_prep_stages[transpose] = stages;
     Carver f(nullptr, 0);
     BlkFormat bf;
     blk_format_layout(f, (R + BLK_ROWS - 1) / BLK_ROWS, stages, &bf);
@@ -861,7 +869,11 @@ extern "C" slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* s
     SLQ_TRY(blk_scratch_layout(c, R, op->nnz, &s));
     if (!scratch || !c.fits()) return fail(SLQ_ERR_WORKSPACE, "blocks: scratch too small");
     int64_t stages = 0;
-    SLQ_TRY(blk_prepare(ptr, ind, R, C, op->nnz, &s, st, &stages));
+    if (op->blk_prep_scratch[transpose] == scratch && scratch)
+        stages = op->blk_prep_stages[transpose];  // prepared by slq_operator_blocks_bytes
+    else
+        SLQ_TRY(blk_prepare(ptr, ind, R, C, op->nnz, &s, st, &stages));
+    op->blk_prep_scratch[transpose] = nullptr;
     const int64_t nblk = (R + BLK_ROWS - 1) / BLK_ROWS;
     Carver f(format, format_bytes);
     BlkFormat bf;
@@ -2939,6 +2951,8 @@ struct RcmBufs {
     uint64_t* keys_alt;
     void* temp;
     size_t temp_bytes;
+    RcmCoopState* coop;  // the one-launch order's level state and barrier
+    int32_t* coop_err;
 };
 
 slq_status rcm_layout(Carver& c, int64_t n, RcmBufs* B)
@@ -2966,6 +2980,8 @@ slq_status rcm_layout(Carver& c, int64_t n, RcmBufs* B)
     B->keys_alt = c.take<uint64_t>(n);
     B->temp_bytes = std::max(t1, t2);
     B->temp = c.take<char>(B->temp_bytes);
+    B->coop = c.take<RcmCoopState>(1);
+    B->coop_err = c.take<int32_t>(4);
     return SLQ_OK;
 }
 
@@ -3033,6 +3049,54 @@ extern "C" slq_status slq_rcm_order_device(int64_t n, int64_t nnz, const int32_t
             db, st);
         if (e != cudaSuccess)
             return fail(SLQ_ERR_CUDA, std::string("cub sort: ") + cudaGetErrorString(e));
+    }
+
+    // every level in one cooperative launch when a warp's sort buffer holds
+    // the widest row's children; else one host round per level (below)
+    if (maxdeg <= 1024 && n <= (int64_t(1) << 30))
+    {
+        int cap = 32;
+        while (cap < maxdeg) cap <<= 1;
+        const int threads = 512;
+        const size_t smem = static_cast<size_t>(threads / 32) * cap * sizeof(uint64_t);
+        int per_sm = 0;
+        bool coop = cudaFuncSetAttribute(k_rcm_coop, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem)) == cudaSuccess &&
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rcm_coop, threads,
+                                                                  smem) == cudaSuccess &&
+                    per_sm >= 1;
+        cudaGetLastError();  // a refused attribute leaves the level rounds
+        if (coop)
+        {
+            SLQ_CK(cudaMemsetAsync(B.coop, 0, sizeof(RcmCoopState), st));
+            SLQ_CK(cudaMemsetAsync(B.coop_err, 0, 4 * sizeof(int32_t), st));
+            int64_t n_arg = n;
+            int maxc = max_components;
+            // about two seconds at the boost clock
+            long long spin_limit = 1LL << 32;
+            int32_t* counts = B.deg_sorted;  // free after the degree sort
+            void* args[] = {(void*)&indptr, (void*)&indices, (void*)&B.degree,
+                            (void*)&B.by_degree, (void*)&n_arg, (void*)&maxc, (void*)&cap,
+                            (void*)&B.pos, (void*)&B.claim, (void*)&B.out, (void*)&counts,
+                            (void*)&B.coop, (void*)&B.coop_err, (void*)&spin_limit};
+            SLQ_CK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_rcm_coop),
+                                               dim3(sms), dim3(threads), args, smem, st));
+            int32_t herr = 0;
+            RcmCoopState hs{};
+            SLQ_CK(cudaMemcpyAsync(&herr, B.coop_err, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                   st));
+            SLQ_CK(cudaMemcpyAsync(&hs, B.coop, sizeof(hs), cudaMemcpyDeviceToHost, st));
+            SLQ_CK(cudaStreamSynchronize(st));
+            if (herr & 64) return SLQ_OK;  // more components than asked for: *done stays 0
+            if (herr & 16)
+                return fail(SLQ_ERR_TIMEOUT, "rcm_order_device: a grid barrier wait ran out");
+            if (herr != 0 || !hs.done || hs.cnt != n)
+                return fail(SLQ_ERR_CUDA, "rcm_order_device: lost track of the visited rows");
+            k_rcm_reverse<<<grid, 256, 0, st>>>(B.out, n, order);
+            SLQ_LAUNCH_CK();
+            *done = 1;
+            return SLQ_OK;
+        }
     }
 
     const int32_t first_init = static_cast<int32_t>(n);

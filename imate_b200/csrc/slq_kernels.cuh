@@ -880,6 +880,281 @@ __global__ void k_rcm_reverse(const int32_t* __restrict__ out, int64_t n,
         order[k] = out[n - 1 - k];
 }
 
+// ---------------------------------------------------------------------------
+// Cuthill-McKee order in one cooperative launch: the same levels, parents
+// and (degree, row) order as the round-per-level kernels above, with every
+// level done inside the kernel between grid barriers instead of by host
+// rounds (a memcpy, a synchronisation and a radix sort per level).  Per
+// level:
+//   A  claim: claim[c] = min(claim[c], k) over the unvisited neighbours c of
+//      every frontier row k (as k_rcm_claim);
+//   B  count: each claimed neighbour is taken once by its parent k
+//      (claim k -> -2 - k) and counted, counts[k - lb];
+//   C  block 0 scans the counts into offsets, sets the next level
+//      [le, le + m) -- or, when the level has no children, starts the next
+//      component at the first unvisited row of the (degree, row) order;
+//   D  each parent lists its children again (claim -2 - k -> INT_MIN), ranks
+//      them by (degree, row) inside its warp and places them at
+//      le + offset + rank.
+// A warp lists at most `cap` children (cap >= the largest row degree, which
+// the host checks).  The grid barrier is a counter and a generation word
+// whose waits give up after `spin_limit` clock cycles (error bit 16), so the
+// kernel always ends.
+// ---------------------------------------------------------------------------
+
+struct RcmCoopState {
+    int64_t lb, le, cnt, cursor;
+    int32_t components, done;
+    uint32_t bar_count, bar_gen;
+};
+
+__device__ __forceinline__ int32_t ldcg_i32(const int32_t* p) { return __ldcg(p); }
+
+// the error word as one value for the whole block (thread 0 reads it)
+__device__ __forceinline__ int32_t rcm_block_err(const int32_t* err, int32_t* slot)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) *slot = *reinterpret_cast<const volatile int32_t*>(err);
+    __syncthreads();
+    return *slot;
+}
+
+__device__ __forceinline__ void rcm_grid_sync(RcmCoopState* st, int32_t* err,
+                                              long long spin_limit)
+{
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        volatile uint32_t* gen = &st->bar_gen;
+        const uint32_t g = *gen;
+        __threadfence();
+        if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1)
+        {
+            atomicExch(&st->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&st->bar_gen, 1u);
+        }
+        else
+        {
+            const long long t0 = clock64();
+            while (*gen == g)
+            {
+                if (clock64() - t0 > spin_limit)
+                {
+                    atomicOr(err, 16);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// block-wide exclusive scan of a[0 .. len) in place (block 0 only); returns
+// the total to every thread of the block
+__device__ int64_t rcm_block_scan(int32_t* a, int64_t len, int32_t* warp_sums)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int64_t carry = 0;
+    for (int64_t base = 0; base < len; base += blockDim.x)
+    {
+        const int64_t i = base + threadIdx.x;
+        const int32_t v = i < len ? ldcg_i32(a + i) : 0;
+        int32_t x = v;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sums[wid] = x;
+        __syncthreads();
+        if (wid == 0)
+        {
+            int32_t s = lane < nw ? warp_sums[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const int32_t y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            if (lane < nw) warp_sums[lane] = s;  // inclusive warp prefix
+        }
+        __syncthreads();
+        const int32_t before = (wid > 0 ? warp_sums[wid - 1] : 0) + x - v;
+        if (i < len) a[i] = static_cast<int32_t>(carry + before);
+        carry += warp_sums[nw - 1];
+        __syncthreads();
+    }
+    return carry;
+}
+
+// block 0: the first unvisited row of by_degree at or after the cursor
+// starts a component at position cnt
+__device__ void rcm_start_component(RcmCoopState* st, const int32_t* __restrict__ by_degree,
+                                    int32_t* __restrict__ pos, int32_t* __restrict__ out,
+                                    int64_t n, int max_components, int32_t* err, int32_t* sh)
+{
+    if (threadIdx.x == 0) sh[0] = INT_MAX;
+    __syncthreads();
+    int64_t cursor = st->cursor;
+    for (;;)
+    {
+        const int64_t i = cursor + threadIdx.x;
+        if (i < n && ldcg_i32(pos + by_degree[i]) < 0) atomicMin(sh, static_cast<int32_t>(i));
+        __syncthreads();
+        const int32_t found = sh[0];
+        if (found != INT_MAX || cursor + blockDim.x >= n) break;
+        cursor += blockDim.x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        const int32_t found = sh[0];
+        if (found == INT_MAX || st->cnt >= n)
+            atomicOr(err, 32);  // lost track of the unvisited rows
+        else if (st->components + 1 > max_components)
+            atomicOr(err, 64);  // more components than asked for
+        else
+        {
+            const int32_t r = by_degree[found];
+            pos[r] = static_cast<int32_t>(st->cnt);
+            out[st->cnt] = r;
+            st->cursor = found + 1;
+            st->lb = st->cnt;
+            st->le = st->cnt + 1;
+            st->cnt += 1;
+            st->components += 1;
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(512, 1)
+    k_rcm_coop(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+               const int32_t* __restrict__ degree, const int32_t* __restrict__ by_degree,
+               int64_t n, int max_components, int cap, int32_t* __restrict__ pos,
+               int32_t* __restrict__ claim, int32_t* __restrict__ out,
+               int32_t* __restrict__ counts, RcmCoopState* st, int32_t* err,
+               long long spin_limit)
+{
+    extern __shared__ uint64_t rcm_sh[];
+    __shared__ int32_t small[40];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    uint64_t* buf = rcm_sh + static_cast<int64_t>(wid) * cap;
+    const int64_t gw = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + wid;
+    const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+
+    if (blockIdx.x == 0) rcm_start_component(st, by_degree, pos, out, n, max_components, err, small);
+    rcm_grid_sync(st, err, spin_limit);
+    for (;;)
+    {
+        if (rcm_block_err(err, small + 32) != 0) return;
+        const int64_t lb = *reinterpret_cast<volatile int64_t*>(&st->lb);
+        const int64_t le = *reinterpret_cast<volatile int64_t*>(&st->le);
+        if (*reinterpret_cast<volatile int32_t*>(&st->done)) return;
+
+        // A: claims
+        for (int64_t k = lb + gw; k < le; k += nwarps)
+        {
+            const int32_t r = ldcg_i32(out + k);
+            const int32_t e1 = __ldg(indptr + r + 1);
+            for (int32_t e = __ldg(indptr + r) + lane; e < e1; e += 32)
+            {
+                const int32_t c = __ldg(indices + e);
+                if (ldcg_i32(pos + c) < 0) atomicMin(claim + c, static_cast<int32_t>(k));
+            }
+        }
+        rcm_grid_sync(st, err, spin_limit);
+        // B: each child taken once by its parent, counted
+        for (int64_t k = lb + gw; k < le; k += nwarps)
+        {
+            const int32_t r = ldcg_i32(out + k);
+            const int32_t kk = static_cast<int32_t>(k);
+            const int32_t e1 = __ldg(indptr + r + 1);
+            int32_t m = 0;
+            for (int32_t e = __ldg(indptr + r) + lane; e < e1; e += 32)
+            {
+                const int32_t c = __ldg(indices + e);
+                if (ldcg_i32(claim + c) == kk && atomicCAS(claim + c, kk, -2 - kk) == kk) ++m;
+            }
+            for (int o = 16; o > 0; o >>= 1) m += __shfl_xor_sync(0xffffffffu, m, o);
+            if (lane == 0)
+            {
+                if (m > cap) atomicOr(err, 128);
+                counts[k - lb] = m;
+            }
+        }
+        rcm_grid_sync(st, err, spin_limit);
+        // C: offsets and the next level (block 0)
+        if (blockIdx.x == 0 && rcm_block_err(err, small + 32) == 0)
+        {
+            const int64_t m = rcm_block_scan(counts, le - lb, small);
+            if (threadIdx.x == 0)
+            {
+                st->lb = le;
+                st->le = le + m;
+                st->cnt = le + m;
+                if (m == 0 && st->cnt >= n) st->done = 1;
+                __threadfence();
+            }
+            __syncthreads();
+            if (m == 0 && le < n)
+                rcm_start_component(st, by_degree, pos, out, n, max_components, err, small);
+        }
+        rcm_grid_sync(st, err, spin_limit);
+        if (rcm_block_err(err, small + 32) != 0) return;
+        // D: children placed at le + offset + rank of (degree, row)
+        for (int64_t k = lb + gw; k < le; k += nwarps)
+        {
+            const int32_t r = ldcg_i32(out + k);
+            const int32_t mark = -2 - static_cast<int32_t>(k);
+            const int32_t e0 = __ldg(indptr + r), e1 = __ldg(indptr + r + 1);
+            int count = 0;
+            for (int32_t eb = e0; eb < e1; eb += 32)
+            {
+                const int32_t e = eb + lane;
+                bool take = false;
+                int32_t c = 0;
+                if (e < e1)
+                {
+                    c = __ldg(indices + e);
+                    take = ldcg_i32(claim + c) == mark && atomicCAS(claim + c, mark, INT_MIN) == mark;
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, take);
+                if (take)
+                {
+                    const int slot = count + __popc(bal & ((1u << lane) - 1u));
+                    if (slot < cap)
+                        buf[slot] = (static_cast<uint64_t>(__ldg(degree + c)) << 32) |
+                                    static_cast<uint32_t>(c);
+                }
+                count += __popc(bal);
+            }
+            __syncwarp();
+            if (count > cap)
+            {
+                if (lane == 0) atomicOr(err, 128);
+                continue;
+            }
+            const int64_t base = le + ldcg_i32(counts + (k - lb));
+            for (int i = lane; i < count; i += 32)
+            {
+                const uint64_t key = buf[i];
+                int rank = 0;
+                for (int j = 0; j < count; ++j) rank += buf[j] < key ? 1 : 0;
+                const int32_t c = static_cast<int32_t>(key & 0xffffffffu);
+                out[base + rank] = c;
+                pos[c] = static_cast<int32_t>(base + rank);
+            }
+            __syncwarp();
+        }
+        rcm_grid_sync(st, err, spin_limit);
+    }
+}
+
 __global__ void k_fill_f64(double* __restrict__ a, int64_t n, double v)
 {
     const int64_t i0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;

@@ -22,8 +22,8 @@
 // not-yet-placed rows of the base order, so that every group except the
 // last has exactly G rows and lines up with the device format's groups.
 // Groups keep the base order's sequence, so the SpMM's gather window stays
-// as local as the base order made it.  Large orders run two such sweeps
-// in parallel from the middle of the base order outwards (see aggregate).
+// as local as the base order made it.  Large orders run up to 8 such
+// sweeps in parallel over segments of the base order (see aggregate).
 
 #include <algorithm>
 #include <atomic>
@@ -32,6 +32,7 @@
 #include <cstring>
 #include <cstdint>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -321,26 +322,35 @@ struct Groups {
     std::vector<int64_t> seed_pos;
 };
 
-// One sweep over the seeds at base positions k0, k0 + step, ... (step +1 or
-// -1, stopping before `stop`); a row may join while state[row] == me (the
-// rows this sweep owns and has not placed yet; placing stores 0).  A
-// group's seed takes its `want` strongest joinable neighbours (selected by
-// strength_key), then theirs, and a group whose neighbourhood runs out is
-// filled with the next unplaced rows of the sweep.  The other sweep's rows
-// are read, never written, so `state` is relaxed atomics.
-template <typename VT>
+// Rows a sweep may place: state[row] == me (the rows this sweep owns and has
+// not placed yet; placing stores 0).  Other sweeps' rows are read, never
+// written, so `state` is relaxed atomics.
+struct SweepOwner {
+    std::atomic<uint8_t>* state;
+    uint8_t me;
+    bool mine(int32_t r) const { return state[r].load(std::memory_order_relaxed) == me; }
+    void take(int32_t r) const { state[r].store(0, std::memory_order_relaxed); }
+};
+
+// One forward sweep over the seeds at base positions k0 .. seed_stop - 1
+// (positions of `base`, NULL = identity) over the rows `own` lets it place.
+// A group's seed takes its `want` strongest placeable neighbours (selected
+// by strength_key), then theirs, and a group whose neighbourhood runs out is
+// filled with the next placeable rows of base positions k0 .. stop - 1.
+template <typename VT, typename Owner>
 void aggregate_sweep(const int32_t* indptr, const int32_t* indices, const VT* data, int G,
-                     const int32_t* base, int64_t k0, int64_t stop, int step, uint8_t me,
-                     std::atomic<uint8_t>* state, Groups& out)
+                     const int32_t* base, int64_t k0, int64_t seed_stop, int64_t stop,
+                     const Owner& own, Groups& out)
 {
+    const int step = 1;
     auto row_at = [&](int64_t k) { return base ? base[k] : static_cast<int32_t>(k); };
-    auto mine = [&](int32_t r) { return state[r].load(std::memory_order_relaxed) == me; };
-    auto take = [&](int32_t r) { state[r].store(0, std::memory_order_relaxed); };
+    auto mine = [&](int32_t r) { return own.mine(r); };
+    auto take = [&](int32_t r) { own.take(r); };
     std::vector<int32_t> group, frontier, next;
     std::vector<uint64_t> keys;
     group.reserve(G);
     int64_t fill_cursor = k0;  // next sweep position for the fallback
-    for (int64_t k = k0; k != stop; k += step)
+    for (int64_t k = k0; k < seed_stop; k += step)
     {
         const int32_t seed = row_at(k);
         if (!mine(seed)) continue;
@@ -398,45 +408,41 @@ void aggregate_sweep(const int32_t* indptr, const int32_t* indices, const VT* da
     }
 }
 
-// Orders of at least 2 x 16384 rows run two sweeps on two threads, both
-// starting at the middle of the base order and moving apart (the first half
-// backwards, the second forwards), so that neither front runs into rows the
-// other has placed; smaller ones one forward sweep.  Groups are then listed
-// by their seeds' base positions, the short groups at the two ends merged
-// and put last.
+// Orders of at least 2 x 16384 rows are cut into K = min(8, n / 16384)
+// segments of the base order; sweep s owns the rows whose base positions
+// lie in segment s and runs forward through it (a row joins only the sweep
+// that owns it), so the K sweeps are independent and run on the pool's
+// threads in any assignment: the result does not depend on the number of
+// threads.  Groups are listed by their seeds' base positions, the short
+// groups at the segments' ends merged and put last.
 template <typename VT>
 void aggregate(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices, const VT* data,
                int G, const int32_t* base, const int32_t* base_pos, int32_t* order)
 {
-    // state[r]: the sweep that owns unplaced row r (1 or 2), 0 once placed
+    // state[r]: the sweep that owns unplaced row r (1 .. K), 0 once placed
     std::vector<std::atomic<uint8_t>> state(static_cast<size_t>(n));
-    Groups sweep[2];
-    if (n >= 2 * 16384 && P.size() >= 2)
-    {
-        const int64_t mid = n / 2;
-        P.run([&](int t, int nt) {
-            int64_t b, e;
-            part_range(n, t, nt, b, e);
-            for (int64_t r = b; r < e; ++r)
-            {
-                const int64_t p = base_pos ? base_pos[r] : r;
-                state[r].store(p < mid ? 1 : 2, std::memory_order_relaxed);
-            }
-        });
-        P.run([&](int t, int) {
-            if (t == 0)
-                aggregate_sweep<VT>(indptr, indices, data, G, base, mid - 1, -1, -1, 1,
-                                    state.data(), sweep[0]);
-            else if (t == 1)
-                aggregate_sweep<VT>(indptr, indices, data, G, base, mid, n, 1, 2, state.data(),
-                                    sweep[1]);
-        });
-    }
-    else
-    {
-        for (int64_t r = 0; r < n; ++r) state[r].store(2, std::memory_order_relaxed);
-        aggregate_sweep<VT>(indptr, indices, data, G, base, 0, n, 1, 2, state.data(), sweep[1]);
-    }
+    const int K = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(8, n / 16384)));
+    const int64_t seg = (n + K - 1) / K;
+    std::vector<Groups> sweep(static_cast<size_t>(K));
+    P.run([&](int t, int nt) {
+        int64_t b, e;
+        part_range(n, t, nt, b, e);
+        for (int64_t r = b; r < e; ++r)
+        {
+            const int64_t p = base_pos ? base_pos[r] : r;
+            state[r].store(static_cast<uint8_t>(1 + p / seg), std::memory_order_relaxed);
+        }
+    });
+    P.run([&](int t, int nt) {
+        for (int s = t; s < K; s += nt)
+        {
+            const int64_t k0 = std::min<int64_t>(n, s * seg);
+            const int64_t k1 = std::min<int64_t>(n, k0 + seg);
+            aggregate_sweep<VT>(indptr, indices, data, G, base, k0, k1, k1,
+                                SweepOwner{state.data(), static_cast<uint8_t>(s + 1)},
+                                sweep[s]);
+        }
+    });
     struct Ref {
         int64_t seed_pos;
         int s;
@@ -444,7 +450,7 @@ void aggregate(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices
     };
     std::vector<Ref> refs;
     std::vector<int32_t> tail;  // rows of the short groups
-    for (int s = 0; s < 2; ++s)
+    for (int s = 0; s < static_cast<int>(sweep.size()); ++s)
     {
         const int64_t ng = static_cast<int64_t>(sweep[s].seed_pos.size());
         for (int64_t i = 0; i < ng; ++i)
@@ -463,6 +469,65 @@ void aggregate(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices
     for (const Ref& rf : refs)
         for (int64_t i = rf.index * G; i < rf.index * G + G; ++i) order[out++] = sweep[rf.s].rows[i];
     for (int32_t r : tail) order[out++] = r;
+}
+
+// Rows of the block being split: the thread's own bit per matrix row (set
+// for the block's rows, cleared after) and, where the bit is set, the row's
+// index in the block (loc) and its placed flag.
+struct BlockOwner {
+    const uint64_t* member;
+    const int16_t* loc;
+    uint8_t* placed;
+    bool mine(int32_t r) const
+    {
+        return ((member[r >> 6] >> (r & 63)) & 1) && !placed[loc[r]];
+    }
+    void take(int32_t r) const { placed[loc[r]] = 1; }
+};
+
+// Blocks of B rows by aggregate(), then every whole block split into groups
+// of G rows by the same sweep over its rows in base order, with the block's
+// rows as the placeable ones.  Blocks run in parallel, each thread with its
+// own membership bits and index table.
+template <typename VT>
+void block_groups(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices,
+                  const VT* data, int B, int G, const int32_t* base, const int32_t* base_pos,
+                  int32_t* order)
+{
+    aggregate<VT>(P, n, indptr, indices, data, B, base, base_pos, order);
+    const int64_t nb = n / B;  // whole blocks; the rest stay last as they are
+    P.run([&](int t, int nt) {
+        int64_t b0, b1;
+        part_range(nb, t, nt, b0, b1);
+        if (b0 >= b1) return;
+        std::vector<int32_t> rows(static_cast<size_t>(B));
+        std::vector<uint64_t> member(static_cast<size_t>((n + 63) / 64), 0);
+        std::unique_ptr<int16_t[]> loc(new int16_t[static_cast<size_t>(n)]);
+        std::vector<uint8_t> placed(static_cast<size_t>(B));
+        Groups g;
+        for (int64_t b = b0; b < b1; ++b)
+        {
+            int32_t* blk = order + b * B;
+            std::copy(blk, blk + B, rows.begin());
+            if (base_pos)
+                std::sort(rows.begin(), rows.end(),
+                          [&](int32_t x, int32_t y) { return base_pos[x] < base_pos[y]; });
+            else
+                std::sort(rows.begin(), rows.end());
+            for (int i = 0; i < B; ++i)
+            {
+                member[rows[i] >> 6] |= uint64_t(1) << (rows[i] & 63);
+                loc[rows[i]] = static_cast<int16_t>(i);
+            }
+            std::fill(placed.begin(), placed.end(), 0);
+            g.rows.clear();
+            g.seed_pos.clear();
+            aggregate_sweep<VT>(indptr, indices, data, G, rows.data(), 0, B, B,
+                                BlockOwner{member.data(), loc.get(), placed.data()}, g);
+            std::copy(g.rows.begin(), g.rows.end(), blk);
+            for (int i = 0; i < B; ++i) member[rows[i] >> 6] = 0;
+        }
+    });
 }
 
 }  // namespace
@@ -489,7 +554,7 @@ extern "C" slq_status slq_group_order(int64_t n, const int32_t* indptr, const in
                                       const void* data, int dtype, int group_rows,
                                       const int32_t* base_order, int32_t* order)
 {
-    if (n < 0 || !indptr || !indices || !order || group_rows < 1 || group_rows > 32)
+    if (n < 0 || !indptr || !indices || !order || group_rows < 1 || group_rows > 1024)
     {
         slq::set_error("group_order: bad arguments");
         return SLQ_ERR_BAD_ARG;
@@ -510,6 +575,36 @@ extern "C" slq_status slq_group_order(int64_t n, const int32_t* indptr, const in
     else
         aggregate<float>(P, n, indptr, indices, static_cast<const float*>(data), group_rows,
                          base_order, bp, order);
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_block_group_order(int64_t n, const int32_t* indptr,
+                                            const int32_t* indices, const void* data, int dtype,
+                                            int block_rows, int group_rows,
+                                            const int32_t* base_order, int32_t* order)
+{
+    if (n < 0 || !indptr || !indices || !order || group_rows < 1 || group_rows > 1024 ||
+        block_rows < group_rows || block_rows > 16384 || block_rows % group_rows != 0)  // int16 loc
+    {
+        slq::set_error("block_group_order: bad arguments");
+        return SLQ_ERR_BAD_ARG;
+    }
+    std::lock_guard<std::mutex> lock(pool_mutex());
+    Pool& P = shared_pool();
+    if (!valid_pattern(P, n, indptr, indices, "block_group_order")) return SLQ_ERR_BAD_CSR;
+    std::vector<int32_t> base_pos;
+    if (base_order && !inverse_perm(n, base_order, base_pos))
+    {
+        slq::set_error("block_group_order: base_order is not a permutation");
+        return SLQ_ERR_BAD_ARG;
+    }
+    const int32_t* bp = base_order ? base_pos.data() : nullptr;
+    if (dtype == SLQ_F64)
+        block_groups<double>(P, n, indptr, indices, static_cast<const double*>(data), block_rows,
+                             group_rows, base_order, bp, order);
+    else
+        block_groups<float>(P, n, indptr, indices, static_cast<const float*>(data), block_rows,
+                            group_rows, base_order, bp, order);
     return SLQ_OK;
 }
 

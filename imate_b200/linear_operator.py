@@ -31,6 +31,66 @@ def _dtype_code(dtype):
                     'GPU; got "%s".' % dtype)
 
 
+class _Stager:
+    """Host-to-device copies through a small ring of page-locked buffers
+    (4 x 16 MB, allocated on first use and kept for the process): chunk i+1
+    is copied into its buffer on the host while chunk i crosses the link, so
+    a large array moves at close to the page-locked rate without pinning a
+    buffer of its own size.  One copy at a time (a lock); every copy is
+    ordered on the device's current stream."""
+
+    CHUNK = 16 << 20
+    SLOTS = 4
+
+    def __init__(self):
+        import threading
+        self.lock = threading.Lock()
+        self.bufs = None
+        self.events = [None] * self.SLOTS
+        self.next = 0
+
+    def upload(self, a, dev):
+        import torch
+        with self.lock:
+            if self.bufs is None:
+                self.bufs = [torch.empty(self.CHUNK, dtype=torch.uint8,
+                                         pin_memory=True)
+                             for _ in range(self.SLOTS)]
+            src = torch.from_numpy(a.reshape(-1).view(np.uint8))
+            out = torch.empty(a.nbytes, dtype=torch.uint8, device=dev)
+            stream = torch.cuda.current_stream(dev)
+            for off in range(0, a.nbytes, self.CHUNK):
+                slot = self.next % self.SLOTS
+                self.next += 1
+                if self.events[slot] is not None:
+                    self.events[slot].synchronize()  # its last copy is done
+                m = min(self.CHUNK, a.nbytes - off)
+                buf = self.bufs[slot][:m]
+                buf.copy_(src[off:off + m])
+                out[off:off + m].copy_(buf, non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+                self.events[slot] = ev
+            return out.view(torch.from_numpy(np.empty(0, a.dtype)).dtype) \
+                .reshape(a.shape)
+
+
+_STAGER = _Stager()
+# arrays of at least this many bytes go through the staging ring
+_STAGE_MIN_BYTES = 4 << 20
+
+
+def to_device(arr, dev, dtype=None):
+    """A host array as a tensor on CUDA device ``dev``: small arrays by a
+    plain copy, large ones through the page-locked staging ring (about five
+    times the pageable rate on a PCIe 5 host link)."""
+    import torch
+    a = np.ascontiguousarray(arr, dtype=dtype)
+    if a.nbytes < _STAGE_MIN_BYTES:
+        return torch.from_numpy(a).to(dev)
+    return _STAGER.upload(a, dev)
+
+
 def _pattern(A):
     """int32 indptr / indices of a CSR matrix, as the host orders take them."""
     return (np.ascontiguousarray(A.indptr, dtype=np.int32),
@@ -72,7 +132,7 @@ def locality_order(A, reorder="auto", device_pattern=None):
     if reorder == "auto":
         if n < 16384 or A.nnz == 0:
             return None
-        spread = order_spread(A)
+        spread = order_spread(A, sample_rows=4096)
         if spread <= 256.0:
             return None
     perm = None
@@ -81,7 +141,8 @@ def locality_order(A, reorder="auto", device_pattern=None):
                                 A.nnz)
     if perm is None:
         perm = rcm_order(A)
-    if reorder == "auto" and order_spread(A, perm) * 4.0 > spread:
+    if reorder == "auto" and \
+            order_spread(A, perm, sample_rows=4096) * 4.0 > spread:
         return None
     return np.ascontiguousarray(perm, dtype=np.int32)
 
@@ -178,6 +239,49 @@ def block_order(A, group_order, group_rows=16, groups_per_block=8):
     return order
 
 
+def block_group_order(A, base_perm, block_rows=128, group_rows=16):
+    """Row order of blocks of ``block_rows`` rows, each of whole groups of
+    ``group_rows`` rows, both aggregated around seeds and their strongest
+    neighbours (``slq_block_group_order``; groups follow ``base_perm``).
+    Serves the tensor-core block format and the row-group format at once.
+    Square matrices only."""
+    A = sp.csr_matrix(A)
+    n = A.shape[0]
+    ip, ind = _pattern(A)
+    data = A.data
+    if data.dtype not in (np.float32, np.float64):
+        data = data.astype(np.float64)
+    data = np.ascontiguousarray(data)
+    dt = _lib.SLQ_F64 if data.dtype == np.float64 else _lib.SLQ_F32
+    base = None if base_perm is None else \
+        np.ascontiguousarray(base_perm, dtype=np.int32)
+    order = np.empty(n, dtype=np.int32)
+    _lib.check(_lib.load().slq_block_group_order(
+        n, ip.ctypes.data, ind.ctypes.data, data.ctypes.data, dt,
+        int(block_rows), int(group_rows),
+        None if base is None else base.ctypes.data, order.ctypes.data))
+    return order
+
+
+# blocks='auto' adds the tensor-core block format to float32 square
+# matrices of at least this order
+BLOCKS_AUTO_MIN_ROWS = 65536
+
+
+def blocks_wanted(blocks, A):
+    """Whether an operator over host matrix A gets the block format:
+    ``blocks`` True (float32 only), False, or 'auto' -- float32 square
+    matrices of order at least BLOCKS_AUTO_MIN_ROWS with at least 8 entries
+    per row, where the tensor-core products beat the row-group kernels."""
+    if blocks == "auto":
+        return bool(A.dtype == np.float32 and A.shape[0] == A.shape[1] and
+                    A.shape[0] >= BLOCKS_AUTO_MIN_ROWS and
+                    A.nnz >= 8 * A.shape[0])
+    if blocks not in (True, False):
+        raise ValueError("blocks must be True, False or 'auto'")
+    return bool(blocks) and A.dtype == np.float32
+
+
 def group_rows_for(A, perm, group_rows="auto", sample=256, aggregate=True):
     """Row-group width for the device format (0 = CSR only) and the row
     order to store the matrix in: (G, perm).
@@ -256,10 +360,8 @@ class _DeviceOperator:
             # first, so that the locality order is computed there, and the
             # values on a helper thread while the host aggregates (both
             # release the GIL)
-            self.indices = torch.from_numpy(
-                np.ascontiguousarray(A.indices, dtype=np.int32)).to(dev)
-            self.indptr = torch.from_numpy(
-                np.ascontiguousarray(A.indptr, dtype=np.int32)).to(dev)
+            self.indices = to_device(A.indices, dev, np.int32)
+            self.indptr = to_device(A.indptr, dev, np.int32)
             pattern = (self.indptr, self.indices)
             if A.dtype in (np.float32, np.float64):
                 import threading
@@ -267,23 +369,33 @@ class _DeviceOperator:
 
                 def _values():
                     try:
-                        box["data"] = torch.from_numpy(
-                            np.ascontiguousarray(A.data)).to(dev)
+                        box["data"] = to_device(A.data, dev)
                     except BaseException as exc:  # re-raised on join
                         box["error"] = exc
                 upload = (threading.Thread(target=_values, daemon=True), box)
                 upload[0].start()
         try:
             base = locality_order(A, reorder, device_pattern=pattern)
-            self.group_rows, perm = group_rows_for(A, base, group_rows,
-                                                   aggregate=aggregate)
-            blocks = blocks and A.dtype == np.float32
-            if blocks and self.group_rows == 16 and perm is not None and \
-                    A.shape[0] == A.shape[1]:
-                # 128-row blocks of eight aggregated 16-row groups whose
-                # column sets overlap (the groups stay whole, so the
-                # row-group format keeps its fill)
-                perm = block_order(A, perm, 16, 8)
+            blocks = blocks_wanted(blocks, A)
+            self.group_rows = None
+            if blocks and aggregate and group_rows in ("auto", 16) and \
+                    A.shape[0] == A.shape[1] and A.shape[0] >= 256 and \
+                    A.nnz >= 8 * A.shape[0]:
+                # 128-row blocks aggregated around seeds, each split into
+                # eight aggregated 16-row groups: one order for the block
+                # format and the row-group format
+                cand = block_group_order(A, base, 128, 16)
+                if group_rows == 16 or _group_fill(A, cand, 16) >= 0.5:
+                    self.group_rows, perm = 16, cand
+            if self.group_rows is None:
+                self.group_rows, perm = group_rows_for(A, base, group_rows,
+                                                       aggregate=aggregate)
+                if blocks and self.group_rows == 16 and perm is not None \
+                        and A.shape[0] == A.shape[1]:
+                    # 128-row blocks of eight 16-row groups whose column
+                    # sets overlap (the groups stay whole, so the row-group
+                    # format keeps its fill)
+                    perm = block_order(A, perm, 16, 8)
         finally:
             if upload is not None:
                 upload[0].join()
@@ -309,12 +421,10 @@ class _DeviceOperator:
         if upload is not None and "data" in upload[1] and A.format == "csr":
             self.data = upload[1]["data"]
         else:
-            self.data = torch.from_numpy(np.ascontiguousarray(A.data)).to(dev)
+            self.data = to_device(A.data, dev)
         if not early:
-            self.indices = torch.from_numpy(
-                np.ascontiguousarray(A.indices, dtype=np.int32)).to(dev)
-            self.indptr = torch.from_numpy(
-                np.ascontiguousarray(A.indptr, dtype=np.int32)).to(dev)
+            self.indices = to_device(A.indices, dev, np.int32)
+            self.indptr = to_device(A.indptr, dev, np.int32)
         self.perm = None
         self.inv = None
         if perm is not None:
@@ -396,7 +506,7 @@ class _DeviceOperator:
         import torch
         self = cls(None, affine, need_transpose)
         A = np.ascontiguousarray(A, dtype=np.float32)
-        self.data = torch.from_numpy(A).to(self.device)
+        self.data = to_device(A, self.device)
         self.indices = None
         self.indptr = None
         self.dtype_code, self.np_dtype = _lib.SLQ_F32, np.dtype(np.float32)
@@ -566,14 +676,17 @@ class Matrix(LinearOperator):
     or 16) adds the row-group format and ``aggregate`` lets its groups be
     formed by neighbour aggregation (see ``group_rows_for``); the format
     itself changes no result bit, the aggregated order only the order of
-    floating-point sums.  ``blocks`` (float32) stores the rows in 128-row
-    blocks of overlapping column sets (``block_order``) and adds the
-    tensor-core block format, which block-wide SpMMs then use; results
-    change only by rounding (TF32 parts, three terms).
+    floating-point sums.  ``blocks`` (float32; 'auto', True or False) stores
+    the rows in 128-row blocks of aggregated 16-row groups
+    (``block_group_order``) and adds the tensor-core block format, which
+    block-wide SpMMs (128 or 256 probes) then use; results change only by
+    rounding (FP16 hi/lo parts of scaled values, FP32 accumulation: samples
+    within about 1e-5 of FP64).  'auto' adds it to float32 square matrices
+    of order at least 65536 (``blocks_wanted``).
     """
 
     def __init__(self, A, reorder="auto", group_rows="auto", aggregate=True,
-                 blocks=False):
+                 blocks="auto"):
         super().__init__()
         self.reorder = reorder
         self.group_rows = group_rows

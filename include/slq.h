@@ -115,18 +115,22 @@ slq_status slq_operator_create(const void* data, const int32_t* indices,
  * cuCSRMatrix::dot, imate/_cu_linear_operator/cu_csr_matrix.cu:278-318).
  * The stored rows of A (transpose = 0) or of A^T (transpose = 1) are cut
  * into blocks of 128 consecutive rows; each block keeps the sorted union of
- * its column indices and its values as a dense 128 x union matrix (TF32
- * parts are taken in the product), so that one SpMM over b = 128 or 256
- * probes runs on the tensor cores (tcgen05 kind::tf32, three terms: about
- * FP32 accuracy).  Its cost follows the union sizes: store the operator with
- * a row order whose consecutive 128-row blocks share columns
- * (slq_block_order).  Built on the device in two calls that use the same
- * scratch: slq_operator_blocks_bytes sizes the format (it synchronizes the
- * stream), slq_operator_add_blocks builds it into `format` (caller memory
- * that must outlive the operator) and attaches it; the scratch can be
- * released after it returns.  Duplicate (row, column) entries are summed.
- * Products at b = 128 / 256 then use it (slq_run, batch plans, the tuner)
- * unless the tuner picked another candidate. */
+ * its column indices (padded to a multiple of 16) and its values as a dense
+ * 128 x union matrix.  Every row is scaled by a power of two and split into
+ * FP16 high and low parts, so one SpMM over b = 128 or 256 probes runs on
+ * the tensor cores (tcgen05 kind::f16, three products hi*hi, hi*lo, lo*hi
+ * of the scaled operands, FP32 accumulation: samples within about 1e-5 of
+ * FP64).  Its cost follows the union sizes: store the operator with a row
+ * order whose consecutive 128-row blocks share columns
+ * (slq_block_group_order, slq_block_order).  Built on the device in two
+ * calls on the same scratch: slq_operator_blocks_bytes prepares the scratch
+ * (sorted keys, unions) and sizes the format (it synchronizes the stream);
+ * slq_operator_add_blocks, given that scratch as it was left, builds the
+ * format into `format` (caller memory that must outlive the operator) and
+ * attaches it (given another scratch it prepares that one first); the
+ * scratch can be released after it returns.  Duplicate (row, column)
+ * entries are summed.  Products at b = 128 / 256 then use it (slq_run,
+ * batch plans, the tuner) unless the tuner picked another candidate. */
 slq_status slq_operator_blocks_scratch_bytes(const slq_op* op, int transpose,
                                              size_t* bytes);
 slq_status slq_operator_blocks_bytes(const slq_op* op, int transpose,
@@ -152,11 +156,11 @@ slq_status slq_rcm_order(int64_t n, const int32_t* indptr,
  * seed of a group of group_rows rows: the seed, its not-yet-placed
  * neighbours by decreasing |a_ij|, their neighbours, and, when the
  * neighbourhood runs out, the next unplaced rows of the base order.  Orders
- * of at least 32768 rows run two sweeps on two host threads, both from the
- * middle of the base order outwards (the first half backwards, the second
- * forwards), each group from one half's rows; groups are then listed by
- * their seeds' base positions, the short groups at the two ends last.  The
- * order depends on n and the inputs only, not on the thread count.
+ * of at least 32768 rows are cut into K = min(8, n / 16384) segments of the
+ * base order swept independently on the host threads, each group from one
+ * segment's rows; groups are then listed by their seeds' base positions,
+ * the short groups at the segments' ends last.  The order depends on n and
+ * the inputs only, not on the thread count.
  * order[k] receives the row at position k; every group but the short ones
  * has exactly group_rows rows, so passing order as slq_operator_create's perm
  * lines the groups up with the row-group format's, whose cost falls with
@@ -185,18 +189,38 @@ slq_status slq_block_order(int64_t n, const int32_t* indptr,
                            int group_rows, int groups_per_block,
                            int32_t* order);
 
+/* Blocks, then groups inside them (host; no counterpart in the reference):
+ * the rows aggregated as slq_group_order does but into blocks of block_rows
+ * rows (a seed and its strongest neighbours, theirs, ...), then the rows of
+ * every whole block, in base order, aggregated the same way into groups of
+ * group_rows rows drawn from that block only.  order[k] receives the row at
+ * position k: every whole block of the tensor-core block format holds whole
+ * row groups, so one order serves both formats.  On the benchmark
+ * correlation matrix (n = 262144, RCM base order) 128-row blocks of 16-row
+ * groups have about 2 % smaller column unions than slq_block_order's blocks
+ * of slq_group_order's groups, with 16-row groups about 3 % larger, at a
+ * fraction of the cost (no group graph).  block_rows must be a multiple of
+ * group_rows, at most 16384.  The order does not depend on the thread
+ * count. */
+slq_status slq_block_group_order(int64_t n, const int32_t* indptr,
+                                 const int32_t* indices, const void* data,
+                                 int dtype, int block_rows, int group_rows,
+                                 const int32_t* base_order, int32_t* order);
+
 /* Workspace for slq_rcm_order_device (device bytes). */
 slq_status slq_rcm_order_device_workspace_bytes(int64_t n, size_t* bytes);
 
 /* slq_rcm_order on the device: the same order for a square CSR pattern of n
  * rows and nnz entries in device memory (int32 indptr / indices, validated
- * first), computed one breadth-first level at a time (one host
- * synchronisation per level and per component); order (device, n entries)
- * receives it.  *done = 1 on success; *done = 0, with SLQ_OK and order
- * undefined, when the pattern has more than max_components connected
- * components or its sort keys (level offset, degree, row) need more than 64
- * bits -- the caller then uses slq_rcm_order.  No counterpart in the
- * reference. */
+ * first); order (device, n entries) receives it.  When no row has more than
+ * 1024 entries every breadth-first level runs inside one cooperative launch
+ * (grid barriers between a level's phases, each wait bounded: a wait that
+ * runs out returns SLQ_ERR_TIMEOUT); otherwise one level per host round (a
+ * synchronisation per level and per component).  *done = 1 on success;
+ * *done = 0, with SLQ_OK and order undefined, when the pattern has more than
+ * max_components connected components or, on the round-per-level path, its
+ * sort keys (level offset, degree, row) need more than 64 bits -- the caller
+ * then uses slq_rcm_order.  No counterpart in the reference. */
 slq_status slq_rcm_order_device(int64_t n, int64_t nnz, const int32_t* indptr,
                                 const int32_t* indices, int max_components,
                                 int32_t* order, int* done, void* workspace,

@@ -3,10 +3,12 @@ sparse SPD correlation matrix with n = 262144 (48.07M nonzeros, diagonal
 shift 0.1), FP32 values, 256 probes from the parity stream, 50 Lanczos steps,
 full reorthogonalisation.
 
-Both device formats run: the default (locality order, aggregated 16-row
-groups, TMA row-group SpMM) and the tensor-core block format (128-row
-blocks, FP16 three-product SpMM).  Bars, on identical probes:
-- default path against the FP64 engine: 1e-6 relative per sample (FP32
+Both device formats run: the row-group path (locality order, aggregated
+16-row groups, TMA row-group SpMM; Matrix(blocks=False)) and the default for
+a float32 matrix of this order, the tensor-core block format (128-row
+blocks of aggregated 16-row groups, FP16 three-product SpMM).  Bars, on
+identical probes:
+- row-group path against the FP64 engine: 1e-6 relative per sample (FP32
   products, FP64 reductions);
 - block path against the FP64 engine: 1e-5 relative per sample (FP16 hi/lo
   products and the tensor core's FP32 accumulation, which shrinks |y| by a
@@ -54,7 +56,7 @@ def test_headline_workload_matches_fp64_and_sparse_lu(cuda, headline_matrix):
     s64 = np.asarray(i64["convergence"]["samples"][:8], float)
     torch.cuda.empty_cache()
 
-    Mr = ib.Matrix(A)
+    Mr = ib.Matrix(A, blocks=False)
     tr_r, ir = _logdet(Mr, 256, 256)
     assert Mr.get_device_operator().group_rows == 16
     assert not Mr.get_device_operator().block_formats
@@ -62,9 +64,11 @@ def test_headline_workload_matches_fp64_and_sparse_lu(cuda, headline_matrix):
     del Mr
     torch.cuda.empty_cache()
 
-    Mb = ib.Matrix(A, blocks=True)
+    Mb = ib.Matrix(A)  # blocks='auto'
     tr_b, ibk = _logdet(Mb, 256, 256)
     assert Mb.get_device_operator().block_formats
+    assert Mb.get_device_operator().group_rows == 16
+    assert "blocks" in ibk["precision"]["spmm"]
     sb = np.asarray(ibk["convergence"]["samples"], float)
     del Mb
     torch.cuda.empty_cache()
