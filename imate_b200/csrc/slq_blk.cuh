@@ -42,9 +42,14 @@
 //   warps 10-17   converters: load the stage's 16 X rows from global memory
 //                 (two stages ahead, into registers), scale and split them
 //                 into FP16 parts and store both in the MN-major 128-byte
-//                 swizzled layout (atoms of 8 K rows x 64 probes).  TMA
-//                 gathers of X rows (one 128-byte box row per gathered row
-//                 segment under the swizzle) measured slower than these loads;
+//                 swizzled layout (atoms of 8 K rows x 64 probes);
+//                 with X already split (PRE: the probe block scaled and split
+//                 into X16[row] = hi[b] | lo[b] by k_x16_split, once per
+//                 Lanczos step) the same warps only copy the rows' 16-byte
+//                 chunks into that layout (no arithmetic, half the stores).
+//                 TMA gathers of the rows (tile::gather4, four 128-byte box
+//                 rows each under the 128-byte swizzle) measured two times
+//                 slower than these loads;
 //   warp 9        MMA issuer: per stage (K = 16) the three products into an
 //                 FP32 accumulator in tensor memory (lane = block row,
 //                 column = probe), two accumulators so the epilogue of one
@@ -310,6 +315,7 @@ struct BlkArgs {
     const int32_t* ucol;
     const float* rsc;
     const __half* img;
+    const __half* x16;         // PRE: X split into FP16 parts, [K][2 NB] (hi | lo)
     const float* X;
     const double* sx;          // per-probe scale s_p of X (norm 1 / s_p), or NULL
     const unsigned int* xmax;  // sx == NULL: per-probe max |x| (float bits)
@@ -337,6 +343,44 @@ __device__ __forceinline__ void split_h4(float4 v, uint2& hi, uint2& lo)
                     *reinterpret_cast<const uint32_t*>(&h23));
     lo = make_uint2(*reinterpret_cast<const uint32_t*>(&l01),
                     *reinterpret_cast<const uint32_t*>(&l23));
+}
+
+// The power-of-two exponent e_p that scales probe p of X into FP16 range:
+// with the probe's scale s_p (|x|_2 = 1 / s_p) every scaled |x| is at most
+// 2^14; without a usable scale, 0.
+__device__ __forceinline__ int blk_x_exp(double sxv)
+{
+    return (sxv > 0.0 && isfinite(sxv)) ? min(max(ilogb(sxv) + 13, -120), 120) : 0;
+}
+
+// X16[r][p] = hi, X16[r][b + p] = lo of 2^e_p X[r][p] (the FP16 parts the
+// block SpMM multiplies), for rows x b probes, b a multiple of 8; thread =
+// 8 probes of one row (two float4 in, one 16-byte store per part).
+__global__ void k_x16_split(const float* __restrict__ X, const double* __restrict__ sx,
+                            int64_t rows, int b, __half* __restrict__ X16)
+{
+    __shared__ float scale[1024];
+    for (int p = threadIdx.x; p < b; p += blockDim.x) scale[p] = ldexpf(1.0f, blk_x_exp(sx[p]));
+    __syncthreads();
+    const int per_row = b >> 3;
+    const int64_t total = rows * per_row;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        const int64_t r = i / per_row;
+        const int p = static_cast<int>(i - r * per_row) * 8;
+        const float4* src = reinterpret_cast<const float4*>(X + r * b + p);
+        float4 a = __ldcs(src), c = __ldcs(src + 1);
+        a = make_float4(a.x * scale[p], a.y * scale[p + 1], a.z * scale[p + 2], a.w * scale[p + 3]);
+        c = make_float4(c.x * scale[p + 4], c.y * scale[p + 5], c.z * scale[p + 6],
+                        c.w * scale[p + 7]);
+        uint2 ha, la, hc, lc;
+        split_h4(a, ha, la);
+        split_h4(c, hc, lc);
+        __half* dst = X16 + r * 2 * b + p;
+        *reinterpret_cast<uint4*>(dst) = make_uint4(ha.x, ha.y, hc.x, hc.y);
+        *reinterpret_cast<uint4*>(dst + b) = make_uint4(la.x, la.y, lc.x, lc.y);
+    }
 }
 
 // Reduce-scatter of 16 per-lane values over the warp's 32 lanes: on return
@@ -411,10 +455,11 @@ __host__ __device__ constexpr uint32_t blk_idesc(uint32_t nb)
     return (1u << 4) | (1u << 16) | ((nb >> 3) << 17) | ((128u >> 4) << 24);
 }
 
-template <int NB>
+template <int NB, bool PRE>
 __global__ void __launch_bounds__(BLK_THREADS, 1)
 k_spmm_blk(const BlkArgs d)
 {
+    constexpr int NT = BLK_THREADS;
     extern __shared__ __align__(1024) unsigned char smem_blk[];
     const uint32_t stage_bytes = blk_stage_bytes(NB);
     const uint32_t x_bytes = blk_x_part(NB);
@@ -459,16 +504,17 @@ k_spmm_blk(const BlkArgs d)
         abort_flag[1] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = tid; i < 4 * 256; i += BLK_THREADS) red[i] = 0.0;
-    for (int p = tid; p < NB; p += BLK_THREADS)
+    for (int i = tid; i < 4 * 256; i += NT) red[i] = 0.0;
+    for (int p = tid; p < NB; p += NT)
     {
         // 2^e_p keeps every scaled |x| <= 2^14: |x| <= |x|_2 = 1 / s_p, or
-        // the measured maximum when no scale is given
+        // the measured maximum when no scale is given (k_x16_split scales
+        // by the same 2^e_p)
         const double sxv = d.sx ? d.sx[p] : 1.0;
         int e = 0;
         if (d.sx)
         {
-            if (sxv > 0.0 && isfinite(sxv)) e = min(max(ilogb(sxv) + 13, -120), 120);
+            e = blk_x_exp(sxv);
         }
         else
         {
@@ -535,7 +581,89 @@ k_spmm_blk(const BlkArgs d)
         }
         __syncwarp();
     }
-    else if (warp >= BLK_CONV0)
+    else if (PRE && warp >= BLK_CONV0)
+    {
+        // copiers (X split beforehand): thread ct takes union row k = ct / 16
+        // of each stage and its 16-byte chunks c = ct % 16 + 16 j of the
+        // row's X16 entry (hi | lo: part c / (NB / 8), probes 8 g .. 8 g + 7,
+        // g = c % (NB / 8)) and copies them (cp.async, no registers) to MN
+        // atom g / 8, K atom k / 8, row k % 8, chunk (g % 8) XOR (k % 8) of
+        // the part's region -- the converters' layout.  A stage is announced
+        // (conv) once this thread's copies of it completed, BLK_CP_AHEAD
+        // stages later, so that many stages of gathers are in flight; the
+        // row indices load BLK_CP_AHEAD stages before they are needed.
+        constexpr int AH = 4;
+        const int ct = tid - BLK_CONV0 * 32;
+        const int k = ct >> 4;
+        constexpr int nj = NB / 64;          // chunks per thread (4 or 2)
+        constexpr int gpp = NB / 8;          // 16-byte chunks per part
+        uint32_t dst[nj];
+#pragma unroll
+        for (int j = 0; j < nj; ++j)
+        {
+            const int c = (ct & 15) + 16 * j;
+            const int part = c / gpp, g = c % gpp;
+            dst[j] = static_cast<uint32_t>(part) * x_bytes + (g >> 3) * 2048 + (k >> 3) * 1024 +
+                     (k & 7) * 128 + (((g & 7) ^ (k & 7)) << 4);
+        }
+        BlkCursor ix;
+        ix.start(d.bstage, d.nblk);
+        int ring[AH];
+#pragma unroll
+        for (int i = 0; i < AH; ++i)
+        {
+            ring[i] = ix.row(d.ucol, d.nblk, k);
+            ix.advance(d.bstage, d.nblk);
+        }
+        auto announce = [&](int64_t done) {
+            // this thread's copies of stage `done` have landed
+            tc::fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&conv[done % BLK_STAGES]);
+        };
+        int64_t it = 0;
+        bool ok = true;
+        for (int64_t blk = blockIdx.x; blk < d.nblk && ok; blk += gridDim.x)
+        {
+            const int s0 = d.bstage[blk], s1 = d.bstage[blk + 1];
+            for (int st = s0; st < s1; ++st, ++it)
+            {
+                const int s = static_cast<int>(it % BLK_STAGES);
+                const uint32_t ph = static_cast<uint32_t>((it / BLK_STAGES) & 1);
+                const int row = ring[0];
+#pragma unroll
+                for (int i = 0; i + 1 < AH; ++i) ring[i] = ring[i + 1];
+                ring[AH - 1] = ix.row(d.ucol, d.nblk, k);
+                ix.advance(d.bstage, d.nblk);
+                bool got = true;
+                if (lane == 0) got = mbar_wait(&empty[s], ph ^ 1u, abort_flag);
+                if (!__shfl_sync(FULL_MASK, got ? 1 : 0, 0))
+                {
+                    if (lane == 0) give_up();
+                    ok = false;
+                    break;
+                }
+                const uint32_t xs0 =
+                    smem_u32(base + static_cast<size_t>(s) * stage_bytes + 2 * BLK_A_PART);
+                const __half* src = d.x16 + int64_t(row) * 2 * NB + (ct & 15) * 8;
+#pragma unroll
+                for (int j = 0; j < nj; ++j)
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;"
+                                 ::"r"(xs0 + dst[j]), "l"(src + 128 * j) : "memory");
+                asm volatile("cp.async.commit_group;" ::: "memory");
+                if (it >= AH)
+                {
+                    asm volatile("cp.async.wait_group %0;" ::"n"(AH) : "memory");
+                    announce(it - AH);
+                }
+            }
+        }
+        // the rest: every copy lands (also after a failed wait)
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        if (ok)
+            for (int64_t done = std::max<int64_t>(0, it - AH); done < it; ++done) announce(done);
+    }
+    else if (!PRE && warp >= BLK_CONV0)
     {
         // converters.  Thread ct takes union row k = ct / 16 of each stage
         // and its float4 slices f = ct % 16 + 16 j (probes 4f .. 4f + 3, MN
@@ -775,7 +903,7 @@ k_spmm_blk(const BlkArgs d)
         tc::tmem_dealloc(tmem, tmem_cols);
     }
     if (d.epi != 0)
-        for (int q = tid; q < NB; q += BLK_THREADS)
+        for (int q = tid; q < NB; q += NT)
         {
             // the per-probe factor of the terms: s_p (alpha), 1 (|y|^2), zs_p
             const double f = d.epi == 1 ? (d.sx ? d.sx[q] : 1.0) : d.epi == 3 ? d.zs[q] : 1.0;

@@ -1088,10 +1088,15 @@ slq_status row_map(CUtensorMap* m, const float* base, int64_t rows, int b)
 }
 
 // The tensor map of one probe-block buffer for the row gathers of the TMA
-// and tensor-core row-group kernels (has_row = false: none).
+// and tensor-core row-group kernels (has_row = false: none), and, for the
+// block SpMM, a buffer that receives the probe block split into FP16 parts
+// (has_x16; x16_b probes per row).
 struct XMaps {
     CUtensorMap row;
     bool has_row = false;
+    __half* x16 = nullptr;
+    int x16_b = 0;
+    bool has_x16 = false;
 };
 
 slq_status make_xmaps(XMaps* m, const float* base, int64_t rows, int b, bool row)
@@ -1100,6 +1105,7 @@ slq_status make_xmaps(XMaps* m, const float* base, int64_t rows, int b, bool row
     m->has_row = row;
     return SLQ_OK;
 }
+
 
 // ---------------------------------------------------------------------------
 // dense FP32 operators (tensor-core product, k_dense_tc)
@@ -1363,8 +1369,13 @@ slq_status spmm_tc_inst(Launcher& L, const CUtensorMap* xmap, const int32_t* gpt
 // SM over the operator's 128-row blocks.
 slq_status spmm_blk_inst(Launcher& L, const slq_op* op, int transpose, int b, const float* X, const double* sx, double shift, float* Y,
                          const float* Z, const double* zc, const double* zs, int epi,
-                         double* partials, int32_t* error, int64_t xrows, int* grid_out)
+                         double* partials, int32_t* error, int64_t xrows, int* grid_out,
+                         const XMaps* maps)
 {
+    // X split into FP16 parts first (one streaming pass) when the caller
+    // gave a buffer for it and X has probe scales: the product then needs
+    // no converter warps
+    const bool pre = maps && maps->has_x16 && maps->x16 && maps->x16_b == b && sx;
     const int64_t rows = transpose ? op->ncols : op->nrows;
     const int64_t nblk = transpose ? op->t_nblk : op->a_nblk;
     // compulsory traffic as for the CSR kernels (the algorithm's bytes, not
@@ -1376,11 +1387,25 @@ slq_status spmm_blk_inst(Launcher& L, const slq_op* op, int transpose, int b, co
     static bool attr = false;
     if (!attr)
     {
-        SLQ_CK(cudaFuncSetAttribute(k_spmm_blk<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SLQ_CK(cudaFuncSetAttribute(k_spmm_blk<128, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(blk_smem_bytes(128))));
-        SLQ_CK(cudaFuncSetAttribute(k_spmm_blk<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SLQ_CK(cudaFuncSetAttribute(k_spmm_blk<256, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(blk_smem_bytes(256))));
+        SLQ_CK(cudaFuncSetAttribute(k_spmm_blk<128, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(blk_smem_bytes(128))));
+        SLQ_CK(cudaFuncSetAttribute(k_spmm_blk<256, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(blk_smem_bytes(256))));
         attr = true;
+    }
+    if (pre)
+    {
+        k_x16_split<<<L.sms * 4, 256, 0, L.st>>>(X, sx, xrows, b, maps->x16);
+        SLQ_LAUNCH_CK();
+        ++L.launches;
     }
     const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(nblk, L.sms)));
     // an X without probe scales: its per-probe maxima first (into the
@@ -1418,10 +1443,15 @@ slq_status spmm_blk_inst(Launcher& L, const slq_op* op, int transpose, int b, co
     d.epi = epi;
     d.partials = partials;
     d.error = error;
-    if (b == 256)
-        k_spmm_blk<256><<<grid, BLK_THREADS, smem, L.st>>>(d);
+    d.x16 = pre ? maps->x16 : nullptr;
+    if (pre && b == 256)
+        k_spmm_blk<256, true><<<grid, BLK_THREADS, smem, L.st>>>(d);
+    else if (pre)
+        k_spmm_blk<128, true><<<grid, BLK_THREADS, smem, L.st>>>(d);
+    else if (b == 256)
+        k_spmm_blk<256, false><<<grid, BLK_THREADS, smem, L.st>>>(d);
     else
-        k_spmm_blk<128><<<grid, BLK_THREADS, smem, L.st>>>(d);
+        k_spmm_blk<128, false><<<grid, BLK_THREADS, smem, L.st>>>(d);
     SLQ_LAUNCH_CK();
     ++L.launches;
     *grid_out = grid;
@@ -1485,7 +1515,7 @@ slq_status spmm_cand(Launcher& L, const slq_op* op, int transpose, const SpmmCan
         {
             if (!error) return fail(SLQ_ERR_BAD_ARG, "block SpMM needs an error word");
             return spmm_blk_inst(L, op, transpose, b, X, sx, shift, Y, Z, zc, zs, epi, partials,
-                                 error, xrows, grid_out);
+                                 error, xrows, grid_out, maps);
         }
         return fail(SLQ_ERR_BAD_ARG, "block SpMM is FP32 only");
     }
@@ -1713,6 +1743,7 @@ slq_status stream_pass(Launcher& L, int64_t n, int b, const VT* W, VT* Wout, int
 
 struct RunPlan {
     int gram, orth, m, bs, b, q;
+    bool x16;             // a buffer for the probe block split into FP16 parts
     int64_t nv, nu;       // probe length, U length (gram)
     int64_t wpp;          // parity words per probe
     int cw, nchunks;      // parity chunking
@@ -1725,6 +1756,7 @@ struct RunBufs {
     void* W;
     void* W2;
     void* T;              // normal-equations runs: A v, [nu][b]
+    __half* X16;          // the SpMM's probe block split into FP16 parts, [nv][2 b]
     double* negshift;     // normal-equations runs: -t per probe
     double* scale_v;
     double* scale_u;
@@ -1797,6 +1829,10 @@ slq_status make_plan(const slq_op* op, const slq_params* p, int q, RunPlan* r)
     b = std::min(next_pow2(b), bmax);
     b = std::min(b, next_pow2(p->max_num_samples));
     r->b = b;
+    // the block SpMM of A v (a float32 block format, b = 128 or 256) takes
+    // v split into FP16 parts beforehand
+    r->x16 = op->dtype == SLQ_F32 && !op->dense && op->a_nblk > 0 && r->gram != 1 &&
+             (b == 128 || b == 256);
     r->wpp = r->nv / 64 + 1;
     r->cw = 64;
     while ((r->wpp + r->cw - 1) / r->cw > 65535) r->cw *= 2;
@@ -1823,6 +1859,7 @@ void carve(Carver& c, const RunPlan& r, int sms, RunBufs* B)
     B->W = (r.gram == 1) ? nullptr : c.take<VT>(vslot);
     B->W2 = (r.gram != 1 && r.orth != 0) ? c.take<VT>(vslot) : nullptr;
     B->T = (r.gram == 2) ? c.take<VT>(static_cast<size_t>(r.nu) * r.b) : nullptr;
+    B->X16 = r.x16 ? c.take<__half>(static_cast<size_t>(r.nv) * 2 * r.b) : nullptr;
     B->negshift = c.take<double>(r.b);
     B->scale_v = c.take<double>(static_cast<size_t>(r.bs) * r.b);
     B->scale_u = c.take<double>(static_cast<size_t>(r.bs) * r.b);
@@ -1898,14 +1935,25 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
     {
         const bool wide = (b == 128 || b == 256);
         const bool row_a = wide && (op->group_rows == 8 || op->group_rows == 16);
-        if (row_a)
+        // the block SpMM's split probe block: one buffer, rewritten before
+        // every product of A v
+        const bool want_x16 = B.X16 != nullptr;
+        if (row_a || want_x16)
         {
             use_tma = true;
             vmaps.resize(bs);
             for (int sl = 0; sl < bs; ++sl)
+            {
                 SLQ_TRY(make_xmaps(&vmaps[sl], V + static_cast<int64_t>(sl) * vslot, r.nv, b,
-                                   true));
-            if (r.gram == 1)
+                                   row_a));
+                if (want_x16)
+                {
+                    vmaps[sl].x16 = B.X16;
+                    vmaps[sl].x16_b = b;
+                    vmaps[sl].has_x16 = true;
+                }
+            }
+            if (r.gram == 1 && row_a)
             {
                 umaps.resize(bs);
                 for (int sl = 0; sl < bs; ++sl)
