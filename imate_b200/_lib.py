@@ -42,7 +42,7 @@ EXPORTS = (
     "slq_batch_info", "slq_batch_destroy", "slq_group_order",
     "slq_rcm_order", "slq_tc_selftest", "slq_tc_selftest_mn",
     "slq_order_spread", "slq_group_fill", "slq_block_order",
-    "slq_block_group_order",
+    "slq_block_group_order", "slq_operator_blocks_info",
     "slq_rcm_order_device_workspace_bytes", "slq_rcm_order_device",
     "slq_dense_operator_workspace_bytes", "slq_dense_operator_create",
     "slq_operator_blocks_scratch_bytes", "slq_operator_blocks_bytes",
@@ -189,6 +189,8 @@ def _declare(lib):
         "slq_block_order": (i32, [i64, vp, vp, vp, i32, i32, vp]),
         "slq_block_group_order": (i32, [i64, vp, vp, vp, i32, i32, i32, vp,
                                         vp]),
+        "slq_operator_blocks_info": (i32, [vp, i32, ctypes.POINTER(i64),
+                                           ctypes.POINTER(i64)]),
         "slq_order_spread": (i32, [i64, vp, vp, vp, i64, vp]),
         "slq_group_fill": (i32, [i64, vp, vp, vp, i32, i64, vp]),
         "slq_rcm_order_device_workspace_bytes": (i32, [i64, vp]),

@@ -491,7 +491,8 @@ k_spmm_blk(const BlkArgs d)
         for (int s = 0; s < BLK_STAGES; ++s)
         {
             mbar_init(&full[s], 1);
-            mbar_init(&conv[s], BLK_CONV_WARPS);  // one arrival per converter warp
+            // one arrival per converter warp, or per copier thread (PRE)
+            mbar_init(&conv[s], PRE ? BLK_CONV_WARPS * 32 : BLK_CONV_WARPS);
             mbar_init(&empty[s], 1);
         }
         for (int i = 0; i < 2; ++i)
@@ -588,10 +589,12 @@ k_spmm_blk(const BlkArgs d)
         // row's X16 entry (hi | lo: part c / (NB / 8), probes 8 g .. 8 g + 7,
         // g = c % (NB / 8)) and copies them (cp.async, no registers) to MN
         // atom g / 8, K atom k / 8, row k % 8, chunk (g % 8) XOR (k % 8) of
-        // the part's region -- the converters' layout.  A stage is announced
-        // (conv) once this thread's copies of it completed, BLK_CP_AHEAD
-        // stages later, so that many stages of gathers are in flight; the
-        // row indices load BLK_CP_AHEAD stages before they are needed.
+        // the part's region -- the converters' layout.  Each thread's copies
+        // of a stage arrive on conv[s] by themselves when they land
+        // (cp.async.mbarrier.arrive.noinc; conv counts the 256 threads), so
+        // a thread moves on to the next free stage at once and up to
+        // BLK_STAGES stages of gathers are in flight; the row indices load
+        // four stages before they are needed.
         constexpr int AH = 4;
         const int ct = tid - BLK_CONV0 * 32;
         const int k = ct >> 4;
@@ -615,12 +618,6 @@ k_spmm_blk(const BlkArgs d)
             ring[i] = ix.row(d.ucol, d.nblk, k);
             ix.advance(d.bstage, d.nblk);
         }
-        auto announce = [&](int64_t done) {
-            // this thread's copies of stage `done` have landed
-            tc::fence_proxy_async_smem();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&conv[done % BLK_STAGES]);
-        };
         int64_t it = 0;
         bool ok = true;
         for (int64_t blk = blockIdx.x; blk < d.nblk && ok; blk += gridDim.x)
@@ -650,18 +647,12 @@ k_spmm_blk(const BlkArgs d)
                 for (int j = 0; j < nj; ++j)
                     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;"
                                  ::"r"(xs0 + dst[j]), "l"(src + 128 * j) : "memory");
-                asm volatile("cp.async.commit_group;" ::: "memory");
-                if (it >= AH)
-                {
-                    asm volatile("cp.async.wait_group %0;" ::"n"(AH) : "memory");
-                    announce(it - AH);
-                }
+                asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];"
+                             ::"r"(smem_u32(&conv[s])) : "memory");
             }
         }
-        // the rest: every copy lands (also after a failed wait)
-        asm volatile("cp.async.wait_group 0;" ::: "memory");
-        if (ok)
-            for (int64_t done = std::max<int64_t>(0, it - AH); done < it; ++done) announce(done);
+        // every copy lands before the thread leaves (also after a failed wait)
+        asm volatile("cp.async.wait_all;" ::: "memory");
     }
     else if (!PRE && warp >= BLK_CONV0)
     {
@@ -776,6 +767,9 @@ k_spmm_blk(const BlkArgs d)
                         ok = false;
                         break;
                     }
+                    // the copiers' cp.async writes (generic proxy) before the
+                    // MMAs read the stage through the async proxy
+                    if (PRE) tc::fence_proxy_async_smem();
                     tc::fence_after_sync();
                     unsigned char* stp = base + static_cast<size_t>(s) * stage_bytes;
                     // A: K-major, no swizzle (K core matrices 128 bytes apart,

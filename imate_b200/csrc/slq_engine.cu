@@ -247,6 +247,7 @@ struct slq_op {
     // 128-row blocks, first stage per block, union columns, row scales,
     // FP16 stage images
     int64_t a_nblk = 0, t_nblk = 0;
+    int64_t a_stages = 0, t_stages = 0;  // 16-column stages of the block formats
     const int32_t* a_bstage = nullptr;
     const int32_t* a_ucol = nullptr;
     const float* a_rsc = nullptr;
@@ -921,6 +922,7 @@ extern "C" slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* s
     if (transpose)
     {
         op->t_nblk = nblk;
+        op->t_stages = stages;
         op->t_bstage = bf.bstage;
         op->t_ucol = bf.ucol;
         op->t_rsc = bf.rsc;
@@ -929,11 +931,23 @@ extern "C" slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* s
     else
     {
         op->a_nblk = nblk;
+        op->a_stages = stages;
         op->a_bstage = bf.bstage;
         op->a_ucol = bf.ucol;
         op->a_rsc = bf.rsc;
         op->a_img = bf.img;
     }
+    return SLQ_OK;
+}
+
+extern "C" slq_status slq_operator_blocks_info(const slq_op* op, int transpose, int64_t* blocks,
+                                               int64_t* stages)
+{
+    if (!op || !blocks || !stages) return fail(SLQ_ERR_BAD_ARG, "blocks_info: NULL argument");
+    if (transpose != 0 && transpose != 1)
+        return fail(SLQ_ERR_BAD_ARG, "blocks_info: transpose must be 0 or 1");
+    *blocks = transpose ? op->t_nblk : op->a_nblk;
+    *stages = transpose ? op->t_stages : op->a_stages;
     return SLQ_OK;
 }
 

@@ -472,6 +472,16 @@ class _DeviceOperator:
             self.add_blocks(need_transpose or fmt == _lib.SLQ_CSC)
         return self
 
+    def blocks_info(self, transpose=False):
+        """(blocks, stages) of the block format of A (or A^T); (0, 0) when
+        the operator has none (``slq_operator_blocks_info``)."""
+        nb = ctypes.c_int64(0)
+        ns = ctypes.c_int64(0)
+        _lib.check(self._lib.slq_operator_blocks_info(
+            self.handle, int(bool(transpose)), ctypes.byref(nb),
+            ctypes.byref(ns)))
+        return int(nb.value), int(ns.value)
+
     def add_blocks(self, with_transpose=False):
         """Attach the tensor-core block format (``slq_operator_add_blocks``:
         128-row blocks of the stored rows, float32) for A and, with

@@ -140,6 +140,13 @@ slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* scratch,
                                    size_t scratch_bytes, void* format,
                                    size_t format_bytes, void* stream);
 
+/* The block format attached to one direction of an operator: its 128-row
+ * blocks and 16-column stages (both 0 when none).  A product over b probes
+ * issues 3 x stages x 128 x 16 x b multiply-adds on the tensor cores
+ * against 2 nnz b useful flops; each stage moves 8 KB of A parts. */
+slq_status slq_operator_blocks_info(const slq_op* op, int transpose,
+                                    int64_t* blocks, int64_t* stages);
+
 /* Reverse Cuthill-McKee order of a square CSR pattern (host arrays; the
  * pattern is taken as symmetric).  Each connected component starts at its
  * lowest-degree row and is visited breadth-first with the children of a row
