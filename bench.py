@@ -587,8 +587,27 @@ def run_engine_arm(args):
             "dtype": "f64", "speedup_mixed_batched": value / world / v64,
             "rel_diff_same_probes": float(np.max(np.abs(s32 - s64) /
                                                  np.abs(s64))),
+            "rel_diff_same_probes_path": "8 probes, block width 8 (row-group "
+                                         "SpMM)",
         }
+        if args.spmm == "block-tc" and args.probes in (128, 256):
+            # the bench's own path (block SpMM at b = 128 / 256) against the
+            # FP64 engine on the same probes
+            kwb = dict(kw, min_num_samples=args.probes,
+                       max_num_samples=args.probes)
+            eb = ib.EngineOptions(block_size=args.probes, rng="parity")
+            _, ib64 = fn(Aop64, engine=eb, **kwb)
+            _, ib32 = fn(Aop, engine=eb, **kwb)
+            t64 = np.asarray(ib64["convergence"]["samples"][:args.probes],
+                             float)
+            t32 = np.asarray(ib32["convergence"]["samples"][:args.probes],
+                             float)
+            line["fp64_plain"]["rel_diff_same_probes_block_spmm"] = float(
+                np.max(np.abs(t32 - t64) / np.abs(t64)))
+            line["fp64_plain"]["mean_rel_diff_same_probes_block_spmm"] = \
+                float(np.mean((t32 - t64) / np.abs(t64)))
         del Aop64
+        torch.cuda.empty_cache()
 
     if rank == 0:
         # end to end through the public API from host arrays
