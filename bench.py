@@ -493,9 +493,15 @@ def run_engine_arm(args):
                 "useful_over_issued": useful / issued,
                 "peak": tp, "peak_source": tp_kind, "unit": "TFLOP/s",
                 "issued_frac": issued / per / 1e12 / tp,
-                "a_image_bytes": nst * 8192.0,
-                "note": "the launch time includes the FP16 split of the probe "
-                        "block (k_x16_split) that precedes each product"}
+                "a_image_bytes": nst * 8192.0}
+        if kstats.get("split", (0,))[0]:
+            nl_x, ms_x, by_x = kstats["split"]
+            spmm_line["split"] = {
+                "kernel": "k_x16_split (FP16 parts of the probe block, once "
+                          "per product)",
+                "ms_per_launch": ms_x / nl_x,
+                "achieved_gbs": (by_x / nl_x) / (ms_x / nl_x * 1e-3) / 1e9,
+                "ms_per_launch_with_product": (ms_x / nl_x) + per * 1e3}
         roofline["spmm"] = spmm_line
 
     line = {

@@ -18,7 +18,7 @@ STATUS_NAMES = {
     5: "NAN", 6: "EIGEN", 7: "UNSUPPORTED", 8: "TIMEOUT",
 }
 SLQ_F32, SLQ_F64 = 0, 1
-ABI_VERSION = 3
+ABI_VERSION = 4
 # per-probe status bits (slq_result.probe_status)
 PROBE_NONFINITE, PROBE_EIGEN, PROBE_NODE, PROBE_SAMPLE = 1, 2, 4, 8
 SLQ_CSR, SLQ_CSC = 0, 1
@@ -86,7 +86,8 @@ class SlqParams(ctypes.Structure):
     ]
 
 
-KERNEL_KINDS = ("spmm", "dots", "reorth", "finalize", "eig", "probe", "other")
+KERNEL_KINDS = ("spmm", "dots", "reorth", "finalize", "eig", "probe", "other",
+                "split")
 
 
 class SlqKernelStat(ctypes.Structure):

@@ -1396,6 +1396,14 @@ slq_status spmm_blk_inst(Launcher& L, const slq_op* op, int transpose, int b, co
     // the block format's)
     const double bytes = op->nnz * 8.0 + (rows + 1) * 4.0 + double(xrows) * b * 4.0 +
                          double(rows) * b * 4.0 * (Z ? 2.0 : 1.0);
+    if (pre)
+    {
+        // its own profile class: one read of X and one write of its parts
+        ProfScope split_prof(SLQ_K_SPLIT, double(xrows) * b * 8.0, L.st);
+        k_x16_split<<<L.sms * 4, 256, 0, L.st>>>(X, sx, xrows, b, maps->x16);
+        SLQ_LAUNCH_CK();
+        ++L.launches;
+    }
     ProfScope prof(SLQ_K_SPMM, bytes, L.st);
     const size_t smem = blk_smem_bytes(b);
     static bool attr = false;
@@ -1415,12 +1423,7 @@ slq_status spmm_blk_inst(Launcher& L, const slq_op* op, int transpose, int b, co
                                     static_cast<int>(blk_smem_bytes(256))));
         attr = true;
     }
-    if (pre)
-    {
-        k_x16_split<<<L.sms * 4, 256, 0, L.st>>>(X, sx, xrows, b, maps->x16);
-        SLQ_LAUNCH_CK();
-        ++L.launches;
-    }
+
     const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(nblk, L.sms)));
     // an X without probe scales: its per-probe maxima first (into the
     // partial-sum buffer past this launch's rows, or, for a product without

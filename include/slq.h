@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define SLQ_ABI_VERSION 3
+#define SLQ_ABI_VERSION 4
 
 typedef enum {
     SLQ_OK = 0,
@@ -550,7 +550,9 @@ void slq_xoshiro_jump_ahead(uint64_t* state, uint64_t k);
  * per-kernel breakdown. */
 typedef enum {
     SLQ_K_SPMM = 0, SLQ_K_DOTS = 1, SLQ_K_REORTH = 2, SLQ_K_FINALIZE = 3,
-    SLQ_K_EIG = 4, SLQ_K_PROBE = 5, SLQ_K_OTHER = 6, SLQ_K_COUNT = 7
+    SLQ_K_EIG = 4, SLQ_K_PROBE = 5, SLQ_K_OTHER = 6,
+    SLQ_K_SPLIT = 7,  /* the FP16 split of the probe block before a block SpMM */
+    SLQ_K_COUNT = 8
 } slq_kernel_kind;
 
 typedef struct {
