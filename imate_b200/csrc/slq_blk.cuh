@@ -316,6 +316,7 @@ struct BlkArgs {
     const float* rsc;
     const __half* img;
     const __half* x16;         // PRE: X split into FP16 parts, [K][2 NB] (hi | lo)
+    const int32_t* xexp;       // PRE: its per-probe exponents (NULL: from sx)
     const float* X;
     const double* sx;          // per-probe scale s_p of X (norm 1 / s_p), or NULL
     const unsigned int* xmax;  // sx == NULL: per-probe max |x| (float bits)
@@ -348,10 +349,7 @@ __device__ __forceinline__ void split_h4(float4 v, uint2& hi, uint2& lo)
 // The power-of-two exponent e_p that scales probe p of X into FP16 range:
 // with the probe's scale s_p (|x|_2 = 1 / s_p) every scaled |x| is at most
 // 2^14; without a usable scale, 0.
-__device__ __forceinline__ int blk_x_exp(double sxv)
-{
-    return (sxv > 0.0 && isfinite(sxv)) ? min(max(ilogb(sxv) + 13, -120), 120) : 0;
-}
+__device__ __forceinline__ int blk_x_exp(double sxv) { return x16_exp(sxv); }
 
 // X16[r][p] = hi, X16[r][b + p] = lo of 2^e_p X[r][p] (the FP16 parts the
 // block SpMM multiplies), for rows x b probes, b a multiple of 8; thread =
@@ -513,7 +511,11 @@ k_spmm_blk(const BlkArgs d)
         // by the same 2^e_p)
         const double sxv = d.sx ? d.sx[p] : 1.0;
         int e = 0;
-        if (d.sx)
+        if (PRE && d.xexp)
+        {
+            e = d.xexp[p];  // the exponent the split block was written with
+        }
+        else if (d.sx)
         {
             e = blk_x_exp(sxv);
         }

@@ -1111,6 +1111,10 @@ struct XMaps {
     __half* x16 = nullptr;
     int x16_b = 0;
     bool has_x16 = false;
+    // x16 already holds this product's X, split by the pass that wrote X
+    // with the exponents x16exp (else the product splits X first)
+    bool x16_ready = false;
+    const int32_t* x16exp = nullptr;
 };
 
 slq_status make_xmaps(XMaps* m, const float* base, int64_t rows, int b, bool row)
@@ -1396,7 +1400,8 @@ slq_status spmm_blk_inst(Launcher& L, const slq_op* op, int transpose, int b, co
     // the block format's)
     const double bytes = op->nnz * 8.0 + (rows + 1) * 4.0 + double(xrows) * b * 4.0 +
                          double(rows) * b * 4.0 * (Z ? 2.0 : 1.0);
-    if (pre)
+    const bool ready = pre && maps->x16_ready && maps->x16exp;
+    if (pre && !ready)
     {
         // its own profile class: one read of X and one write of its parts
         ProfScope split_prof(SLQ_K_SPLIT, double(xrows) * b * 8.0, L.st);
@@ -1461,6 +1466,7 @@ slq_status spmm_blk_inst(Launcher& L, const slq_op* op, int transpose, int b, co
     d.partials = partials;
     d.error = error;
     d.x16 = pre ? maps->x16 : nullptr;
+    d.xexp = ready ? maps->x16exp : nullptr;
     if (pre && b == 256)
         k_spmm_blk<256, true><<<grid, BLK_THREADS, smem, L.st>>>(d);
     else if (pre)
@@ -1690,7 +1696,9 @@ slq_status stream_pass(Launcher& L, int64_t n, int b, const VT* W, VT* Wout, int
                        const VT* Vj, const double* sj, const double* aj, const VT* Vm,
                        const double* sm, const double* bm, const VT* basis, int64_t slot_elems,
                        int bs, int last, int J, const VT* coef, int want_norm,
-                       double* partials, int32_t* error, int* grid_out)
+                       double* partials, int32_t* error, int* grid_out,
+                       double* wn2_out = nullptr, const double* wn2_in = nullptr,
+                       int wn2_grid = 0, __half* x16 = nullptr, int32_t* x16exp = nullptr)
 {
     constexpr int R = (sizeof(VT) == 4) ? 16 : 8;
     constexpr size_t SMEM_MAX = 232448;
@@ -1737,6 +1745,11 @@ slq_status stream_pass(Launcher& L, int64_t n, int b, const VT* W, VT* Wout, int
     a.partials = partials;
     a.error = error;
     a.fail_first_wait = 0;
+    a.wn2_out = wn2_out;
+    a.wn2_in = wn2_in;
+    a.wn2_grid = wn2_grid;
+    a.x16 = x16;
+    a.x16exp = x16exp;
     if (g_fail_stream_waits.load() > 0 && g_fail_stream_waits.fetch_sub(1) > 0)
         a.fail_first_wait = 1;
     const int gy = b / PT;
@@ -1745,7 +1758,8 @@ slq_status stream_pass(Launcher& L, int64_t n, int b, const VT* W, VT* Wout, int
     const int npre = 1 + (do_update ? (Vm ? 2 : 1) : 0);
     const int skip = (MODE == 0 && do_update) ? (Vm ? 2 : 1) : 0;
     const int reads = npre + std::max(0, J - skip);
-    const int writes = (MODE == 1 || do_update) ? 1 : 0;
+    // the split parts: 2 x 2 bytes per element, one float vector's bytes
+    const int writes = ((MODE == 1 || do_update) ? 1 : 0) + (x16 ? 1 : 0);
     ProfScope prof(MODE == 0 ? SLQ_K_DOTS : SLQ_K_REORTH, vb * (reads + writes), L.st);
     k_stream<VT, MODE, R><<<dim3(gx, gy), STREAM_THREADS, smem, L.st>>>(a);
     SLQ_LAUNCH_CK();
@@ -1774,6 +1788,8 @@ struct RunBufs {
     void* W2;
     void* T;              // normal-equations runs: A v, [nu][b]
     __half* X16;          // the SpMM's probe block split into FP16 parts, [nv][2 b]
+    int32_t* X16exp;      // its per-probe exponents when a streaming pass wrote it
+    double* wn2;          // |w|^2 partials of the dots pass for that split, [sms][b]
     double* negshift;     // normal-equations runs: -t per probe
     double* scale_v;
     double* scale_u;
@@ -1877,6 +1893,8 @@ void carve(Carver& c, const RunPlan& r, int sms, RunBufs* B)
     B->W2 = (r.gram != 1 && r.orth != 0) ? c.take<VT>(vslot) : nullptr;
     B->T = (r.gram == 2) ? c.take<VT>(static_cast<size_t>(r.nu) * r.b) : nullptr;
     B->X16 = r.x16 ? c.take<__half>(static_cast<size_t>(r.nv) * 2 * r.b) : nullptr;
+    B->X16exp = r.x16 ? c.take<int32_t>(r.b) : nullptr;
+    B->wn2 = r.x16 ? c.take<double>(static_cast<size_t>(sms) * r.b) : nullptr;
     B->negshift = c.take<double>(r.b);
     B->scale_v = c.take<double>(static_cast<size_t>(r.bs) * r.b);
     B->scale_u = c.take<double>(static_cast<size_t>(r.bs) * r.b);
@@ -1992,7 +2010,12 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
                                const VT* Vj, const double* sj, const double* aj, const VT* Vm,
                                const double* sm, const double* bm, const VT* basis,
                                int64_t slot_elems, const double* scales, int last, int J,
-                               int* nparts) -> slq_status {
+                               int* nparts, bool split) -> slq_status {
+        // split: the last pass also writes w_out split into FP16 parts for
+        // the block SpMM (B.X16), scaled by the norm the first dots pass
+        // measures of the updated w
+        split = split && B.X16 && do_update;
+        int dg0 = 0;
         for (int c0 = 0; c0 < J; c0 += MAX_J)
         {
             const int Jc = std::min(MAX_J, J - c0);
@@ -2001,7 +2024,8 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
             SLQ_TRY(stream_pass<VT, 0>(L, n, b, first ? w_in_first : w_work, w_work,
                                        first ? do_update : 0, Vj, sj, aj, Vm, sm, bm, basis,
                                        slot_elems, bs, last - c0, Jc, nullptr, 0, B.partials,
-                                       B.error, &dg));
+                                       B.error, &dg, (split && first) ? B.wn2 : nullptr));
+            if (first) dg0 = dg;
             SLQ_TRY(finalize<VT>(L, B.partials, dg, Jc * b, FIN_COEF, nullptr,
                                  coef + static_cast<int64_t>(c0) * b, scales, b, bs, last - c0,
                                  nullptr, nullptr, nullptr, 0, 0.0, 0));
@@ -2011,11 +2035,14 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
         {
             const int Jc = std::min(MAX_J, J - c0);
             const bool lastc = (c0 + MAX_J >= J);
+            const bool sp = split && lastc;
             SLQ_TRY(stream_pass<VT, 1>(L, n, b, w_work, lastc ? w_out : w_work, 0, nullptr,
                                        nullptr, nullptr, nullptr, nullptr, nullptr, basis,
                                        slot_elems, bs, last - c0, Jc,
                                        coef + static_cast<int64_t>(c0) * b, lastc ? 1 : 0,
-                                       B.partials, B.error, &rg));
+                                       B.partials, B.error, &rg, nullptr,
+                                       sp ? B.wn2 : nullptr, sp ? dg0 : 0,
+                                       sp ? B.X16 : nullptr, sp ? B.X16exp : nullptr));
         }
         *nparts = rg;
         return SLQ_OK;
@@ -2024,10 +2051,19 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
     if (r.gram != 1)
     {
         VT* T = static_cast<VT*>(B.T);
+        // B.X16 holds v_j split into FP16 parts when the previous step's last
+        // reorthogonalisation pass wrote it (else the product splits v_j)
+        bool x16_ready = false;
         for (int j = 0; j < m; ++j)
         {
             VT* vj = Vs(j);
             int sg = 0;
+            if (use_tma && B.X16)
+            {
+                XMaps& mv = vmaps[((j % bs) + bs) % bs];
+                mv.x16_ready = x16_ready;
+                mv.x16exp = B.X16exp;
+            }
             if (r.gram == 0)
             {
                 SLQ_TRY(op_spmm<VT>(L, op, 0, b, vj, sv_of(j), shift, W, nullptr, nullptr,
@@ -2043,6 +2079,7 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
                 SLQ_TRY(op_spmm<VT>(L, op, 1, b, T, nullptr, 0.0, W, vj, B.negshift, sv_of(j),
                                     3, B.partials, &sg, nullptr, B.error));
             }
+            x16_ready = false;
             double* aj = B.alpha + static_cast<int64_t>(j) * b;
             SLQ_TRY(finalize<VT>(L, B.partials, sg, b, FIN_STORE, aj, nullptr, nullptr, b, bs, 0,
                                  nullptr, nullptr, nullptr, 0, 0.0, j));
@@ -2062,7 +2099,8 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
             else
             {
                 SLQ_TRY(reorthogonalize(r.nv, W, W2, Vs(j + 1), 1, vj, sv_of(j), aj, vm, sm, bm,
-                                        V, vslot, B.scale_v, j, J, &nparts));
+                                        V, vslot, B.scale_v, j, J, &nparts, true));
+                x16_ready = B.X16 != nullptr;
             }
             SLQ_TRY(finalize<VT>(L, B.partials, nparts, b, FIN_NORM,
                                  B.beta + static_cast<int64_t>(j) * b, nullptr, nullptr, b, bs, 0,
@@ -2088,7 +2126,7 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
             if (Ju > 0)
                 SLQ_TRY(reorthogonalize(r.nu, uj, uj, uj, 0, nullptr, nullptr, nullptr, nullptr,
                                         nullptr, nullptr, U, uslot, B.scale_u, j - 1, Ju,
-                                        &nparts));
+                                        &nparts, false));
             double* aj = B.alpha + static_cast<int64_t>(j) * b;
             SLQ_TRY(finalize<VT>(L, B.partials, nparts, b, FIN_NORM, aj, nullptr, nullptr, b, bs,
                                  0, su_of(j), B.active, B.size, 0, 0.0, j));
@@ -2101,7 +2139,8 @@ slq_status krylov_block(Launcher& L, const slq_op* op, const slq_params* p, cons
             nparts = sgv;
             if (Jv > 0)
                 SLQ_TRY(reorthogonalize(r.nv, vn, vn, vn, 0, nullptr, nullptr, nullptr, nullptr,
-                                        nullptr, nullptr, V, vslot, B.scale_v, j, Jv, &nparts));
+                                        nullptr, nullptr, V, vslot, B.scale_v, j, Jv, &nparts,
+                                        false));
             SLQ_TRY(finalize<VT>(L, B.partials, nparts, b, FIN_NORM,
                                  B.beta + static_cast<int64_t>(j) * b, nullptr, nullptr, b, bs, 0,
                                  sv_of(j + 1), B.active, B.size, 1, thr, j));

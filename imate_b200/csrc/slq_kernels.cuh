@@ -21,6 +21,7 @@
 #ifndef SLQ_KERNELS_CUH_
 #define SLQ_KERNELS_CUH_
 
+#include <cuda_fp16.h>
 #include <climits>
 #include <cstdint>
 #include <cuda.h>
@@ -1264,6 +1265,23 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
         : "memory");
 }
 
+// The exponent e_p that scales a probe of norm 1 / s into FP16 range for
+// the block SpMM (every scaled |x| <= 2^14); 0 without a usable scale.
+__device__ __forceinline__ int x16_exp(double s)
+{
+    return (s > 0.0 && isfinite(s)) ? min(max(ilogb(s) + 13, -120), 120) : 0;
+}
+
+// hi = rn_f16(v), lo = rn_f16(v - hi) of one scaled element of the split
+// block X16[row] = hi[b] | lo[b]
+__device__ __forceinline__ void x16_store(__half* x16, int64_t row, int b, int p, float v)
+{
+    const __half h = __float2half_rn(v);
+    const __half l = __float2half_rn(v - __half2float(h));
+    x16[row * 2 * b + p] = h;
+    x16[row * 2 * b + b + p] = l;
+}
+
 template <typename VT>
 struct StreamArgs {
     int64_t n;            // rows
@@ -1290,6 +1308,17 @@ struct StreamArgs {
     double* partials;     // dots: [grid.x][J][b]; reorth: [grid.x][b]
     int32_t* error;       // set to 1 when a wait runs out
     int fail_first_wait;  // test hook: the consumers' first wait runs out at once
+    // the block SpMM's split probe block, written by the pass that writes the
+    // next Krylov vector (float only): dots with do_update write the partial
+    // sums of |w|^2 of the updated w, [grid.x][b] (wn2_out); the last reorth
+    // pass reduces them (wn2_in, wn2_grid rows), takes 2^e_p with e_p from
+    // that norm (an upper bound of the final one, so every scaled element
+    // fits), and writes x16[row] = hi | lo of 2^e_p w and x16exp[p] = e_p
+    double* wn2_out;
+    const double* wn2_in;
+    int wn2_grid;
+    __half* x16;
+    int32_t* x16exp;
 };
 
 // MODE 0: dots, MODE 1: reorth.  R = rows per consumer thread per tile.
@@ -1423,6 +1452,23 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
         }
         double nacc = 0.0;
         bool ok = true;
+        // the split probe block (MODE 1 with x16): this probe's 2^e_p from
+        // the reduced |w|^2 partials of the dots pass (a fixed order)
+        bool x16_on = false;
+        float x16_scale = 1.0f;
+        if constexpr (MODE == 1 && sizeof(VT) == 4)
+        {
+            if (a.x16 && a.wn2_in)
+            {
+                double n2 = 0.0;
+                for (int g = 0; g < a.wn2_grid; ++g)
+                    n2 += a.wn2_in[static_cast<int64_t>(g) * b + p0 + pl];
+                const int e = (n2 > 0.0 && isfinite(n2)) ? x16_exp(1.0 / sqrt(n2)) : 0;
+                x16_scale = ldexpf(1.0f, e);
+                x16_on = true;
+                if (roff == 0 && blockIdx.x == 0) a.x16exp[p0 + pl] = e;
+            }
+        }
         const int lane = tid & 31;
         auto release = [&](int st) {
             __syncwarp();
@@ -1548,6 +1594,7 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
                         const VT wr = static_cast<VT>(w[k]);
                         w[k] = static_cast<double>(wr);
                         a.Wout[(row0 + roff + k * RSTEP) * b + p0 + pl] = wr;
+                        nacc += w[k] * w[k];
                         lj += vj[k] * w[k];
                         if (a.Vm)
                             lm += static_cast<double>(st[(roff + k * RSTEP) * PT + pl]) * w[k];
@@ -1566,7 +1613,10 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
                     const VT wr = static_cast<VT>(w[k]);
                     const double d = static_cast<double>(wr);
                     nacc += d * d;
-                    a.Wout[(row0 + roff + k * RSTEP) * b + p0 + pl] = wr;
+                    const int64_t row = row0 + roff + k * RSTEP;
+                    a.Wout[row * b + p0 + pl] = wr;
+                    if (x16_on)
+                        x16_store(a.x16, row, b, p0 + pl, static_cast<float>(wr) * x16_scale);
                 }
             }
         }
@@ -1594,6 +1644,7 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
                         const VT wr = static_cast<VT>(wv);
                         wv = static_cast<double>(wr);
                         a.Wout[o] = wr;
+                        nacc += wv * wv;
                         if (J > 0) extra[tid] += x * wv;
                         if (a.Vm && J > 1) extra[STREAM_CONSUMERS + tid] += y * wv;
                     }
@@ -1611,10 +1662,11 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
                     const double d = static_cast<double>(wr);
                     nacc += d * d;
                     a.Wout[o] = wr;
+                    if (x16_on) x16_store(a.x16, r, b, p0 + pl, static_cast<float>(wr) * x16_scale);
                 }
             }
         }
-        if (MODE == 1) red[tid] = nacc;
+        red[tid] = nacc;
     }
     __syncthreads();
 
@@ -1637,6 +1689,15 @@ __global__ void __launch_bounds__(STREAM_THREADS, 1) k_stream(const StreamArgs<V
             double sum = 0.0;
             for (int r = 0; r < RSTEP; ++r) sum += red[r * PT + q];
             a.partials[static_cast<int64_t>(blockIdx.x) * b + p0 + q] = sum;
+        }
+    }
+    if (MODE == 0 && a.wn2_out)
+    {
+        for (int q = tid; q < PT; q += STREAM_CONSUMERS)
+        {
+            double sum = 0.0;
+            for (int r = 0; r < RSTEP; ++r) sum += red[r * PT + q];
+            a.wn2_out[static_cast<int64_t>(blockIdx.x) * b + p0 + q] = sum;
         }
     }
 }
