@@ -168,15 +168,16 @@ bool valid_pattern(Pool& P, int64_t n, const int32_t* indptr, const int32_t* ind
         }
     const int64_t e0 = indptr[0], e1 = indptr[n];
     std::atomic<bool> bad(false);
+    // one unsigned comparison per index, or-ed without a branch so the loop
+    // vectorises (a negative index is a large unsigned one)
+    const uint32_t un = static_cast<uint32_t>(n);
     P.run([&](int t, int nt) {
         int64_t b, e;
         part_range(e1 - e0, t, nt, b, e);
-        for (int64_t k = e0 + b; k < e0 + e; ++k)
-            if (indices[k] < 0 || indices[k] >= n)
-            {
-                bad.store(true, std::memory_order_relaxed);
-                return;
-            }
+        const uint32_t* ix = reinterpret_cast<const uint32_t*>(indices + e0);
+        uint32_t any = 0;
+        for (int64_t k = b; k < e; ++k) any |= static_cast<uint32_t>(ix[k] >= un);
+        if (any) bad.store(true, std::memory_order_relaxed);
     });
     if (bad.load())
     {
