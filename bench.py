@@ -2,10 +2,10 @@
 """Benchmark: SLQ logdet probe*steps/s on B200 (mixed precision, batched).
 
 Workload (one "step" = one SLQ logdet run over one block of probes on the
-resident matrix): the sparse SPD correlation matrix of the BASELINE's second
-configuration -- n = 262144 points uniform in [0,1]^2 (numpy PCG64 seed 1),
+resident matrix): the sparse SPD correlation matrix of the headline
+workload -- n = 262144 points uniform in [0,1]^2 (numpy PCG64 seed 1),
 kernel exp(-r/0.005) zeroed below 0.05 -- with the diagonal shift 0.1 in place
-of the configuration's 1e-3, which leaves the matrix indefinite (smallest Ritz
+of the specified 1e-3, which leaves the matrix indefinite (smallest Ritz
 value -0.0548, logdet undefined); 48.07M nonzeros, FP32 values, int32
 indices.  256 Rademacher probes (parity stream, seed 0), lanczos_degree 50,
 full reorthogonalisation.  Inputs (matrix 385 MB, Krylov basis 13.4 GB) are
@@ -18,7 +18,8 @@ e2e        same metric through the public API from host scipy arrays: the
            timed region.
 roofline   dominant kernel class: algorithmic bytes per launch / mean launch
            time (CUDA events inside the timed region), vs the measured HBM
-           copy bandwidth.
+           copy bandwidth; roofline.spmm the same for the SpMM, with the
+           tensor-core work it issues on the block format.
 cpu_baseline  the reference's own CPU SLQ (oracle/_ref, built from its
            sources) on the host cores, on a bounded sample of the workload.
 
