@@ -37,7 +37,10 @@
 //                      stride byte offset 256 between 8-row groups)
 // so one stage of A is one contiguous 8 KB bulk copy.
 //
-// Kernel k_spmm_blk (persistent, one CTA per SM, blocks dealt round-robin):
+// Kernel k_spmm_blk (persistent, one CTA per SM; CTA c takes slots c, c +
+// grid, ... of the format's slot order, which keeps every wave of grid slots
+// to one run of consecutive blocks -- the X rows they gather stay in L2 --
+// and balances the CTAs' stage counts within each wave):
 //   warp 8        producer: per stage, one cp.async.bulk of the A parts;
 //   warps 10-17   converters: load the stage's 16 X rows from global memory
 //                 (two stages ahead, into registers), scale and split them
@@ -312,6 +315,7 @@ struct BlkArgs {
     int64_t nblk;              // 128-row blocks
     int NB;                    // probes = b (128 or 256)
     const int32_t* bstage;
+    const int32_t* order;      // block of each slot (CTA c takes slots c, c + grid, ...)
     const int32_t* ucol;
     const float* rsc;
     const __half* img;
@@ -411,15 +415,18 @@ __device__ __forceinline__ float reduce_scatter16(float (&a)[16], int lane)
 // Position in a CTA's stage sequence: its blocks blockIdx.x, + gridDim.x, ...
 // and each block's stages in order.
 struct BlkCursor {
-    int64_t blk;
+    int64_t slot;  // this CTA's slots: blockIdx.x, + gridDim.x, ...
     int st, s1;
+    const int32_t* order;
 
-    __device__ void start(const int32_t* bstage, int64_t nblk)
+    __device__ void start(const int32_t* bstage, const int32_t* ord, int64_t nblk)
     {
-        blk = blockIdx.x;
+        order = ord;
+        slot = blockIdx.x;
         st = s1 = 0;
-        if (blk < nblk)
+        if (slot < nblk)
         {
+            const int64_t blk = order[slot];
             st = bstage[blk];
             s1 = bstage[blk + 1];
         }
@@ -427,12 +434,13 @@ struct BlkCursor {
 
     __device__ void advance(const int32_t* bstage, int64_t nblk)
     {
-        if (blk >= nblk) return;
+        if (slot >= nblk) return;
         if (++st >= s1)
         {
-            blk += gridDim.x;
-            if (blk < nblk)
+            slot += gridDim.x;
+            if (slot < nblk)
             {
+                const int64_t blk = order[slot];
                 st = bstage[blk];
                 s1 = bstage[blk + 1];
             }
@@ -442,7 +450,7 @@ struct BlkCursor {
     // union row k of the current stage (-1 past the end)
     __device__ int row(const int32_t* ucol, int64_t nblk, int k) const
     {
-        return blk < nblk ? ucol[int64_t(st) * BLK_BK + k] : -1;
+        return slot < nblk ? ucol[int64_t(st) * BLK_BK + k] : -1;
     }
 };
 
@@ -555,8 +563,9 @@ k_spmm_blk(const BlkArgs d)
         {
             int64_t it = 0;
             bool ok = true;
-            for (int64_t blk = blockIdx.x; blk < d.nblk && ok; blk += gridDim.x)
+            for (int64_t slot = blockIdx.x; slot < d.nblk && ok; slot += gridDim.x)
             {
+                const int64_t blk = d.order[slot];
                 const int s0 = d.bstage[blk], s1 = d.bstage[blk + 1];
                 for (int st = s0; st < s1; ++st, ++it)
                 {
@@ -612,7 +621,7 @@ k_spmm_blk(const BlkArgs d)
                      (k & 7) * 128 + (((g & 7) ^ (k & 7)) << 4);
         }
         BlkCursor ix;
-        ix.start(d.bstage, d.nblk);
+        ix.start(d.bstage, d.order, d.nblk);
         int ring[AH];
 #pragma unroll
         for (int i = 0; i < AH; ++i)
@@ -622,8 +631,9 @@ k_spmm_blk(const BlkArgs d)
         }
         int64_t it = 0;
         bool ok = true;
-        for (int64_t blk = blockIdx.x; blk < d.nblk && ok; blk += gridDim.x)
+        for (int64_t slot = blockIdx.x; slot < d.nblk && ok; slot += gridDim.x)
         {
+            const int64_t blk = d.order[slot];
             const int s0 = d.bstage[blk], s1 = d.bstage[blk + 1];
             for (int st = s0; st < s1; ++st, ++it)
             {
@@ -684,8 +694,8 @@ k_spmm_blk(const BlkArgs d)
         // stage cursors: the one being converted and the one whose row index
         // is loading
         BlkCursor cur, ix;
-        cur.start(d.bstage, d.nblk);
-        ix.start(d.bstage, d.nblk);
+        cur.start(d.bstage, d.order, d.nblk);
+        ix.start(d.bstage, d.order, d.nblk);
         float4 b0[4], b1[4];
         // prologue: rows of stages 0 and 1 loading, the index of stage 2
         load_x(ix.row(d.ucol, d.nblk, k), b0);
@@ -731,10 +741,10 @@ k_spmm_blk(const BlkArgs d)
             ix.advance(d.bstage, d.nblk);
             return true;
         };
-        while (ok && cur.blk < d.nblk)
+        while (ok && cur.slot < d.nblk)
         {
             ok = step(b0);
-            if (!ok || cur.blk >= d.nblk) break;
+            if (!ok || cur.slot >= d.nblk) break;
             ok = step(b1);
         }
     }
@@ -745,8 +755,9 @@ k_spmm_blk(const BlkArgs d)
             const uint32_t idesc = blk_idesc(static_cast<uint32_t>(NB));
             int64_t it = 0, lb = 0;
             bool ok = true;
-            for (int64_t blk = blockIdx.x; blk < d.nblk && ok; blk += gridDim.x, ++lb)
+            for (int64_t slot = blockIdx.x; slot < d.nblk && ok; slot += gridDim.x, ++lb)
             {
+                const int64_t blk = d.order[slot];
                 const int buf = static_cast<int>(lb & 1);
                 if (lb >= 2 &&
                     !mbar_wait(&acc_empty[buf], static_cast<uint32_t>(((lb >> 1) - 1) & 1),
@@ -816,8 +827,9 @@ k_spmm_blk(const BlkArgs d)
         const float wz = d.epi == 3 ? 1.0f : 0.0f;
         const int my_col = blk_col(lane);
         int64_t lb = 0;
-        for (int64_t blk = blockIdx.x; blk < d.nblk; blk += gridDim.x, ++lb)
+        for (int64_t slot = blockIdx.x; slot < d.nblk; slot += gridDim.x, ++lb)
         {
+            const int64_t blk = d.order[slot];
             const int buf = static_cast<int>(lb & 1);
             const int64_t row = blk * BLK_ROWS + 32 * qd + lane;
             const float rs = d.rsc[row];  // 2^-f_r (padding rows hold 1)

@@ -256,6 +256,8 @@ struct slq_op {
     const int32_t* t_ucol = nullptr;
     const float* t_rsc = nullptr;
     const __half* t_img = nullptr;
+    const int32_t* a_order = nullptr;
+    const int32_t* t_order = nullptr;
     // slq_operator_dot's error word and per-probe maxima of X for the block
     // kernel (inside the first format buffer)
     int32_t* blk_error = nullptr;
@@ -782,6 +784,7 @@ struct BlkFormat {
     int32_t* error;
     unsigned int* xmax;  // [256]
     int32_t* bstage;
+    int32_t* order;      // [nblk] block of each slot of the kernel's waves
     int32_t* ucol;
     float* rsc;
     __half* img;
@@ -792,9 +795,47 @@ void blk_format_layout(Carver& c, int64_t nblk, int64_t stages, BlkFormat* f)
     f->error = c.take<int32_t>(1);
     f->xmax = c.take<unsigned int>(256);
     f->bstage = c.take<int32_t>(nblk + 1);
+    f->order = c.take<int32_t>(nblk);
     f->ucol = c.take<int32_t>(stages * BLK_BK);
     f->rsc = c.take<float>(nblk * BLK_ROWS);
     f->img = c.take<__half>(stages * BLK_IMG_STAGE);
+}
+
+// The slot order of the block SpMM's G CTAs (CTA c takes slots c, c + G,
+// ...): wave w = slots w G .. w G + G - 1 holds blocks w G .. w G + G - 1,
+// consecutive blocks so that a wave's X rows stay in L2, and within each
+// wave the blocks with the most stages go to the CTAs with the least work
+// so far (longest first onto the least loaded).  The last, partial wave can
+// only use CTAs 0 .. rem - 1; it is dealt first.  Deterministic.
+void blk_balance(const int32_t* bstage, int64_t nblk, int G, int32_t* order)
+{
+    if (nblk <= 0) return;
+    G = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(G, nblk)));
+    const int64_t W = (nblk + G - 1) / G;
+    std::vector<int64_t> load(static_cast<size_t>(G), 0);
+    std::vector<int32_t> blocks, ctas;
+    auto deal = [&](int64_t w) {
+        const int64_t b0 = w * G, b1 = std::min<int64_t>(nblk, b0 + G);
+        const int n = static_cast<int>(b1 - b0);
+        blocks.resize(static_cast<size_t>(n));
+        ctas.resize(static_cast<size_t>(n));
+        for (int i = 0; i < n; ++i) blocks[i] = static_cast<int32_t>(b0 + i);
+        for (int i = 0; i < n; ++i) ctas[i] = i;
+        std::sort(blocks.begin(), blocks.end(), [&](int32_t x, int32_t y) {
+            const int sx = bstage[x + 1] - bstage[x], sy = bstage[y + 1] - bstage[y];
+            return sx != sy ? sx > sy : x < y;
+        });
+        std::sort(ctas.begin(), ctas.end(), [&](int32_t x, int32_t y) {
+            return load[x] != load[y] ? load[x] < load[y] : x < y;
+        });
+        for (int i = 0; i < n; ++i)
+        {
+            order[b0 + ctas[i]] = blocks[i];
+            load[ctas[i]] += bstage[blocks[i] + 1] - bstage[blocks[i]];
+        }
+    };
+    if (nblk % G != 0) deal(W - 1);
+    for (int64_t w = 0; w < ((nblk % G != 0) ? W - 1 : W); ++w) deal(w);
 }
 
 slq_status blk_source(const slq_op* op, int transpose, const int32_t** ptr, const int32_t** ind,
@@ -914,6 +955,18 @@ extern "C" slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* s
     SLQ_CK(cudaMemsetAsync(bf.error, 0, sizeof(int32_t), st));
     // the scratch may be released once the build has run
     SLQ_CK(cudaStreamSynchronize(st));
+    {
+        // the kernel's slot order, balanced for this device's SM count
+        std::vector<int32_t> hb(static_cast<size_t>(nblk + 1)), ho(static_cast<size_t>(nblk));
+        SLQ_CK(cudaMemcpyAsync(hb.data(), bf.bstage, sizeof(int32_t) * (nblk + 1),
+                               cudaMemcpyDeviceToHost, st));
+        SLQ_CK(cudaStreamSynchronize(st));
+        blk_balance(hb.data(), nblk, sms, ho.data());
+        if (nblk > 0)
+            SLQ_CK(cudaMemcpyAsync(bf.order, ho.data(), sizeof(int32_t) * nblk,
+                                   cudaMemcpyHostToDevice, st));
+        SLQ_CK(cudaStreamSynchronize(st));  // ho is released on return
+    }
     if (!op->blk_error)
     {
         op->blk_error = bf.error;
@@ -924,6 +977,7 @@ extern "C" slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* s
         op->t_nblk = nblk;
         op->t_stages = stages;
         op->t_bstage = bf.bstage;
+        op->t_order = bf.order;
         op->t_ucol = bf.ucol;
         op->t_rsc = bf.rsc;
         op->t_img = bf.img;
@@ -933,6 +987,7 @@ extern "C" slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* s
         op->a_nblk = nblk;
         op->a_stages = stages;
         op->a_bstage = bf.bstage;
+        op->a_order = bf.order;
         op->a_ucol = bf.ucol;
         op->a_rsc = bf.rsc;
         op->a_img = bf.img;
@@ -1451,6 +1506,7 @@ slq_status spmm_blk_inst(Launcher& L, const slq_op* op, int transpose, int b, co
     d.nblk = nblk;
     d.NB = b;
     d.bstage = transpose ? op->t_bstage : op->a_bstage;
+    d.order = transpose ? op->t_order : op->a_order;
     d.ucol = transpose ? op->t_ucol : op->a_ucol;
     d.rsc = transpose ? op->t_rsc : op->a_rsc;
     d.img = transpose ? op->t_img : op->a_img;
