@@ -362,6 +362,8 @@ struct PermBufs {
     uint64_t* keys_out;
     int32_t* pos_in;
     int32_t* pos_out;
+    int32_t* deg;       // [n + 1] row lengths in B's order
+    int32_t* flag;      // [4]: largest row length
     void* temp;
     size_t temp_bytes;
 };
@@ -375,8 +377,17 @@ slq_status perm_layout(Carver& c, int64_t n, int64_t nnz, int dtype, PermBufs* t
         static_cast<int32_t*>(nullptr), static_cast<int>(std::max<int64_t>(nnz, 1)));
     if (e != cudaSuccess)
         return fail(SLQ_ERR_CUDA, std::string("cub sort sizing: ") + cudaGetErrorString(e));
+    size_t scan_bytes = 0;
+    e = cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, static_cast<const int32_t*>(nullptr),
+                                      static_cast<int32_t*>(nullptr),
+                                      static_cast<int>(n + 1));
+    if (e != cudaSuccess)
+        return fail(SLQ_ERR_CUDA, std::string("cub scan sizing: ") + cudaGetErrorString(e));
+    temp_bytes = std::max(temp_bytes, scan_bytes);
     t->inv = c.take<int32_t>(n);
     t->p_ptr = c.take<int32_t>(n + 1);
+    t->deg = c.take<int32_t>(n + 1);
+    t->flag = c.take<int32_t>(4);
     t->p_ind = c.take<int32_t>(nnz);
     t->p_data = c.take<char>(nnz * dsize(dtype));
     t->keys_in = c.take<uint64_t>(nnz);
@@ -399,6 +410,37 @@ slq_status permute_csr(const int32_t* ptr, const int32_t* ind, const void* data,
     const int grid = sms * 4;
     k_inverse_perm<<<grid, 256, 0, st>>>(perm, n, t->inv);
     SLQ_LAUNCH_CK();
+    // rows of at most PERM_ROW_MAX entries: each row relabelled and sorted in
+    // one warp (no global sort); else one radix sort of (row, column) keys
+    SLQ_CK(cudaMemsetAsync(t->flag, 0, sizeof(int32_t), st));
+    k_perm_deg<<<grid, 256, 0, st>>>(ptr, perm, n, t->deg, t->flag);
+    SLQ_LAUNCH_CK();
+    int32_t maxdeg = 0;
+    SLQ_CK(cudaMemcpyAsync(&maxdeg, t->flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    SLQ_CK(cudaStreamSynchronize(st));
+    if (maxdeg <= PERM_ROW_MAX)
+    {
+        size_t tb = t->temp_bytes;
+        cudaError_t e = cub::DeviceScan::ExclusiveSum(t->temp, tb, t->deg, t->p_ptr,
+                                                      static_cast<int>(n + 1), st);
+        if (e != cudaSuccess)
+            return fail(SLQ_ERR_CUDA, std::string("cub scan: ") + cudaGetErrorString(e));
+        if (nnz > 0)
+        {
+            const int rg = static_cast<int>(std::min<int64_t>((n + PERM_WARPS - 1) / PERM_WARPS,
+                                                              int64_t(sms) * 16));
+            if (dtype == SLQ_F64)
+                k_perm_rows<double><<<rg, PERM_WARPS * 32, 0, st>>>(
+                    ptr, ind, static_cast<const double*>(data), perm, t->inv, t->p_ptr, n,
+                    t->p_ind, static_cast<double*>(t->p_data));
+            else
+                k_perm_rows<float><<<rg, PERM_WARPS * 32, 0, st>>>(
+                    ptr, ind, static_cast<const float*>(data), perm, t->inv, t->p_ptr, n,
+                    t->p_ind, static_cast<float*>(t->p_data));
+            SLQ_LAUNCH_CK();
+        }
+        return SLQ_OK;
+    }
     if (nnz > 0)
     {
         k_perm_keys<<<grid, 256, 0, st>>>(ptr, ind, t->inv, n, t->keys_in, t->pos_in);

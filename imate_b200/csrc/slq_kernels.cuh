@@ -715,6 +715,89 @@ __global__ void k_perm_keys(const int32_t* __restrict__ indptr,
     }
 }
 
+// deg[i] = row length of A's row perm[i] (deg[n] = 0, for the exclusive
+// scan into B's row pointer); *maxdeg = the largest
+__global__ void k_perm_deg(const int32_t* __restrict__ indptr, const int32_t* __restrict__ perm,
+                           int64_t n, int32_t* __restrict__ deg, int32_t* __restrict__ maxdeg)
+{
+    int32_t m = 0;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i <= n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        int32_t d = 0;
+        if (i < n)
+        {
+            const int32_t r = perm[i];
+            d = indptr[r + 1] - indptr[r];
+        }
+        deg[i] = d;
+        m = max(m, d);
+    }
+    atomicMax(maxdeg, m);
+}
+
+// Rows of B = P A P^T, one warp per row i of B (A's row perm[i], at most
+// PERM_ROW_MAX entries): the entries relabelled (column inv[c]) and sorted by
+// (new column, position in the row) with a bitonic network in the warp's
+// shared-memory slice -- the order a stable sort of (row, column) keys
+// gives, so B is the same bit for bit.
+constexpr int PERM_ROW_MAX = 1024;
+constexpr int PERM_WARPS = 4;
+
+template <typename VT>
+__global__ void __launch_bounds__(PERM_WARPS * 32)
+    k_perm_rows(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                const VT* __restrict__ data, const int32_t* __restrict__ perm,
+                const int32_t* __restrict__ inv, const int32_t* __restrict__ p_ptr, int64_t n,
+                int32_t* __restrict__ p_ind, VT* __restrict__ p_data)
+{
+    __shared__ uint64_t keys[PERM_WARPS][PERM_ROW_MAX];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    uint64_t* buf = keys[w];
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * PERM_WARPS + w; i < n;
+         i += static_cast<int64_t>(gridDim.x) * PERM_WARPS)
+    {
+        const int32_t r = perm[i];
+        const int32_t e0 = indptr[r];
+        const int len = indptr[r + 1] - e0;
+        if (len <= 0) continue;
+        int m = 1;
+        while (m < len) m <<= 1;
+        for (int t = lane; t < m; t += 32)
+            buf[t] = t < len ? (static_cast<uint64_t>(static_cast<uint32_t>(inv[indices[e0 + t]])) << 32) |
+                                   static_cast<uint32_t>(t)
+                             : ~uint64_t(0);
+        __syncwarp();
+        for (int k = 2; k <= m; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1)
+            {
+                for (int t = lane; t < m; t += 32)
+                {
+                    const int u = t ^ j;
+                    if (u > t)
+                    {
+                        const uint64_t a = buf[t], b = buf[u];
+                        if ((a > b) == ((t & k) == 0))
+                        {
+                            buf[t] = b;
+                            buf[u] = a;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        const int64_t o = p_ptr[i];
+        for (int t = lane; t < len; t += 32)
+        {
+            const uint64_t key = buf[t];
+            p_ind[o + t] = static_cast<int32_t>(key >> 32);
+            p_data[o + t] = data[e0 + static_cast<int32_t>(key & 0xffffffffu)];
+        }
+        __syncwarp();
+    }
+}
+
 template <typename VT>
 __global__ void k_perm_gather(const uint64_t* __restrict__ sorted_keys,
                               const int32_t* __restrict__ sorted_pos,
