@@ -366,16 +366,29 @@ class _DeviceOperator:
             if A.dtype in (np.float32, np.float64):
                 import threading
                 box = {}
+                # its own stream, so that the copies run beside the locality
+                # order's kernels instead of queueing behind them
+                side = torch.cuda.Stream(device=dev)
 
                 def _values():
                     try:
-                        box["data"] = to_device(A.data, dev)
+                        with torch.cuda.stream(side):
+                            box["data"] = to_device(A.data, dev)
                     except BaseException as exc:  # re-raised on join
                         box["error"] = exc
                 upload = (threading.Thread(target=_values, daemon=True), box)
                 upload[0].start()
         try:
             base = locality_order(A, reorder, device_pattern=pattern)
+            # the values' upload overlaps the locality order (mostly device
+            # work); it ends before the host orders below, whose threads it
+            # would otherwise compete with
+            if upload is not None:
+                upload[0].join()
+                main = torch.cuda.current_stream(dev)
+                main.wait_stream(side)
+                if "data" in upload[1]:
+                    upload[1]["data"].record_stream(main)
             blocks = blocks_wanted(blocks, A)
             self.group_rows = None
             if blocks and aggregate and group_rows in ("auto", 16) and \
