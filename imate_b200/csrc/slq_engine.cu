@@ -117,6 +117,19 @@ inline int next_pow2(int x)
 
 inline size_t dsize(int dtype) { return dtype == SLQ_F64 ? 8 : 4; }
 
+// A small read of device memory into pageable host memory, issued once the
+// stream's work has finished.  A pageable read queued behind running kernels
+// holds the calling thread in the driver until they end, and another host
+// thread's page-locked upload (the values' upload beside the operator's
+// set-up) was measured waiting behind it for the kernels' whole duration.
+inline cudaError_t read_back(void* host, const void* dev, size_t bytes, cudaStream_t st)
+{
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e;
+}
+
 // Per-kernel event timing (slq_profile_begin / slq_profile_end).
 struct ProfRecord {
     int kind;
@@ -416,8 +429,7 @@ slq_status permute_csr(const int32_t* ptr, const int32_t* ind, const void* data,
     k_perm_deg<<<grid, 256, 0, st>>>(ptr, perm, n, t->deg, t->flag);
     SLQ_LAUNCH_CK();
     int32_t maxdeg = 0;
-    SLQ_CK(cudaMemcpyAsync(&maxdeg, t->flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    SLQ_CK(cudaStreamSynchronize(st));
+    SLQ_CK(read_back(&maxdeg, t->flag, sizeof(int32_t), st));
     if (maxdeg <= PERM_ROW_MAX)
     {
         size_t tb = t->temp_bytes;
@@ -600,8 +612,7 @@ extern "C" slq_status slq_operator_create(const void* data, const int32_t* indic
         k_check_csr<<<sms * 4, 256, 0, st>>>(indptr, indices, srows, scols, nnz, flag);
         SLQ_LAUNCH_CK();
         int32_t h = 0;
-        SLQ_CK(cudaMemcpyAsync(&h, flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-        SLQ_CK(cudaStreamSynchronize(st));
+        SLQ_CK(read_back(&h, flag, sizeof(int32_t), st));
         if (h & 1) return fail(SLQ_ERR_BAD_CSR, "index pointer must start at 0 and end at nnz");
         if (h & 2) return fail(SLQ_ERR_BAD_CSR, "index pointer must be non-decreasing");
         if (h & 4) return fail(SLQ_ERR_BAD_CSR, "index out of range");
@@ -816,8 +827,7 @@ slq_status blk_prepare(const int32_t* ptr, const int32_t* ind, int64_t R, int64_
     if (e != cudaSuccess)
         return fail(SLQ_ERR_CUDA, std::string("cub scan (blocks): ") + cudaGetErrorString(e));
     int32_t total = 0;
-    SLQ_CK(cudaMemcpyAsync(&total, s->bstage + nblk, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    SLQ_CK(cudaStreamSynchronize(st));
+    SLQ_CK(read_back(&total, s->bstage + nblk, sizeof(int32_t), st));
     *stages = total;
     return SLQ_OK;
 }
@@ -1000,9 +1010,7 @@ extern "C" slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* s
     {
         // the kernel's slot order, balanced for this device's SM count
         std::vector<int32_t> hb(static_cast<size_t>(nblk + 1)), ho(static_cast<size_t>(nblk));
-        SLQ_CK(cudaMemcpyAsync(hb.data(), bf.bstage, sizeof(int32_t) * (nblk + 1),
-                               cudaMemcpyDeviceToHost, st));
-        SLQ_CK(cudaStreamSynchronize(st));
+        SLQ_CK(read_back(hb.data(), bf.bstage, sizeof(int32_t) * (nblk + 1), st));
         blk_balance(hb.data(), nblk, sms, ho.data());
         if (nblk > 0)
             SLQ_CK(cudaMemcpyAsync(bf.order, ho.data(), sizeof(int32_t) * nblk,
@@ -3233,8 +3241,7 @@ extern "C" slq_status slq_rcm_order_device(int64_t n, int64_t nnz, const int32_t
     k_rcm_init<<<grid, 256, 0, st>>>(indptr, n, B.degree, B.rows, B.pos, B.claim, B.flag + 3);
     SLQ_LAUNCH_CK();
     int32_t h[4] = {0, 0, 0, 0};
-    SLQ_CK(cudaMemcpyAsync(h, B.flag, sizeof(h), cudaMemcpyDeviceToHost, st));
-    SLQ_CK(cudaStreamSynchronize(st));
+    SLQ_CK(read_back(h, B.flag, sizeof(h), st));
     if (h[0] & 1) return fail(SLQ_ERR_BAD_CSR, "rcm_order_device: index pointer must start at 0 and end at nnz");
     if (h[0] & 2) return fail(SLQ_ERR_BAD_CSR, "rcm_order_device: index pointer must be non-decreasing");
     if (h[0] & 4) return fail(SLQ_ERR_BAD_CSR, "rcm_order_device: index out of range");
@@ -3285,10 +3292,8 @@ extern "C" slq_status slq_rcm_order_device(int64_t n, int64_t nnz, const int32_t
                                                dim3(sms), dim3(threads), args, smem, st));
             int32_t herr = 0;
             RcmCoopState hs{};
-            SLQ_CK(cudaMemcpyAsync(&herr, B.coop_err, sizeof(int32_t), cudaMemcpyDeviceToHost,
-                                   st));
-            SLQ_CK(cudaMemcpyAsync(&hs, B.coop, sizeof(hs), cudaMemcpyDeviceToHost, st));
-            SLQ_CK(cudaStreamSynchronize(st));
+            SLQ_CK(read_back(&herr, B.coop_err, sizeof(int32_t), st));
+            SLQ_CK(read_back(&hs, B.coop, sizeof(hs), st));
             if (herr & 64) return SLQ_OK;  // more components than asked for: *done stays 0
             if (herr & 16)
                 return fail(SLQ_ERR_TIMEOUT, "rcm_order_device: a grid barrier wait ran out");
@@ -3313,8 +3318,7 @@ extern "C" slq_status slq_rcm_order_device(int64_t n, int64_t nnz, const int32_t
         k_rcm_start<<<1, 1, 0, st>>>(B.by_degree, B.flag + 2, B.pos, B.out, cnt, n);
         SLQ_LAUNCH_CK();
         int32_t first = 0;
-        SLQ_CK(cudaMemcpyAsync(&first, B.flag + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-        SLQ_CK(cudaStreamSynchronize(st));
+        SLQ_CK(read_back(&first, B.flag + 2, sizeof(int32_t), st));
         if (first >= n) return fail(SLQ_ERR_CUDA, "rcm_order_device: lost track of the visited rows");
         cursor = first + 1;
         int64_t lb = cnt, le = cnt + 1;
@@ -3332,8 +3336,7 @@ extern "C" slq_status slq_rcm_order_device(int64_t n, int64_t nnz, const int32_t
                                                    B.claim, nb, db, B.keys, B.flag + 1);
             SLQ_LAUNCH_CK();
             int32_t m = 0;
-            SLQ_CK(cudaMemcpyAsync(&m, B.flag + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-            SLQ_CK(cudaStreamSynchronize(st));
+            SLQ_CK(read_back(&m, B.flag + 1, sizeof(int32_t), st));
             if (m < 0 || cnt + m > n)
                 return fail(SLQ_ERR_CUDA, "rcm_order_device: level count out of range");
             if (m > 0)

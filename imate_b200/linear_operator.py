@@ -11,6 +11,8 @@ workspace, with a deterministic device transpose.
 """
 
 import ctypes
+import os
+from concurrent import futures
 
 import numpy as np
 import scipy.sparse as sp
@@ -80,6 +82,33 @@ _STAGER = _Stager()
 _STAGE_MIN_BYTES = 4 << 20
 
 
+_SIDE_STREAMS = {}
+_UPLOADER = []
+# a forked child has none of the parent's threads
+os.register_at_fork(after_in_child=_UPLOADER.clear)
+
+
+def _uploader():
+    """The thread that uploads a matrix's values beside its set-up, kept for
+    the process: a thread started per matrix spent milliseconds bringing up
+    its own team of host copy threads on its first copy."""
+    if not _UPLOADER:
+        _UPLOADER.append(futures.ThreadPoolExecutor(
+            max_workers=1, thread_name_prefix="slq-upload"))
+    return _UPLOADER[0]
+
+
+def _side_stream(dev):
+    """One upload stream per device, kept for the process: the caching
+    allocator keeps its blocks per stream, so a stream made per call would
+    take fresh device memory for every upload."""
+    import torch
+    s = _SIDE_STREAMS.get(dev.index)
+    if s is None:
+        s = _SIDE_STREAMS[dev.index] = torch.cuda.Stream(device=dev)
+    return s
+
+
 def to_device(arr, dev, dtype=None):
     """A host array as a tensor on CUDA device ``dev``: small arrays by a
     plain copy, large ones through the page-locked staging ring (about five
@@ -113,7 +142,7 @@ def order_spread(A, perm=None, sample_rows=20000):
     return float(out.value)
 
 
-def locality_order(A, reorder="auto", device_pattern=None):
+def locality_order(A, reorder="auto", device_pattern=None, spread=None):
     """Reverse Cuthill-McKee order (``rcm_order``) of a square sparse matrix,
     or None.
 
@@ -124,6 +153,8 @@ def locality_order(A, reorder="auto", device_pattern=None):
     square matrix, False never.  ``device_pattern`` = (indptr, indices), A's
     CSR arrays as int32 CUDA tensors, computes the order on the device
     (``rcm_order_device``; the host computes it when that declines).
+    ``spread``, if given, is ``order_spread(A, sample_rows=4096)``, already
+    computed by the caller.
     """
     if reorder is False or A.shape[0] != A.shape[1]:
         return None
@@ -132,7 +163,8 @@ def locality_order(A, reorder="auto", device_pattern=None):
     if reorder == "auto":
         if n < 16384 or A.nnz == 0:
             return None
-        spread = order_spread(A, sample_rows=4096)
+        if spread is None:
+            spread = order_spread(A, sample_rows=4096)
         if spread <= 256.0:
             return None
     perm = None
@@ -355,40 +387,42 @@ class _DeviceOperator:
                  A.nnz <= np.iinfo(np.int32).max)
         pattern = None
         upload = None
+        spread = None
+        if early and reorder == "auto" and A.shape[0] >= 16384 and A.nnz:
+            # the natural order's spread, before the uploads below compete
+            # with it for the host cores
+            spread = order_spread(A, sample_rows=4096)
         if early:
             # canonical CSR goes to the device as it is: upload the pattern
             # first, so that the locality order is computed there, and the
             # values on a helper thread while the host aggregates (both
             # release the GIL)
-            self.indices = to_device(A.indices, dev, np.int32)
+            # (the small index pointer first: a plain copy waits for the
+            # stream's earlier copies)
             self.indptr = to_device(A.indptr, dev, np.int32)
+            self.indices = to_device(A.indices, dev, np.int32)
             pattern = (self.indptr, self.indices)
             if A.dtype in (np.float32, np.float64):
-                import threading
-                box = {}
                 # its own stream, so that the copies run beside the locality
                 # order's kernels instead of queueing behind them
-                side = torch.cuda.Stream(device=dev)
+                side = _side_stream(dev)
 
                 def _values():
-                    try:
-                        with torch.cuda.stream(side):
-                            box["data"] = to_device(A.data, dev)
-                    except BaseException as exc:  # re-raised on join
-                        box["error"] = exc
-                upload = (threading.Thread(target=_values, daemon=True), box)
-                upload[0].start()
+                    with torch.cuda.stream(side):
+                        return to_device(A.data, dev)
+                upload = _uploader().submit(_values)
         try:
-            base = locality_order(A, reorder, device_pattern=pattern)
+            base = locality_order(A, reorder, device_pattern=pattern,
+                                  spread=spread)
             # the values' upload overlaps the locality order (mostly device
             # work); it ends before the host orders below, whose threads it
             # would otherwise compete with
             if upload is not None:
-                upload[0].join()
+                futures.wait([upload])
                 main = torch.cuda.current_stream(dev)
                 main.wait_stream(side)
-                if "data" in upload[1]:
-                    upload[1]["data"].record_stream(main)
+                if upload.exception() is None:
+                    upload.result().record_stream(main)
             blocks = blocks_wanted(blocks, A)
             self.group_rows = None
             if blocks and aggregate and group_rows in ("auto", 16) and \
@@ -411,9 +445,9 @@ class _DeviceOperator:
                     perm = block_order(A, perm, 16, 8)
         finally:
             if upload is not None:
-                upload[0].join()
-        if upload is not None and "error" in upload[1]:
-            raise upload[1]["error"]
+                futures.wait([upload])
+        if upload is not None and upload.exception() is not None:
+            raise upload.exception()
         if perm is not None and A.format != "csr":
             A = A.tocsr()
         fmt = _lib.SLQ_CSC if A.format == "csc" else _lib.SLQ_CSR
@@ -431,8 +465,8 @@ class _DeviceOperator:
         if max(A.shape) > np.iinfo(np.int32).max or \
                 self.nnz > np.iinfo(np.int32).max:
             raise ValueError("matrix too large for 32-bit indices")
-        if upload is not None and "data" in upload[1] and A.format == "csr":
-            self.data = upload[1]["data"]
+        if upload is not None and A.format == "csr":
+            self.data = upload.result()
         else:
             self.data = to_device(A.data, dev)
         if not early:
