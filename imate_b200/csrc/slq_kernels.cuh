@@ -738,11 +738,85 @@ __global__ void k_perm_deg(const int32_t* __restrict__ indptr, const int32_t* __
 
 // Rows of B = P A P^T, one warp per row i of B (A's row perm[i], at most
 // PERM_ROW_MAX entries): the entries relabelled (column inv[c]) and sorted by
-// (new column, position in the row) with a bitonic network in the warp's
-// shared-memory slice -- the order a stable sort of (row, column) keys
-// gives, so B is the same bit for bit.
+// (new column, position in the row) with a bitonic network held in the
+// warp's registers -- the order a stable sort of (row, column) keys gives,
+// so B is the same bit for bit.  Key t of the row sits in lane t % 32,
+// register t / 32: exchanges across lanes are shuffles, those across
+// registers stay in the lane, and the loads and stores are coalesced.  Each
+// row runs the smallest network (32, 64, ..., 1024 keys) that holds it.
 constexpr int PERM_ROW_MAX = 1024;
-constexpr int PERM_WARPS = 4;
+constexpr int PERM_WARPS = 8;
+
+// Bitonic sort of the warp's 32 * KPL keys into increasing order.
+template <int KPL>
+__device__ __forceinline__ void warp_bitonic(uint64_t (&a)[KPL], int lane)
+{
+    constexpr int M = 32 * KPL;
+#pragma unroll
+    for (int k = 2; k <= M; k <<= 1)
+    {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1)
+        {
+            if (j >= 32)
+            {
+                const int jr = j >> 5;
+#pragma unroll
+                for (int r = 0; r < KPL; ++r)
+                {
+                    if (r & jr) continue;
+                    const bool up = ((((r << 5) | lane) & k) == 0);
+                    const uint64_t x = a[r], y = a[r | jr];
+                    const bool sw = (x > y) == up;
+                    a[r] = sw ? y : x;
+                    a[r | jr] = sw ? x : y;
+                }
+            }
+            else
+            {
+                const bool lower = (lane & j) == 0;
+#pragma unroll
+                for (int r = 0; r < KPL; ++r)
+                {
+                    const uint64_t y = __shfl_xor_sync(0xffffffffu, a[r], j);
+                    const bool up = ((((r << 5) | lane) & k) == 0);
+                    const uint64_t lo = a[r] < y ? a[r] : y;
+                    const uint64_t hi = a[r] < y ? y : a[r];
+                    a[r] = (up == lower) ? lo : hi;
+                }
+            }
+        }
+    }
+}
+
+template <typename VT, int KPL>
+__device__ __forceinline__ void perm_row(const int32_t* __restrict__ indices,
+                                         const VT* __restrict__ data,
+                                         const int32_t* __restrict__ inv, int32_t e0, int len,
+                                         int64_t o, int lane, int32_t* __restrict__ p_ind,
+                                         VT* __restrict__ p_data)
+{
+    uint64_t a[KPL];
+#pragma unroll
+    for (int r = 0; r < KPL; ++r)
+    {
+        const int t = (r << 5) | lane;
+        a[r] = t < len ? (static_cast<uint64_t>(static_cast<uint32_t>(inv[indices[e0 + t]])) << 32) |
+                             static_cast<uint32_t>(t)
+                       : ~uint64_t(0);
+    }
+    warp_bitonic<KPL>(a, lane);
+#pragma unroll
+    for (int r = 0; r < KPL; ++r)
+    {
+        const int t = (r << 5) | lane;
+        if (t < len)
+        {
+            p_ind[o + t] = static_cast<int32_t>(a[r] >> 32);
+            p_data[o + t] = data[e0 + static_cast<int32_t>(a[r] & 0xffffffffu)];
+        }
+    }
+}
 
 template <typename VT>
 __global__ void __launch_bounds__(PERM_WARPS * 32)
@@ -751,50 +825,24 @@ __global__ void __launch_bounds__(PERM_WARPS * 32)
                 const int32_t* __restrict__ inv, const int32_t* __restrict__ p_ptr, int64_t n,
                 int32_t* __restrict__ p_ind, VT* __restrict__ p_data)
 {
-    __shared__ uint64_t keys[PERM_WARPS][PERM_ROW_MAX];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
-    uint64_t* buf = keys[w];
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * PERM_WARPS + w; i < n;
          i += static_cast<int64_t>(gridDim.x) * PERM_WARPS)
     {
         const int32_t r = perm[i];
         const int32_t e0 = indptr[r];
         const int len = indptr[r + 1] - e0;
-        if (len <= 0) continue;
-        int m = 1;
-        while (m < len) m <<= 1;
-        for (int t = lane; t < m; t += 32)
-            buf[t] = t < len ? (static_cast<uint64_t>(static_cast<uint32_t>(inv[indices[e0 + t]])) << 32) |
-                                   static_cast<uint32_t>(t)
-                             : ~uint64_t(0);
-        __syncwarp();
-        for (int k = 2; k <= m; k <<= 1)
-            for (int j = k >> 1; j > 0; j >>= 1)
-            {
-                for (int t = lane; t < m; t += 32)
-                {
-                    const int u = t ^ j;
-                    if (u > t)
-                    {
-                        const uint64_t a = buf[t], b = buf[u];
-                        if ((a > b) == ((t & k) == 0))
-                        {
-                            buf[t] = b;
-                            buf[u] = a;
-                        }
-                    }
-                }
-                __syncwarp();
-            }
         const int64_t o = p_ptr[i];
-        for (int t = lane; t < len; t += 32)
-        {
-            const uint64_t key = buf[t];
-            p_ind[o + t] = static_cast<int32_t>(key >> 32);
-            p_data[o + t] = data[e0 + static_cast<int32_t>(key & 0xffffffffu)];
-        }
-        __syncwarp();
+        // len is the same in every lane: the branch is warp-uniform
+        if (len <= 0) continue;
+        if (len <= 32) perm_row<VT, 1>(indices, data, inv, e0, len, o, lane, p_ind, p_data);
+        else if (len <= 64) perm_row<VT, 2>(indices, data, inv, e0, len, o, lane, p_ind, p_data);
+        else if (len <= 128) perm_row<VT, 4>(indices, data, inv, e0, len, o, lane, p_ind, p_data);
+        else if (len <= 256) perm_row<VT, 8>(indices, data, inv, e0, len, o, lane, p_ind, p_data);
+        else if (len <= 512) perm_row<VT, 16>(indices, data, inv, e0, len, o, lane, p_ind, p_data);
+        else if (len <= PERM_ROW_MAX)
+            perm_row<VT, 32>(indices, data, inv, e0, len, o, lane, p_ind, p_data);
     }
 }
 

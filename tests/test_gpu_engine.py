@@ -319,6 +319,52 @@ def test_reordered_operator_products(cuda):
     assert np.max(np.abs(y - want)) < 1e-12 * np.max(np.abs(want))
 
 
+def _spread_rows_matrix(n, longest, seed):
+    """Symmetric sparse matrix whose row lengths run from a few entries to
+    about ``longest`` (every size of the device permutation's per-row
+    sorting network)."""
+    rng = np.random.default_rng(seed)
+    rows, cols = [], []
+    for i in range(n):
+        k = int(rng.integers(1, 40)) if i % 50 else int(rng.integers(40, longest))
+        c = rng.choice(n, size=k, replace=False)
+        rows.append(np.full(k, i))
+        cols.append(c)
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    S = sp.csr_matrix((rng.uniform(0.1, 1.0, r.size), (r, c)), shape=(n, n))
+    A = (S + S.T + sp.identity(n) * (2.0 * longest)).tocsr()
+    A.sort_indices()
+    return A
+
+
+@pytest.mark.parametrize("longest", [900, 1400])
+def test_device_permutation_equals_host_permuted_csr(cuda, longest):
+    # rows of up to 1,024 entries are sorted one warp per row, longer
+    # patterns by one radix sort of (row, column) keys: either way the
+    # operator holds A[p][:, p] with sorted rows, so its products equal
+    # those of the host-permuted matrix bit for bit
+    A = _spread_rows_matrix(3000, longest, 11)
+    deg = np.diff(A.indptr)
+    assert deg.min() >= 1 and (deg.max() > 1024) == (longest > 1024)
+    # rows for every network size: 32, 64, ..., 1,024 keys
+    assert {int(np.ceil(np.log2(max(d, 32) / 32))) for d in deg if d <= 1024} \
+        == {0, 1, 2, 3, 4, 5}
+    M = ib.Matrix(A, reorder=True, group_rows=8)
+    op = M.get_device_operator()
+    assert op.perm is not None
+    p = op.perm.cpu().numpy().astype(np.int64)
+    Ap = A[p][:, p].tocsr()
+    Ap.sort_indices()
+    H = ib.Matrix(Ap, reorder=False, group_rows=8, aggregate=False)
+    oph = H.get_device_operator()
+    assert oph.perm is None and oph.group_rows == op.group_rows
+    x = np.random.default_rng(2).standard_normal((3000, 5))
+    y = _dot(op, x)
+    yh = _dot(oph, x[p])
+    assert np.array_equal(y[p], yh)
+
+
 @pytest.mark.parametrize("orth", [0, -1])
 def test_reordered_lanczos_matches_reference(cuda, golden, corr_small, orth):
     # a symmetric permutation changes only summation order
