@@ -18,7 +18,7 @@ STATUS_NAMES = {
     5: "NAN", 6: "EIGEN", 7: "UNSUPPORTED", 8: "TIMEOUT",
 }
 SLQ_F32, SLQ_F64 = 0, 1
-ABI_VERSION = 4
+ABI_VERSION = 5
 # per-probe status bits (slq_result.probe_status)
 PROBE_NONFINITE, PROBE_EIGEN, PROBE_NODE, PROBE_SAMPLE = 1, 2, 4, 8
 SLQ_CSR, SLQ_CSC = 0, 1
@@ -47,6 +47,7 @@ EXPORTS = (
     "slq_dense_operator_workspace_bytes", "slq_dense_operator_create",
     "slq_operator_blocks_scratch_bytes", "slq_operator_blocks_bytes",
     "slq_operator_add_blocks", "slq_debug_fail_stream_waits",
+    "slq_debug_blocks_sorted_keys",
 )
 TUNE_MAX_CANDIDATES = 16
 SPMM_KINDS = ("csr", "row-group", "row-group-tma", "row-group-tc", "block-tc")
@@ -205,6 +206,7 @@ def _declare(lib):
         "slq_operator_blocks_bytes": (i32, [vp, i32, vp, sz, vp, psz]),
         "slq_operator_add_blocks": (i32, [vp, i32, vp, sz, vp, sz, vp]),
         "slq_debug_fail_stream_waits": (i32, [i32]),
+        "slq_debug_blocks_sorted_keys": (i32, [i32]),
         "slq_tc_selftest_mn": (i32, [vp, vp, vp, i32, vp, vp]),
     }
     for name, (res, args) in sig.items():

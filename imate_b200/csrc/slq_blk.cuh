@@ -133,6 +133,232 @@ __global__ void k_blk_keys(const int32_t* __restrict__ ptr, const int32_t* __res
     }
 }
 
+// Block unions by bitmap.  A block's rows are consecutive CSR rows, so its
+// entries are one range of the index array; its union columns are the set
+// bits of a bitmap over its column range [lo, hi] in shared memory, in
+// increasing column order: the order the sorted (block, column) keys give,
+// so both ways build the same format.  A block whose columns span more than
+// BLK_UNION_SPAN sets *wide and the build takes the sorted-key path.  One
+// CTA of BLK_UNION_THREADS threads per block.
+constexpr int BLK_UNION_WORDS = 8192;  // 32 KB of bits: spans of up to 262,144 columns
+constexpr int64_t BLK_UNION_SPAN = int64_t(BLK_UNION_WORDS) * 32;
+constexpr int BLK_UNION_THREADS = 256;
+constexpr int BLK_UNION_GROUPS = BLK_UNION_WORDS / 8;  // prefix counts per 8 words
+
+struct BlkUnionSmem {
+    uint32_t bits[BLK_UNION_WORDS];
+    int32_t pre8[BLK_UNION_GROUPS];  // set bits in words [0, 8 g)
+    int32_t red[2 * (BLK_UNION_THREADS / 32) + 2];
+};
+
+// the block's smallest and largest column (hi = -1 for an empty block);
+// every thread of the CTA receives both
+__device__ __forceinline__ void blk_col_range(const int32_t* __restrict__ ind, int64_t e0,
+                                              int64_t e1, BlkUnionSmem& sm, int32_t& lo,
+                                              int32_t& hi)
+{
+    constexpr int NW = BLK_UNION_THREADS / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int32_t l = INT_MAX, h = -1;
+    for (int64_t e = e0 + threadIdx.x; e < e1; e += BLK_UNION_THREADS)
+    {
+        const int32_t c = ind[e];
+        l = min(l, c);
+        h = max(h, c);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        l = min(l, __shfl_xor_sync(FULL_MASK, l, off));
+        h = max(h, __shfl_xor_sync(FULL_MASK, h, off));
+    }
+    if (lane == 0)
+    {
+        sm.red[w] = l;
+        sm.red[NW + w] = h;
+    }
+    __syncthreads();
+    if (w == 0)
+    {
+        l = lane < NW ? sm.red[lane] : INT_MAX;
+        h = lane < NW ? sm.red[NW + lane] : -1;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            l = min(l, __shfl_xor_sync(FULL_MASK, l, off));
+            h = max(h, __shfl_xor_sync(FULL_MASK, h, off));
+        }
+        if (lane == 0)
+        {
+            sm.red[2 * NW] = l;
+            sm.red[2 * NW + 1] = h;
+        }
+    }
+    __syncthreads();
+    lo = sm.red[2 * NW];
+    hi = sm.red[2 * NW + 1];
+    __syncthreads();  // red is written again by the caller
+}
+
+// the block's bitmap over `words` words from column lo
+__device__ __forceinline__ void blk_bitmap(const int32_t* __restrict__ ind, int64_t e0, int64_t e1,
+                                           int32_t lo, int words, BlkUnionSmem& sm)
+{
+    for (int w = threadIdx.x; w < words; w += BLK_UNION_THREADS) sm.bits[w] = 0u;
+    __syncthreads();
+    for (int64_t e = e0 + threadIdx.x; e < e1; e += BLK_UNION_THREADS)
+    {
+        const uint32_t off = static_cast<uint32_t>(ind[e] - lo);
+        atomicOr(&sm.bits[off >> 5], 1u << (off & 31));
+    }
+    __syncthreads();
+}
+
+// cnt[b] = union size of block b; *wide = 1 if a block spans too many
+// columns (cnt is then rebuilt by the sorted-key path)
+__global__ void __launch_bounds__(BLK_UNION_THREADS)
+    k_blk_ucount(const int32_t* __restrict__ ptr, const int32_t* __restrict__ ind, int64_t rows,
+                 int64_t nblk, int32_t* __restrict__ cnt, int32_t* __restrict__ wide)
+{
+    __shared__ BlkUnionSmem sm;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int64_t b = blockIdx.x; b < nblk; b += gridDim.x)
+    {
+        const int64_t r0 = b * BLK_ROWS, r1 = min(rows, r0 + BLK_ROWS);
+        const int64_t e0 = ptr[r0], e1 = ptr[r1];
+        int32_t lo, hi;
+        blk_col_range(ind, e0, e1, sm, lo, hi);
+        const int64_t span = hi < 0 ? 0 : int64_t(hi) - lo + 1;  // the same in every thread
+        if (span == 0 || span > BLK_UNION_SPAN)
+        {
+            if (threadIdx.x == 0)
+            {
+                cnt[b] = 0;
+                if (span > BLK_UNION_SPAN) atomicOr(wide, 1);
+            }
+            continue;
+        }
+        const int words = static_cast<int>((span + 31) >> 5);
+        blk_bitmap(ind, e0, e1, lo, words, sm);
+        int32_t c = 0;
+        for (int k = threadIdx.x; k < words; k += BLK_UNION_THREADS) c += __popc(sm.bits[k]);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(FULL_MASK, c, off);
+        if (lane == 0) sm.red[w] = c;
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            int32_t t = 0;
+            for (int k = 0; k < BLK_UNION_THREADS / 32; ++k) t += sm.red[k];
+            cnt[b] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// union index of the column at offset `off` from lo (bits and pre8 built)
+__device__ __forceinline__ int32_t blk_union_index(const BlkUnionSmem& sm, uint32_t off)
+{
+    const int wd = static_cast<int>(off >> 5);
+    int32_t u = sm.pre8[wd >> 3];
+    for (int k = wd & ~7; k < wd; ++k) u += __popc(sm.bits[k]);
+    return u + __popc(sm.bits[wd] & ((1u << (off & 31)) - 1u));
+}
+
+// Per block (spans checked by k_blk_ucount): its union columns into ucol
+// from stage bstage[b], the last stage padded with copies of the largest
+// union column (0 for an empty block), and its values into the zeroed FP32
+// staging images tmp[stage][128][16] (atomic adds only sum duplicate
+// (row, column) entries).  One warp per row for the values.
+__global__ void __launch_bounds__(BLK_UNION_THREADS)
+    k_blk_ufill(const int32_t* __restrict__ ptr, const int32_t* __restrict__ ind,
+                const float* __restrict__ vals, int64_t rows, int64_t nblk,
+                const int32_t* __restrict__ bstage, int32_t* __restrict__ ucol,
+                float* __restrict__ tmp)
+{
+    __shared__ BlkUnionSmem sm;
+    constexpr int NW = BLK_UNION_THREADS / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int64_t b = blockIdx.x; b < nblk; b += gridDim.x)
+    {
+        const int64_t r0 = b * BLK_ROWS, r1 = min(rows, r0 + BLK_ROWS);
+        const int64_t e0 = ptr[r0], e1 = ptr[r1];
+        const int64_t base = static_cast<int64_t>(bstage[b]) * BLK_BK;
+        const int64_t end = static_cast<int64_t>(bstage[b + 1]) * BLK_BK;
+        int32_t lo, hi;
+        blk_col_range(ind, e0, e1, sm, lo, hi);
+        if (hi < 0)
+        {
+            for (int64_t j = base + threadIdx.x; j < end; j += BLK_UNION_THREADS) ucol[j] = 0;
+            continue;
+        }
+        const int64_t span = int64_t(hi) - lo + 1;
+        if (span > BLK_UNION_SPAN) continue;  // k_blk_ucount flagged it: not this path
+        const int words = static_cast<int>((span + 31) >> 5);
+        blk_bitmap(ind, e0, e1, lo, words, sm);
+        // prefix counts per 8 words: each thread sums whole groups, then one
+        // exclusive scan over the threads' totals
+        const int groups = (words + 7) >> 3;
+        const int per = (groups + BLK_UNION_THREADS - 1) / BLK_UNION_THREADS;
+        const int g0 = min(groups, static_cast<int>(threadIdx.x) * per);
+        const int g1 = min(groups, g0 + per);
+        int32_t t = 0;
+        for (int g = g0; g < g1; ++g)
+        {
+            int32_t s8 = 0;
+            for (int k = g * 8; k < min(words, g * 8 + 8); ++k) s8 += __popc(sm.bits[k]);
+            sm.pre8[g] = s8;  // group total for now
+            t += s8;
+        }
+        int32_t incl = t;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1)
+        {
+            const int32_t v = __shfl_up_sync(FULL_MASK, incl, off);
+            if (lane >= off) incl += v;
+        }
+        if (lane == 31) sm.red[w] = incl;
+        __syncthreads();
+        int32_t before = incl - t;
+        for (int k = 0; k < w; ++k) before += sm.red[k];
+        for (int g = g0; g < g1; ++g)
+        {
+            const int32_t s8 = sm.pre8[g];
+            sm.pre8[g] = before;
+            before += s8;
+        }
+        __syncthreads();
+        int32_t total = 0;  // the block's union size
+        for (int k = 0; k < NW; ++k) total += sm.red[k];
+        // union columns in increasing order, then the last stage's padding
+        for (int k = threadIdx.x; k < words; k += BLK_UNION_THREADS)
+        {
+            uint32_t m = sm.bits[k];
+            if (!m) continue;
+            int32_t u = blk_union_index(sm, static_cast<uint32_t>(k) << 5);
+            while (m)
+            {
+                const int bit = __ffs(m) - 1;
+                ucol[base + u++] = lo + k * 32 + bit;
+                m &= m - 1u;
+            }
+        }
+        for (int64_t j = base + total + threadIdx.x; j < end; j += BLK_UNION_THREADS) ucol[j] = hi;
+        // values
+        for (int64_t row = r0 + w; row < r1; row += NW)
+        {
+            const int rr = static_cast<int>(row & (BLK_ROWS - 1));
+            for (int64_t e = ptr[row] + lane; e < ptr[row + 1]; e += 32)
+            {
+                const int32_t u = blk_union_index(sm, static_cast<uint32_t>(ind[e] - lo));
+                const int64_t stage = bstage[b] + u / BLK_BK;
+                atomicAdd(&tmp[(stage * BLK_ROWS + rr) * BLK_BK + u % BLK_BK], vals[e]);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // flags[i] = 1 where sorted key i starts a new (block, column) pair
 __global__ void k_blk_flags(const uint64_t* __restrict__ keys, int64_t nnz,
                             int32_t* __restrict__ flags)

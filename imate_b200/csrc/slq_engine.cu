@@ -93,6 +93,9 @@ int g_num_sms = 0;
 // test hook (slq_debug_fail_stream_waits): streaming launches left whose
 // first wait is to run out at once
 std::atomic<int> g_fail_stream_waits{0};
+// test hook (slq_debug_blocks_sorted_keys): build block unions by sorting
+// (block, column) keys even where the bitmap path applies
+std::atomic<int> g_blk_sorted_keys{0};
 
 slq_status device_sms(int* sms)
 {
@@ -280,6 +283,7 @@ struct slq_op {
     // slq_operator_add_blocks on the same scratch does not sort again
     const void* blk_prep_scratch[2] = {nullptr, nullptr};
     int64_t blk_prep_stages[2] = {0, 0};
+    bool blk_prep_bitmap[2] = {false, false};
     // autotuned SpMM candidate per direction and log2(block width); -1 = built-in
     int8_t tuned[2][11];
     slq_op()
@@ -779,10 +783,12 @@ slq_status blk_scratch_layout(Carver& c, int64_t rows, int64_t nnz, BlkScratch* 
     return SLQ_OK;
 }
 
-// Sorted (block, column) keys, union sizes and first stages of an R x C CSR
-// matrix in the scratch; *stages receives the total (host synchronisation).
+// Union sizes and first stages of the 128-row blocks of an R x C CSR
+// matrix in the scratch, by per-block bitmaps (*bitmap = true) or, where a
+// block's columns span too far, by sorted (block, column) keys; *stages
+// receives the total (host synchronisation).
 slq_status blk_prepare(const int32_t* ptr, const int32_t* ind, int64_t R, int64_t C, int64_t nnz,
-                       BlkScratch* s, cudaStream_t st, int64_t* stages)
+                       BlkScratch* s, cudaStream_t st, int64_t* stages, bool* bitmap)
 {
     int sms = 0;
     SLQ_TRY(device_sms(&sms));
@@ -791,7 +797,21 @@ slq_status blk_prepare(const int32_t* ptr, const int32_t* ind, int64_t R, int64_
     const int cbits = bits_for(std::max<int64_t>(C - 1, 1));
     const int bbits = bits_for(std::max<int64_t>(nblk - 1, 1));
     SLQ_CK(cudaMemsetAsync(s->cnt, 0, sizeof(int32_t) * (nblk + 1), st));
-    if (nnz > 0)
+    *bitmap = false;
+    if (nnz > 0 && nblk > 0 && g_blk_sorted_keys.load() == 0)
+    {
+        // the word that flags a block too wide for its bitmap (the flags
+        // array is free on this path)
+        SLQ_CK(cudaMemsetAsync(s->flags, 0, sizeof(int32_t), st));
+        k_blk_ucount<<<static_cast<int>(std::min<int64_t>(nblk, int64_t(sms) * 6)),
+                       BLK_UNION_THREADS, 0, st>>>(ptr, ind, R, nblk, s->cnt, s->flags);
+        SLQ_LAUNCH_CK();
+        int32_t wide = 0;
+        SLQ_CK(read_back(&wide, s->flags, sizeof(int32_t), st));
+        *bitmap = wide == 0;
+        if (!*bitmap) SLQ_CK(cudaMemsetAsync(s->cnt, 0, sizeof(int32_t) * (nblk + 1), st));
+    }
+    if (nnz > 0 && !*bitmap)
     {
         k_blk_keys<<<grid, 256, 0, st>>>(ptr, ind, R, cbits, s->keys_in, s->pos_in, s->rr);
         SLQ_LAUNCH_CK();
@@ -938,10 +958,13 @@ extern "C" slq_status slq_operator_blocks_bytes(const slq_op* op, int transpose,
     SLQ_TRY(blk_scratch_layout(c, R, op->nnz, &s));
     if (!scratch || !c.fits()) return fail(SLQ_ERR_WORKSPACE, "blocks: scratch too small");
     int64_t stages = 0;
-    SLQ_TRY(blk_prepare(ptr, ind, R, C, op->nnz, &s, static_cast<cudaStream_t>(stream), &stages));
+    bool bitmap = false;
+    SLQ_TRY(blk_prepare(ptr, ind, R, C, op->nnz, &s, static_cast<cudaStream_t>(stream), &stages,
+                        &bitmap));
     slq_op* mop = const_cast<slq_op*>(op);  // the preparation cache only
     mop->blk_prep_scratch[transpose] = scratch;
     mop->blk_prep_stages[transpose] = stages;
+    mop->blk_prep_bitmap[transpose] = bitmap;
     Carver f(nullptr, 0);
     BlkFormat bf;
     blk_format_layout(f, (R + BLK_ROWS - 1) / BLK_ROWS, stages, &bf);
@@ -963,10 +986,15 @@ extern "C" slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* s
     SLQ_TRY(blk_scratch_layout(c, R, op->nnz, &s));
     if (!scratch || !c.fits()) return fail(SLQ_ERR_WORKSPACE, "blocks: scratch too small");
     int64_t stages = 0;
+    bool bitmap = false;
     if (op->blk_prep_scratch[transpose] == scratch && scratch)
-        stages = op->blk_prep_stages[transpose];  // prepared by slq_operator_blocks_bytes
+    {
+        // prepared by slq_operator_blocks_bytes
+        stages = op->blk_prep_stages[transpose];
+        bitmap = op->blk_prep_bitmap[transpose];
+    }
     else
-        SLQ_TRY(blk_prepare(ptr, ind, R, C, op->nnz, &s, st, &stages));
+        SLQ_TRY(blk_prepare(ptr, ind, R, C, op->nnz, &s, st, &stages, &bitmap));
     op->blk_prep_scratch[transpose] = nullptr;
     const int64_t nblk = (R + BLK_ROWS - 1) / BLK_ROWS;
     Carver f(format, format_bytes);
@@ -985,21 +1013,32 @@ extern "C" slq_status slq_operator_add_blocks(slq_op* op, int transpose, void* s
     SLQ_CK(cudaMemsetAsync(bf.img, 0, sizeof(__half) * stages * BLK_IMG_STAGE, st));
     k_blk_rowscale<<<grid, 256, 0, st>>>(ptr, val, R, nblk * BLK_ROWS, s.fsc, bf.rsc);
     SLQ_LAUNCH_CK();
-    if (op->nnz > 0)
+    if (bitmap)
     {
-        k_blk_ucol<<<grid, 256, 0, st>>>(s.keys_out, s.flags, s.uidx, op->nnz, cbits, s.ufirst,
-                                         bf.bstage, bf.ucol);
+        // union columns, padding and values of each block from its bitmap
+        k_blk_ufill<<<static_cast<int>(std::min<int64_t>(nblk, int64_t(sms) * 6)),
+                      BLK_UNION_THREADS, 0, st>>>(ptr, ind, val, R, nblk, bf.bstage, bf.ucol,
+                                                  reinterpret_cast<float*>(bf.img));
         SLQ_LAUNCH_CK();
     }
-    k_blk_pad<<<std::max<int64_t>(1, std::min<int64_t>(grid, (nblk + 255) / 256)), 256, 0, st>>>(
-        s.cnt, bf.bstage, nblk, bf.ucol);
-    SLQ_LAUNCH_CK();
-    if (op->nnz > 0)
+    else
     {
-        k_blk_scatter<<<grid, 256, 0, st>>>(s.keys_out, s.pos_out, s.uidx, op->nnz, cbits,
-                                            s.ufirst, bf.bstage, val, s.rr,
-                                            reinterpret_cast<float*>(bf.img));
+        if (op->nnz > 0)
+        {
+            k_blk_ucol<<<grid, 256, 0, st>>>(s.keys_out, s.flags, s.uidx, op->nnz, cbits,
+                                             s.ufirst, bf.bstage, bf.ucol);
+            SLQ_LAUNCH_CK();
+        }
+        k_blk_pad<<<std::max<int64_t>(1, std::min<int64_t>(grid, (nblk + 255) / 256)), 256, 0,
+                    st>>>(s.cnt, bf.bstage, nblk, bf.ucol);
         SLQ_LAUNCH_CK();
+        if (op->nnz > 0)
+        {
+            k_blk_scatter<<<grid, 256, 0, st>>>(s.keys_out, s.pos_out, s.uidx, op->nnz, cbits,
+                                                s.ufirst, bf.bstage, val, s.rr,
+                                                reinterpret_cast<float*>(bf.img));
+            SLQ_LAUNCH_CK();
+        }
     }
     k_blk_split<<<std::max<int64_t>(1, std::min<int64_t>(stages, int64_t(sms) * 8)), 256, 0, st>>>(
         bf.img, bf.bstage, nblk, s.fsc, stages);
@@ -3752,6 +3791,13 @@ extern "C" slq_status slq_tc_selftest_mn(const float* a, const float* b, float* 
 }
 
 extern "C" int slq_abi_version(void) { return SLQ_ABI_VERSION; }
+
+extern "C" slq_status slq_debug_blocks_sorted_keys(int on)
+{
+    if (on != 0 && on != 1) return fail(SLQ_ERR_BAD_ARG, "debug_blocks_sorted_keys: on must be 0 or 1");
+    g_blk_sorted_keys.store(on);
+    return SLQ_OK;
+}
 
 extern "C" slq_status slq_debug_fail_stream_waits(int count)
 {

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define SLQ_ABI_VERSION 4
+#define SLQ_ABI_VERSION 5
 
 typedef enum {
     SLQ_OK = 0,
@@ -124,7 +124,9 @@ slq_status slq_operator_create(const void* data, const int32_t* indices,
  * order whose consecutive 128-row blocks share columns
  * (slq_block_group_order, slq_block_order).  Built on the device in two
  * calls on the same scratch: slq_operator_blocks_bytes prepares the scratch
- * (sorted keys, unions) and sizes the format (it synchronizes the stream);
+ * (the union sizes, from a bitmap of each block's columns in shared memory,
+ * or from sorted (block, column) keys where a block's columns span more
+ * than 262,144) and sizes the format (it synchronizes the stream);
  * slq_operator_add_blocks, given that scratch as it was left, builds the
  * format into `format` (caller memory that must outlive the operator) and
  * attaches it (given another scratch it prepares that one first); the
@@ -608,6 +610,13 @@ int slq_abi_version(void);
  * SLQ_ERR_TIMEOUT -- so the failure path can be exercised without a fault.
  * 0 switches it off. */
 slq_status slq_debug_fail_stream_waits(int count);
+
+/* Test hook (no counterpart in the reference): 1 builds the block format's
+ * union columns by sorting (block, column) keys, the path the build
+ * otherwise takes only for a block whose columns span more than 262,144;
+ * 0 (the default) lets it use per-block bitmaps.  Both give the same
+ * format. */
+slq_status slq_debug_blocks_sorted_keys(int on);
 
 #ifdef __cplusplus
 }

@@ -212,3 +212,60 @@ def test_block_candidate_listed_only_with_the_format(cuda):
     # float64 operators never get the block format
     M64 = ib.Matrix(A.astype(np.float64), blocks=True)
     assert not M64.get_device_operator().block_formats
+
+
+def _wide_matrix():
+    """n = 300,000, diagonal plus three entries that make block 0 reach from
+    column 0 to column n - 1: a span above the 262,144 columns of a block's
+    bitmap, so the build takes the sorted-key path."""
+    n = 300000
+    i = np.arange(n)
+    rows = np.r_[i, 0, 5, 127]
+    cols = np.r_[i, n - 1, n - 2, 200000]
+    vals = np.r_[1.0 + np.random.default_rng(4).random(n), 0.5, -0.25, 2.0]
+    return sp.csr_matrix((vals, (rows, cols)), shape=(n, n), dtype=np.float32)
+
+
+def _corr_matrix():
+    return ib.correlation_matrix(20000, scale=0.01, threshold=0.05, shift=0.1,
+                                 seed=2, dtype=np.float32)
+
+
+@pytest.mark.parametrize("case", ["ragged", "wide", "corr"])
+def test_block_unions_by_bitmap_equal_sorted_keys(cuda, case):
+    # the block format built from per-block column bitmaps (the default) is
+    # the one built from sorted (block, column) keys: same blocks and stages,
+    # products equal bit for bit in both directions
+    import torch
+    from imate_b200 import _lib
+    lib = _lib.load()
+    A = {"ragged": _ragged_matrix, "wide": _wide_matrix,
+         "corr": _corr_matrix}[case]()
+    opts = {} if case == "corr" else dict(reorder=False, group_rows=0)
+    X = torch.from_numpy(np.random.default_rng(5).standard_normal(
+        (A.shape[0], 128)).astype(np.float32)).cuda()
+    got = []
+    for sorted_keys in (1, 0):
+        _lib.check(lib.slq_debug_blocks_sorted_keys(sorted_keys))
+        try:
+            M = ib.Matrix(A, blocks=True, **opts)
+            op = M.get_device_operator(need_transpose=True)
+        finally:
+            _lib.check(lib.slq_debug_blocks_sorted_keys(0))
+        assert len(op.block_formats) == 2
+        got.append((op.blocks_info(False), op.blocks_info(True),
+                    op.dot(X).cpu().numpy(),
+                    op.dot(X, transpose=True).cpu().numpy()))
+    assert got[0][0] == got[1][0] and got[0][1] == got[1][1]
+    assert np.array_equal(got[0][2], got[1][2])
+    assert np.array_equal(got[0][3], got[1][3])
+    if case == "wide":
+        want = A.astype(np.float64) @ X.cpu().numpy().astype(np.float64)
+        assert np.max(np.abs(got[1][2] - want)) < 1e-5 * np.max(np.abs(want))
+
+
+def test_block_unions_hook_rejects_bad_values(cuda):
+    from imate_b200 import _lib
+    lib = _lib.load()
+    assert lib.slq_debug_blocks_sorted_keys(2) == 1  # bad argument
+    assert lib.slq_debug_blocks_sorted_keys(0) == 0
