@@ -150,10 +150,8 @@ inline void part_range(int64_t total, int t, int n, int64_t& begin, int64_t& end
     end = total * (t + 1) / n;
 }
 
-// indptr monotone from a non-negative start and every column index in
-// [0, n): the checks that make the host loops below safe
-bool valid_pattern(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices,
-                   const char* who)
+// indptr starts non-negative and never decreases
+bool valid_indptr(int64_t n, const int32_t* indptr, const char* who)
 {
     if (indptr[0] < 0)
     {
@@ -166,22 +164,44 @@ bool valid_pattern(Pool& P, int64_t n, const int32_t* indptr, const int32_t* ind
             slq::set_error(std::string(who) + ": indptr is not monotone");
             return false;
         }
+    return true;
+}
+
+// part t of nt of the check that every column index (of a pattern whose
+// indptr passed valid_indptr) lies in [0, n): one unsigned comparison per
+// index, or-ed without a branch so the loop vectorises (a negative index is
+// a large unsigned one); true if this part holds a bad one
+bool indices_out_of_range(int64_t n, const int32_t* indptr, const int32_t* indices, int t, int nt)
+{
     const int64_t e0 = indptr[0], e1 = indptr[n];
-    std::atomic<bool> bad(false);
-    // one unsigned comparison per index, or-ed without a branch so the loop
-    // vectorises (a negative index is a large unsigned one)
+    int64_t b, e;
+    part_range(e1 - e0, t, nt, b, e);
+    const uint32_t* ix = reinterpret_cast<const uint32_t*>(indices + e0);
     const uint32_t un = static_cast<uint32_t>(n);
+    uint32_t any = 0;
+    for (int64_t k = b; k < e; ++k) any |= static_cast<uint32_t>(ix[k] >= un);
+    return any != 0;
+}
+
+void set_range_error(const char* who)
+{
+    slq::set_error(std::string(who) + ": column index out of range");
+}
+
+// indptr monotone from a non-negative start and every column index in
+// [0, n): the checks that make the host loops below safe
+bool valid_pattern(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices,
+                   const char* who)
+{
+    if (!valid_indptr(n, indptr, who)) return false;
+    std::atomic<bool> bad(false);
     P.run([&](int t, int nt) {
-        int64_t b, e;
-        part_range(e1 - e0, t, nt, b, e);
-        const uint32_t* ix = reinterpret_cast<const uint32_t*>(indices + e0);
-        uint32_t any = 0;
-        for (int64_t k = b; k < e; ++k) any |= static_cast<uint32_t>(ix[k] >= un);
-        if (any) bad.store(true, std::memory_order_relaxed);
+        if (indices_out_of_range(n, indptr, indices, t, nt))
+            bad.store(true, std::memory_order_relaxed);
     });
     if (bad.load())
     {
-        slq::set_error(std::string(who) + ": column index out of range");
+        set_range_error(who);
         return false;
     }
     return true;
@@ -351,11 +371,14 @@ inline void prefetch_row(const int32_t* indptr, const int32_t* indices, const VT
 // A group's seed takes its `want` strongest placeable neighbours (selected
 // by strength_key), then theirs, and a group whose neighbourhood runs out is
 // filled with the next placeable rows of base positions k0 .. stop - 1.
+// A column index outside [0, n) is never placeable, so the sweep may run
+// before, or beside, the check of the whole pattern's indices.
 template <typename VT, typename Owner>
-void aggregate_sweep(const int32_t* indptr, const int32_t* indices, const VT* data, int G,
-                     const int32_t* base, int64_t k0, int64_t seed_stop, int64_t stop,
+void aggregate_sweep(int64_t n, const int32_t* indptr, const int32_t* indices, const VT* data,
+                     int G, const int32_t* base, int64_t k0, int64_t seed_stop, int64_t stop,
                      const Owner& own, Groups& out)
 {
+    const uint32_t un = static_cast<uint32_t>(n);
     const int step = 1;
     auto row_at = [&](int64_t k) { return base ? base[k] : static_cast<int32_t>(k); };
     auto mine = [&](int32_t r) { return own.mine(r); };
@@ -389,8 +412,9 @@ void aggregate_sweep(const int32_t* indptr, const int32_t* indices, const VT* da
                 for (int32_t e = e0; e < e1; ++e)
                 {
                     const int32_t c = indices[e];
+                    const bool in = static_cast<uint32_t>(c) < un;
                     keys[m] = strength_key(data ? static_cast<float>(data[e]) : 1.0f, c);
-                    m += mine(c) ? 1 : 0;
+                    m += (in && mine(in ? c : 0)) ? 1 : 0;
                 }
                 keys.resize(static_cast<size_t>(m));
                 if (m > want)
@@ -431,9 +455,16 @@ void aggregate_sweep(const int32_t* indptr, const int32_t* indices, const VT* da
 // threads in any assignment: the result does not depend on the number of
 // threads.  Groups are listed by their seeds' base positions, the short
 // groups at the segments' ends merged and put last.
+//
+// With `check`, the column indices of the whole pattern (whose indptr the
+// caller has checked) are checked too: on the pool threads beyond the K
+// sweeping ones, beside the sweeps, or before them when there are none.
+// Returns false (the error set, `order` unspecified) for an index outside
+// [0, n).
 template <typename VT>
-void aggregate(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices, const VT* data,
-               int G, const int32_t* base, const int32_t* base_pos, int32_t* order)
+bool aggregate(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices, const VT* data,
+               int G, const int32_t* base, const int32_t* base_pos, int32_t* order, bool check,
+               const char* who)
 {
     // state[r]: the sweep that owns unplaced row r (1 .. K), 0 once placed
     std::vector<std::atomic<uint8_t>> state(static_cast<size_t>(n));
@@ -449,16 +480,41 @@ void aggregate(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices
             state[r].store(static_cast<uint8_t>(1 + p / seg), std::memory_order_relaxed);
         }
     });
+    std::atomic<bool> bad(false);
+    const bool beside = check && P.size() > K;
+    if (check && !beside)
+    {
+        P.run([&](int t, int nt) {
+            if (indices_out_of_range(n, indptr, indices, t, nt))
+                bad.store(true, std::memory_order_relaxed);
+        });
+        if (bad.load())
+        {
+            set_range_error(who);
+            return false;
+        }
+    }
     P.run([&](int t, int nt) {
-        for (int s = t; s < K; s += nt)
+        if (beside && t >= K)
+        {
+            if (indices_out_of_range(n, indptr, indices, t - K, nt - K))
+                bad.store(true, std::memory_order_relaxed);
+            return;
+        }
+        for (int s = t; s < K; s += beside ? K : nt)
         {
             const int64_t k0 = std::min<int64_t>(n, s * seg);
             const int64_t k1 = std::min<int64_t>(n, k0 + seg);
-            aggregate_sweep<VT>(indptr, indices, data, G, base, k0, k1, k1,
+            aggregate_sweep<VT>(n, indptr, indices, data, G, base, k0, k1, k1,
                                 SweepOwner{state.data(), static_cast<uint8_t>(s + 1)},
                                 sweep[s]);
         }
     });
+    if (bad.load())
+    {
+        set_range_error(who);
+        return false;
+    }
     struct Ref {
         int64_t seed_pos;
         int s;
@@ -485,6 +541,7 @@ void aggregate(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices
     for (const Ref& rf : refs)
         for (int64_t i = rf.index * G; i < rf.index * G + G; ++i) order[out++] = sweep[rf.s].rows[i];
     for (int32_t r : tail) order[out++] = r;
+    return true;
 }
 
 // Rows of the block being split: the thread's own bit per matrix row (set
@@ -506,11 +563,12 @@ struct BlockOwner {
 // rows as the placeable ones.  Blocks run in parallel, each thread with its
 // own membership bits and index table.
 template <typename VT>
-void block_groups(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices,
+bool block_groups(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indices,
                   const VT* data, int B, int G, const int32_t* base, const int32_t* base_pos,
-                  int32_t* order)
+                  int32_t* order, const char* who)
 {
-    aggregate<VT>(P, n, indptr, indices, data, B, base, base_pos, order);
+    if (!aggregate<VT>(P, n, indptr, indices, data, B, base, base_pos, order, true, who))
+        return false;
     const int64_t nb = n / B;  // whole blocks; the rest stay last as they are
     P.run([&](int t, int nt) {
         int64_t b0, b1;
@@ -541,12 +599,13 @@ void block_groups(Pool& P, int64_t n, const int32_t* indptr, const int32_t* indi
             std::fill(placed.begin(), placed.end(), 0);
             g.rows.clear();
             g.seed_pos.clear();
-            aggregate_sweep<VT>(indptr, indices, data, G, rows.data(), 0, B, B,
+            aggregate_sweep<VT>(n, indptr, indices, data, G, rows.data(), 0, B, B,
                                 BlockOwner{member.data(), loc.get(), placed.data()}, g);
             std::copy(g.rows.begin(), g.rows.end(), blk);
             for (int i = 0; i < B; ++i) member[rows[i] >> 6] = 0;
         }
     });
+    return true;
 }
 
 }  // namespace
@@ -580,7 +639,7 @@ extern "C" slq_status slq_group_order(int64_t n, const int32_t* indptr, const in
     }
     std::lock_guard<std::mutex> lock(pool_mutex());
     Pool& P = shared_pool();
-    if (!valid_pattern(P, n, indptr, indices, "group_order")) return SLQ_ERR_BAD_CSR;
+    if (!valid_indptr(n, indptr, "group_order")) return SLQ_ERR_BAD_CSR;
     std::vector<int32_t> base_pos;
     if (base_order && !inverse_perm(n, base_order, base_pos))
     {
@@ -588,13 +647,14 @@ extern "C" slq_status slq_group_order(int64_t n, const int32_t* indptr, const in
         return SLQ_ERR_BAD_ARG;
     }
     const int32_t* bp = base_order ? base_pos.data() : nullptr;
-    if (dtype == SLQ_F64)
-        aggregate<double>(P, n, indptr, indices, static_cast<const double*>(data), group_rows,
-                          base_order, bp, order);
-    else
-        aggregate<float>(P, n, indptr, indices, static_cast<const float*>(data), group_rows,
-                         base_order, bp, order);
-    return SLQ_OK;
+    // the column indices are checked beside the sweeps
+    const bool ok =
+        dtype == SLQ_F64
+            ? aggregate<double>(P, n, indptr, indices, static_cast<const double*>(data),
+                                group_rows, base_order, bp, order, true, "group_order")
+            : aggregate<float>(P, n, indptr, indices, static_cast<const float*>(data),
+                               group_rows, base_order, bp, order, true, "group_order");
+    return ok ? SLQ_OK : SLQ_ERR_BAD_CSR;
 }
 
 extern "C" slq_status slq_block_group_order(int64_t n, const int32_t* indptr,
@@ -610,7 +670,7 @@ extern "C" slq_status slq_block_group_order(int64_t n, const int32_t* indptr,
     }
     std::lock_guard<std::mutex> lock(pool_mutex());
     Pool& P = shared_pool();
-    if (!valid_pattern(P, n, indptr, indices, "block_group_order")) return SLQ_ERR_BAD_CSR;
+    if (!valid_indptr(n, indptr, "block_group_order")) return SLQ_ERR_BAD_CSR;
     std::vector<int32_t> base_pos;
     if (base_order && !inverse_perm(n, base_order, base_pos))
     {
@@ -618,13 +678,16 @@ extern "C" slq_status slq_block_group_order(int64_t n, const int32_t* indptr,
         return SLQ_ERR_BAD_ARG;
     }
     const int32_t* bp = base_order ? base_pos.data() : nullptr;
-    if (dtype == SLQ_F64)
-        block_groups<double>(P, n, indptr, indices, static_cast<const double*>(data), block_rows,
-                             group_rows, base_order, bp, order);
-    else
-        block_groups<float>(P, n, indptr, indices, static_cast<const float*>(data), block_rows,
-                            group_rows, base_order, bp, order);
-    return SLQ_OK;
+    // the column indices are checked beside the block sweeps
+    const bool ok =
+        dtype == SLQ_F64
+            ? block_groups<double>(P, n, indptr, indices, static_cast<const double*>(data),
+                                   block_rows, group_rows, base_order, bp, order,
+                                   "block_group_order")
+            : block_groups<float>(P, n, indptr, indices, static_cast<const float*>(data),
+                                  block_rows, group_rows, base_order, bp, order,
+                                  "block_group_order");
+    return ok ? SLQ_OK : SLQ_ERR_BAD_CSR;
 }
 
 extern "C" slq_status slq_block_order(int64_t n, const int32_t* indptr, const int32_t* indices,
@@ -829,9 +892,11 @@ extern "C" slq_status slq_group_fill(int64_t n, const int32_t* indptr, const int
         int64_t b, e;
         part_range(m, t, nt, b, e);
         std::vector<int32_t> cols;
+        std::vector<uint64_t> seen;  // bitmap over a group's column range
         for (int64_t i = b; i < e; ++i)
         {
             cols.clear();
+            int32_t lo = INT32_MAX, hi = -1;
             for (int g = 0; g < G; ++g)
             {
                 const int64_t k = picks[i] * G + g;
@@ -841,12 +906,31 @@ extern "C" slq_status slq_group_fill(int64_t n, const int32_t* indptr, const int
                     bad.store(true, std::memory_order_relaxed);
                     return;
                 }
+                for (int32_t x = indptr[r]; x < indptr[r + 1]; ++x)
+                {
+                    lo = std::min(lo, indices[x]);
+                    hi = std::max(hi, indices[x]);
+                }
                 cols.insert(cols.end(), indices + indptr[r], indices + indptr[r + 1]);
             }
             if (cols.empty()) continue;
             const int64_t nnz = static_cast<int64_t>(cols.size());
-            std::sort(cols.begin(), cols.end());
-            const int64_t uni = std::unique(cols.begin(), cols.end()) - cols.begin();
+            // distinct columns: a bitmap over [lo, hi] when that is at most
+            // 64 bits per entry, else sorting
+            int64_t uni = 0;
+            const int64_t words = (static_cast<int64_t>(hi) - lo) / 64 + 1;
+            if (words <= nnz)
+            {
+                seen.assign(static_cast<size_t>(words), 0);
+                for (const int32_t c : cols)
+                    seen[static_cast<size_t>((c - lo) >> 6)] |= uint64_t(1) << ((c - lo) & 63);
+                for (const uint64_t w : seen) uni += __builtin_popcountll(w);
+            }
+            else
+            {
+                std::sort(cols.begin(), cols.end());
+                uni = std::unique(cols.begin(), cols.end()) - cols.begin();
+            }
             ratio[i] = static_cast<double>(nnz) / (static_cast<double>(G) * static_cast<double>(uni));
         }
     });
