@@ -784,9 +784,12 @@ k_spmm_blk(const BlkArgs d)
 
     if (warp == BLK_PRODUCER)
     {
-        // producer: the A parts of every stage, one 8 KB bulk copy each
+        // producer: the A parts of every stage, one 8 KB bulk copy each,
+        // read once per product: they leave L2 first, before the X rows
+        // that neighbouring blocks gather again
         if (lane == 0)
         {
+            const uint64_t a_policy = l2_evict_first_policy();
             int64_t it = 0;
             bool ok = true;
             for (int64_t slot = blockIdx.x; slot < d.nblk && ok; slot += gridDim.x)
@@ -805,8 +808,8 @@ k_spmm_blk(const BlkArgs d)
                     }
                     unsigned char* stp = base + static_cast<size_t>(s) * stage_bytes;
                     mbar_expect_tx(&full[s], static_cast<uint32_t>(2 * BLK_A_PART));
-                    bulk_copy_g2s(stp, d.img + int64_t(st) * BLK_IMG_STAGE, 2 * BLK_A_PART,
-                                  &full[s]);
+                    bulk_copy_g2s_hint(stp, d.img + int64_t(st) * BLK_IMG_STAGE, 2 * BLK_A_PART,
+                                       &full[s], a_policy);
                 }
             }
             // the copies in flight land before the CTA leaves
