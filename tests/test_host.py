@@ -459,3 +459,28 @@ def test_block_group_order_nests_groups_in_blocks(lib):
     assert whole <= n
     with pytest.raises(_lib.SlqError):
         block_group_order(A, base, 100, 16)  # not a multiple
+
+
+@pytest.mark.parametrize("bad_col", [-1, 40000, 2 ** 31 - 1])
+@pytest.mark.parametrize("where", ["first", "middle", "last"])
+def test_block_group_order_rejects_out_of_range_columns(lib, bad_col, where):
+    # the index check runs beside the aggregation sweeps (2 sweeps for
+    # n = 40000 leave the other pool threads to it) or before them; either
+    # way one bad column anywhere makes the call fail, and the sweeps never
+    # index with it
+    A = sp.csr_matrix(ib.correlation_matrix(40000, scale=0.01, threshold=0.05,
+                                            shift=0.1, seed=4,
+                                            dtype="float32"))
+    n = A.shape[0]
+    ip = np.ascontiguousarray(A.indptr, dtype=np.int32)
+    ind = np.ascontiguousarray(A.indices, dtype=np.int32).copy()
+    data = np.ascontiguousarray(A.data)
+    k = {"first": 0, "middle": ind.size // 2, "last": ind.size - 1}[where]
+    ind[k] = bad_col
+    out = np.empty(n, np.int32)
+    for fn, args in ((lib.slq_block_group_order, (128, 16)),
+                     (lib.slq_group_order, (16,))):
+        st = fn(n, ip.ctypes.data, ind.ctypes.data, data.ctypes.data,
+                _lib.SLQ_F32, *args, None, out.ctypes.data)
+        assert st == 2  # SLQ_ERR_BAD_CSR
+        assert b"out of range" in lib.slq_last_error()
