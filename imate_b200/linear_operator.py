@@ -295,6 +295,18 @@ def block_group_order(A, base_perm, block_rows=128, group_rows=16):
     return order
 
 
+def _fallback_order(A, base, group_rows, aggregate, blocks):
+    """(group rows, row order) from the sampled row-group statistics
+    (``group_rows_for``), the 16-row groups merged into 128-row blocks
+    (``block_order``) when the operator gets the block format."""
+    G, perm = group_rows_for(A, base, group_rows, aggregate=aggregate)
+    if blocks and G == 16 and perm is not None and A.shape[0] == A.shape[1]:
+        # 128-row blocks of eight 16-row groups whose column sets overlap
+        # (the groups stay whole, so the row-group format keeps its fill)
+        perm = block_order(A, perm, 16, 8)
+    return G, perm
+
+
 # blocks='auto' adds the tensor-core block format to float32 square
 # matrices of at least this order
 BLOCKS_AUTO_MIN_ROWS = 65536
@@ -387,6 +399,7 @@ class _DeviceOperator:
                  A.nnz <= np.iinfo(np.int32).max)
         pattern = None
         upload = None
+        pending_fill = None
         spread = None
         if early and reorder == "auto" and A.shape[0] >= 16384 and A.nnz:
             # the natural order's spread, before the uploads below compete
@@ -432,17 +445,15 @@ class _DeviceOperator:
                 # eight aggregated 16-row groups: one order for the block
                 # format and the row-group format
                 cand = block_group_order(A, base, 128, 16)
-                if group_rows == 16 or _group_fill(A, cand, 16) >= 0.5:
-                    self.group_rows, perm = 16, cand
+                self.group_rows, perm = 16, cand
+                if group_rows != 16:
+                    # the check that its 16-row groups fill well (else the
+                    # orders of _fallback_order) runs on the upload thread,
+                    # idle by now, beside the device build with it
+                    pending_fill = _uploader().submit(_group_fill, A, cand, 16)
             if self.group_rows is None:
-                self.group_rows, perm = group_rows_for(A, base, group_rows,
-                                                       aggregate=aggregate)
-                if blocks and self.group_rows == 16 and perm is not None \
-                        and A.shape[0] == A.shape[1]:
-                    # 128-row blocks of eight 16-row groups whose column
-                    # sets overlap (the groups stay whole, so the row-group
-                    # format keeps its fill)
-                    perm = block_order(A, perm, 16, 8)
+                self.group_rows, perm = _fallback_order(A, base, group_rows,
+                                                        aggregate, blocks)
         finally:
             if upload is not None:
                 futures.wait([upload])
@@ -472,6 +483,27 @@ class _DeviceOperator:
         if not early:
             self.indices = to_device(A.indices, dev, np.int32)
             self.indptr = to_device(A.indptr, dev, np.int32)
+        try:
+            self._build(perm, fmt, affine, need_transpose, check_indices,
+                        blocks)
+        finally:
+            if pending_fill is not None:
+                futures.wait([pending_fill])
+        if pending_fill is not None and pending_fill.result() < 0.5:
+            # the candidate's 16-row groups fill poorly: rebuild with the
+            # orders the row-group statistics pick
+            self._destroy()
+            self.group_rows, perm = _fallback_order(A, base, group_rows,
+                                                    aggregate, blocks)
+            self._build(perm, fmt, affine, need_transpose, check_indices,
+                        blocks)
+
+    def _build(self, perm, fmt, affine, need_transpose, check_indices,
+               blocks):
+        """The device operator over the uploaded arrays in row order
+        ``perm`` (None = as stored), with the block format if ``blocks``."""
+        import torch
+        dev = self.device
         self.perm = None
         self.inv = None
         if perm is not None:
@@ -482,6 +514,15 @@ class _DeviceOperator:
         self._create(fmt, affine, need_transpose, check_indices)
         if blocks:
             self.add_blocks(need_transpose or fmt == _lib.SLQ_CSC)
+
+    def _destroy(self):
+        """Release the engine's operator and the formats built for it."""
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            self._lib.slq_operator_destroy(h)
+            self.handle = ctypes.c_void_p(None)
+        self.block_formats = []
+        self.workspace = None
 
     @classmethod
     def from_device(cls, indptr, indices, data, shape, affine=False,

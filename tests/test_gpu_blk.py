@@ -269,3 +269,34 @@ def test_block_unions_hook_rejects_bad_values(cuda):
     lib = _lib.load()
     assert lib.slq_debug_blocks_sorted_keys(2) == 1  # bad argument
     assert lib.slq_debug_blocks_sorted_keys(0) == 0
+
+
+def test_block_candidate_order_rejected_for_poor_fill(cuda):
+    # an unstructured matrix: the block/group candidate order fills its
+    # 16-row groups poorly, so the operator built with it beside the fill
+    # check is rebuilt with the row-group statistics' order -- the operator
+    # that order gives directly, with products equal to scipy's
+    import torch
+    from imate_b200.linear_operator import (_fallback_order, _group_fill,
+                                            block_group_order, locality_order)
+    n = 4096
+    B = sp.random(n, n, density=0.006, random_state=12, format="csr")
+    A = (B + B.T + sp.identity(n) * 4.0).tocsr().astype(np.float32)
+    A.sort_indices()
+    assert A.nnz >= 8 * n
+    base = locality_order(A)
+    cand = block_group_order(A, base, 128, 16)
+    assert _group_fill(A, cand, 16) < 0.5
+    G, perm = _fallback_order(A, base, "auto", True, True)
+    M = ib.Matrix(A, blocks=True)
+    op = M.get_device_operator()
+    assert op.group_rows == G
+    if perm is None:
+        assert op.perm is None
+    else:
+        assert np.array_equal(op.perm.cpu().numpy(), perm)
+    X = np.random.default_rng(6).standard_normal((n, 128)).astype(np.float32)
+    Y = op.dot(torch.from_numpy(X).cuda()).cpu().numpy()
+    want = A.astype(np.float64) @ X.astype(np.float64)
+    scale = abs(A.astype(np.float64)) @ np.abs(X.astype(np.float64))
+    assert np.max(np.abs(Y - want) / scale) < RTOL_BLOCK
